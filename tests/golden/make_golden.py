@@ -1,0 +1,270 @@
+"""Generate the golden fixtures of tests/golden/ by running the REFERENCE implementation.
+
+Run once in an environment where the reference source is importable (it is not needed on a GPU
+host; the fixtures it writes are committed):
+
+    PYTHONPATH=<reference>/src NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py \
+        --reference <reference>
+
+Every fixture stores the inputs and the reference's outputs of one hot-path function on seeded
+inputs: neighbour lists (find_neighbours_numba), tighten, density_numba, compute_density,
+forces_numba, disc_forces_numba, glf_step_many, beta_cool, coupled.step and blocks.advance.
+The inputs follow the reference's own tests (tests/sim/test_neighbours.py:15-19, 102-130;
+tests/sim/test_density.py:21-27; tests/sim/test_forces.py:21-26) or the seeded cloud of the
+benchmark workloads.
+"""
+
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SEED = 20261014  # the reference's test seed (tests/conftest.py:7)
+
+
+def _uneven(rng, n, box):
+    pos = rng.uniform(0, box, size=(n, 3))
+    h = np.exp(rng.uniform(np.log(0.01), np.log(0.3), n)) * box / 8
+    return pos, h
+
+
+def _blob(rng, n=2000):
+    core = rng.normal(0.0, 0.15, size=(n // 2, 3))
+    bg = rng.uniform(-1.0, 1.0, size=(n - n // 2, 3))
+    return np.concatenate([core, bg]), np.full(n, 1.0 / n)
+
+
+def _save(name, **arrays):
+    path = os.path.join(HERE, name)
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e3:.0f} kB)")
+
+
+def lists_fixture(nbmod):
+    out = {}
+    cases = ["open_uneven", "periodic_cube", "periodic_long_box", "isolated_large_h", "clump_and_halo"]
+    for case in cases:
+        rng = np.random.default_rng(SEED)
+        if case == "open_uneven":
+            pos, h = _uneven(rng, 3000, 2.0)
+            box = None
+        elif case == "periodic_cube":
+            pos, h = _uneven(rng, 3000, 2.0)
+            box = 2.0
+        elif case == "periodic_long_box":
+            box = np.array([2.0, 0.125, 0.125])
+            pos = rng.uniform(0, 1, (4000, 3)) * box
+            h = rng.uniform(0.005, 0.03, 4000)
+        elif case == "isolated_large_h":
+            pos = np.concatenate([rng.uniform(0, 1, (2000, 3)), [[5.0, 5.0, 5.0], [-3.0, 0.5, 0.5]]])
+            h = np.concatenate([np.full(2000, 0.04), [4.0, 2.5]])
+            box = None
+        else:
+            pos = np.concatenate([rng.normal(0, 0.02, (2000, 3)), rng.uniform(-1, 1, (500, 3))])
+            h = np.concatenate([np.full(2000, 0.005), np.full(500, 0.5)])
+            box = None
+        nb = nbmod.find_neighbours_numba(pos, h, box=box)
+        ref = nbmod.find_neighbours(pos, h, box=box)
+        assert np.array_equal(nb.offset, ref.offset) and np.array_equal(nb.index, ref.index)
+        out[f"{case}_pos"] = pos
+        out[f"{case}_h"] = h
+        out[f"{case}_box"] = np.zeros(3) if box is None else np.broadcast_to(box, (3,)).astype(float)
+        out[f"{case}_offset"] = nb.offset.astype(np.int64)
+        out[f"{case}_index"] = nb.index.astype(np.int32)
+    out["cases"] = np.array(cases)
+    _save("lists.npz", **out)
+
+
+def cloud_lists_fixture(nbmod, ics):
+    """The 4,096-particle benchmark cloud: reference cell grid and lists at h_search = 1.4 h."""
+    ic = ics.cloud(4096)
+    hs = ic.h * 1.4
+    nb = nbmod.find_neighbours_numba(ic.x, hs)
+    # reference grid geometry (sim/neighbours.py:251-266) and cell of each particle
+    lo = ic.x.min(axis=0)
+    span = ic.x.max(axis=0) - lo
+    cell = max(0.5 * 2.0 * float(np.median(hs)), float(np.max(span)) / 160.0, 1e-300)
+    ncell = np.maximum(np.floor(span / cell).astype(np.int64) + 1, 1)
+    inv = np.full(3, 1.0 / cell)
+    start, order = nbmod._build_grid(ic.x, lo, inv, ncell)
+    tight = nbmod.tighten(nb, ic.x, ic.h)
+    _save("cloud_lists.npz", pos=ic.x, h_search=hs, h=ic.h, offset=nb.offset,
+          index=nb.index.astype(np.int32), grid_start=start, grid_order=order.astype(np.int32),
+          ncell=ncell, lo=lo, inv_cell=inv, tight_offset=tight.offset,
+          tight_index=tight.index.astype(np.int32))  # fmt: skip
+
+
+def density_fixture(sph, nbmod):
+    rng = np.random.default_rng(SEED)
+    pos, mass = _blob(rng)
+    h0 = np.full(len(pos), 0.05)
+    first = sph.compute_density(pos, mass, h0, h_max=0.5)
+    h_search = first.h * 1.25
+    nb = nbmod.find_neighbours(pos, h_search)
+    rows = np.sort(rng.choice(len(pos), 700, replace=False))
+    fast = sph.density_numba(pos, mass, first.h, nb, h_search, tol=1e-12, h_max=0.5)
+    part = sph.density_numba(pos, mass, first.h, nb, h_search, tol=1e-12, h_max=0.5, rows=rows)
+    cub = sph.density_numba(pos, mass, first.h, nb, h_search, kernel_name="cubic", eta=1.2,
+                            tol=1e-4, h_max=0.5)  # fmt: skip
+    _save("density.npz", pos=pos, mass=mass, h_first=first.h, rho_first=first.rho,
+          omega_first=first.omega, flags_first=first.flags, h_search=h_search,
+          offset=nb.offset, index=nb.index.astype(np.int32), rows=rows,
+          h=fast.h, rho=fast.rho, omega=fast.omega, iters=fast.iterations, flags=fast.flags,
+          rows_h=part.h, rows_rho=part.rho, cubic_h=cub.h, cubic_rho=cub.rho,
+          cubic_omega=cub.omega, cubic_flags=cub.flags, cubic_iters=cub.iterations)  # fmt: skip
+
+
+def forces_fixture(sph, nbmod):
+    rng = np.random.default_rng(SEED)
+    pos, mass = _blob(rng)
+    u = rng.uniform(0.5, 1.5, len(pos))
+    vel = rng.normal(0.0, 0.3, size=pos.shape)
+    d = sph.compute_density(pos, mass, np.full(len(pos), 0.05), h_max=0.5)
+    p = (5.0 / 3.0 - 1.0) * d.rho * u
+    cs = np.sqrt(10.0 / 9.0 * u)
+    alpha = rng.uniform(0.0, 1.0, len(pos))
+    nb = nbmod.tighten(d.neighbours, pos, d.h)
+    rows = np.sort(rng.choice(len(pos), 600, replace=False))
+    out = dict(pos=pos, vel=vel, mass=mass, h=d.h, rho=d.rho, omega=d.omega, pressure=p, u=u,
+               c_s=cs, alpha=alpha, offset=nb.offset, index=nb.index.astype(np.int32), rows=rows)
+    plain = sph.forces_numba(pos, vel, mass, d.h, d.rho, d.omega, p, nb)
+    out.update(plain_acc=plain.acc, plain_dudt=plain.dudt, plain_vsig=plain.vsig_max)
+    for sig in (0, 1):
+        shock = sph.ShockCapturing(beta=2.0, alpha_u=0.5, conductivity_signal=sig)
+        f = sph.forces_numba(pos, vel, mass, d.h, d.rho, d.omega, p, nb, u=u, c_s=cs, alpha=alpha,
+                             shock=shock)  # fmt: skip
+        out.update({f"cond{sig}_acc": f.acc, f"cond{sig}_dudt": f.dudt,
+                    f"cond{sig}_vsig": f.vsig_max, f"cond{sig}_visc": f.dudt_visc,
+                    f"cond{sig}_cond": f.dudt_cond})  # fmt: skip
+    fr = sph.forces_numba(pos, vel, mass, d.h, d.rho, d.omega, p, nb, u=u, c_s=cs, alpha=alpha,
+                          shock=sph.ShockCapturing(alpha_u=0.5, conductivity_signal=1), rows=rows)
+    out.update(rows_acc=fr.acc, rows_dudt=fr.dudt, rows_vsig=fr.vsig_max)
+    a_d, u_d = sph.disc_forces_numba(pos, vel, mass, d.h, d.rho, d.omega, cs, 0.5, nb)
+    out.update(disc_acc=a_d, disc_dudt=u_d)
+    cub = sph.forces_numba(pos, vel, mass, d.h, d.rho, d.omega, p, nb, kernel_name="cubic", u=u,
+                           c_s=cs, alpha=alpha)  # fmt: skip
+    out.update(cubic_acc=cub.acc, cubic_dudt=cub.dudt, cubic_vsig=cub.vsig_max)
+    _save("forces.npz", **out)
+
+
+def glf_fixture(integ, gravity):
+    rng = np.random.default_rng(SEED)
+    n = 200
+    r = np.exp(rng.uniform(np.log(6.0), np.log(5000.0), n))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    x = d * r[:, None]
+    t = np.cross(d, rng.normal(size=(n, 3)))
+    t /= np.linalg.norm(t, axis=1)[:, None]
+    v = (t * rng.uniform(0.5, 1.2, n)[:, None] + d * rng.uniform(-0.3, 0.3, n)[:, None]) \
+        * np.sqrt(1.0 / r)[:, None]  # fmt: skip
+    p = gravity.gn_p_from_v(x, v)
+    dt = 0.005 * r**1.5
+    x1, p1, it = integ.glf_step_many(x, p, dt)
+    _save("glf.npz", x=x, p=p, dt=dt, x1=x1, p1=p1, iters=it, v=v,
+          v_from_p=gravity.gn_v_from_p(x, p), ham=gravity.gn_hamiltonian(x, p))  # fmt: skip
+
+
+def cooling_fixture(cooling):
+    rng = np.random.default_rng(SEED)
+    u = np.exp(rng.uniform(np.log(1e-10), np.log(1e-4), 500))
+    uf = np.full(500, 2.0e-9)
+    dt = np.exp(rng.uniform(0.0, np.log(1e5), 500))
+    r = rng.uniform(10.0, 5000.0, 500)
+    tc = cooling.cooling_time(r, 230.0)
+    _save("cooling.npz", u=u, u_floor=uf, dt=dt, r=r, t_cool=tc,
+          u_new=cooling.beta_cool(u, uf, dt, tc))  # fmt: skip
+
+
+def _state_arrays(prefix, st, fields):
+    return {f"{prefix}_{f}": np.array(getattr(st, f), copy=True) for f in fields}
+
+
+def coupled_fixture(coupled, ics, hydro_cfg):
+    """The 4,096-particle cloud (cubic kernel, eta 1.2, alpha = 1, beta = 2, GN hole, no
+    cooling): initialise and three shared steps of stable_dt."""
+    ic = ics.cloud(4096)
+    hc = hydro_cfg(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                   conductivity_signal=1, alpha_u=0.05, h_max=200.0)  # fmt: skip
+    cc = coupled.CoupledConfig(hydro=hc)
+    st = coupled.initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, cc)
+    fields = ["x", "p", "u", "h", "rho", "a_hydro", "dudt", "vsig_max", "c_s"]
+    out = dict(x0=ic.x, v0=ic.v, u0=ic.u, mass=ic.mass, h0=ic.h)
+    out.update(_state_arrays("init", st, fields))
+    dts = []
+    for k in range(3):
+        dt = coupled.stable_dt(st, cc)
+        dts.append(dt)
+        st = coupled.step(st, cc, dt)
+        out.update(_state_arrays(f"step{k + 1}", st, fields))
+        led = coupled.ledger(st, cc)
+        out[f"step{k + 1}_energy"] = led["energy"]
+        out[f"step{k + 1}_angmom"] = led["angmom"]
+    out["dts"] = np.array(dts)
+    out["builds"] = st.neighbour_cache.builds
+    out["reuses"] = st.neighbour_cache.reuses
+    _save("coupled.npz", **out)
+
+
+def blocks_fixture(blocks, coupled, ics, hydro_cfg):
+    """A 2,048-particle cloud warm enough to spread over several levels: block steps with the
+    limiter, beta-cooling, conductivity, forced level offsets 0-3; 16 system steps."""
+    ic = ics.cloud(2048, radius=20.0, total_mass=1e-3, t_kelvin=3e8, r_peri=60.0, r_apo=400.0,
+                   seed=7)  # fmt: skip
+    rng = np.random.default_rng(SEED)
+    v = ic.v + rng.normal(0.0, 0.002, ic.v.shape)
+    hc = hydro_cfg(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                   conductivity_signal=1, alpha_u=0.05, h_max=200.0)  # fmt: skip
+    cc = coupled.CoupledConfig(hydro=hc, cooling_beta=230.0)
+    bc = blocks.BlockConfig(coupled=cc, dt_max=64.0)
+    offset = rng.integers(0, 4, len(ic.x))  # forced extra levels (the reference's test hook)
+    st = blocks.initialise(ic.x, v, ic.u, ic.mass, ic.h, bc, t_stop=1e9, level_offset=offset)
+    fields = ["x", "p", "u", "h", "rho", "omega", "a_hydro", "dudt", "level", "n_beg", "n_end",
+              "x_beg", "p_half", "u_half", "vsig_max"]
+    out = dict(x0=ic.x, v0=v, u0=ic.u, mass=ic.mass, h0=ic.h, level_offset=offset)
+    out.update(_state_arrays("init", st, fields))
+    actives = []
+    for k in range(16):
+        rows = blocks.advance(st, bc)
+        actives.append(len(rows))
+    out.update(_state_arrays("final", st, fields))
+    led = blocks.ledger(st, bc)
+    out["final_energy"] = led["energy"]
+    out["final_e_radiated"] = led["e_radiated"]
+    out["final_n"] = st.n
+    out["active_counts"] = np.array(actives)
+    out["builds"] = st.neighbour_cache.builds
+    out["reuses"] = st.neighbour_cache.reuses
+    out["woken"] = st.woken
+    _save("blocks.npz", **out)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", required=True, help="root of the reference checkout")
+    args = ap.parse_args()
+    sys.path.insert(0, os.path.join(args.reference, "src"))
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from nebula.physics import cooling, gravity
+    from nebula.sim import blocks, coupled, integrator, sph
+    from nebula.sim import neighbours as nbmod
+    from nebula.sim.hydro import HydroConfig
+
+    from blackhole_nebula_simulator_b200 import ics
+
+    lists_fixture(nbmod)
+    cloud_lists_fixture(nbmod, ics)
+    density_fixture(sph, nbmod)
+    forces_fixture(sph, nbmod)
+    glf_fixture(integrator, gravity)
+    cooling_fixture(cooling)
+    coupled_fixture(coupled, ics, HydroConfig)
+    blocks_fixture(blocks, coupled, ics, HydroConfig)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,198 @@
+"""The CPU oracle against the reference's own outputs (golden fixtures): pins the checker.
+
+Lists and cells must match exactly; floating-point kernels to the tolerances the reference's
+tests use between its Numba kernels and its readable twins (rtol 1e-12), since the oracle's
+operation order follows the reference's.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import cooling as ocool
+from oracle import native, steps
+from oracle.sph import C_NORM, compute_density
+from tests.conftest import check, golden
+
+
+def _nb(off, idx, box=None):
+    return native.Neighbours(np.asarray(off, np.int64), np.asarray(idx, np.int64), box)
+
+
+@pytest.mark.parametrize(
+    "case", ["open_uneven", "periodic_cube", "periodic_long_box", "isolated_large_h",
+             "clump_and_halo"])  # fmt: skip
+def test_lists_match_reference(case):
+    g = golden("lists.npz")
+    box = g[f"{case}_box"]
+    nb = native.find_neighbours(g[f"{case}_pos"], g[f"{case}_h"], box=None if not box.any() else box)
+    check(f"{case}: offsets", g[f"{case}_offset"], nb.offset)
+    check(f"{case}: indices", g[f"{case}_index"].astype(np.int64), nb.index)
+
+
+def test_cloud_cells_and_lists_match_reference():
+    g = golden("cloud_lists.npz")
+    cell, lo, inv, nc = native.grid_cells(g["pos"], g["h_search"])
+    check("grid dims", g["ncell"], nc)
+    check("grid lo", g["lo"], lo)
+    # the reference's counting sort: order lists particles cell by cell, index ascending
+    order = np.argsort(cell, kind="stable")
+    check("cell order", g["grid_order"].astype(np.int64), order)
+    start = np.searchsorted(cell[order], np.arange(int(np.prod(nc)) + 1))
+    check("cell starts", g["grid_start"], start)
+    nb = native.find_neighbours(g["pos"], g["h_search"])
+    check("cloud lists offsets", g["offset"], nb.offset)
+    check("cloud lists indices", g["index"].astype(np.int64), nb.index)
+    t = native.tighten(nb, g["pos"], g["h"])
+    check("tightened offsets", g["tight_offset"], t.offset)
+    check("tightened indices", g["tight_index"].astype(np.int64), t.index)
+
+
+def test_density_matches_reference():
+    g = golden("density.npz")
+    nb = _nb(g["offset"], g["index"])
+    h, rho, om, it, fl = native.density(g["pos"], g["mass"], g["h_first"], nb, g["h_search"], 1,
+                                        C_NORM[1], 1.6, tol=1e-12, h_max=0.5)  # fmt: skip
+    check("h", g["h"], h, rtol=1e-12)
+    check("rho", g["rho"], rho, rtol=1e-12)
+    check("omega", g["omega"], om, rtol=1e-12)
+    check("flags", g["flags"], fl)
+    h2, rho2, *_ = native.density(g["pos"], g["mass"], g["h_first"], nb, g["h_search"], 1,
+                                  C_NORM[1], 1.6, tol=1e-12, h_max=0.5, rows=g["rows"])  # fmt: skip
+    check("rows h", g["rows_h"], h2, rtol=1e-12)
+    h3, rho3, om3, it3, fl3 = native.density(g["pos"], g["mass"], g["h_first"], nb, g["h_search"],
+                                             0, C_NORM[0], 1.2, tol=1e-4, h_max=0.5)  # fmt: skip
+    check("cubic h", g["cubic_h"], h3, rtol=1e-12)
+    check("cubic rho", g["cubic_rho"], rho3, rtol=1e-12)
+    check("cubic omega", g["cubic_omega"], om3, rtol=1e-12)
+    check("cubic flags", g["cubic_flags"], fl3)
+    check("cubic iterations", g["cubic_iters"], it3)
+
+
+def test_compute_density_matches_reference():
+    g = golden("density.npz")
+    res = compute_density(g["pos"], g["mass"], np.full(len(g["pos"]), 0.05), h_max=0.5)
+    check("compute_density h", g["h_first"], res.h, rtol=1e-12)
+    check("compute_density rho", g["rho_first"], res.rho, rtol=1e-12)
+    check("compute_density flags", g["flags_first"], res.flags)
+
+
+@pytest.mark.parametrize("sig", [0, 1])
+def test_forces_match_reference(sig):
+    g = golden("forces.npz")
+    nb = _nb(g["offset"], g["index"])
+    args = (g["pos"], g["vel"], g["mass"], g["h"], g["rho"], g["omega"], g["pressure"], nb)
+    acc, dudt, vsig, vh, ch = native.forces(*args, 1, C_NORM[1], u=g["u"], c_s=g["c_s"],
+                                            alpha=g["alpha"], alpha_u=0.5, cond_signal=sig)
+    check("acc", g[f"cond{sig}_acc"], acc, rtol=1e-12, per_vector=True)
+    scale = np.abs(g[f"cond{sig}_dudt"]).max()
+    check("dudt", g[f"cond{sig}_dudt"] / scale, dudt / scale, atol=1e-12)
+    check("vsig", g[f"cond{sig}_vsig"], vsig, rtol=1e-14)
+    check("visc heat", g[f"cond{sig}_visc"] / scale, vh / scale, atol=1e-12)
+    check("cond heat", g[f"cond{sig}_cond"] / scale, ch / scale, atol=1e-12)
+
+
+def test_forces_plain_rows_disc_cubic_match_reference():
+    g = golden("forces.npz")
+    nb = _nb(g["offset"], g["index"])
+    base = (g["pos"], g["vel"], g["mass"], g["h"], g["rho"], g["omega"], g["pressure"], nb)
+    acc, dudt, vsig, _, _ = native.forces(*base, 1, C_NORM[1])
+    check("plain acc", g["plain_acc"], acc, rtol=1e-12, per_vector=True)
+    check("plain dudt", g["plain_dudt"], dudt, rtol=1e-11, atol=1e-14)
+    acc, dudt, vsig, _, _ = native.forces(*base, 1, C_NORM[1], u=g["u"], c_s=g["c_s"],
+                                          alpha=g["alpha"], alpha_u=0.5, cond_signal=1,
+                                          rows=g["rows"])  # fmt: skip
+    check("rows acc", g["rows_acc"], acc, rtol=1e-12, per_vector=True)
+    check("rows vsig", g["rows_vsig"], vsig, rtol=1e-14)
+    a_d, u_d = native.disc_forces(g["pos"], g["vel"], g["mass"], g["h"], g["rho"], g["omega"],
+                                  g["c_s"], 0.5, nb, 1, C_NORM[1])  # fmt: skip
+    check("disc acc", g["disc_acc"], a_d, rtol=1e-12, per_vector=True)
+    check("disc dudt", g["disc_dudt"], u_d, rtol=1e-11, atol=1e-14 * np.abs(g["disc_dudt"]).max())
+    acc, dudt, vsig, _, _ = native.forces(*base, 0, C_NORM[0], u=g["u"], c_s=g["c_s"],
+                                          alpha=g["alpha"])  # fmt: skip
+    check("cubic acc", g["cubic_acc"], acc, rtol=1e-12, per_vector=True)
+
+
+def test_glf_matches_reference():
+    g = golden("glf.npz")
+    x1, p1, it = native.glf_step_many(g["x"], g["p"], g["dt"])
+    check("x1", g["x1"], x1, rtol=1e-15, per_vector=True)
+    check("p1", g["p1"], p1, rtol=1e-15, per_vector=True)
+    check("iterations", g["iters"], it)
+    check("v from p", g["v_from_p"], native.gn_v_from_p(g["x"], g["p"]), rtol=1e-15,
+          per_vector=True)  # fmt: skip
+    check("p from v", g["p"], steps.gn_p_from_v(g["x"], g["v"]), rtol=1e-15, per_vector=True)
+    check("hamiltonian", g["ham"], steps.gn_hamiltonian(g["x"], g["p"]), rtol=1e-13)
+
+
+def test_glf_failures_flagged():
+    x = np.array([[6.0, 0.0, 0.0]])
+    p = steps.gn_p_from_v(x, np.array([[0.0, 0.4, 0.0]]))
+    with pytest.raises(native.GLFConvergenceError, match="did not converge"):
+        native.glf_step_many(x, p, 50.0)
+    with pytest.raises(native.GLFConvergenceError, match="inside r"):
+        native.glf_step_many(np.array([[2.4, 0.0, 0.0]]), p, 0.1)
+
+
+def test_beta_cooling_matches_reference():
+    g = golden("cooling.npz")
+    check("beta_cool", g["u_new"], ocool.beta_cool(g["u"], g["u_floor"], g["dt"], g["t_cool"]),
+          rtol=1e-15)  # fmt: skip
+    check("cooling time", g["t_cool"], ocool.cooling_time(g["r"], 230.0), rtol=1e-15)
+
+
+def _cfg():
+    from blackhole_nebula_simulator_b200.config import CoupledConfig, HydroConfig
+
+    hc = HydroConfig(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                     conductivity_signal=1, alpha_u=0.05, h_max=200.0)  # fmt: skip
+    return hc, CoupledConfig
+
+
+def test_shared_steps_match_reference():
+    g = golden("coupled.npz")
+    hc, CC = _cfg()
+    cc = CC(hydro=hc)
+    st = steps.coupled_initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], cc)
+    for f in ("h", "rho", "dudt"):
+        check(f"init {f}", g[f"init_{f}"], getattr(st, f), rtol=1e-10, atol=1e-30)
+    check("init acc", g["init_a_hydro"], st.a_hydro, rtol=1e-9, per_vector=True)
+    for k in range(3):
+        dt = steps.coupled_stable_dt(st, cc)
+        check(f"dt {k}", g["dts"][k], dt, rtol=1e-12)
+        st = steps.coupled_step(st, cc, dt)
+        check(f"step {k + 1} x", g[f"step{k + 1}_x"], st.x, rtol=1e-14, per_vector=True)
+        check(f"step {k + 1} p", g[f"step{k + 1}_p"], st.p, rtol=1e-12, per_vector=True)
+        check(f"step {k + 1} u", g[f"step{k + 1}_u"], st.u, rtol=1e-10)
+        check(f"step {k + 1} h", g[f"step{k + 1}_h"], st.h, rtol=1e-10)
+        check(f"step {k + 1} acc", g[f"step{k + 1}_a_hydro"], st.a_hydro, rtol=1e-8,
+              per_vector=True)  # fmt: skip
+        led = steps.coupled_ledger(st, cc)
+        check(f"step {k + 1} energy", g[f"step{k + 1}_energy"], led["energy"], rtol=1e-13)
+    check("cache builds", int(g["builds"]), st.neighbour_cache.builds)
+    check("cache reuses", int(g["reuses"]), st.neighbour_cache.reuses)
+
+
+def test_block_steps_match_reference():
+    from blackhole_nebula_simulator_b200.config import BlockConfig
+
+    g = golden("blocks.npz")
+    hc, CC = _cfg()
+    bc = BlockConfig(coupled=CC(hydro=hc, cooling_beta=230.0), dt_max=64.0)
+    st = steps.blocks_initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc, t_stop=1e9,
+                                 level_offset=g["level_offset"])  # fmt: skip
+    check("init levels", g["init_level"], st.level)
+    check("init n_end", g["init_n_end"], st.n_end)
+    actives = [len(steps.blocks_advance(st, bc)) for _ in range(len(g["active_counts"]))]
+    check("active counts", g["active_counts"], np.array(actives))
+    check("final tick", int(g["final_n"]), st.n)
+    check("final levels", g["final_level"], st.level)
+    check("final n_end", g["final_n_end"], st.n_end)
+    check("final x", g["final_x"], st.x, rtol=1e-13, per_vector=True)
+    check("final p", g["final_p"], st.p, rtol=1e-11, per_vector=True)
+    check("final u", g["final_u"], st.u, rtol=1e-9)
+    check("final h", g["final_h"], st.h, rtol=1e-9)
+    check("final energy", float(g["final_energy"]), steps.blocks_ledger(st, bc)["energy"],
+          rtol=1e-12)  # fmt: skip
+    check("final e_radiated", float(g["final_e_radiated"]), st.e_radiated, rtol=1e-9)
+    check("cache builds", int(g["builds"]), st.neighbour_cache.builds)
+    check("cache reuses", int(g["reuses"]), st.neighbour_cache.reuses)
