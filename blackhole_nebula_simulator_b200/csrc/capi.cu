@@ -1,0 +1,361 @@
+// extern "C" entry points of libnebula_b200.so (declared in include/nebula_b200.h).
+#include <cub/cub.cuh>
+
+#include <new>
+
+#include "../../include/nebula_b200.h"
+#include "common.cuh"
+#include "cooling.cuh"
+#include "engine.cuh"
+#include "gravity.cuh"
+#include "sph.cuh"
+#include "steps.cuh"
+
+struct nb_ctx {
+  nbk::Engine E;
+};
+
+using nbk::Engine;
+
+namespace {
+
+cudaStream_t S(void* stream) { return (cudaStream_t)stream; }
+
+int begin(nb_ctx* ctx) {
+  if (!ctx) return NB_ERR_INPUT;
+  Engine& E = ctx->E;
+  E.last_error[0] = 0;
+  NB_CUDA(cudaSetDevice(E.device));
+  return 0;
+}
+
+__global__ void k_beta(int64_t n, const double* __restrict__ u, const double* __restrict__ uf,
+                       const double* __restrict__ dt, const double* __restrict__ tc,
+                       double* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = nbk::beta_cool_one(u[i], uf[i], dt[i], tc[i]);
+}
+
+__global__ void k_brems(int64_t n, const double* __restrict__ u, const double* __restrict__ rho,
+                        const double* __restrict__ dt, double dt_scalar, nbk::BremsParams bp,
+                        double* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = nbk::brems_cool_one(u[i], rho[i], dt ? dt[i] : dt_scalar, bp);
+}
+
+// sim/neighbours.py:284-323 on caller lists
+__global__ void k_tighten(int64_t nrows, const int64_t* __restrict__ rows, const double* __restrict__ pos,
+                          const double* __restrict__ h, const int64_t* __restrict__ off,
+                          const int64_t* __restrict__ idx, int64_t* __restrict__ counts,
+                          const int64_t* __restrict__ out_off, int64_t* __restrict__ out_idx) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows ? rows[q] : q;
+  int64_t m = 0;
+  for (int64_t e = off[i]; e < off[i + 1]; ++e) {
+    int64_t j = idx[e];
+    double d2 = nbk::d2_exact(pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1],
+                              pos[3 * j + 2] - pos[3 * i + 2]);
+    double rr = 2.0 * fmax(h[i], h[j]);
+    if (d2 < rr * rr) {
+      if (out_off) out_idx[out_off[i] + m] = j;
+      m += 1;
+    }
+  }
+  if (!out_off) counts[i] = m;
+}
+
+double cnorm_of(int kid) { return kid == 0 ? 1.0 / M_PI : 495.0 / (256.0 * M_PI); }
+
+nbk::BremsParams brems_params(const nb_params* prm) {
+  nbk::BremsParams b;
+  b.tfac = prm->brems_tfac;
+  b.b = prm->brems_b;
+  b.kappa = prm->brems_kappa;
+  b.u_floor = prm->u_floor;
+  b.t_floor = prm->brems_t_floor;
+  return b;
+}
+
+int check_params(Engine& E, const nb_params* prm) {
+  if (!prm) return nbk::set_host_error(E, "params missing"), NB_ERR_INPUT;
+  if (prm->kernel_id != 0 && prm->kernel_id != 1) {
+    nbk::set_host_error(E, "kernel_id must be 0 (cubic) or 1 (wendland_c4)");
+    return NB_ERR_INPUT;
+  }
+  if (prm->precision != 0 && prm->precision != 1) {
+    nbk::set_host_error(E, "precision must be 0 (fp64) or 1 (fp32)");
+    return NB_ERR_INPUT;
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nb_version(void) { return 1; }
+
+nb_ctx* nb_create(int device) {
+  nb_ctx* c = new (std::nothrow) nb_ctx();
+  if (!c) return nullptr;
+  c->E.device = device;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete c;
+    return nullptr;
+  }
+  if (c->E.ensure_n(1) != 0) {
+    c->E.release();
+    delete c;
+    return nullptr;
+  }
+  return c;
+}
+
+void nb_destroy(nb_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->E.device);
+  cudaDeviceSynchronize();
+  ctx->E.release();
+  delete ctx;
+}
+
+const char* nb_last_error(nb_ctx* ctx) { return ctx ? ctx->E.last_error : "no context"; }
+
+int nb_reset_cache(nb_ctx* ctx) {
+  NB_TRY(begin(ctx));
+  ctx->E.ws.cache.valid = false;
+  return 0;
+}
+
+int nb_find_neighbours(nb_ctx* ctx, int64_t n, const double* pos, const double* h,
+                       int64_t* offset, int64_t* total, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (n < 0 || n > 2000000000) return nbk::set_host_error(E, "n out of range"), NB_ERR_INPUT;
+  NB_TRY(nbk::build_lists(E, n, pos, h, S(stream)));
+  *total = E.lists.total;
+  if (n == 0) {
+    NB_CUDA(cudaMemsetAsync(offset, 0, sizeof(int64_t), S(stream)));
+    return 0;
+  }
+  return nbk::export_lists_offsets(E, offset, S(stream));
+}
+
+int nb_neighbours_export(nb_ctx* ctx, int64_t* offset, int64_t* index, void* stream) {
+  NB_TRY(begin(ctx));
+  return nbk::export_lists(ctx->E, offset, index, S(stream));
+}
+
+int nb_tighten(nb_ctx* ctx, int64_t n, const double* pos, const double* h, const int64_t* offset,
+               const int64_t* index, int64_t nrows, const int64_t* rows, int64_t* counts,
+               const int64_t* out_off, int64_t* out_idx, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (!out_off) NB_CUDA(cudaMemsetAsync(counts, 0, sizeof(int64_t) * n, S(stream)));
+  if (nrows > 0)
+    k_tighten<<<nbk::grid_for(nrows), NB_THREADS, 0, S(stream)>>>(nrows, rows, pos, h, offset,
+                                                                  index, counts, out_off, out_idx);
+  NB_CUDA(cudaGetLastError());
+  return nbk::check_device_error(E, S(stream));
+}
+
+int nb_density(nb_ctx* ctx, int64_t n, const double* pos, const double* mass,
+               const double* h_start, const double* h_search, const int64_t* offset,
+               const int64_t* index, int64_t nrows, const int64_t* rows, int kernel_id,
+               double eta, double tol, double h_max, double* h_out, double* rho, double* omega,
+               int64_t* iters, int64_t* flags, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (kernel_id != 0 && kernel_id != 1) return nbk::set_host_error(E, "bad kernel_id"), NB_ERR_INPUT;
+  NB_TRY(E.ws.ensure(E, n));
+  nbk::pack_pos(n, pos, nullptr, E.ws.pk0, S(stream));
+  nbk::DensityParams dp{kernel_id, cnorm_of(kernel_id), eta, tol, h_max};
+  nbk::launch_density64<int64_t>(rows ? nrows : n, rows, E.ws.pk0, mass, h_start, h_search,
+                                 offset, index, dp, nullptr, h_out, rho, omega, iters, flags,
+                                 S(stream));
+  NB_CUDA(cudaGetLastError());
+  return nbk::check_device_error(E, S(stream));
+}
+
+int nb_forces(nb_ctx* ctx, int64_t n, const double* pos, const double* vel, const double* mass,
+              const double* h, const double* rho, const double* omega, const double* pressure,
+              const double* u, const double* c_s, const double* alpha, const int64_t* offset,
+              const int64_t* index, int64_t nrows, const int64_t* rows, int kernel_id,
+              double beta, double alpha_u, int cond_signal, double* acc, double* dudt,
+              double* vsig_max, double* vheat, double* cheat, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (kernel_id != 0 && kernel_id != 1) return nbk::set_host_error(E, "bad kernel_id"), NB_ERR_INPUT;
+  NB_TRY(E.ws.ensure(E, n));
+  nbk::Workspace& W = E.ws;
+  cudaStream_t st = S(stream);
+  nbk::pack_pos(n, pos, nullptr, W.pk0, st);
+  nbk::pack_vm(n, vel, mass, W.pk1, st);
+  nbk::pack4(n, h, rho, omega, pressure, W.pk2, st);
+  nbk::pack4(n, u, c_s, alpha, nullptr, W.pk3, st);
+  nbk::ForceParams fp{};
+  fp.kid = kernel_id;
+  fp.cnorm = cnorm_of(kernel_id);
+  fp.use_sph = 1;
+  fp.use_visc = alpha != nullptr && c_s != nullptr;
+  fp.use_cond = fp.use_visc && u != nullptr;
+  fp.cond_signal = cond_signal;
+  fp.beta = beta;
+  fp.alpha_u = alpha_u;
+  fp.use_disc = 0;
+  fp.tighten = 0;
+  nbk::ForceOut fo;
+  fo.acc = acc;
+  fo.dudt = dudt;
+  fo.vsig = vsig_max;
+  fo.vheat = vheat;
+  fo.cheat = cheat;
+  nbk::launch_forces64<int64_t>(rows ? nrows : n, rows, W.pk0, W.pk1, W.pk2, W.pk3, offset, index,
+                                fp, nullptr, fo, st);
+  NB_CUDA(cudaGetLastError());
+  return nbk::check_device_error(E, st);
+}
+
+int nb_disc_forces(nb_ctx* ctx, int64_t n, const double* pos, const double* vel,
+                   const double* mass, const double* h, const double* rho, const double* omega,
+                   const double* c_s, double alpha_av, const int64_t* offset, const int64_t* index,
+                   int64_t nrows, const int64_t* rows, int kernel_id, double* acc, double* dudt,
+                   void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (kernel_id != 0 && kernel_id != 1) return nbk::set_host_error(E, "bad kernel_id"), NB_ERR_INPUT;
+  NB_TRY(E.ws.ensure(E, n));
+  nbk::Workspace& W = E.ws;
+  cudaStream_t st = S(stream);
+  nbk::pack_pos(n, pos, nullptr, W.pk0, st);
+  nbk::pack_vm(n, vel, mass, W.pk1, st);
+  nbk::pack4(n, h, rho, omega, nullptr, W.pk2, st);
+  nbk::pack4(n, nullptr, c_s, nullptr, nullptr, W.pk3, st);
+  nbk::ForceParams fp{};
+  fp.kid = kernel_id;
+  fp.cnorm = cnorm_of(kernel_id);
+  fp.use_sph = 0;
+  fp.use_disc = 1;
+  fp.disc_alpha_av = alpha_av;
+  fp.tighten = 0;
+  nbk::ForceOut fo;
+  fo.dacc = acc;
+  fo.ddudt = dudt;
+  nbk::launch_forces64<int64_t>(rows ? nrows : n, rows, W.pk0, W.pk1, W.pk2, W.pk3, offset, index,
+                                fp, nullptr, fo, st);
+  NB_CUDA(cudaGetLastError());
+  return nbk::check_device_error(E, st);
+}
+
+int nb_glf_step_many(nb_ctx* ctx, int64_t n, const double* x, const double* p, const double* dt,
+                     double dt_scalar, double* x1, double* p1, int64_t* iters, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  NB_TRY(E.ws.ensure(E, n));
+  cudaStream_t st = S(stream);
+  int64_t* it = iters ? iters : E.ws.iters;
+  nbk::launch_glf(n, x, p, dt, dt_scalar, x1, p1, it, st);
+  NB_CUDA(cudaGetLastError());
+  if (n == 0) return 0;
+  size_t tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceReduce::Min(E.cub_tmp, tmp, it, E.ws.d_i64, (int)n, st));
+  NB_CUDA(cudaMemcpyAsync(E.ws.h_i64, E.ws.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  int64_t w = E.ws.h_i64[0];
+  if (w >= 0) return 0;
+  nbk::set_host_error(E, w == -1   ? "stage 1 (p_half) did not converge in 10 iterations: time step too large"
+                         : w == -2 ? "stage 2 (x1) did not converge in 10 iterations: time step too large"
+                                   : "particle inside r = 2.5");
+  return w == -1 ? NB_ERR_GLF_P_HALF : w == -2 ? NB_ERR_GLF_X1 : NB_ERR_GLF_RADIUS;
+}
+
+int nb_gn_v_from_p(nb_ctx* ctx, int64_t n, const double* x, const double* p, double* v, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  nbk::launch_v_from_p(n, x, p, v, S(stream));
+  NB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int nb_gn_p_from_v(nb_ctx* ctx, int64_t n, const double* x, const double* v, double* p, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  nbk::launch_p_from_v(n, x, v, p, S(stream));
+  NB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int nb_beta_cool(nb_ctx* ctx, int64_t n, const double* u, const double* u_floor, const double* dt,
+                 const double* t_cool, double* out, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (n > 0) k_beta<<<nbk::grid_for(n), NB_THREADS, 0, S(stream)>>>(n, u, u_floor, dt, t_cool, out);
+  NB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int nb_brems_cool(nb_ctx* ctx, int64_t n, const double* u, const double* rho, const double* dt,
+                  double dt_scalar, const nb_params* prm, double* out, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (!prm) return nbk::set_host_error(E, "params missing"), NB_ERR_INPUT;
+  if (n > 0)
+    k_brems<<<nbk::grid_for(n), NB_THREADS, 0, S(stream)>>>(n, u, rho, dt, dt_scalar,
+                                                            brems_params(prm), out);
+  NB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int nb_ledger(nb_ctx* ctx, int64_t n, const double* x, const double* p, const double* u,
+              const double* mass, double* out, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  cudaStream_t st = S(stream);
+  NB_TRY(E.ws.ensure(E, std::max<int64_t>(n, 1)));
+  nbk::launch_ledger(n, x, p, u, mass, E.red, E.ws.d_tmp, st);
+  NB_CUDA(cudaMemcpyAsync(E.ws.h_dbl, E.ws.d_tmp, sizeof(double) * 9, cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  for (int t = 0; t < 9; ++t) out[t] = E.ws.h_dbl[t];
+  return 0;
+}
+
+int nb_coupled_initialise(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* stream) {
+  NB_TRY(begin(ctx));
+  NB_TRY(check_params(ctx->E, prm));
+  return nbk::coupled_initialise(ctx->E, st, prm, S(stream));
+}
+
+int nb_coupled_step(nb_ctx* ctx, nb_state* st, const nb_params* prm, double dt, void* stream) {
+  NB_TRY(begin(ctx));
+  NB_TRY(check_params(ctx->E, prm));
+  return nbk::coupled_step(ctx->E, st, prm, dt, S(stream));
+}
+
+int nb_coupled_stable_dt(nb_ctx* ctx, nb_state* st, const nb_params* prm, double* dt_out,
+                         void* stream) {
+  NB_TRY(begin(ctx));
+  NB_TRY(check_params(ctx->E, prm));
+  return nbk::coupled_stable_dt(ctx->E, st, prm, dt_out, S(stream));
+}
+
+int nb_block_initialise(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* stream) {
+  NB_TRY(begin(ctx));
+  NB_TRY(check_params(ctx->E, prm));
+  return nbk::block_initialise(ctx->E, st, prm, S(stream));
+}
+
+int nb_block_advance(nb_ctx* ctx, nb_state* st, const nb_params* prm, int64_t* rows_out,
+                     void* stream) {
+  NB_TRY(begin(ctx));
+  NB_TRY(check_params(ctx->E, prm));
+  return nbk::block_advance(ctx->E, st, prm, rows_out, S(stream));
+}
+
+int nb_block_land(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* stream) {
+  NB_TRY(begin(ctx));
+  NB_TRY(check_params(ctx->E, prm));
+  return nbk::block_land(ctx->E, st, prm, S(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,637 @@
+// The step runtime: list cache with the reference's reuse test, density for given rows with the
+// search-doubling loop, the fused EOS + force pass, and the shared-step and block-step drivers.
+//
+// State arrays stay in the caller's particle order.  Each list build sorts the particles in
+// Morton order; the pair passes read packed copies in that order (coalesced, cache-friendly) and
+// scatter their results back to the caller's order.
+#include <cub/cub.cuh>
+
+#include <cmath>
+#include <vector>
+
+#include "../../include/nebula_b200.h"
+#include "common.cuh"
+#include "cooling.cuh"
+#include "engine.cuh"
+#include "gravity.cuh"
+#include "sph.cuh"
+#include "steps.cuh"
+
+namespace nbk {
+
+// ---------------------------------------------------------------- workspace
+template <typename T>
+static int grow(Engine& E, T*& p, int64_t& cap, int64_t want) {
+  if (want <= cap && p) return 0;
+  int64_t c = std::max<int64_t>(want + want / 4, 1024);
+  if (p) cudaFree(p);
+  p = nullptr;
+  NB_CUDA(cudaMalloc((void**)&p, sizeof(T) * (size_t)c));
+  cap = c;
+  return 0;
+}
+
+int Engine::ensure_cub(size_t bytes) {
+  Engine& E = *this;
+  if (bytes <= cub_bytes && cub_tmp) return 0;
+  if (cub_tmp) cudaFree(cub_tmp);
+  cub_tmp = nullptr;
+  size_t b = bytes + bytes / 4 + 4096;
+  NB_CUDA(cudaMalloc(&cub_tmp, b));
+  cub_bytes = b;
+  return 0;
+}
+
+int Engine::ensure_n(int64_t n) {
+  Engine& E = *this;
+  if (!d_err) {
+    NB_CUDA(cudaMalloc((void**)&d_err, sizeof(int) * 4));
+    NB_CUDA(cudaMemset(d_err, 0, sizeof(int) * 4));
+    NB_CUDA(cudaMallocHost((void**)&h_err, sizeof(int) * 4));
+    NB_CUDA(cudaMalloc((void**)&bbox, sizeof(double) * 8));
+    NB_CUDA(cudaMallocHost((void**)&h_red, sizeof(double) * 64));
+  }
+  if (n <= cap_n && keys_a) return 0;
+  int64_t c = std::max<int64_t>(n + n / 4, 1024);
+  auto fr = [](void* p) {
+    if (p) cudaFree(p);
+  };
+  fr(bbox_part); fr(keys_a); fr(keys_b); fr(vals_a); fr(counts); fr(red);
+  fr(lists.perm); fr(lists.inv_perm); fr(lists.spos); fr(lists.off);
+  NB_CUDA(cudaMalloc((void**)&bbox_part, sizeof(double) * 6 * 1184));
+  NB_CUDA(cudaMalloc((void**)&keys_a, sizeof(uint64_t) * c));
+  NB_CUDA(cudaMalloc((void**)&keys_b, sizeof(uint64_t) * c));
+  NB_CUDA(cudaMalloc((void**)&vals_a, sizeof(int32_t) * c));
+  NB_CUDA(cudaMalloc((void**)&counts, sizeof(int64_t) * (c + 1)));
+  NB_CUDA(cudaMalloc((void**)&red, sizeof(double) * 16 * 1184));
+  NB_CUDA(cudaMalloc((void**)&lists.perm, sizeof(int32_t) * c));
+  NB_CUDA(cudaMalloc((void**)&lists.inv_perm, sizeof(int32_t) * c));
+  NB_CUDA(cudaMalloc((void**)&lists.spos, sizeof(double4) * c));
+  NB_CUDA(cudaMalloc((void**)&lists.off, sizeof(int64_t) * (c + 1)));
+  cap_n = c;
+  lists.n = 0;
+  return ensure_cub(cub_bytes_needed(c, 0));
+}
+
+int Engine::ensure_nodes(int64_t m) { return grow2(m); }
+
+int Engine::grow2(int64_t m) {
+  Engine& E = *this;
+  if (m <= cap_nodes && node_lo) return 0;
+  int64_t c = std::max<int64_t>(m + m / 4, 256);
+  if (node_lo) cudaFree(node_lo);
+  if (node_hi) cudaFree(node_hi);
+  NB_CUDA(cudaMalloc((void**)&node_lo, sizeof(double4) * c));
+  NB_CUDA(cudaMalloc((void**)&node_hi, sizeof(double4) * c));
+  cap_nodes = c;
+  return 0;
+}
+
+int Engine::ensure_list_capacity(int64_t m) {
+  Engine& E = *this;
+  NB_TRY(grow(E, lists.idx, cap_list, std::max<int64_t>(m, 1)));
+  return 0;
+}
+
+int Engine::ensure_sort_keys(int64_t m) {
+  Engine& E = *this;
+  NB_TRY(grow(E, sort_keys, cap_sort, m));
+  return ensure_cub(cub_bytes_needed(cap_n, m));
+}
+
+void Engine::release() {
+  void* ps[] = {d_err, bbox, bbox_part, keys_a, keys_b, vals_a, counts, node_lo, node_hi,
+                cub_tmp, sort_keys, red, lists.perm, lists.inv_perm, lists.spos, lists.off,
+                lists.idx};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  if (h_err) cudaFreeHost(h_err);
+  if (h_red) cudaFreeHost(h_red);
+  ws.release();
+}
+
+int check_device_error(Engine& E, cudaStream_t st) {
+  NB_CUDA(cudaMemcpyAsync(E.h_err, E.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(cudaGetLastError());
+  int code = E.h_err[0];
+  if (code == 0) return 0;
+  NB_CUDA(cudaMemsetAsync(E.d_err, 0, sizeof(int), st));
+  const char* msg = "device error";
+  int ret = NB_ERR_INPUT;
+  switch (code) {
+    case ERR_LIST_OVERFLOW: msg = "neighbour list longer than counted"; ret = -3; break;
+    case ERR_TRAVERSAL_STACK: msg = "tree traversal stack exhausted"; ret = -3; break;
+    case ERR_BAD_INDEX: msg = "index outside [0, n)"; ret = NB_ERR_INPUT; break;
+    case ERR_NONPOSITIVE_U: msg = "non-positive internal energy"; ret = NB_ERR_NONPOSITIVE_U; break;
+    case ERR_LEVEL: msg = "a particle needs a level beyond K_MAX = 40"; ret = NB_ERR_LEVEL; break;
+    case ERR_LIMITER: msg = "level limiter did not settle"; ret = -3; break;
+    case ERR_DT: msg = "time steps must be positive"; ret = NB_ERR_DT; break;
+  }
+  std::snprintf(E.last_error, sizeof(E.last_error), "%s", msg);
+  return ret;
+}
+
+// ---------------------------------------------------------------- small kernels
+__global__ void k_mask_rows(int64_t nrows, const int64_t* __restrict__ rows, int64_t n,
+                            uint8_t* __restrict__ mask, int* err) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows[q];
+  if (i < 0 || i >= n) {
+    set_error(err, ERR_BAD_INDEX);
+    return;
+  }
+  mask[i] = 1;
+}
+
+__global__ void k_rows_to_sorted(int64_t nrows, const int64_t* __restrict__ rows,
+                                 const int32_t* __restrict__ inv_perm, int64_t* __restrict__ out) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  out[q] = inv_perm[rows[q]];
+}
+
+// h_search = min(min(h_guess, h_max) * skin, cap) (sim/sph.py:373)
+__global__ void k_hsearch(int64_t n, const double* __restrict__ hg, double h_max, double skin,
+                          double* __restrict__ hs) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  hs[i] = fmin(hg[i], h_max) * skin;
+}
+
+__global__ void k_disp(int64_t n, const double* __restrict__ x, const double* __restrict__ xr,
+                       double* __restrict__ disp, int32_t* __restrict__ iota) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double dx = x[3 * i] - xr[3 * i], dy = x[3 * i + 1] - xr[3 * i + 1], dz = x[3 * i + 2] - xr[3 * i + 2];
+  disp[i] = sqrt(dx * dx + dy * dy + dz * dz);
+  iota[i] = (int32_t)i;
+}
+
+// h_eff = hs - (disp + d_rest)/2; fail if a row has h_eff <= h_guess/2 or another particle
+// h_guess > h_eff (sim/sph.py:134-138).  Also fills h_lim (rows: h_eff, others: h_guess).
+__global__ void k_reuse_test(int64_t n, const double* __restrict__ hs, const double* __restrict__ disp,
+                             double d_rest, const double* __restrict__ hg,
+                             const uint8_t* __restrict__ is_row, double* __restrict__ h_eff,
+                             double* __restrict__ h_lim, int* __restrict__ fail) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double he = hs[i] - 0.5 * (disp[i] + d_rest);
+  h_eff[i] = he;
+  bool row = is_row[i];
+  h_lim[i] = row ? he : hg[i];
+  bool bad = row ? !(he > 0.5 * hg[i]) : !(hg[i] <= he);
+  if (bad) atomicOr(fail, 1);
+}
+
+// sim/sph.py:85-111: every particle k within 2 max(h_lim_j, h_lim_k) of a fast particle j must be
+// in j's list.  One block per fast particle; binary search in the (sorted) row.
+__global__ void k_fast_complete(int64_t n, int nfast, const int32_t* __restrict__ fast,
+                                const double* __restrict__ x, const double* __restrict__ h_lim,
+                                const int32_t* __restrict__ inv_perm, const int64_t* __restrict__ off,
+                                const int32_t* __restrict__ idx, int* __restrict__ fail) {
+  int q = blockIdx.x;
+  if (q >= nfast) return;
+  int64_t j = fast[q];
+  int64_t row = inv_perm[j];
+  int64_t lo = off[row], hi = off[row + 1];
+  double xj0 = x[3 * j], xj1 = x[3 * j + 1], xj2 = x[3 * j + 2];
+  for (int64_t k = threadIdx.x; k < n; k += blockDim.x) {
+    double d2 = d2_exact(x[3 * k] - xj0, x[3 * k + 1] - xj1, x[3 * k + 2] - xj2);
+    double rr = 2.0 * fmax(h_lim[j], h_lim[k]);
+    if (d2 <= rr * rr) {
+      int32_t key = inv_perm[k];
+      int64_t a = lo, b = hi;
+      while (a < b) {
+        int64_t m = (a + b) >> 1;
+        if (idx[m] < key)
+          a = m + 1;
+        else
+          b = m;
+      }
+      if (a >= hi || idx[a] != key) atomicOr(fail, 1);
+    }
+  }
+}
+
+__global__ void k_gather_d(int64_t n, const int32_t* __restrict__ perm, const double* __restrict__ a,
+                           double* __restrict__ out) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  out[k] = a[perm[k]];
+}
+
+// sorted packs for the pair passes
+__global__ void k_pack_sorted(int64_t n, const int32_t* __restrict__ perm,
+                              const double* __restrict__ x, const double* __restrict__ w,
+                              double4* __restrict__ out) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int64_t i = perm[k];
+  out[k] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], w ? w[i] : 0.0);
+}
+
+__global__ void k_pack_sorted4(int64_t n, const int32_t* __restrict__ perm, const double* __restrict__ a,
+                               const double* __restrict__ b, const double* __restrict__ c,
+                               const double* __restrict__ d, double4* __restrict__ out) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int64_t i = perm[k];
+  out[k] = make_double4(a ? a[i] : 0.0, b ? b[i] : 0.0, c ? c[i] : 0.0, d ? d[i] : 0.0);
+}
+
+// FP32 positions: integer cell of a uniform grid (edge `cell`, at most 1024 per axis, corner lo)
+// packed 10 bits per axis, and the float offset from the cell centre.
+__global__ void k_pack_sorted32(int64_t n, const int32_t* __restrict__ perm,
+                                const double* __restrict__ x, const double* __restrict__ box6,
+                                double cell, float4* __restrict__ out) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int64_t i = perm[k];
+  int c[3];
+  float o[3];
+  for (int a = 0; a < 3; ++a) {
+    double t = (x[3 * i + a] - box6[a]) / cell;
+    int ci = (int)floor(t);
+    ci = min(max(ci, 0), 1023);
+    c[a] = ci;
+    o[a] = (float)(x[3 * i + a] - (box6[a] + (ci + 0.5) * cell));
+  }
+  out[k] = make_float4(o[0], o[1], o[2], __int_as_float((c[0] << 20) | (c[1] << 10) | c[2]));
+}
+
+// ideal-gas EOS (physics/eos.py:21-28) for every particle; u <= 0 is an error
+__global__ void k_eos(int64_t n, const double* __restrict__ rho, const double* __restrict__ u,
+                      double gamma, double* __restrict__ P, double* __restrict__ cs, int* err) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double ui = u[i];
+  if (!(ui > 0.0)) set_error(err, ERR_NONPOSITIVE_U);
+  P[i] = (gamma - 1.0) * rho[i] * ui;
+  cs[i] = sqrt(gamma * (gamma - 1.0) * ui);
+}
+
+// after the force pass: add the disc viscosity, nu, alpha and v_sig of the rows
+__global__ void k_combine_rows(int64_t nrows, const int64_t* __restrict__ rows, int use_visc,
+                               double disc_alpha_av,
+                               const double* __restrict__ dacc, const double* __restrict__ ddudt,
+                               const double* __restrict__ cs, const double* __restrict__ h,
+                               const double* __restrict__ vsig_f, double* __restrict__ acc,
+                               double* __restrict__ dudt, double* __restrict__ vsig,
+                               double* __restrict__ nu) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows[q];
+  if (disc_alpha_av > 0) {
+    for (int c = 0; c < 3; ++c) acc[3 * i + c] += dacc[3 * i + c];
+    dudt[i] += ddudt[i];
+    if (nu) nu[i] = disc_alpha_av * cs[i] * h[i] / 10.0;
+  }
+  vsig[i] = use_visc ? vsig_f[i] : cs[i];
+}
+
+// touched sets: mark the rows and their list entries (optionally only interacting pairs)
+__global__ void k_mark(int64_t nrows, const int64_t* __restrict__ rows,
+                       const int32_t* __restrict__ perm, const int32_t* __restrict__ inv_perm,
+                       const int64_t* __restrict__ off, const int32_t* __restrict__ idx, int tight,
+                       const double* __restrict__ x, const double* __restrict__ h,
+                       uint8_t* __restrict__ mark) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows[q];
+  int64_t k = inv_perm[i];
+  mark[i] = 1;
+  double xi0 = x[3 * i], xi1 = x[3 * i + 1], xi2 = x[3 * i + 2], hi = h[i];
+  for (int64_t e = off[k]; e < off[k + 1]; ++e) {
+    int64_t j = perm[idx[e]];
+    if (tight) {
+      double d2 = d2_exact(x[3 * j] - xi0, x[3 * j + 1] - xi1, x[3 * j + 2] - xi2);
+      double rr = 2.0 * fmax(hi, h[j]);
+      if (!(d2 < rr * rr)) continue;
+    }
+    mark[j] = 1;
+  }
+}
+
+__global__ void k_mask_and_not(int64_t n, const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
+                               uint8_t* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = a[i] && !b[i];
+}
+
+__global__ void k_mask_or(int64_t n, const uint8_t* __restrict__ a, uint8_t* __restrict__ b) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  b[i] = b[i] | a[i];
+}
+
+__global__ void k_iota64(int64_t n, int64_t* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = i;
+}
+
+// rows with flag 2 (FLAG_SEARCH_TOO_SMALL): double their search; every row restarts from its h
+// (sim/sph.py:378-386)
+__global__ void k_grow(int64_t nrows, const int64_t* __restrict__ rows, const int64_t* __restrict__ flags,
+                       const double* __restrict__ h_res, double* __restrict__ hs,
+                       double* __restrict__ hg, int* __restrict__ count) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows[q];
+  if (flags[i] == 2) {
+    hs[i] = hs[i] * 2.0;
+    atomicAdd(count, 1);
+  }
+  hg[i] = h_res[i];
+}
+
+__global__ void k_count_flag2(int64_t nrows, const int64_t* __restrict__ rows,
+                              const int64_t* __restrict__ flags, int* __restrict__ count) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  if (flags[rows[q]] == 2) atomicAdd(count, 1);
+}
+
+__global__ void k_max_rows(int64_t nrows, const int64_t* __restrict__ rows, const double* __restrict__ a,
+                           double* __restrict__ b) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows[q];
+  b[i] = fmax(b[i], a[i]);
+}
+
+// ---------------------------------------------------------------- cache + density
+int Workspace::ensure(Engine& E, int64_t n) {
+  if (n <= cap && d_a) return 0;
+  release();
+  int64_t c = std::max<int64_t>(n + n / 4, 1024);
+  double** dd[] = {&d_a, &d_b, &d_c, &d_hg, &d_hs, &d_heff, &d_hlim, &d_disp, &d_P, &d_cs,
+                   &d_vsig, &d_ddudt, &d_dm, &d_tmp, &d_uh};
+  for (double** p : dd) NB_CUDA(cudaMalloc((void**)p, sizeof(double) * c));
+  double** d3[] = {&v_flow, &v_pred, &v_eval, &v_dacc, &v_tmp};
+  for (double** p : d3) NB_CUDA(cudaMalloc((void**)p, sizeof(double) * 3 * c));
+  double4** d4[] = {&pk0, &pk1, &pk2, &pk3};
+  for (double4** p : d4) NB_CUDA(cudaMalloc((void**)p, sizeof(double4) * c));
+  NB_CUDA(cudaMalloc((void**)&pk32, sizeof(float4) * c));
+  int64_t** i8[] = {&rows, &rows_s, &rows2, &iters, &flags, &need, &i_tmp, &pairs};
+  for (int64_t** p : i8) NB_CUDA(cudaMalloc((void**)p, sizeof(int64_t) * (c + 1)));
+  uint8_t** u1[] = {&m_rows, &m_done, &m_need, &m_tmp};
+  for (uint8_t** p : u1) NB_CUDA(cudaMalloc((void**)p, c));
+  NB_CUDA(cudaMalloc((void**)&i32a, sizeof(int32_t) * c));
+  NB_CUDA(cudaMalloc((void**)&i32b, sizeof(int32_t) * c));
+  NB_CUDA(cudaMalloc((void**)&dk_b, sizeof(double) * c));
+  NB_CUDA(cudaMalloc((void**)&d_int, sizeof(int) * 16));
+  NB_CUDA(cudaMalloc((void**)&d_i64, sizeof(int64_t) * 16));
+  NB_CUDA(cudaMallocHost((void**)&h_int, sizeof(int) * 16));
+  NB_CUDA(cudaMallocHost((void**)&h_i64, sizeof(int64_t) * 16));
+  NB_CUDA(cudaMallocHost((void**)&h_dbl, sizeof(double) * 80));
+  cap = c;
+  if (cache.cap < c) {
+    if (cache.x_ref) cudaFree(cache.x_ref);
+    if (cache.hs) cudaFree(cache.hs);
+    NB_CUDA(cudaMalloc((void**)&cache.x_ref, sizeof(double) * 3 * c));
+    NB_CUDA(cudaMalloc((void**)&cache.hs, sizeof(double) * c));
+    cache.cap = c;
+    cache.valid = false;
+  }
+  size_t need = cub_bytes_needed(c, 0);
+  size_t a = 0;
+  cub::DeviceRadixSort::SortPairsDescending((void*)nullptr, a, (double*)nullptr, (double*)nullptr,
+                                            (int32_t*)nullptr, (int32_t*)nullptr, (int)c);
+  size_t b = 0;
+  cub::DeviceReduce::Min((void*)nullptr, b, (int64_t*)nullptr, (int64_t*)nullptr, (int)c);
+  size_t d = 0;
+  cub::DeviceReduce::Sum((void*)nullptr, d, (double*)nullptr, (double*)nullptr, (int)c);
+  return E.ensure_cub(std::max(std::max(need, a), std::max(b, d)) + 4096);
+}
+
+void Workspace::release() {
+  void* ps[] = {d_a, d_b, d_c, d_hg, d_hs, d_heff, d_hlim, d_disp, d_P, d_cs, d_vsig, d_ddudt,
+                d_dm, d_tmp, d_uh, v_flow, v_pred, v_eval, v_dacc, v_tmp, pk0, pk1, pk2, pk3, pk32,
+                rows, rows_s, rows2, iters, flags, need, i_tmp, pairs, m_rows, m_done, m_need,
+                m_tmp, i32a, i32b, dk_b, d_int, d_i64};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  if (h_int) cudaFreeHost(h_int);
+  if (h_i64) cudaFreeHost(h_i64);
+  if (h_dbl) cudaFreeHost(h_dbl);
+  *this = Workspace{cache};
+}
+
+static int read_int(Engine& E, int* d, int* out, cudaStream_t st) {
+  NB_CUDA(cudaMemcpyAsync(E.ws.h_int, d, sizeof(int), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  *out = E.ws.h_int[0];
+  return 0;
+}
+
+// Density pass of `rows` on the current lists with the given search radii; results into the
+// caller-order arrays h_out, rho, omega and the scratch flags/iters.
+static int density_on_lists(Engine& E, int64_t n, const double* x, const double* mass,
+                            const double* h_start, const double* h_search, int64_t nrows,
+                            const int64_t* rows, const nb_params* prm, double* h_out,
+                            double* rho, double* omega, cudaStream_t st) {
+  Workspace& W = E.ws;
+  Lists& L = E.lists;
+  if (nrows == 0) return 0;
+  k_rows_to_sorted<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.inv_perm, W.rows_s);
+  k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, mass, W.d_a);
+  k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, h_start, W.d_b);
+  k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, h_search, W.d_c);
+  DensityParams dp{prm->kernel_id, prm->cnorm, prm->eta, prm->tol, prm->h_max};
+  if (prm->precision == 1) {
+    double span = 0;
+    NB_CUDA(cudaMemcpyAsync(W.h_dbl, E.bbox, sizeof(double) * 6, cudaMemcpyDeviceToHost, st));
+    NB_CUDA(cudaStreamSynchronize(st));
+    for (int a = 0; a < 3; ++a) span = std::max(span, W.h_dbl[3 + a] - W.h_dbl[a]);
+    double cell = std::max(span / 1000.0, 1e-30);
+    k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, E.bbox, cell, W.pk32);
+    launch_density32<int32_t>(nrows, W.rows_s, W.pk32, (float)cell, W.d_a, W.d_b, W.d_c, L.off,
+                              L.idx, dp, L.perm, h_out, rho, omega, W.iters, W.flags, st);
+  } else {
+    k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, nullptr, W.pk0);
+    launch_density64<int32_t>(nrows, W.rows_s, W.pk0, W.d_a, W.d_b, W.d_c, L.off, L.idx, dp,
+                              L.perm, h_out, rho, omega, W.iters, W.flags, st);
+  }
+  NB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// sim/sph.py:117-147 (_reuse_limits): returns 1 with W.d_heff filled if the cached lists are
+// provably complete for the search limits h_eff, else 0.
+static int reuse_limits(Engine& E, int64_t n, const double* x, const double* hg, int* ok,
+                        cudaStream_t st) {
+  Workspace& W = E.ws;
+  Cache& C = W.cache;
+  *ok = 0;
+  k_disp<<<grid_for(n), NB_THREADS, 0, st>>>(n, x, C.x_ref, W.d_disp, W.i32a);
+  size_t tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceRadixSort::SortPairsDescending(E.cub_tmp, tmp, W.d_disp, W.dk_b, W.i32a,
+                                                    W.i32b, (int)n, 0, 64, st));
+  int top = (int)std::min<int64_t>(n, 65);
+  NB_CUDA(cudaMemcpyAsync(W.h_dbl, W.dk_b, sizeof(double) * top, cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  static const int FAST[] = {0, 1, 2, 4, 8, 16, 32, 64};
+  for (int nf : FAST) {
+    if (nf >= top) break;
+    double d_rest = W.h_dbl[nf];
+    NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
+    k_reuse_test<<<grid_for(n), NB_THREADS, 0, st>>>(n, C.hs, W.d_disp, d_rest, hg, W.m_rows,
+                                                     W.d_heff, W.d_hlim, W.d_int);
+    int fail = 0;
+    NB_TRY(read_int(E, W.d_int, &fail, st));
+    if (fail) continue;
+    if (nf == 0) {
+      *ok = 1;
+      return 0;
+    }
+    NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
+    k_fast_complete<<<nf, NB_THREADS, 0, st>>>(n, nf, W.i32b, x, W.d_hlim, E.lists.inv_perm,
+                                               E.lists.off, E.lists.idx, W.d_int);
+    NB_TRY(read_int(E, W.d_int, &fail, st));
+    if (!fail) {
+      *ok = 1;
+      return 0;
+    }
+  }
+  return 0;
+}
+
+// sim/sph.py:329-387 (compute_density) for `rows` (caller order, W.rows is NOT used here): reuse
+// the cached lists while provably complete, else rebuild with search h_guess * skin and double
+// the search of rows whose root lies beyond it, up to 12 rounds.  h (in/out, caller order) is the
+// guess for every particle; rows get their solved h, and rho / omega.
+int compute_density(Engine& E, int64_t n, const double* x, const double* mass, double* h,
+                    double* rho, double* omega, int64_t nrows, const int64_t* rows,
+                    const nb_params* prm, int64_t* builds, int64_t* reuses, cudaStream_t st) {
+  Workspace& W = E.ws;
+  Cache& C = W.cache;
+  NB_TRY(W.ensure(E, n));
+  NB_CUDA(cudaMemsetAsync(W.m_rows, 0, n, st));
+  k_mask_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, n, W.m_rows, E.d_err);
+  NB_CUDA(cudaMemcpyAsync(W.d_hg, h, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  if (C.valid && C.n == n && n > 0 && E.lists.n == n) {
+    int ok = 0;
+    NB_TRY(reuse_limits(E, n, x, W.d_hg, &ok, st));
+    if (ok) {
+      NB_TRY(density_on_lists(E, n, x, mass, W.d_hg, W.d_heff, nrows, rows, prm, h, rho, omega, st));
+      NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
+      k_count_flag2<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, W.flags, W.d_int);
+      int grow_n = 0;
+      NB_TRY(read_int(E, W.d_int, &grow_n, st));
+      if (grow_n == 0) {
+        *reuses += 1;
+        return check_device_error(E, st);
+      }
+      k_max_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, h, W.d_hg);
+    }
+  }
+  k_hsearch<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.d_hg, prm->h_max, prm->skin, W.d_hs);
+  for (int round = 0; round < 12; ++round) {
+    NB_TRY(build_lists(E, n, x, W.d_hs, st));
+    *builds += 1;
+    NB_TRY(density_on_lists(E, n, x, mass, W.d_hg, W.d_hs, nrows, rows, prm, h, rho, omega, st));
+    NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
+    k_grow<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, W.flags, h, W.d_hs, W.d_hg, W.d_int);
+    int grow_n = 0;
+    NB_TRY(read_int(E, W.d_int, &grow_n, st));
+    if (grow_n == 0) {
+      NB_CUDA(cudaMemcpyAsync(C.x_ref, x, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, st));
+      NB_CUDA(cudaMemcpyAsync(C.hs, W.d_hs, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+      C.valid = true;
+      C.n = n;
+      return check_device_error(E, st);
+    }
+  }
+  std::snprintf(E.last_error, sizeof(E.last_error),
+                "smoothing lengths kept outgrowing the neighbour search");
+  return NB_ERR_SEARCH;
+}
+
+void mark_rows(Engine& E, int64_t nrows, const int64_t* rows, int tight, const double* x,
+               const double* h, uint8_t* mark, cudaStream_t st) {
+  if (nrows <= 0) return;
+  Lists& L = E.lists;
+  k_mark<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.perm, L.inv_perm, L.off, L.idx,
+                                                 tight, x, h, mark);
+}
+
+void mask_and_not(int64_t n, const uint8_t* a, const uint8_t* b, uint8_t* out, cudaStream_t st) {
+  if (n > 0) k_mask_and_not<<<grid_for(n), NB_THREADS, 0, st>>>(n, a, b, out);
+}
+
+void mask_or(int64_t n, const uint8_t* a, uint8_t* b, cudaStream_t st) {
+  if (n > 0) k_mask_or<<<grid_for(n), NB_THREADS, 0, st>>>(n, a, b);
+}
+
+int select_mask(Engine& E, int64_t n, const uint8_t* mask, int64_t* out, int64_t* count,
+                cudaStream_t st) {
+  Workspace& W = E.ws;
+  k_iota64<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.i_tmp);
+  size_t tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceSelect::Flagged(E.cub_tmp, tmp, W.i_tmp, mask, out, W.d_i64, (int)n, st));
+  NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  *count = W.h_i64[0];
+  return 0;
+}
+
+// Fused EOS + force pass for `rows` (caller order) with interacting pairs only (the tightened
+// lists of sim/neighbours.py:284-323, tested on the fly).  Writes a_hydro, dudt, vsig_max,
+// visc_heating (and nu) at the rows.  P and c_s of every particle go to W.d_P / W.d_cs.
+int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, int64_t nrows,
+                  const int64_t* rows, const nb_params* prm, cudaStream_t st) {
+  Workspace& W = E.ws;
+  Lists& L = E.lists;
+  int64_t n = s->n;
+  k_eos<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->rho, u, prm->gamma, W.d_P, W.d_cs, E.d_err);
+  if (nrows == 0) return check_device_error(E, st);
+  k_rows_to_sorted<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.inv_perm, W.rows_s);
+  k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, vel, s->mass, W.pk1);
+  k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->h, s->rho, s->omega, W.d_P, W.pk2);
+  k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, W.pk3);
+  ForceParams fp{};
+  fp.kid = prm->kernel_id;
+  fp.cnorm = prm->cnorm;
+  fp.use_sph = 1;
+  fp.use_visc = prm->viscosity;
+  fp.use_cond = prm->viscosity && prm->conductivity;
+  fp.cond_signal = prm->cond_signal;
+  fp.beta = prm->beta;
+  fp.alpha_u = prm->alpha_u;
+  fp.use_disc = prm->disc_alpha_av > 0;
+  fp.disc_alpha_av = prm->disc_alpha_av;
+  fp.tighten = 1;
+  ForceOut fo;
+  fo.acc = s->a_hydro;
+  fo.dudt = s->dudt;
+  fo.vsig = W.d_vsig;
+  fo.vheat = s->visc_heating;
+  fo.dacc = W.v_dacc;
+  fo.ddudt = W.d_ddudt;
+  fo.pairs = W.pairs;
+  if (prm->precision == 1) {
+    NB_CUDA(cudaMemcpyAsync(W.h_dbl, E.bbox, sizeof(double) * 6, cudaMemcpyDeviceToHost, st));
+    NB_CUDA(cudaStreamSynchronize(st));
+    double span = 0;
+    for (int a = 0; a < 3; ++a) span = std::max(span, W.h_dbl[3 + a] - W.h_dbl[a]);
+    // the grid must cover the current positions: recompute the box when particles moved
+    double cell = std::max(span / 1000.0, 1e-30);
+    k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, E.bbox, cell, W.pk32);
+    launch_forces32<int32_t>(nrows, W.rows_s, W.pk32, (float)cell, W.pk1, W.pk2, W.pk3, L.off,
+                             L.idx, fp, L.perm, fo, st);
+  } else {
+    k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, nullptr, W.pk0);
+    launch_forces64<int32_t>(nrows, W.rows_s, W.pk0, W.pk1, W.pk2, W.pk3, L.off, L.idx, fp,
+                             L.perm, fo, st);
+  }
+  k_combine_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(
+      nrows, rows, prm->viscosity, prm->disc_alpha_av, W.v_dacc, W.d_ddudt, W.d_cs, s->h,
+      W.d_vsig, s->a_hydro, s->dudt, s->vsig_max, s->nu);
+  NB_CUDA(cudaGetLastError());
+  return check_device_error(E, st);
+}
+
+}  // namespace nbk

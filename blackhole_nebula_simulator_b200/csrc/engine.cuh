@@ -1,0 +1,125 @@
+// The engine context behind the C-ABI: device workspace that grows on demand and is reused,
+// the cached neighbour lists of the last build, and error reporting.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+
+#include "common.cuh"
+
+namespace nbk {
+
+constexpr int MAX_LEVELS = 16;
+
+// Symmetric lists of the last build, in sorted (Morton) order: row k belongs to the particle
+// perm[k] of the caller's order; entries are sorted positions.
+struct Lists {
+  int64_t n = 0, total = 0;
+  int32_t* perm = nullptr;      // sorted position -> caller index
+  int32_t* inv_perm = nullptr;  // caller index -> sorted position
+  double4* spos = nullptr;      // sorted (x, y, z, h_search)
+  int64_t* off = nullptr;       // n + 1
+  int32_t* idx = nullptr;       // total
+};
+
+struct Engine;
+
+// Cached lists of the last build: positions and search radii they were built with
+// (sim/sph.py:62-82, NeighbourCache).
+struct Cache {
+  bool valid = false;
+  int64_t n = 0;
+  double* x_ref = nullptr;
+  double* hs = nullptr;
+  int64_t cap = 0;
+};
+
+// Per-particle scratch of the step runtime (caller order unless noted).
+struct Workspace {
+  Cache cache;
+  int64_t cap = 0;
+  double *d_a = nullptr, *d_b = nullptr, *d_c = nullptr, *d_hg = nullptr, *d_hs = nullptr,
+         *d_heff = nullptr, *d_hlim = nullptr, *d_disp = nullptr, *d_P = nullptr,
+         *d_cs = nullptr, *d_vsig = nullptr, *d_ddudt = nullptr, *d_dm = nullptr,
+         *d_tmp = nullptr, *d_uh = nullptr;
+  double *v_flow = nullptr, *v_pred = nullptr, *v_eval = nullptr, *v_dacc = nullptr,
+         *v_tmp = nullptr;  // (n, 3)
+  double4 *pk0 = nullptr, *pk1 = nullptr, *pk2 = nullptr, *pk3 = nullptr;  // sorted packs
+  float4* pk32 = nullptr;
+  int64_t *rows = nullptr, *rows_s = nullptr, *rows2 = nullptr, *iters = nullptr,
+          *flags = nullptr, *need = nullptr, *i_tmp = nullptr, *pairs = nullptr;
+  uint8_t *m_rows = nullptr, *m_done = nullptr, *m_need = nullptr, *m_tmp = nullptr;
+  int32_t *i32a = nullptr, *i32b = nullptr;
+  double* dk_b = nullptr;
+  int* d_int = nullptr;
+  int64_t* d_i64 = nullptr;
+  int* h_int = nullptr;
+  int64_t* h_i64 = nullptr;
+  double* h_dbl = nullptr;
+  int ensure(Engine& E, int64_t n);
+  void release();
+};
+
+struct Engine {
+  int device = 0;
+  int* d_err = nullptr;
+  int* h_err = nullptr;  // pinned
+  char last_error[512] = {0};
+  int64_t cap_n = 0, cap_nodes = 0, cap_list = 0, cap_sort = 0;
+  double* bbox_part = nullptr;
+  double* bbox = nullptr;
+  uint64_t* keys_a = nullptr;
+  uint64_t* keys_b = nullptr;
+  int32_t* vals_a = nullptr;
+  int64_t* counts = nullptr;
+  double4* node_lo = nullptr;
+  double4* node_hi = nullptr;
+  void* cub_tmp = nullptr;
+  size_t cub_bytes = 0;
+  int64_t* sort_keys = nullptr;
+  double* red = nullptr;      // reduction partials (doubles)
+  double* h_red = nullptr;    // pinned host copy of small reductions
+  Lists lists;
+  Workspace ws;
+
+  int ensure_n(int64_t n);
+  int ensure_nodes(int64_t m);
+  int grow2(int64_t m);
+  int ensure_list_capacity(int64_t m);
+  int ensure_sort_keys(int64_t m);
+  int ensure_cub(size_t bytes);
+  void release();
+};
+
+size_t cub_bytes_needed(int64_t n, int64_t m);
+int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaStream_t st);
+int export_lists_offsets(Engine& E, int64_t* off_out, cudaStream_t st);
+int export_lists(Engine& E, int64_t* off_out, int64_t* idx_out, cudaStream_t st);
+
+inline int set_host_error(Engine& E, const char* msg) {
+  std::snprintf(E.last_error, sizeof(E.last_error), "%s", msg);
+  return -1;
+}
+
+int check_device_error(Engine& E, cudaStream_t st);
+
+}  // namespace nbk
+
+#define NB_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t _e = (call);                                                                 \
+    if (_e != cudaSuccess) {                                                                 \
+      std::snprintf(E.last_error, sizeof(E.last_error), "CUDA error %s at %s:%d: %s",        \
+                    cudaGetErrorName(_e), __FILE__, __LINE__, cudaGetErrorString(_e));       \
+      return -2;                                                                             \
+    }                                                                                        \
+  } while (0)
+
+#define NB_TRY(expr)        \
+  do {                      \
+    int _r = (expr);        \
+    if (_r != 0) return _r; \
+  } while (0)

@@ -1,0 +1,370 @@
+// Neighbour lists on the GPU: Morton-sorted particles, an implicit 8-ary tree of boxes over
+// leaves of 32 consecutive sorted particles, and a warp-per-leaf traversal that writes exact
+// symmetric lists.
+//
+// The set is the reference's (sim/neighbours.py:240-281, find_neighbours_numba):
+//     N(i) = { j : r_ij^2 < (2 h_i)^2  or  r_ij^2 < (2 h_j)^2 },  i itself included,
+// with r_ij^2 = dx*dx + dy*dy + dz*dz, dx = x_j - x_i, evaluated in double with the reference's
+// rounding (no fused multiply-add), so the lists are identical bit for bit.  The tree only
+// prunes: a node is skipped when the distance between its box and the query leaf's box is at
+// least 2 max(h_query_max, h_node_max) (with a 1e-12 relative margin on the safe side), which
+// can never drop a pair the test above accepts.
+//
+// Rows come out in sorted (Morton) order with each row's entries in ascending sorted index.
+#include <cub/cub.cuh>
+
+#include "common.cuh"
+#include "engine.cuh"
+
+namespace nbk {
+
+static constexpr int LEAF = 32;
+static constexpr int FAN = 8;
+static constexpr int STACK = 96;
+
+// ---------------------------------------------------------------- bounding box
+__global__ void k_bbox_partial(int64_t n, const double* __restrict__ pos, double* __restrict__ part) {
+  __shared__ double s[6][NB_THREADS];
+  double mn[3] = {1e308, 1e308, 1e308}, mx[3] = {-1e308, -1e308, -1e308};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    for (int c = 0; c < 3; ++c) {
+      double v = pos[3 * i + c];
+      mn[c] = fmin(mn[c], v);
+      mx[c] = fmax(mx[c], v);
+    }
+  }
+  for (int c = 0; c < 3; ++c) {
+    s[c][threadIdx.x] = mn[c];
+    s[3 + c][threadIdx.x] = mx[c];
+  }
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int c = 0; c < 3; ++c) {
+        s[c][threadIdx.x] = fmin(s[c][threadIdx.x], s[c][threadIdx.x + w]);
+        s[3 + c][threadIdx.x] = fmax(s[3 + c][threadIdx.x], s[3 + c][threadIdx.x + w]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < 6; ++c) part[6 * blockIdx.x + c] = s[c][0];
+}
+
+__global__ void k_bbox_final(int nb, const double* __restrict__ part, double* __restrict__ box6) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double r[6] = {1e308, 1e308, 1e308, -1e308, -1e308, -1e308};
+  for (int b = 0; b < nb; ++b)
+    for (int c = 0; c < 3; ++c) {
+      r[c] = fmin(r[c], part[6 * b + c]);
+      r[3 + c] = fmax(r[3 + c], part[6 * b + 3 + c]);
+    }
+  for (int c = 0; c < 6; ++c) box6[c] = r[c];
+}
+
+// ---------------------------------------------------------------- Morton keys
+__device__ __forceinline__ uint64_t spread21(uint64_t v) {
+  v &= 0x1fffffull;
+  v = (v | (v << 32)) & 0x1f00000000ffffull;
+  v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+  v = (v | (v << 8)) & 0x100f00f00f00f00full;
+  v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+  v = (v | (v << 2)) & 0x1249249249249249ull;
+  return v;
+}
+
+__global__ void k_morton(int64_t n, const double* __restrict__ pos, const double* __restrict__ box6,
+                         uint64_t* __restrict__ keys, int32_t* __restrict__ vals) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double span = fmax(fmax(box6[3] - box6[0], box6[4] - box6[1]), box6[5] - box6[2]);
+  double scale = span > 0 ? 2097151.0 / span : 0.0;
+  uint64_t q[3];
+  for (int c = 0; c < 3; ++c) {
+    double t = (pos[3 * i + c] - box6[c]) * scale;
+    t = fmin(fmax(t, 0.0), 2097151.0);
+    q[c] = (uint64_t)t;
+  }
+  keys[i] = (spread21(q[0]) << 2) | (spread21(q[1]) << 1) | spread21(q[2]);
+  vals[i] = (int32_t)i;
+}
+
+__global__ void k_gather_sorted(int64_t n, const int32_t* __restrict__ perm,
+                                const double* __restrict__ pos, const double* __restrict__ hs,
+                                double4* __restrict__ spos, int32_t* __restrict__ inv_perm) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int32_t i = perm[k];
+  spos[k] = make_double4(pos[3 * (int64_t)i], pos[3 * (int64_t)i + 1], pos[3 * (int64_t)i + 2], hs[i]);
+  inv_perm[i] = (int32_t)k;
+}
+
+// ---------------------------------------------------------------- tree of boxes
+__global__ void k_leaf_boxes(int64_t n, int64_t nleaf, const double4* __restrict__ spos,
+                             double4* __restrict__ lo, double4* __restrict__ hi) {
+  int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (l >= nleaf) return;
+  int64_t a = l * LEAF, b = min(a + LEAF, n);
+  double4 mn = make_double4(1e308, 1e308, 1e308, 0.0), mx = make_double4(-1e308, -1e308, -1e308, 0.0);
+  for (int64_t k = a; k < b; ++k) {
+    double4 p = spos[k];
+    mn.x = fmin(mn.x, p.x);
+    mn.y = fmin(mn.y, p.y);
+    mn.z = fmin(mn.z, p.z);
+    mx.x = fmax(mx.x, p.x);
+    mx.y = fmax(mx.y, p.y);
+    mx.z = fmax(mx.z, p.z);
+    mn.w = fmax(mn.w, p.w);  // lo.w carries the largest h of the node
+  }
+  lo[l] = mn;
+  hi[l] = mx;
+}
+
+__global__ void k_level_up(int64_t nchild, int64_t nparent, const double4* __restrict__ clo,
+                           const double4* __restrict__ chi, double4* __restrict__ plo,
+                           double4* __restrict__ phi) {
+  int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= nparent) return;
+  double4 mn = make_double4(1e308, 1e308, 1e308, 0.0), mx = make_double4(-1e308, -1e308, -1e308, 0.0);
+  for (int64_t c = p * FAN; c < min((p + 1) * FAN, nchild); ++c) {
+    double4 a = clo[c], b = chi[c];
+    mn.x = fmin(mn.x, a.x);
+    mn.y = fmin(mn.y, a.y);
+    mn.z = fmin(mn.z, a.z);
+    mn.w = fmax(mn.w, a.w);
+    mx.x = fmax(mx.x, b.x);
+    mx.y = fmax(mx.y, b.y);
+    mx.z = fmax(mx.z, b.z);
+  }
+  plo[p] = mn;
+  phi[p] = mx;
+}
+
+struct TreeView {
+  const double4* lo;
+  const double4* hi;
+  int64_t level_off[MAX_LEVELS + 1];
+  int64_t level_size[MAX_LEVELS];
+  int nlevels;
+};
+
+__device__ __forceinline__ double box_gap2(double4 alo, double4 ahi, double4 blo, double4 bhi) {
+  double gx = fmax(fmax(blo.x - ahi.x, alo.x - bhi.x), 0.0);
+  double gy = fmax(fmax(blo.y - ahi.y, alo.y - bhi.y), 0.0);
+  double gz = fmax(fmax(blo.z - ahi.z, alo.z - bhi.z), 0.0);
+  return gx * gx + gy * gy + gz * gz;
+}
+
+// Warp per query leaf.  pass 0 counts each row's entries, pass 1 writes them.  Node entries on
+// the stack are (level << 40) | index; children are pushed highest first so leaves are reached in
+// ascending order, which keeps every row sorted.
+template <int PASS>
+__global__ void __launch_bounds__(NB_THREADS) k_lists(int64_t n, int64_t nleaf, TreeView tv,
+                                                      const double4* __restrict__ spos,
+                                                      int64_t* __restrict__ counts,
+                                                      const int64_t* __restrict__ off,
+                                                      int32_t* __restrict__ idx, int* err) {
+  __shared__ int64_t stack_s[NB_THREADS / 32][STACK];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int64_t leaf = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (leaf >= nleaf) return;  // warp-uniform
+  int64_t* stack = stack_s[wib];
+  int64_t k = leaf * LEAF + lane;
+  bool valid = k < n;
+  double4 me = valid ? spos[k] : make_double4(0, 0, 0, 0);
+  double ri = 2.0 * me.w;
+  double r2i = __dmul_rn(ri, ri);
+  const double4 qlo = tv.lo[leaf], qhi = tv.hi[leaf];
+  const double qh = qlo.w;
+  int64_t m = 0, base = 0, cap = 0;
+  if (PASS == 1 && valid) {
+    base = off[k];
+    cap = off[k + 1] - base;
+  }
+  int sp = 0;
+  if (lane == 0) stack[0] = ((int64_t)(tv.nlevels - 1) << 40);
+  sp = 1;
+  __syncwarp();
+  while (sp > 0) {
+    int64_t e = stack[sp - 1];
+    __syncwarp();
+    sp -= 1;
+    int lvl = (int)(e >> 40);
+    int64_t node = e & ((1ll << 40) - 1);
+    if (lvl == 0) {
+      // candidate leaf: lanes load its particles, every query lane tests all of them
+      int64_t cb = node * LEAF;
+      int64_t kk = cb + lane;
+      double4 c = kk < n ? spos[kk] : make_double4(0, 0, 0, 0);
+      int cnt = (int)min((int64_t)LEAF, n - cb);
+      for (int t = 0; t < cnt; ++t) {
+        double cx = __shfl_sync(0xffffffffu, c.x, t);
+        double cy = __shfl_sync(0xffffffffu, c.y, t);
+        double cz = __shfl_sync(0xffffffffu, c.z, t);
+        double ch = __shfl_sync(0xffffffffu, c.w, t);
+        if (!valid) continue;
+        double d2 = d2_exact(cx - me.x, cy - me.y, cz - me.z);
+        double rj = 2.0 * ch;
+        if (d2 < r2i || d2 < __dmul_rn(rj, rj)) {
+          if (PASS == 1) {
+            if (m < cap)
+              idx[base + m] = (int32_t)(cb + t);
+            else
+              set_error(err, ERR_LIST_OVERFLOW);
+          }
+          m += 1;
+        }
+      }
+      continue;
+    }
+    // internal node: lanes 0..FAN-1 test one child each against the query leaf's box
+    int64_t c0 = node * FAN;
+    int64_t csize = tv.level_size[lvl - 1];
+    int64_t child = c0 + lane;
+    bool hit = false;
+    if (lane < FAN && child < csize) {
+      int64_t g = tv.level_off[lvl - 1] + child;
+      double4 blo = tv.lo[g], bhi = tv.hi[g];
+      double reach = 2.0 * fmax(qh, blo.w);
+      hit = box_gap2(qlo, qhi, blo, bhi) < reach * reach * (1.0 + 1e-12);
+    }
+    unsigned mask = __ballot_sync(0xffffffffu, hit);
+    int nh = __popc(mask);
+    if (sp + nh > STACK) {
+      set_error(err, ERR_TRAVERSAL_STACK);
+      break;
+    }
+    if (hit) {
+      // highest child first on the stack: its position counts the set bits above this lane
+      int above = __popc(mask & ~((2u << lane) - 1u));
+      stack[sp + above] = ((int64_t)(lvl - 1) << 40) | child;
+    }
+    __syncwarp();
+    sp += nh;
+  }
+  if (PASS == 0 && valid) counts[k] = m;
+}
+
+// ---------------------------------------------------------------- export to original order
+__global__ void k_export_counts(int64_t n, const int32_t* __restrict__ inv_perm,
+                                const int64_t* __restrict__ off_s, int64_t* __restrict__ cnt_o) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int32_t k = inv_perm[i];
+  cnt_o[i] = off_s[k + 1] - off_s[k];
+}
+
+__global__ void k_export_fill(int64_t n, const int32_t* __restrict__ perm,
+                              const int64_t* __restrict__ off_s, const int32_t* __restrict__ idx_s,
+                              const int64_t* __restrict__ off_o, int64_t* __restrict__ idx_o) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int64_t i = perm[k];
+  int64_t dst = off_o[i];
+  for (int64_t e = off_s[k]; e < off_s[k + 1]; ++e) idx_o[dst++] = perm[idx_s[e]];
+}
+
+// ---------------------------------------------------------------- host orchestration
+int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaStream_t st) {
+  NB_TRY(E.ensure_n(n));
+  if (n == 0) {
+    E.lists.n = 0;
+    E.lists.total = 0;
+    NB_CUDA(cudaMemsetAsync(E.lists.off, 0, sizeof(int64_t), st));
+    return 0;
+  }
+  Lists& L = E.lists;
+  // bounding box and Morton keys
+  int nbb = (int)std::min<int64_t>(grid_for(n), 1184);
+  k_bbox_partial<<<nbb, NB_THREADS, 0, st>>>(n, pos, E.bbox_part);
+  k_bbox_final<<<1, 32, 0, st>>>(nbb, E.bbox_part, E.bbox);
+  k_morton<<<grid_for(n), NB_THREADS, 0, st>>>(n, pos, E.bbox, E.keys_a, E.vals_a);
+  size_t tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceRadixSort::SortPairs(E.cub_tmp, tmp, E.keys_a, E.keys_b, E.vals_a, L.perm,
+                                          (int)n, 0, 63, st));
+  k_gather_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, pos, hs, L.spos, L.inv_perm);
+  // tree
+  int64_t nleaf = (n + LEAF - 1) / LEAF;
+  TreeView tv;
+  int64_t size = nleaf, offs = 0;
+  int nl = 0;
+  while (true) {
+    tv.level_off[nl] = offs;
+    tv.level_size[nl] = size;
+    offs += size;
+    nl += 1;
+    if (size == 1 || nl == MAX_LEVELS) break;
+    size = (size + FAN - 1) / FAN;
+  }
+  tv.level_off[nl] = offs;
+  tv.nlevels = nl;
+  if (tv.level_size[nl - 1] != 1) return set_host_error(E, "tree deeper than MAX_LEVELS");
+  NB_TRY(E.ensure_nodes(offs));
+  k_leaf_boxes<<<grid_for(nleaf), NB_THREADS, 0, st>>>(n, nleaf, L.spos, E.node_lo, E.node_hi);
+  for (int l = 1; l < nl; ++l)
+    k_level_up<<<grid_for(tv.level_size[l]), NB_THREADS, 0, st>>>(
+        tv.level_size[l - 1], tv.level_size[l], E.node_lo + tv.level_off[l - 1],
+        E.node_hi + tv.level_off[l - 1], E.node_lo + tv.level_off[l], E.node_hi + tv.level_off[l]);
+  tv.lo = E.node_lo;
+  tv.hi = E.node_hi;
+  // count, scan, fill
+  unsigned gb = grid_for(nleaf * 32);
+  k_lists<0><<<gb, NB_THREADS, 0, st>>>(n, nleaf, tv, L.spos, E.counts, nullptr, nullptr, E.d_err);
+  NB_CUDA(cudaMemsetAsync(L.off, 0, sizeof(int64_t), st));
+  tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, E.counts, L.off + 1, (int)n, st));
+  int64_t total = 0;
+  NB_CUDA(cudaMemcpyAsync(&total, L.off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  NB_TRY(E.ensure_list_capacity(total));
+  k_lists<1><<<gb, NB_THREADS, 0, st>>>(n, nleaf, tv, L.spos, nullptr, L.off, L.idx, E.d_err);
+  L.n = n;
+  L.total = total;
+  return check_device_error(E, st);
+}
+
+// Offsets (n + 1) of the last build's lists in the caller's order.
+int export_lists_offsets(Engine& E, int64_t* off_out, cudaStream_t st) {
+  Lists& L = E.lists;
+  int64_t n = L.n;
+  NB_CUDA(cudaMemsetAsync(off_out, 0, sizeof(int64_t), st));
+  if (n == 0) return 0;
+  k_export_counts<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.inv_perm, L.off, E.counts);
+  size_t tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, E.counts, off_out + 1, (int)n, st));
+  return check_device_error(E, st);
+}
+
+// Entries of the last build's lists in the caller's order and numbering, each row ascending;
+// off_out must hold the offsets from export_lists_offsets.
+int export_lists(Engine& E, int64_t* off_out, int64_t* idx_out, cudaStream_t st) {
+  Lists& L = E.lists;
+  int64_t n = L.n;
+  if (n == 0) return 0;
+  size_t tmp = E.cub_bytes;
+  k_export_fill<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, L.off, L.idx, off_out, idx_out);
+  if (L.total > 0) {
+    NB_TRY(E.ensure_sort_keys(L.total));
+    NB_CUDA(cudaMemcpyAsync(E.sort_keys, idx_out, sizeof(int64_t) * L.total,
+                            cudaMemcpyDeviceToDevice, st));
+    tmp = E.cub_bytes;
+    NB_CUDA(cub::DeviceSegmentedSort::SortKeys(E.cub_tmp, tmp, E.sort_keys, idx_out, L.total,
+                                                (int)n, off_out, off_out + 1, st));
+  }
+  return check_device_error(E, st);
+}
+
+size_t cub_bytes_needed(int64_t n, int64_t m) {
+  size_t a = 0, b = 0, c = 0, d = 0;
+  cub::DeviceRadixSort::SortPairs((void*)nullptr, a, (uint64_t*)nullptr, (uint64_t*)nullptr,
+                                  (int32_t*)nullptr, (int32_t*)nullptr, (int)n, 0, 63);
+  cub::DeviceScan::InclusiveSum((void*)nullptr, b, (int64_t*)nullptr, (int64_t*)nullptr, (int)n);
+  if (m > 0)
+    cub::DeviceSegmentedSort::SortKeys((void*)nullptr, c, (int64_t*)nullptr, (int64_t*)nullptr,
+                                       m, (int)n, (int64_t*)nullptr, (int64_t*)nullptr);
+  cub::DeviceSelect::Flagged((void*)nullptr, d, (int64_t*)nullptr, (const uint8_t*)nullptr,
+                             (int64_t*)nullptr, (int64_t*)nullptr, (int)n);
+  return std::max(std::max(a, b), std::max(c, d)) + 256;
+}
+
+}  // namespace nbk

@@ -1,0 +1,42 @@
+// FP32 instantiations of the pair passes (fused multiply-add allowed: the FP32 path is judged
+// against the FP64 oracle by its stated tolerance, not bit for bit).
+#include "sph_impl.cuh"
+
+namespace nbk {
+
+template <typename I>
+void launch_density32(int64_t nrows, const int64_t* rows, const float4* pos, float cell,
+                      const double* mass, const double* h_start, const double* h_search,
+                      const int64_t* off, const I* idx, DensityParams prm, const int32_t* out_map,
+                      double* h_out, double* rho, double* omega, int64_t* iters, int64_t* flags,
+                      cudaStream_t st) {
+  if (nrows <= 0) return;
+  Pos32 geo{pos, cell};
+  k_density<float, Pos32, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+      nrows, rows, geo, mass, h_start, h_search, off, idx, prm, out_map, h_out, rho, omega, iters,
+      flags);
+}
+
+template <typename I>
+void launch_forces32(int64_t nrows, const int64_t* rows, const float4* pos, float cell,
+                     const double4* vm, const double4* hydro, const double4* aux,
+                     const int64_t* off, const I* idx, ForceParams prm, const int32_t* out_map,
+                     ForceOut out, cudaStream_t st) {
+  if (nrows <= 0) return;
+  Pos32 geo{pos, cell};
+  k_forces<float, Pos32, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+      nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
+}
+
+
+template void launch_density32<int32_t>(int64_t, const int64_t*, const float4*, float,
+                                        const double*, const double*, const double*,
+                                        const int64_t*, const int32_t*, DensityParams,
+                                        const int32_t*, double*, double*, double*, int64_t*,
+                                        int64_t*, cudaStream_t);
+template void launch_forces32<int32_t>(int64_t, const int64_t*, const float4*, float,
+                                       const double4*, const double4*, const double4*,
+                                       const int64_t*, const int32_t*, ForceParams,
+                                       const int32_t*, ForceOut, cudaStream_t);
+
+}  // namespace nbk

@@ -1,0 +1,81 @@
+// FP64 instantiations of the pair passes (compiled without fused multiply-add: the FP64 path
+// rounds like the reference).
+#include "sph_impl.cuh"
+
+namespace nbk {
+
+template <typename I>
+void launch_density64(int64_t nrows, const int64_t* rows, const double4* pos, const double* mass,
+                      const double* h_start, const double* h_search, const int64_t* off,
+                      const I* idx, DensityParams prm, const int32_t* out_map, double* h_out,
+                      double* rho, double* omega, int64_t* iters, int64_t* flags, cudaStream_t st) {
+  if (nrows <= 0) return;
+  Pos64 geo{pos};
+  k_density<double, Pos64, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+      nrows, rows, geo, mass, h_start, h_search, off, idx, prm, out_map, h_out, rho, omega, iters,
+      flags);
+}
+
+template <typename I>
+void launch_forces64(int64_t nrows, const int64_t* rows, const double4* pos, const double4* vm,
+                     const double4* hydro, const double4* aux, const int64_t* off, const I* idx,
+                     ForceParams prm, const int32_t* out_map, ForceOut out, cudaStream_t st) {
+  if (nrows <= 0) return;
+  Pos64 geo{pos};
+  k_forces<double, Pos64, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+      nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
+}
+
+template void launch_density64<int64_t>(int64_t, const int64_t*, const double4*, const double*,
+                                        const double*, const double*, const int64_t*,
+                                        const int64_t*, DensityParams, const int32_t*, double*,
+                                        double*, double*, int64_t*, int64_t*, cudaStream_t);
+template void launch_density64<int32_t>(int64_t, const int64_t*, const double4*, const double*,
+                                        const double*, const double*, const int64_t*,
+                                        const int32_t*, DensityParams, const int32_t*, double*,
+                                        double*, double*, int64_t*, int64_t*, cudaStream_t);
+template void launch_forces64<int64_t>(int64_t, const int64_t*, const double4*, const double4*,
+                                       const double4*, const double4*, const int64_t*,
+                                       const int64_t*, ForceParams, const int32_t*, ForceOut,
+                                       cudaStream_t);
+template void launch_forces64<int32_t>(int64_t, const int64_t*, const double4*, const double4*,
+                                       const double4*, const double4*, const int64_t*,
+                                       const int32_t*, ForceParams, const int32_t*, ForceOut,
+                                       cudaStream_t);
+
+// ---------------------------------------------------------------- packing (caller order)
+__global__ void k_pack_pos(int64_t n, const double* __restrict__ pos, const double* __restrict__ w,
+                           double4* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], w ? w[i] : 0.0);
+}
+
+__global__ void k_pack4(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                        const double* __restrict__ c, const double* __restrict__ d,
+                        double4* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = make_double4(a ? a[i] : 0.0, b ? b[i] : 0.0, c ? c[i] : 0.0, d ? d[i] : 0.0);
+}
+
+__global__ void k_pack_vm(int64_t n, const double* __restrict__ vel, const double* __restrict__ m,
+                          double4* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = make_double4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], m[i]);
+}
+
+
+void pack_pos(int64_t n, const double* pos, const double* w, double4* out, cudaStream_t st) {
+  if (n > 0) k_pack_pos<<<grid_for(n), NB_THREADS, 0, st>>>(n, pos, w, out);
+}
+void pack4(int64_t n, const double* a, const double* b, const double* c, const double* d,
+           double4* out, cudaStream_t st) {
+  if (n > 0) k_pack4<<<grid_for(n), NB_THREADS, 0, st>>>(n, a, b, c, d, out);
+}
+void pack_vm(int64_t n, const double* vel, const double* m, double4* out, cudaStream_t st) {
+  if (n > 0) k_pack_vm<<<grid_for(n), NB_THREADS, 0, st>>>(n, vel, m, out);
+}
+
+}  // namespace nbk

@@ -1,0 +1,281 @@
+// SPH pair passes on neighbour lists (implementation, included by sph64.cu and sph32.cu): the h-rho Newton solve and the fused pressure + artificial
+// viscosity (+ conductivity, + disc viscosity) force and du/dt pass.
+//
+// Both run one thread per row over CSR lists.  They are templated on the list index type so the
+// same code serves the caller-order int64 lists of the operator API and the engine's sorted int32
+// lists, and on the arithmetic: FP64 (every pair term in double) or FP32 (positions as float
+// offsets from cell centres, float pair terms, Kahan-compensated sums, the Newton update and all
+// per-particle state in double).
+#pragma once
+#include "common.cuh"
+#include "engine.cuh"
+#include "sph.cuh"
+
+namespace nbk {
+
+// ---------------------------------------------------------------- position differences
+// FP64: packed (x, y, z, w) doubles.  dx = x_j - x_i as the reference forms it.
+struct Pos64 {
+  const double4* p;
+  __device__ __forceinline__ void diff(int64_t i, int64_t j, double& dx, double& dy,
+                                       double& dz) const {
+    double4 a = p[i], b = p[j];
+    dx = b.x - a.x;
+    dy = b.y - a.y;
+    dz = b.z - a.z;
+  }
+};
+
+// FP32: per particle the integer cell of a uniform grid of edge `cell` and the float offset from
+// that cell's centre; dx = (c_j - c_i) cell + (o_j - o_i) keeps full float precision at any
+// distance from the origin.
+struct Pos32 {
+  const float4* p;  // (ox, oy, oz, packed cell: 10 bits per axis)
+  float cell;
+  __device__ __forceinline__ void diff(int64_t i, int64_t j, float& dx, float& dy,
+                                       float& dz) const {
+    float4 a = p[i], b = p[j];
+    int ca = __float_as_int(a.w), cb = __float_as_int(b.w);
+    float ex = (float)(((cb >> 20) & 1023) - ((ca >> 20) & 1023));
+    float ey = (float)(((cb >> 10) & 1023) - ((ca >> 10) & 1023));
+    float ez = (float)((cb & 1023) - (ca & 1023));
+    dx = fmaf(ex, cell, b.x - a.x);
+    dy = fmaf(ey, cell, b.y - a.y);
+    dz = fmaf(ez, cell, b.z - a.z);
+  }
+};
+
+__device__ __forceinline__ double sqdist(double dx, double dy, double dz) { return d2_exact(dx, dy, dz); }
+__device__ __forceinline__ float sqdist(float dx, float dy, float dz) {
+  return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+}
+
+template <typename R>
+struct Acc;
+template <>
+struct Acc<double> {
+  double s = 0.0;
+  __device__ __forceinline__ void add(double v) { s += v; }
+  __device__ __forceinline__ double get() const { return s; }
+};
+template <>
+struct Acc<float> {
+  Kahan k;
+  __device__ __forceinline__ void add(float v) { k.add(v); }
+  __device__ __forceinline__ double get() const { return (double)k.s; }
+};
+
+// ---------------------------------------------------------------- density
+// Reference sim/sph.py:215-297 (_sums, _distances, _density_kernel): Newton-Raphson on
+// f(h) = sum_j m_j W(r_ij, h) - m_i (eta/h)^3 inside a bisection bracket, tol * h0, at most 50
+// iterations; the cap test near the search limit; Omega = 1 + h/(3 rho) sum m dW/dh (1 at h_max).
+template <typename R, typename PosT, typename I>
+__device__ void density_sums(const PosT& geo, int64_t i, const int64_t* off, const I* idx,
+                             const double* mass, R r2max, R h, int kid, R cnorm, double& rs_out,
+                             double& dws_out) {
+  Acc<R> rs, dws;
+  R inv_h = R(1) / h;
+  R ih2 = inv_h * inv_h;
+  R ih3 = ih2 * inv_h;
+  R ih4 = ih2 * ih2;
+  for (int64_t e = off[i]; e < off[i + 1]; ++e) {
+    int64_t j = (int64_t)idx[e];
+    R dx, dy, dz;
+    geo.diff(i, j, dx, dy, dz);
+    R d2 = sqdist(dx, dy, dz);
+    if (!(d2 < r2max)) continue;
+    R q = sqrt(d2) * inv_h;
+    if (q < R(2)) {
+      R fq = kernel_f<R>(q, kid);
+      R m = (R)mass[j];
+      rs.add(m * cnorm * ih3 * fq);
+      dws.add(m * (-cnorm * ih4 * (R(3) * fq + q * kernel_df<R>(q, kid))));
+    }
+  }
+  rs_out = rs.get();
+  dws_out = dws.get();
+}
+
+template <typename R, typename PosT, typename I>
+__global__ void __launch_bounds__(NB_THREADS)
+    k_density(int64_t nrows, const int64_t* __restrict__ rows, PosT geo,
+              const double* __restrict__ mass, const double* __restrict__ h_start,
+              const double* __restrict__ h_search, const int64_t* __restrict__ off,
+              const I* __restrict__ idx, DensityParams prm, const int32_t* __restrict__ out_map,
+              double* __restrict__ h_out, double* __restrict__ rho, double* __restrict__ omega,
+              int64_t* __restrict__ iters, int64_t* __restrict__ flags) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows ? rows[q] : q;
+  int64_t o = out_map ? (int64_t)out_map[i] : q;
+  double m_i = mass[i];
+  double hs = fmin(h_search[i], prm.h_max);
+  double r_max = 2.0 * hs;
+  R r2max = (R)(r_max * r_max);
+  double lo = 0.0, hi = hs;
+  double h = fmin(h_start[i], hi);
+  double h0 = h;
+  int flag = 3, it = 0;
+  const double eta = prm.eta, e3 = eta * eta * eta;
+  const int kid = prm.kid;
+  const R cn = (R)prm.cnorm;
+  while (it < 50) {
+    it += 1;
+    double rs, dws;
+    density_sums<R>(geo, i, off, idx, mass, r2max, (R)h, kid, cn, rs, dws);
+    double t = eta / h;
+    double f = rs - m_i * (t * t * t);
+    double h2 = h * h;
+    double df = dws + 3.0 * m_i * e3 / (h2 * h2);
+    if (f > 0)
+      hi = h;
+    else
+      lo = h;
+    double h_new = df > 0 ? h - f / df : 0.5 * (lo + hi);
+    if (!(lo <= h_new && h_new <= hi)) h_new = 0.5 * (lo + hi);
+    if (fabs(h_new - h) < prm.tol * h0) {
+      h = h_new;
+      flag = 0;
+      break;
+    }
+    h = h_new;
+  }
+  if (h >= hs * (1 - 1e-3)) {
+    double rs_lim, dummy;
+    density_sums<R>(geo, i, off, idx, mass, r2max, (R)hs, kid, cn, rs_lim, dummy);
+    double t = eta / hs;
+    if (rs_lim - m_i * (t * t * t) < 0) {
+      h = hs;
+      flag = hs >= prm.h_max ? 1 : 2;
+    }
+  }
+  double rs, dws;
+  density_sums<R>(geo, i, off, idx, mass, r2max, (R)h, kid, cn, rs, dws);
+  h_out[o] = h;
+  rho[o] = rs;
+  omega[o] = flag == 1 ? 1.0 : 1.0 + h / (3.0 * rs) * dws;
+  if (iters) iters[o] = it;
+  if (flags) flags[o] = flag;
+}
+
+// ---------------------------------------------------------------- forces
+// Reference sim/sph.py:519-652 (_forces_kernel, no reconstruction) and sim/sph.py:1084-1117
+// (_disc_kernel).  r_ab = x_a - x_b; F(h) = dW/dr; pair terms antisymmetric.
+template <typename R>
+__device__ __forceinline__ R dwdr(R r, R h, int kid, R cnorm) {
+  R h2 = h * h;
+  return cnorm / (h2 * h2) * kernel_df<R>(r / h, kid);
+}
+
+template <typename R, typename PosT, typename I>
+__global__ void __launch_bounds__(NB_THREADS)
+    k_forces(int64_t nrows, const int64_t* __restrict__ rows, PosT geo,
+             const double4* __restrict__ vm,    // (vx, vy, vz, mass)
+             const double4* __restrict__ hydro, // (h, rho, omega, P)
+             const double4* __restrict__ aux,   // (u, c_s, alpha, unused)
+             const int64_t* __restrict__ off, const I* __restrict__ idx, ForceParams prm,
+             const int32_t* __restrict__ out_map, ForceOut out) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t a = rows ? rows[q] : q;
+  int64_t o = out_map ? (int64_t)out_map[a] : q;
+  const double4 va = vm[a], ha = hydro[a], xa = aux[a];
+  const R h_a = (R)ha.x, rho_a = (R)ha.y, om_a = (R)ha.z, P_a = (R)ha.w;
+  const R inv_or_a = R(1) / (om_a * rho_a);
+  const R inv_orr_a = R(1) / (om_a * rho_a * rho_a);
+  const R cs_a = (R)xa.y, al_a = (R)xa.z, u_a = (R)xa.x;
+  const R beta = (R)prm.beta, alpha_u = (R)prm.alpha_u, aav = (R)prm.disc_alpha_av;
+  const R cn = (R)prm.cnorm;
+  const int kid = prm.kid;
+  Acc<R> ax, ay, az, work, heat, vheat, cheat, dax, day, daz, dheat;
+  R vmax = prm.use_visc ? cs_a : R(0);
+  int64_t npairs = 0;
+  for (int64_t e = off[a]; e < off[a + 1]; ++e) {
+    int64_t b = (int64_t)idx[e];
+    if (b == a) continue;
+    R ddx, ddy, ddz;
+    geo.diff(a, b, ddx, ddy, ddz);  // x_b - x_a
+    const double4 hb4 = hydro[b];
+    const R h_b = (R)hb4.x;
+    R d2 = sqdist(ddx, ddy, ddz);
+    if (prm.tighten) {
+      R rr = R(2) * (h_a > h_b ? h_a : h_b);
+      if (!(d2 < rr * rr)) continue;
+    }
+    npairs += 1;
+    const double4 vb = vm[b];
+    const R rho_b = (R)hb4.y, om_b = (R)hb4.z, P_b = (R)hb4.w;
+    const R m_b = (R)vb.w;
+    R r = sqrt(d2);
+    R rx = -ddx / r, ry = -ddy / r, rz = -ddz / r;  // r_hat of x_a - x_b
+    R fa = dwdr<R>(r, h_a, kid, cn);
+    R fb = dwdr<R>(r, h_b, kid, cn);
+    R vdotr = ((R)va.x - (R)vb.x) * rx + ((R)va.y - (R)vb.y) * ry + ((R)va.z - (R)vb.z) * rz;
+    R num_a = P_a, num_b = P_b;
+    R inv_orr_b = R(1) / (om_b * rho_b * rho_b);
+    if (prm.use_sph) {
+      if (prm.use_visc) {
+        const double4 xb = aux[b];
+        R vsig_a = al_a * cs_a + beta * fabs(vdotr);
+        R vsig_b = (R)xb.z * (R)xb.y + beta * fabs(vdotr);
+        if (vsig_a > vmax) vmax = vsig_a;
+        if (vdotr < R(0)) {
+          num_a += R(-0.5) * rho_a * vsig_a * vdotr;
+          num_b += R(-0.5) * rho_b * vsig_b * vdotr;
+          R dh = m_b * vsig_a * R(0.5) * vdotr * vdotr * fa * inv_or_a;
+          heat.add(-dh);
+          vheat.add(-dh);
+        }
+        if (prm.use_cond) {
+          R vu;
+          if (prm.cond_signal == 0)
+            vu = sqrt(fabs(P_a - P_b) / (R(0.5) * (rho_a + rho_b)));
+          else
+            vu = fabs(vdotr);
+          R dc = m_b * alpha_u * vu * (u_a - (R)xb.x) * R(0.5) *
+                 (fa * inv_or_a + fb / (om_b * rho_b));
+          heat.add(dc);
+          cheat.add(dc);
+        }
+      }
+      R f = m_b * (num_a * inv_orr_a * fa + num_b * inv_orr_b * fb);
+      ax.add(-f * rx);
+      ay.add(-f * ry);
+      az.add(-f * rz);
+      work.add(m_b * vdotr * fa);
+    }
+    if (prm.use_disc) {
+      const double4 xb = aux[b];
+      R qa = -rho_a * h_a / (R(2) * r) * aav * cs_a * vdotr * inv_orr_a;
+      R qb = -rho_b * h_b / (R(2) * r) * aav * (R)xb.y * vdotr * inv_orr_b;
+      R f = m_b * (qa * fa + qb * fb);
+      dax.add(-f * rx);
+      day.add(-f * ry);
+      daz.add(-f * rz);
+      dheat.add(m_b * qa * vdotr * fa);
+    }
+  }
+  if (prm.use_sph) {
+    double du = (double)P_a * (double)inv_or_a / (double)rho_a * work.get() + heat.get();
+    if (out.acc) {
+      out.acc[3 * o + 0] = ax.get();
+      out.acc[3 * o + 1] = ay.get();
+      out.acc[3 * o + 2] = az.get();
+    }
+    if (out.dudt) out.dudt[o] = du;
+    if (out.vsig) out.vsig[o] = (double)vmax;
+    if (out.vheat) out.vheat[o] = vheat.get();
+    if (out.cheat) out.cheat[o] = cheat.get();
+  }
+  if (prm.use_disc) {
+    if (out.dacc) {
+      out.dacc[3 * o + 0] = dax.get();
+      out.dacc[3 * o + 1] = day.get();
+      out.dacc[3 * o + 2] = daz.get();
+    }
+    if (out.ddudt) out.ddudt[o] = dheat.get();
+  }
+  if (out.pairs) out.pairs[o] = npairs;
+}
+
+}  // namespace nbk

@@ -1,0 +1,637 @@
+// The reference's step drivers on device state: the hydro evaluation of active rows and their
+// neighbours (sim/blocks.py:217-315; sim/coupled.py:145-195), the shared kick-flow-kick step
+// (sim/coupled.py:198-258), and the block-timestep system step with levels, limiter, wake-up and
+// opening kicks on the int64 tick timeline (sim/blocks.py:318-563, sim/timesteps.py:21-59).
+//
+// Compiled without fused multiply-add: every kick, drift and cooling update rounds like the
+// reference's NumPy expressions.
+#include <cub/cub.cuh>
+
+#include "common.cuh"
+#include "cooling.cuh"
+#include "engine.cuh"
+#include "gravity.cuh"
+#include "steps.cuh"
+
+namespace nbk {
+
+__device__ __forceinline__ int64_t ticks_of(int64_t level) { return (int64_t)1 << (K_MAX - level); }
+
+__device__ __forceinline__ double norm3(const double* v) {
+  return sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+}
+
+__global__ void k_fill_u8(int64_t n, uint8_t v, uint8_t* __restrict__ m) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) m[i] = v;
+}
+
+__global__ void k_any_nonpositive(int64_t n, const double* __restrict__ u, int* err) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n && !(u[i] > 0.0)) set_error(err, ERR_NONPOSITIVE_U);
+}
+
+__global__ void k_set_rows(int64_t nrows, const int64_t* __restrict__ rows, double v,
+                           double* __restrict__ a) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q < nrows) a[rows[q]] = v;
+}
+
+__global__ void k_iota(int64_t n, int64_t* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = i;
+}
+
+// ---------------------------------------------------------------- hydro of the active rows
+// sim/blocks.py:217-239 (_density_touched) and 242-315 (_hydro_rows): density for the rows and
+// every neighbour in the cached lists, widened until every interacting neighbour is fresh; then
+// the fused EOS + force pass for the rows.
+int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, const int64_t* rows,
+               const double* vel, const double* u, cudaStream_t st) {
+  Workspace& W = E.ws;
+  int64_t n = s->n;
+  NB_TRY(W.ensure(E, n));
+  k_any_nonpositive<<<grid_for(n), NB_THREADS, 0, st>>>(n, u, E.d_err);
+  NB_TRY(check_device_error(E, st));
+  // todo = every particle without a cache, else rows and their cached-list neighbours
+  if (!W.cache.valid || W.cache.n != n || E.lists.n != n) {
+    k_fill_u8<<<grid_for(n), NB_THREADS, 0, st>>>(n, 1, W.m_need);
+  } else {
+    NB_CUDA(cudaMemsetAsync(W.m_need, 0, n, st));
+    mark_rows(E, nrows, rows, 0, s->x, s->h, W.m_need, st);
+  }
+  NB_CUDA(cudaMemsetAsync(W.m_done, 0, n, st));
+  bool settled = false;
+  for (int it = 0; it < 8; ++it) {
+    int64_t ntodo = 0;
+    NB_TRY(select_mask(E, n, W.m_need, W.rows2, &ntodo, st));
+    if (ntodo == 0) {
+      settled = true;
+      break;
+    }
+    NB_TRY(compute_density(E, n, s->x, s->mass, s->h, s->rho, s->omega, ntodo, W.rows2, prm,
+                           &s->builds, &s->reuses, st));
+    mask_or(n, W.m_need, W.m_done, st);
+    // interacting neighbours of the rows at the current h
+    NB_CUDA(cudaMemsetAsync(W.m_tmp, 0, n, st));
+    mark_rows(E, nrows, rows, 1, s->x, s->h, W.m_tmp, st);
+    mask_and_not(n, W.m_tmp, W.m_done, W.m_need, st);
+  }
+  if (!settled) {
+    int64_t ntodo = 0;
+    NB_TRY(select_mask(E, n, W.m_need, W.rows2, &ntodo, st));
+    if (ntodo != 0) {
+      std::snprintf(E.last_error, sizeof(E.last_error),
+                    "neighbour set of the active particles did not settle");
+      return NB_ERR_TOUCHED;
+    }
+  }
+  if (prm->viscosity)
+    k_set_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, prm->alpha_const, s->alpha);
+  return engine_forces(E, s, vel, u, nrows, rows, prm, st);
+}
+
+// ---------------------------------------------------------------- shared step
+__global__ void k_kick_half(int64_t n, const double* __restrict__ p, const double* __restrict__ a,
+                            const double* __restrict__ u, const double* __restrict__ dudt,
+                            double half, double* __restrict__ p_out, double* __restrict__ u_out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int c = 0; c < 3; ++c) p_out[3 * i + c] = p[3 * i + c] + half * a[3 * i + c];
+  u_out[i] = u[i] + half * dudt[i];
+}
+
+// cooling over dt at mid-step (sim/coupled.py:244-251): u_half <- cooled, dm = m (u_half - u_new)
+__global__ void k_cool_shared(int64_t n, int law, const double* __restrict__ x0,
+                              const double* __restrict__ x1, const double* __restrict__ rho,
+                              const double* __restrict__ m, double dt, double beta,
+                              double u_floor, BremsParams bp, double* __restrict__ u_half,
+                              double* __restrict__ dm) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double uh = u_half[i], un;
+  if (law == 1) {
+    double r_mid = 0.5 * (norm3(x0 + 3 * i) + norm3(x1 + 3 * i));
+    double t_cool = beta / pow(r_mid, -1.5);
+    un = beta_cool_one(uh, u_floor, dt, t_cool);
+  } else {
+    un = brems_cool_one(uh, rho[i], dt, bp);
+  }
+  dm[i] = m[i] * (uh - un);
+  u_half[i] = un;
+}
+
+__global__ void k_pred_shared(int64_t n, const double* __restrict__ p_flow,
+                              const double* __restrict__ a, const double* __restrict__ u_half,
+                              const double* __restrict__ dudt, double half,
+                              double* __restrict__ p_pred, double* __restrict__ u_pred) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int c = 0; c < 3; ++c) p_pred[3 * i + c] = p_flow[3 * i + c] + half * a[3 * i + c];
+  u_pred[i] = u_half[i] + half * dudt[i];
+}
+
+static BremsParams brems_of(const nb_params* prm) {
+  BremsParams b;
+  b.tfac = prm->brems_tfac;
+  b.b = prm->brems_b;
+  b.kappa = prm->brems_kappa;
+  b.u_floor = prm->u_floor;
+  b.t_floor = prm->brems_t_floor;
+  return b;
+}
+
+static int glf_status(Engine& E, int64_t n, const int64_t* iters, cudaStream_t st) {
+  size_t tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceReduce::Min(E.cub_tmp, tmp, iters, E.ws.d_i64, (int)n, st));
+  NB_CUDA(cudaMemcpyAsync(E.ws.h_i64, E.ws.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  int64_t worst = E.ws.h_i64[0];
+  if (worst >= 0) return 0;
+  const char* msg = worst == -1   ? "stage 1 (p_half) did not converge in 10 iterations: time step too large"
+                    : worst == -2 ? "stage 2 (x1) did not converge in 10 iterations: time step too large"
+                                  : "particle inside r = 2.5";
+  std::snprintf(E.last_error, sizeof(E.last_error), "%s", msg);
+  return worst == -1 ? NB_ERR_GLF_P_HALF : worst == -2 ? NB_ERR_GLF_X1 : NB_ERR_GLF_RADIUS;
+}
+
+static int sum_doubles(Engine& E, int64_t n, const double* a, double* out, cudaStream_t st) {
+  if (n <= 0) {
+    *out = 0.0;
+    return 0;
+  }
+  size_t tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceReduce::Sum(E.cub_tmp, tmp, a, E.ws.d_tmp, (int)n, st));
+  NB_CUDA(cudaMemcpyAsync(E.ws.h_dbl, E.ws.d_tmp, sizeof(double), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  *out = E.ws.h_dbl[0];
+  return 0;
+}
+
+int coupled_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st) {
+  Workspace& W = E.ws;
+  int64_t n = s->n;
+  NB_TRY(W.ensure(E, n));
+  W.cache.valid = false;
+  k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
+  launch_v_from_p(n, s->x, s->p, W.v_eval, st);
+  NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st));
+  return 0;
+}
+
+int coupled_step(Engine& E, nb_state* s, const nb_params* prm, double dt, cudaStream_t st) {
+  Workspace& W = E.ws;
+  int64_t n = s->n;
+  NB_TRY(W.ensure(E, n));
+  double half = 0.5 * dt;
+  // p_half, u_half; gravity flow over dt
+  double* u_half = W.d_uh;
+  k_kick_half<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->p, s->a_hydro, s->u, s->dudt, half,
+                                                  W.v_tmp, u_half);
+  launch_glf(n, s->x, W.v_tmp, nullptr, dt, W.v_pred, W.v_flow, W.iters, st);
+  NB_TRY(glf_status(E, n, W.iters, st));
+  if (prm->cooling == 1 || prm->cooling == 2) {
+    k_cool_shared<<<grid_for(n), NB_THREADS, 0, st>>>(n, prm->cooling, s->x, W.v_pred, s->rho,
+                                                      s->mass, dt, prm->cooling_beta,
+                                                      prm->u_floor, brems_of(prm), u_half, W.d_dm);
+    double de = 0;
+    NB_TRY(sum_doubles(E, n, W.d_dm, &de, st));
+    s->e_radiated += de;
+  }
+  // predicted state: x1, p_flow, u_half + dt/2 dudt; predictor momentum for velocities
+  NB_CUDA(cudaMemcpyAsync(s->x, W.v_pred, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, st));
+  k_pred_shared<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.v_flow, s->a_hydro, u_half, s->dudt,
+                                                    half, W.v_tmp, s->u);
+  launch_v_from_p(n, s->x, W.v_tmp, W.v_eval, st);
+  k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
+  NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st));
+  // closing kick with the new forces
+  k_pred_shared<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.v_flow, s->a_hydro, u_half, s->dudt,
+                                                    half, s->p, s->u);
+  s->particle_steps += n;
+  s->last_active = n;
+  NB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// sim/coupled.py:213-226: min over particles of C_cour h / v_sig, C_force sqrt(h / |a|),
+// viscous 0.25 h^2 / nu and eta_orb r^(3/2).
+__global__ void k_stable_dt(int64_t n, const double* __restrict__ h, const double* __restrict__ vsig,
+                            const double* __restrict__ a, const double* __restrict__ nu,
+                            const double* __restrict__ x, double courant, double c_force,
+                            double eta_orb, double* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double dt = courant * (h[i] / vsig[i]);
+  double amag = norm3(a + 3 * i);
+  if (amag > 0) dt = fmin(dt, c_force * sqrt(h[i] / amag));
+  if (nu && nu[i] > 0) dt = fmin(dt, 0.25 * h[i] * h[i] / nu[i]);
+  double r = norm3(x + 3 * i);
+  dt = fmin(dt, eta_orb * pow(r, 1.5));
+  out[i] = dt;
+}
+
+int coupled_stable_dt(Engine& E, nb_state* s, const nb_params* prm, double* dt, cudaStream_t st) {
+  Workspace& W = E.ws;
+  int64_t n = s->n;
+  NB_TRY(W.ensure(E, n));
+  k_stable_dt<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->h, s->vsig_max, s->a_hydro,
+                                                  prm->disc_alpha_av > 0 ? s->nu : nullptr, s->x,
+                                                  prm->courant, prm->c_force, prm->eta_orb, W.d_b);
+  size_t tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceReduce::Min(E.cub_tmp, tmp, W.d_b, W.d_tmp, (int)n, st));
+  NB_CUDA(cudaMemcpyAsync(W.h_dbl, W.d_tmp, sizeof(double), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  *dt = W.h_dbl[0];
+  return 0;
+}
+
+// ---------------------------------------------------------------- block steps
+// gravity flow of every particle to tick n_next from its step start, the predictor momentum,
+// and the active flags (sim/blocks.py:506-517)
+__global__ void k_block_flow(int64_t n, int64_t n_next, double tick,
+                             const double* __restrict__ x_beg, const double* __restrict__ p_half,
+                             const int64_t* __restrict__ n_beg, const int64_t* __restrict__ n_end,
+                             const double* __restrict__ a, double* __restrict__ x,
+                             double* __restrict__ p_flow, double* __restrict__ p_pred,
+                             int64_t* __restrict__ iters, uint8_t* __restrict__ active) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = (double)(n_next - n_beg[i]) * tick;
+  double half_len = 0.5 * (double)(n_end[i] - n_beg[i]) * tick;
+  double xb[3] = {x_beg[3 * i], x_beg[3 * i + 1], x_beg[3 * i + 2]};
+  double pb[3] = {p_half[3 * i], p_half[3 * i + 1], p_half[3 * i + 2]};
+  double xo[3], po[3];
+  iters[i] = glf_one(xb, pb, s, xo, po);
+  double lag = s - half_len;
+  for (int c = 0; c < 3; ++c) {
+    x[3 * i + c] = xo[c];
+    p_flow[3 * i + c] = po[c];
+    p_pred[3 * i + c] = po[c] + lag * a[3 * i + c];
+  }
+  active[i] = n_end[i] == n_next;
+}
+
+// cooling at mid-step of every particle over its elapsed time s (exact laws), radiated energy of
+// the active rows, and the predicted u (sim/blocks.py:518-538)
+__global__ void k_block_cool(int64_t n, int law, int64_t n_next, double tick,
+                             const int64_t* __restrict__ n_beg, const int64_t* __restrict__ n_end,
+                             const double* __restrict__ x_beg, const double* __restrict__ x,
+                             const double* __restrict__ rho, const double* __restrict__ m,
+                             const double* __restrict__ dudt, double beta, double u_floor,
+                             BremsParams bp, double* __restrict__ u_half, double* __restrict__ u,
+                             double* __restrict__ lum, double* __restrict__ dm) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = (double)(n_next - n_beg[i]) * tick;
+  double half_len = 0.5 * (double)(n_end[i] - n_beg[i]) * tick;
+  double uh = u_half[i];
+  bool act = n_end[i] == n_next;
+  double uc = uh;
+  if (law == 1) {
+    double r_mid = 0.5 * (norm3(x_beg + 3 * i) + norm3(x + 3 * i));
+    double t_cool = beta / pow(r_mid, -1.5);
+    uc = beta_cool_one(uh, u_floor, s, t_cool);
+  } else if (law == 2) {
+    uc = brems_cool_one(uh, rho[i], s, bp);
+  }
+  if (law != 0) {
+    double d = act ? m[i] * (uh - uc) : 0.0;
+    dm[i] = d;
+    if (act) {
+      lum[i] = d / (2.0 * half_len);
+      u_half[i] = uc;
+    }
+  }
+  u[i] = uc + (s - half_len) * dudt[i];
+}
+
+// closing kicks of the rows (sim/blocks.py:544-547)
+__global__ void k_block_close(int64_t nrows, const int64_t* __restrict__ rows, double tick,
+                              const int64_t* __restrict__ n_beg, const int64_t* __restrict__ n_end,
+                              const double* __restrict__ p_flow, const double* __restrict__ a,
+                              const double* __restrict__ u_half, const double* __restrict__ dudt,
+                              double* __restrict__ p_pred, double* __restrict__ u) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows[q];
+  double half_len = 0.5 * (double)(n_end[i] - n_beg[i]) * tick;
+  for (int c = 0; c < 3; ++c) p_pred[3 * i + c] = p_flow[3 * i + c] + half_len * a[3 * i + c];
+  u[i] = u_half[i] + half_len * dudt[i];
+}
+
+// wanted level of the rows: orbit, Courant, force and viscous criteria (sim/blocks.py:318-334),
+// level_for_dt (sim/timesteps.py:26-39), forced offset, allowed_level (sim/timesteps.py:47-59)
+__global__ void k_wanted_levels(int64_t nrows, const int64_t* __restrict__ rows, int64_t tick_n,
+                                double dt_max, const double* __restrict__ h,
+                                const double* __restrict__ vsig, const double* __restrict__ a,
+                                const double* __restrict__ nu, const double* __restrict__ x,
+                                double courant, double c_force, double eta_orb,
+                                const int64_t* __restrict__ offset, int64_t* __restrict__ level,
+                                int* err) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows[q];
+  double hi = h[i];
+  double dt = courant * hi / vsig[i];
+  double amag = norm3(a + 3 * i);
+  if (amag > 0) dt = fmin(dt, c_force * sqrt(hi / amag));
+  if (nu && nu[i] > 0) dt = fmin(dt, 0.25 * (hi * hi) / nu[i]);
+  dt = fmin(dt, eta_orb * pow(norm3(x + 3 * i), 1.5));
+  if (!(dt > 0)) {
+    set_error(err, ERR_DT);
+    return;
+  }
+  double kd = ceil(log2(dt_max / dt) - 1e-12);
+  int64_t k = (int64_t)kd;
+  if (k < 0) k = 0;
+  if (k <= 62 && dt_max / exp2((double)k) > dt) k += 1;
+  if (k > K_MAX) {
+    set_error(err, ERR_LEVEL);
+    return;
+  }
+  k += offset ? offset[i] : 0;
+  int64_t cur = level[i];
+  int64_t nw = k >= cur ? k : cur;
+  if (k < cur) {
+    for (int64_t kk = k; kk < cur; ++kk) {
+      if (kk >= 0 && kk <= K_MAX && tick_n % ticks_of(kk) == 0) {
+        nw = kk;
+        break;
+      }
+    }
+  }
+  level[i] = nw;
+}
+
+// one sweep of the level limiter over the rows' interacting pairs (sim/blocks.py:337-353); the
+// least fixed point above the start is unique, so in-place sweeps reach the reference's levels
+__global__ void k_limit_sweep(int64_t nrows, const int64_t* __restrict__ rows,
+                              const int32_t* __restrict__ perm, const int32_t* __restrict__ inv_perm,
+                              const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
+                              const double* __restrict__ x, const double* __restrict__ h,
+                              int64_t max_gap, int64_t* level, int* changed) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows[q];
+  int64_t k = inv_perm[i];
+  double xi0 = x[3 * i], xi1 = x[3 * i + 1], xi2 = x[3 * i + 2], hi = h[i];
+  int64_t need = ((volatile int64_t*)level)[i];
+  for (int64_t e = off[k]; e < off[k + 1]; ++e) {
+    int64_t j = perm[idx[e]];
+    double d2 = d2_exact(x[3 * j] - xi0, x[3 * j + 1] - xi1, x[3 * j + 2] - xi2);
+    double rr = 2.0 * fmax(hi, h[j]);
+    if (!(d2 < rr * rr)) continue;
+    int64_t lj = ((volatile int64_t*)level)[j];
+    if (lj - max_gap > need) need = lj - max_gap;
+  }
+  if (need > ((volatile int64_t*)level)[i]) {
+    atomicMax((long long*)&level[i], (long long)need);
+    *changed = 1;
+  }
+}
+
+// _land (sim/blocks.py:383-393) and the K_MAX check of _choose_levels
+__global__ void k_land(int64_t nrows, const int64_t* __restrict__ rows, int64_t tick_n,
+                       int64_t n_stop, int64_t* __restrict__ level, int* err) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows[q];
+  int64_t k = level[i];
+  if (tick_n < n_stop) {
+    for (int guard = 0; guard < 64; ++guard) {
+      int64_t kk = k < K_MAX ? k : K_MAX;
+      if (!(tick_n + ticks_of(kk) > n_stop)) break;
+      k += 1;
+    }
+  }
+  if (k > K_MAX) set_error(err, ERR_LEVEL);
+  level[i] = k;
+}
+
+// _wake_targets (sim/blocks.py:356-364): need[j] = max over active i of level_i - max_gap
+__global__ void k_wake_need(int64_t nrows, const int64_t* __restrict__ rows,
+                            const int32_t* __restrict__ perm, const int32_t* __restrict__ inv_perm,
+                            const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
+                            const double* __restrict__ x, const double* __restrict__ h,
+                            const int64_t* __restrict__ level, int64_t max_gap,
+                            int64_t* __restrict__ need) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows[q];
+  int64_t k = inv_perm[i];
+  double xi0 = x[3 * i], xi1 = x[3 * i + 1], xi2 = x[3 * i + 2], hi = h[i];
+  long long v = (long long)(level[i] - max_gap);
+  for (int64_t e = off[k]; e < off[k + 1]; ++e) {
+    int64_t j = perm[idx[e]];
+    double d2 = d2_exact(x[3 * j] - xi0, x[3 * j + 1] - xi1, x[3 * j + 2] - xi2);
+    double rr = 2.0 * fmax(hi, h[j]);
+    if (!(d2 < rr * rr)) continue;
+    atomicMax((long long*)&need[j], v);
+  }
+}
+
+// _cut_steps / _cut_to (sim/blocks.py:404-431): shorten running steps longer than `need` allows
+__global__ void k_cut_steps(int64_t n, int64_t tick_n, double tick, const int64_t* __restrict__ need,
+                            const double* __restrict__ a, const double* __restrict__ dudt,
+                            int64_t* __restrict__ level, int64_t* __restrict__ n_end,
+                            double* __restrict__ p_half, double* __restrict__ u_half,
+                            unsigned long long* __restrict__ woken) {
+  int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  int64_t nd = need[j];
+  if (!(n_end[j] > tick_n && nd > level[j])) return;
+  int64_t t_new = ticks_of(nd);
+  int64_t end_new = (tick_n / t_new + 1) * t_new;
+  level[j] = nd;
+  if (end_new < n_end[j]) {
+    double d_len = (double)(end_new - n_end[j]) * tick;
+    for (int c = 0; c < 3; ++c) p_half[3 * j + c] += 0.5 * d_len * a[3 * j + c];
+    u_half[j] += 0.5 * d_len * dudt[j];
+    n_end[j] = end_new;
+    atomicAdd(woken, 1ull);
+  }
+}
+
+// _open (sim/blocks.py:443-452)
+__global__ void k_open(int64_t nrows, const int64_t* __restrict__ rows, int64_t tick_n, double tick,
+                       const int64_t* __restrict__ level, const double* __restrict__ x,
+                       const double* __restrict__ p, const double* __restrict__ u,
+                       const double* __restrict__ a, const double* __restrict__ dudt,
+                       int64_t* __restrict__ n_beg, int64_t* __restrict__ n_end,
+                       double* __restrict__ x_beg, double* __restrict__ p_half,
+                       double* __restrict__ u_half) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows[q];
+  int64_t t = ticks_of(level[i]);
+  double length = (double)t * tick;
+  n_beg[i] = tick_n;
+  n_end[i] = tick_n + t;
+  for (int c = 0; c < 3; ++c) {
+    x_beg[3 * i + c] = x[3 * i + c];
+    p_half[3 * i + c] = p[3 * i + c] + 0.5 * length * a[3 * i + c];
+  }
+  u_half[i] = u[i] + 0.5 * length * dudt[i];
+}
+
+__global__ void k_fill_i64(int64_t n, int64_t v, int64_t* __restrict__ a) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
+// sim/blocks.py:367-380 (_choose_levels) followed by _open for the rows
+static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows,
+                                  const int64_t* rows, cudaStream_t st) {
+  Workspace& W = E.ws;
+  Lists& L = E.lists;
+  int64_t n = s->n;
+  if (nrows == 0) return 0;
+  k_wanted_levels<<<grid_for(nrows), NB_THREADS, 0, st>>>(
+      nrows, rows, s->tick_n, prm->dt_max, s->h, s->vsig_max, s->a_hydro,
+      prm->disc_alpha_av > 0 ? s->nu : nullptr, s->x, prm->courant, prm->c_force, prm->eta_orb,
+      s->level_offset, s->level, E.d_err);
+  NB_TRY(check_device_error(E, st));
+  if (prm->limiter) {
+    bool settled = false;
+    for (int sweep = 0; sweep < 4096; ++sweep) {
+      NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
+      k_limit_sweep<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.perm, L.inv_perm, L.off,
+                                                            L.idx, s->x, s->h, prm->max_gap,
+                                                            s->level, W.d_int);
+      NB_CUDA(cudaMemcpyAsync(W.h_int, W.d_int, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NB_CUDA(cudaStreamSynchronize(st));
+      if (W.h_int[0] == 0) {
+        settled = true;
+        break;
+      }
+    }
+    if (!settled) return set_host_error(E, "level limiter did not settle");
+  }
+  k_land<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, s->tick_n, s->n_stop, s->level, E.d_err);
+  NB_TRY(check_device_error(E, st));
+  if (prm->limiter) {
+    k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, -1, W.need);
+    k_wake_need<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.perm, L.inv_perm, L.off,
+                                                        L.idx, s->x, s->h, s->level, prm->max_gap,
+                                                        W.need);
+    NB_CUDA(cudaMemsetAsync(W.d_i64, 0, sizeof(int64_t), st));
+    k_cut_steps<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->tick_n, s->tick, W.need, s->a_hydro,
+                                                    s->dudt, s->level, s->n_end, s->p_half,
+                                                    s->u_half, (unsigned long long*)W.d_i64);
+    NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    NB_CUDA(cudaStreamSynchronize(st));
+    s->woken += W.h_i64[0];
+  }
+  k_open<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, s->tick_n, s->tick, s->level, s->x,
+                                                 s->p, s->u, s->a_hydro, s->dudt, s->n_beg,
+                                                 s->n_end, s->x_beg, s->p_half, s->u_half);
+  NB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// sim/blocks.py:455-499 (initialise): the caller has filled x, p (from v), u, mass, h, alpha and
+// zeroed the rest; every particle is evaluated, gets its level and opens its first step.
+int block_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st) {
+  Workspace& W = E.ws;
+  int64_t n = s->n;
+  NB_TRY(W.ensure(E, n));
+  W.cache.valid = false;
+  k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
+  launch_v_from_p(n, s->x, s->p, W.v_eval, st);
+  NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st));
+  k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, 0, s->level);
+  return choose_levels_and_open(E, s, prm, n, W.rows, st);
+}
+
+// sim/blocks.py:502-563 (advance): one system step to the earliest step end.  rows_out (optional,
+// device, n) receives the active rows; their number is s->last_active.
+int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_out,
+                  cudaStream_t st) {
+  Workspace& W = E.ws;
+  int64_t n = s->n;
+  NB_TRY(W.ensure(E, n));
+  size_t tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceReduce::Min(E.cub_tmp, tmp, s->n_end, W.d_i64, (int)n, st));
+  NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  int64_t n_next = W.h_i64[0];
+  // flow of every particle from its step start; predictor momenta; active flags
+  k_block_flow<<<grid_for(n, 128), 128, 0, st>>>(n, n_next, s->tick, s->x_beg, s->p_half, s->n_beg,
+                                                 s->n_end, s->a_hydro, s->x, W.v_flow, W.v_pred,
+                                                 W.iters, W.m_rows);
+  NB_TRY(glf_status(E, n, W.iters, st));
+  int64_t nrows = 0;
+  NB_TRY(select_mask(E, n, W.m_rows, W.rows, &nrows, st));
+  k_block_cool<<<grid_for(n), NB_THREADS, 0, st>>>(
+      n, prm->cooling == 1 ? 1 : (prm->cooling >= 2 ? 2 : 0), n_next, s->tick, s->n_beg,
+      s->n_end, s->x_beg, s->x, s->rho, s->mass, s->dudt, prm->cooling_beta, prm->u_floor,
+      brems_of(prm), s->u_half, s->u, s->luminosity, W.d_dm);
+  if (prm->cooling != 0) {
+    double de = 0;
+    NB_TRY(sum_doubles(E, n, W.d_dm, &de, st));
+    s->e_radiated += de;
+  }
+  s->tick_n = n_next;
+  launch_v_from_p(n, s->x, W.v_pred, W.v_eval, st);
+  NB_TRY(hydro_rows(E, s, prm, nrows, W.rows, W.v_eval, s->u, st));
+  k_block_close<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, W.rows, s->tick, s->n_beg, s->n_end,
+                                                       W.v_flow, s->a_hydro, s->u_half, s->dudt,
+                                                       W.v_pred, s->u);
+  NB_CUDA(cudaMemcpyAsync(s->p, W.v_pred, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, st));
+  NB_TRY(choose_levels_and_open(E, s, prm, nrows, W.rows, st));
+  if (rows_out && nrows > 0)
+    NB_CUDA(cudaMemcpyAsync(rows_out, W.rows, sizeof(int64_t) * nrows, cudaMemcpyDeviceToDevice, st));
+  s->last_active = nrows;
+  s->particle_steps += nrows;
+  return 0;
+}
+
+// run()'s prologue (sim/blocks.py:727-734): re-open the steps opened at this tick that would end
+// past n_stop so they land on it
+__global__ void k_fresh(int64_t n, int64_t tick_n, int64_t n_stop, const int64_t* __restrict__ n_beg,
+                        const int64_t* __restrict__ n_end, uint8_t* __restrict__ m) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) m[i] = n_beg[i] == tick_n && n_end[i] > n_stop;
+}
+
+__global__ void k_open_only(int64_t nrows, const int64_t* __restrict__ rows, int64_t tick_n,
+                            double tick, const int64_t* __restrict__ level,
+                            const double* __restrict__ x, const double* __restrict__ p,
+                            const double* __restrict__ u, const double* __restrict__ a,
+                            const double* __restrict__ dudt, int64_t* __restrict__ n_beg,
+                            int64_t* __restrict__ n_end, double* __restrict__ x_beg,
+                            double* __restrict__ p_half, double* __restrict__ u_half) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows[q];
+  int64_t t = ticks_of(level[i]);
+  double length = (double)t * tick;
+  n_beg[i] = tick_n;
+  n_end[i] = tick_n + t;
+  for (int c = 0; c < 3; ++c) {
+    x_beg[3 * i + c] = x[3 * i + c];
+    p_half[3 * i + c] = p[3 * i + c] + 0.5 * length * a[3 * i + c];
+  }
+  u_half[i] = u[i] + 0.5 * length * dudt[i];
+}
+
+int block_land(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st) {
+  (void)prm;
+  Workspace& W = E.ws;
+  int64_t n = s->n;
+  NB_TRY(W.ensure(E, n));
+  k_fresh<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->tick_n, s->n_stop, s->n_beg, s->n_end, W.m_tmp);
+  int64_t nf = 0;
+  NB_TRY(select_mask(E, n, W.m_tmp, W.rows2, &nf, st));
+  if (nf == 0) return 0;
+  k_land<<<grid_for(nf), NB_THREADS, 0, st>>>(nf, W.rows2, s->tick_n, s->n_stop, s->level, E.d_err);
+  NB_TRY(check_device_error(E, st));
+  k_open_only<<<grid_for(nf), NB_THREADS, 0, st>>>(nf, W.rows2, s->tick_n, s->tick, s->level, s->x,
+                                                   s->p, s->u, s->a_hydro, s->dudt, s->n_beg,
+                                                   s->n_end, s->x_beg, s->p_half, s->u_half);
+  NB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace nbk

@@ -1,0 +1,37 @@
+// Step runtime entry points shared between engine.cu, steps.cu and capi.cu.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/nebula_b200.h"
+#include "engine.cuh"
+
+namespace nbk {
+
+constexpr int K_MAX = 40;
+
+int compute_density(Engine& E, int64_t n, const double* x, const double* mass, double* h,
+                    double* rho, double* omega, int64_t nrows, const int64_t* rows,
+                    const nb_params* prm, int64_t* builds, int64_t* reuses, cudaStream_t st);
+int select_mask(Engine& E, int64_t n, const uint8_t* mask, int64_t* out, int64_t* count,
+                cudaStream_t st);
+int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, int64_t nrows,
+                  const int64_t* rows, const nb_params* prm, cudaStream_t st);
+
+int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, const int64_t* rows,
+               const double* vel, const double* u, cudaStream_t st);
+int coupled_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st);
+int coupled_step(Engine& E, nb_state* s, const nb_params* prm, double dt, cudaStream_t st);
+int coupled_stable_dt(Engine& E, nb_state* s, const nb_params* prm, double* dt, cudaStream_t st);
+int block_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st);
+int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_out,
+                  cudaStream_t st);
+int block_land(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st);
+
+// launchers of engine.cu kernels used by steps.cu
+void mark_rows(Engine& E, int64_t nrows, const int64_t* rows, int tight, const double* x,
+               const double* h, uint8_t* mark, cudaStream_t st);
+void mask_and_not(int64_t n, const uint8_t* a, const uint8_t* b, uint8_t* out, cudaStream_t st);
+void mask_or(int64_t n, const uint8_t* a, uint8_t* b, cudaStream_t st);
+
+}  // namespace nbk

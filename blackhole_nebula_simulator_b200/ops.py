@@ -1,0 +1,217 @@
+"""The reference's inner operators on the GPU, same names, arguments and results.
+
+Each function replaces one reference function one for one (file:line in its docstring) and runs
+the sm_100a kernels of libnebula_b200.so.  Inputs may be NumPy arrays or tensors; results are
+float64 / int64 CUDA tensors (``.cpu().numpy()`` gives the reference's arrays).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib
+from .config import C_NORM, DEFAULT_ETA, DEFAULT_KERNEL, KERNEL_IDS, ShockCapturing
+from .device import ctx, dev_f64, dev_i64, ptr, stream
+
+GLFConvergenceError = _lib.GLFConvergenceError
+
+FLAG_OK, FLAG_AT_H_MAX, FLAG_SEARCH_TOO_SMALL, FLAG_NO_CONVERGENCE = 0, 1, 2, 3
+
+
+def _call(name, *args):
+    c = ctx()
+    _lib.check(c, getattr(_lib.lib(), name)(c, *args))
+
+
+@dataclass
+class Neighbours:
+    """CSR lists (sim/neighbours.py:22-36): neighbours of i are index[offset[i]:offset[i+1]]."""
+
+    offset: torch.Tensor
+    index: torch.Tensor
+    box: object = None
+
+    def of(self, i: int) -> torch.Tensor:
+        return self.index[int(self.offset[i]) : int(self.offset[i + 1])]
+
+    @property
+    def counts(self) -> torch.Tensor:
+        return torch.diff(self.offset)
+
+
+def find_neighbours(pos, h, box=None) -> Neighbours:
+    """sim/neighbours.py:240-281 (find_neighbours_numba): symmetric lists {j : r_ij < 2 max(h_i,
+    h_j)}, self included, rows sorted.  Periodic boxes are not part of the CUDA path."""
+    if box is not None:
+        raise NotImplementedError("periodic boxes are not part of the CUDA SPH path")
+    pos = dev_f64(pos)
+    h = dev_f64(h)
+    n = len(pos)
+    off = torch.empty(n + 1, dtype=torch.int64, device=pos.device)
+    total = ctypes.c_int64(0)
+    _call("nb_find_neighbours", n, ptr(pos), ptr(h), ptr(off), ctypes.byref(total), stream())
+    idx = torch.empty(max(total.value, 1), dtype=torch.int64, device=pos.device)
+    _call("nb_neighbours_export", ptr(off), ptr(idx), stream())
+    return Neighbours(off, idx[: total.value], None)
+
+
+def tighten(nb: Neighbours, pos, h, rows=None) -> Neighbours:
+    """sim/neighbours.py:306-323: keep r < 2 max(h_i, h_j), lists for ``rows`` only."""
+    pos = dev_f64(pos)
+    h = dev_f64(h)
+    n = len(pos)
+    rows_t = torch.arange(n, device=pos.device) if rows is None else dev_i64(rows)
+    counts = torch.zeros(n, dtype=torch.int64, device=pos.device)
+    off_in, idx_in = dev_i64(nb.offset), dev_i64(nb.index)
+    _call("nb_tighten", n, ptr(pos), ptr(h), ptr(off_in), ptr(idx_in), len(rows_t), ptr(rows_t),
+          ptr(counts), None, None, stream())  # fmt: skip
+    off = torch.zeros(n + 1, dtype=torch.int64, device=pos.device)
+    torch.cumsum(counts, 0, out=off[1:])
+    total = int(off[-1])
+    idx = torch.empty(max(total, 1), dtype=torch.int64, device=pos.device)
+    _call("nb_tighten", n, ptr(pos), ptr(h), ptr(off_in), ptr(idx_in), len(rows_t), ptr(rows_t),
+          ptr(counts), ptr(off), ptr(idx), stream())  # fmt: skip
+    return Neighbours(off, idx[:total], nb.box)
+
+
+@dataclass
+class DensityResult:
+    h: torch.Tensor
+    rho: torch.Tensor
+    omega: torch.Tensor
+    iterations: torch.Tensor
+    flags: torch.Tensor
+    neighbours: Neighbours
+
+
+def density_numba(pos, mass, h_start, nb: Neighbours, h_search, kernel_name=DEFAULT_KERNEL,
+                  eta=DEFAULT_ETA, tol=1e-4, h_max=math.inf, rows=None) -> DensityResult:  # fmt: skip
+    """sim/sph.py:300-326: the density pass on given lists; results in rows order."""
+    pos = dev_f64(pos)
+    n = len(pos)
+    kid = KERNEL_IDS[kernel_name]
+    rows_t = None if rows is None else dev_i64(rows)
+    m = n if rows_t is None else len(rows_t)
+    d = pos.device
+    h_out, rho, om = (torch.empty(m, dtype=torch.float64, device=d) for _ in range(3))
+    it, fl = (torch.empty(m, dtype=torch.int64, device=d) for _ in range(2))
+    mass_t, hs_t, hsr_t = dev_f64(mass, (n,)), dev_f64(h_start, (n,)), dev_f64(h_search, (n,))
+    off, idx = dev_i64(nb.offset), dev_i64(nb.index)
+    _call("nb_density", n, ptr(pos), ptr(mass_t), ptr(hs_t), ptr(hsr_t), ptr(off), ptr(idx), m,
+          ptr(rows_t), kid, float(eta), float(tol), float(h_max), ptr(h_out), ptr(rho), ptr(om),
+          ptr(it), ptr(fl), stream())  # fmt: skip
+    return DensityResult(h_out, rho, om, it, fl, nb)
+
+
+@dataclass
+class ForceResult:
+    acc: torch.Tensor
+    dudt: torch.Tensor
+    vsig_max: torch.Tensor
+    dudt_visc: torch.Tensor = None
+    dudt_cond: torch.Tensor = None
+
+
+def forces_numba(pos, vel, mass, h, rho, omega, pressure, nb: Neighbours,
+                 kernel_name=DEFAULT_KERNEL, u=None, c_s=None, alpha=None,
+                 shock: ShockCapturing = ShockCapturing(), rows=None, grad_v=None) -> ForceResult:  # fmt: skip
+    """sim/sph.py:655-690 without velocity reconstruction (shock.reconstruction must be off)."""
+    use_visc = alpha is not None and c_s is not None
+    if use_visc and shock.reconstruction:
+        raise NotImplementedError("velocity reconstruction is not part of the CUDA SPH path")
+    pos = dev_f64(pos)
+    n = len(pos)
+    rows_t = None if rows is None else dev_i64(rows)
+    m = n if rows_t is None else len(rows_t)
+    d = pos.device
+    acc = torch.empty((m, 3), dtype=torch.float64, device=d)
+    dudt, vsig, vh, ch = (torch.empty(m, dtype=torch.float64, device=d) for _ in range(4))
+    opt = lambda a: None if a is None else dev_f64(a, (n,))  # noqa: E731
+    off, idx = dev_i64(nb.offset), dev_i64(nb.index)
+    args = [dev_f64(vel), dev_f64(mass, (n,)), dev_f64(h), dev_f64(rho), dev_f64(omega),
+            dev_f64(pressure), opt(u if use_visc else None), opt(c_s if use_visc else None),
+            opt(alpha if use_visc else None)]  # fmt: skip
+    _call("nb_forces", n, ptr(pos), *[ptr(a) for a in args], ptr(off), ptr(idx), m, ptr(rows_t),
+          KERNEL_IDS[kernel_name], float(shock.beta), float(shock.alpha_u),
+          int(shock.conductivity_signal), ptr(acc), ptr(dudt), ptr(vsig), ptr(vh), ptr(ch),
+          stream())  # fmt: skip
+    if not use_visc:
+        vh.zero_()
+        ch.zero_()
+    return ForceResult(acc, dudt, vsig, vh, ch)
+
+
+def disc_forces_numba(pos, vel, mass, h, rho, omega, c_s, alpha_av, nb: Neighbours,
+                      kernel_name=DEFAULT_KERNEL, rows=None):  # fmt: skip
+    """sim/sph.py:1120-1137: (acc (rows, 3), du/dt (rows,)) of the disc viscosity."""
+    pos = dev_f64(pos)
+    n = len(pos)
+    rows_t = None if rows is None else dev_i64(rows)
+    m = n if rows_t is None else len(rows_t)
+    acc = torch.empty((m, 3), dtype=torch.float64, device=pos.device)
+    dudt = torch.empty(m, dtype=torch.float64, device=pos.device)
+    off, idx = dev_i64(nb.offset), dev_i64(nb.index)
+    _call("nb_disc_forces", n, ptr(pos), ptr(dev_f64(vel)), ptr(dev_f64(mass, (n,))),
+          ptr(dev_f64(h)), ptr(dev_f64(rho)), ptr(dev_f64(omega)), ptr(dev_f64(c_s)),
+          float(alpha_av), ptr(off), ptr(idx), m, ptr(rows_t), KERNEL_IDS[kernel_name], ptr(acc),
+          ptr(dudt), stream())  # fmt: skip
+    return acc, dudt
+
+
+def glf_step_many(x, p, dt):
+    """sim/integrator.py:188-198: one generalized-leapfrog step per particle; (x1, p1, iters).
+    Raises GLFConvergenceError like the reference."""
+    x = dev_f64(x)
+    p = dev_f64(p)
+    n = len(x)
+    x1, p1 = torch.empty_like(x), torch.empty_like(p)
+    it = torch.empty(n, dtype=torch.int64, device=x.device)
+    if isinstance(dt, (int, float)):
+        _call("nb_glf_step_many", n, ptr(x), ptr(p), None, float(dt), ptr(x1), ptr(p1), ptr(it),
+              stream())  # fmt: skip
+    else:
+        dtt = dev_f64(dt, (n,))
+        _call("nb_glf_step_many", n, ptr(x), ptr(p), ptr(dtt), 0.0, ptr(x1), ptr(p1), ptr(it),
+              stream())  # fmt: skip
+    return x1, p1, it
+
+
+def gn_v_from_p(x, p):
+    """sim/fastphys.py:35-42: v = A p + C (p.x) x."""
+    x = dev_f64(x)
+    v = torch.empty_like(x)
+    _call("nb_gn_v_from_p", len(x), ptr(x), ptr(dev_f64(p)), ptr(v), stream())
+    return v
+
+
+def gn_p_from_v(x, v):
+    """physics/gravity.py:66-77: p = f v + g rdot x/r."""
+    x = dev_f64(x)
+    p = torch.empty_like(x)
+    _call("nb_gn_p_from_v", len(x), ptr(x), ptr(dev_f64(v)), ptr(p), stream())
+    return p
+
+
+def beta_cool(u, u_floor, dt, t_cool):
+    """physics/cooling.py:33-40: u_floor + (u - u_floor) exp(-dt / t_cool)."""
+    u = dev_f64(u)
+    n = len(u)
+    out = torch.empty_like(u)
+    _call("nb_beta_cool", n, ptr(u), ptr(dev_f64(u_floor, (n,))), ptr(dev_f64(dt, (n,))),
+          ptr(dev_f64(t_cool, (n,))), ptr(out), stream())  # fmt: skip
+    return out
+
+
+def ledger_sums(x, p, u, mass) -> dict:
+    """sim/coupled.py:261-270 sums on the device: energy sum m (H + u) (without radiated energy),
+    sum m |H|, angular momentum, momentum, mass."""
+    x = dev_f64(x)
+    out = (ctypes.c_double * 9)()
+    _call("nb_ledger", len(x), ptr(x), ptr(dev_f64(p)), ptr(dev_f64(u)), ptr(dev_f64(mass)), out,
+          stream())  # fmt: skip
+    v = list(out)
+    return {"energy": v[0], "abs_h": v[1], "angmom": v[2:5], "momentum": v[5:8], "mass": v[8]}

@@ -1,0 +1,167 @@
+/*
+ * nebula_b200.h — C ABI of libnebula_b200.so, the sm_100a SPH step of Blackhole-Nebula-Simulator.
+ *
+ * Every array argument is a DEVICE pointer (e.g. torch.Tensor.data_ptr() of a CUDA tensor) in
+ * the caller's particle order, C-contiguous: positions, velocities and momenta are (n, 3)
+ * float64, per-particle scalars (n,) float64, neighbour lists CSR int64 (offset n+1, index
+ * total).  "rows" selects particles (int64 indices) whose results are written in rows order,
+ * exactly like the reference's ``rows`` argument.  `stream` is a cudaStream_t (NULL: the legacy
+ * default stream).  Nothing calls exit() or traps on the device.
+ *
+ * Return value: 0 = success; NB_ERR_* > 0 = a domain error that maps to one of the reference's
+ * exceptions (message in nb_last_error); < 0 = a CUDA or host error (message in nb_last_error).
+ */
+#ifndef NEBULA_B200_H
+#define NEBULA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* domain errors (reference exception in brackets) */
+#define NB_ERR_GLF_P_HALF 11      /* [GLFConvergenceError] stage 1 did not converge */
+#define NB_ERR_GLF_X1 12          /* [GLFConvergenceError] stage 2 did not converge */
+#define NB_ERR_GLF_RADIUS 13      /* [GLFConvergenceError] particle inside r = 2.5 */
+#define NB_ERR_SEARCH 20          /* [RuntimeError] smoothing lengths kept outgrowing the search */
+#define NB_ERR_TOUCHED 21         /* [RuntimeError] neighbour set of the active particles did not settle */
+#define NB_ERR_NONPOSITIVE_U 22   /* [FloatingPointError] non-positive internal energy */
+#define NB_ERR_LEVEL 23           /* [ValueError] a level beyond K_MAX */
+#define NB_ERR_DT 24              /* [ValueError] time steps must be positive */
+#define NB_ERR_UNSUPPORTED 25     /* [NotImplementedError] option outside the CUDA path */
+#define NB_ERR_INPUT 26           /* [ValueError] bad argument */
+
+#if defined(__GNUC__)
+#define NB_API __attribute__((visibility("default")))
+#else
+#define NB_API
+#endif
+
+typedef struct nb_ctx nb_ctx;
+
+/* Physics and numerics of one run: the fields of the reference's HydroConfig, CoupledConfig and
+ * BlockConfig that the CUDA path implements (sim/hydro.py:53-98, sim/coupled.py:62-75,
+ * sim/blocks.py:83-100). */
+typedef struct nb_params {
+  int kernel_id;          /* 0 cubic spline, 1 Wendland C4 */
+  double cnorm, eta, tol, h_max, skin;
+  double gamma;
+  int viscosity, conductivity, cond_signal;
+  double alpha_const, beta, alpha_u;
+  double disc_alpha_av;   /* > 0: disc viscosity (Option B) */
+  double courant, c_force, eta_orb;
+  int precision;          /* 0: FP64 pair arithmetic, 1: FP32 (cell offsets, Kahan sums) */
+  int cooling;            /* 0 none, 1 beta-cooling, 2 bremsstrahlung (exact), 3 brems via MLP */
+  double cooling_beta;    /* beta of beta-cooling */
+  double u_floor;         /* code u at the floor temperature */
+  double brems_tfac, brems_b, brems_kappa, brems_t_floor;
+  double dt_max;          /* block steps: level-0 step */
+  int limiter, max_gap;
+} nb_params;
+
+/* Device state of a run (the fields of the reference's GasState / BlockState that the step
+ * reads or writes).  Block-step fields may be NULL for the shared step. */
+typedef struct nb_state {
+  int64_t n;
+  double *x, *p, *u, *mass, *h, *alpha, *a_hydro, *dudt, *rho, *omega, *c_s, *vsig_max, *nu;
+  double *visc_heating;
+  int64_t *level, *n_beg, *n_end, *level_offset;
+  double *x_beg, *p_half, *u_half, *luminosity;
+  int64_t tick_n, n_stop;
+  double t0, tick;
+  double e_radiated;
+  int64_t particle_steps, woken, last_active, pairs;
+  int64_t builds, reuses;
+} nb_state;
+
+/* ---------------------------------------------------------------- context */
+NB_API nb_ctx* nb_create(int device);
+NB_API void nb_destroy(nb_ctx* ctx);
+NB_API const char* nb_last_error(nb_ctx* ctx);
+NB_API int nb_version(void);
+
+/* ---------------------------------------------------------------- operators
+ * One-for-one replacements of the reference's inner functions (sim/neighbours.py, sim/sph.py,
+ * sim/integrator.py, sim/fastphys.py, physics/cooling.py). */
+
+/* find_neighbours_numba (sim/neighbours.py:240-281): builds the symmetric lists
+ * {j : r_ij < 2 max(h_i, h_j)} (no periodic box) and writes offset (n+1) and *total (host).
+ * nb_neighbours_export then writes index (total) with every row sorted ascending. */
+NB_API int nb_find_neighbours(nb_ctx* ctx, int64_t n, const double* pos, const double* h, int64_t* offset,
+                       int64_t* total, void* stream);
+NB_API int nb_neighbours_export(nb_ctx* ctx, int64_t* offset, int64_t* index, void* stream);
+
+/* tighten (sim/neighbours.py:284-323), two calls: out_off == NULL writes counts (n) of the kept
+ * entries per row; then with out_off (n+1, the caller's prefix sum) writes out_idx. */
+NB_API int nb_tighten(nb_ctx* ctx, int64_t n, const double* pos, const double* h, const int64_t* offset,
+               const int64_t* index, int64_t nrows, const int64_t* rows, int64_t* counts,
+               const int64_t* out_off, int64_t* out_idx, void* stream);
+
+/* density_numba (sim/sph.py:300-326): results (nrows) in rows order (rows NULL: all n). */
+NB_API int nb_density(nb_ctx* ctx, int64_t n, const double* pos, const double* mass,
+               const double* h_start, const double* h_search, const int64_t* offset,
+               const int64_t* index, int64_t nrows, const int64_t* rows, int kernel_id,
+               double eta, double tol, double h_max, double* h_out, double* rho, double* omega,
+               int64_t* iters, int64_t* flags, void* stream);
+
+/* forces_numba without reconstruction (sim/sph.py:655-690).  u NULL: no conductivity; alpha or
+ * c_s NULL: no viscosity.  vheat / cheat may be NULL. */
+NB_API int nb_forces(nb_ctx* ctx, int64_t n, const double* pos, const double* vel, const double* mass,
+              const double* h, const double* rho, const double* omega, const double* pressure,
+              const double* u, const double* c_s, const double* alpha, const int64_t* offset,
+              const int64_t* index, int64_t nrows, const int64_t* rows, int kernel_id,
+              double beta, double alpha_u, int cond_signal, double* acc, double* dudt,
+              double* vsig_max, double* vheat, double* cheat, void* stream);
+
+/* disc_forces_numba (sim/sph.py:1120-1137). */
+NB_API int nb_disc_forces(nb_ctx* ctx, int64_t n, const double* pos, const double* vel,
+                   const double* mass, const double* h, const double* rho, const double* omega,
+                   const double* c_s, double alpha_av, const int64_t* offset, const int64_t* index,
+                   int64_t nrows, const int64_t* rows, int kernel_id, double* acc, double* dudt,
+                   void* stream);
+
+/* glf_step_many (sim/integrator.py:188-198): dt (n) or, when dt is NULL, dt_scalar for all.
+ * iters: iterations, or -1 / -2 / -3 for a failed particle (status NB_ERR_GLF_*). */
+NB_API int nb_glf_step_many(nb_ctx* ctx, int64_t n, const double* x, const double* p, const double* dt,
+                     double dt_scalar, double* x1, double* p1, int64_t* iters, void* stream);
+
+/* gn_v_from_p_nb (sim/fastphys.py:35-42) and gn_p_from_v (physics/gravity.py:66-77). */
+NB_API int nb_gn_v_from_p(nb_ctx* ctx, int64_t n, const double* x, const double* p, double* v, void* stream);
+NB_API int nb_gn_p_from_v(nb_ctx* ctx, int64_t n, const double* x, const double* v, double* p, void* stream);
+
+/* beta_cool (physics/cooling.py:33-40), elementwise. */
+NB_API int nb_beta_cool(nb_ctx* ctx, int64_t n, const double* u, const double* u_floor, const double* dt,
+                 const double* t_cool, double* out, void* stream);
+
+/* Exact bremsstrahlung cooling at fixed rho over dt (no reference counterpart; the law is
+ * documented in cooling.cuh).  dt NULL: dt_scalar for all. */
+NB_API int nb_brems_cool(nb_ctx* ctx, int64_t n, const double* u, const double* rho, const double* dt,
+                  double dt_scalar, const nb_params* prm, double* out, void* stream);
+
+/* Ledger sums (sim/coupled.py:261-270) into out[9] on the host: sum m (H + u), sum m |H|,
+ * angular momentum (3), momentum (3), mass. */
+NB_API int nb_ledger(nb_ctx* ctx, int64_t n, const double* x, const double* p, const double* u,
+              const double* mass, double* out, void* stream);
+
+/* ---------------------------------------------------------------- step runtime
+ * The reference's step entry points (sim/coupled.py:198-258, sim/blocks.py:455-563) on device
+ * state.  The list cache (and its reuse test, sim/sph.py:62-147) lives in the context. */
+NB_API int nb_coupled_initialise(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* stream);
+NB_API int nb_coupled_step(nb_ctx* ctx, nb_state* st, const nb_params* prm, double dt, void* stream);
+NB_API int nb_coupled_stable_dt(nb_ctx* ctx, nb_state* st, const nb_params* prm, double* dt_out,
+                         void* stream);
+NB_API int nb_block_initialise(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* stream);
+NB_API int nb_block_advance(nb_ctx* ctx, nb_state* st, const nb_params* prm, int64_t* rows_out,
+                     void* stream);
+/* Re-open the steps just opened so they land on n_stop (sim/blocks.py:722-734, run's prologue). */
+NB_API int nb_block_land(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* stream);
+
+/* Drop the cached neighbour lists (the next density call rebuilds them). */
+NB_API int nb_reset_cache(nb_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEBULA_B200_H */

@@ -357,8 +357,9 @@ static inline void sums(const double* r, const double* m, int64_t cnt, double h,
                         double cnorm, double* rs_out, double* dws_out) {
   double rs = 0.0, dws = 0.0;
   double inv_h = 1.0 / h;
-  double ih3 = inv_h * inv_h * inv_h;
-  double ih4 = ih3 * inv_h;
+  double ih2 = inv_h * inv_h;
+  double ih3 = ih2 * inv_h;  /* x**3 and x**4 as Numba evaluates integer powers */
+  double ih4 = ih2 * ih2;
   for (int64_t k = 0; k < cnt; ++k) {
     double q = r[k] * inv_h;
     if (q < 2.0) {
@@ -421,8 +422,8 @@ void or_density(int64_t n, const double* pos, const double* mass, const double* 
         sums(r, m, cnt, h, kid, cnorm, &rs, &dws);
         double t = eta / h;
         double f = rs - m_i * (t * t * t);
-        double h4 = h * h * h * h;
-        double df = dws + 3.0 * m_i * e3 / h4;
+        double h2 = h * h;
+        double df = dws + 3.0 * m_i * e3 / (h2 * h2);
         if (f > 0)
           hi = h;
         else
@@ -463,8 +464,8 @@ void or_density(int64_t n, const double* pos, const double* mass, const double* 
  * sim/sph.py:519-652 (_dwdr, _forces_kernel) without velocity reconstruction: pressure force,
  * P dV work, signal-velocity viscosity with shock heating, optional conductivity. */
 static inline double dwdr(double r, double h, int kid, double cnorm) {
-  double h4 = h * h * h * h;
-  return cnorm / h4 * kernel_df(r / h, kid);
+  double h2 = h * h;
+  return cnorm / (h2 * h2) * kernel_df(r / h, kid);
 }
 
 void or_forces(const double* pos, const double* vel, const double* mass, const double* h,
@@ -576,7 +577,7 @@ void or_disc_forces(const double* pos, const double* vel, const double* mass, co
 static inline void dh_dx(double x0, double x1, double x2, double p0, double p1, double p2,
                          double* g) {
   double r = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
-  double r2 = r * r, r3 = r2 * r, r4 = r3 * r, r5 = r4 * r;
+  double r2 = r * r, r3 = r2 * r, r4 = r2 * r2, r5 = r4 * r;
   double c = -2.0 * (r - 2.0) / r4;
   double da = 2.0 / (r * r);
   double dc = (6.0 * r - 16.0) / r5;
@@ -591,7 +592,7 @@ static inline void dh_dx(double x0, double x1, double x2, double p0, double p1, 
 static inline void dh_dp(double x0, double x1, double x2, double p0, double p1, double p2,
                          double* v) {
   double r = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
-  double r4 = r * r * r * r;
+  double r2 = r * r, r4 = r2 * r2;
   double a = (r - 2.0) / r;
   double c = -2.0 * (r - 2.0) / r4;
   double cpx = c * (p0 * x0 + p1 * x1 + p2 * x2);
