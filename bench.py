@@ -1,0 +1,334 @@
+"""Benchmark of the SPH step: particle-steps/s of block-timestep system steps on one B200.
+
+One "step" is one system step (blocks.advance): the GN gravity flow of every particle, density
+for the active rows and their neighbours, the fused force + du/dt pass for the active rows,
+cooling, kicks and new levels.  value = active particles summed over the K timed system steps of
+all ranks / the slowest rank's device time (CUDA events on the launching stream).
+
+Workloads (seeded synthetic inputs; there is no dataset):
+  torus   4,194,304 particles, Gaussian torus R=100 a=40 sigma=15, T=1e9 K, disc viscosity
+          alpha_SS = 0.1, bremsstrahlung cooling, block steps (dt_max 256)   [default]
+  streams 1,048,576 particles, two colliding cylinders at r=1664, 1e-10 g/cm^3, bremsstrahlung
+  cloud   262,144-particle cloud on a GN orbit (block steps)
+Inputs (~1 GB of particle state at 4M) are larger than the 126 MB L2, so no flush is needed.
+
+--impl reference times the reference's algorithm on the host cores instead: the CPU oracle port
+(oracle/, C + OpenMP, all host threads) on a bounded sample of the same workload.
+Multi-GPU: replicas only (each rank runs an independent seeded run; no collective in the step).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA x clock
+FP64_NOMINAL_TFLOPS = FP32_NOMINAL_TFLOPS / 2.0
+FLOP_PER_DENSITY_EVAL = 25.0  # distance + kernel + two sums per pair evaluation
+FLOP_PER_FORCE_PAIR = 75.0  # pressure + viscosity + P dV (+20 with disc viscosity)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return {"hbm_gbs": p["hbm_gbs"], "bf16_tflops": p["bf16_tflops"], "source": "measured"}
+    return {**PEAKS_FALLBACK, "source": "fallback"}
+
+
+def workload(name: str, n: int | None, precision: str, seed_shift: int = 0):
+    from blackhole_nebula_simulator_b200 import ics
+    from blackhole_nebula_simulator_b200.config import BlockConfig, CoupledConfig, HydroConfig
+
+    common = dict(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                  conductivity_signal=1, alpha_u=0.05, h_max=200.0, precision=precision)  # fmt: skip
+    if name == "torus":
+        n = n or 4_194_304
+        ic = ics.torus(n, seed=4 + seed_shift)
+        alpha_av = 10.0 * 0.1 * 15.0 / float(np.mean(ic.h))  # alpha_SS = 0.1, H = sigma = 15
+        hc = HydroConfig(disc_alpha_av=alpha_av, **common)
+        bc = BlockConfig(coupled=CoupledConfig(hydro=hc, cooling="brems"), dt_max=256.0)
+    elif name == "streams":
+        n = n or 1_048_576
+        ic = ics.streams(n, seed=3 + seed_shift)
+        bc = BlockConfig(coupled=CoupledConfig(hydro=HydroConfig(**common), cooling="brems"),
+                         dt_max=4096.0)  # fmt: skip
+    elif name == "cloud":
+        n = n or 262_144
+        ic = ics.cloud(n, seed=1 + seed_shift)
+        bc = BlockConfig(coupled=CoupledConfig(hydro=HydroConfig(**common)), dt_max=4096.0)
+    else:
+        raise ValueError(name)
+    return ic, bc
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")  # fmt: skip
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)  # fmt: skip
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([s.strip() for s in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 3 + k and r[3 + k].lower() == "active"})  # fmt: skip
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows)}
+
+
+def profile_read(ctx):
+    import ctypes
+
+    from blackhole_nebula_simulator_b200 import _lib
+
+    out = (ctypes.c_double * 16)()
+    _lib.check(ctx, _lib.lib().nb_profile_read(ctx, out))
+    names = ["lists", "density", "forces", "flow"]
+    return {names[c]: {"ms": out[4 * c], "launches": int(out[4 * c + 1]), "units": out[4 * c + 2],
+                       "pairs": out[4 * c + 3]} for c in range(4)}  # fmt: skip
+
+
+def roofline(prof, precision, disc, pk):
+    """Dominant kernel: its algorithmic bytes per launch over its event-timed duration."""
+    dom = max(prof, key=lambda k: prof[k]["ms"])
+    d = prof[dom]
+    if d["launches"] == 0:
+        return None, dom
+    ms = d["ms"] / d["launches"]
+    rec = 112.0 if precision == "fp32" else 128.0  # packed per-particle records of a pair pass
+    units = d["units"] / d["launches"]
+    pairs = d["pairs"] / d["launches"]
+    if dom == "forces":
+        bytes_ = units * (rec + 48.0) + pairs * 4.0
+        flops = pairs * (FLOP_PER_FORCE_PAIR + (20.0 if disc else 0.0))
+    elif dom == "density":
+        bytes_ = units * (48.0 + 40.0) + pairs * 4.0
+        flops = pairs * FLOP_PER_DENSITY_EVAL
+    elif dom == "lists":
+        bytes_ = units * (32.0 + 8.0) + pairs * 4.0
+        flops = 0.0
+    else:  # flow: x_beg, p_half, n_beg, n_end, a read; x, p_flow, p_pred written
+        bytes_ = units * (48.0 + 16.0 + 24.0 + 72.0 + 8.0)
+        flops = 0.0
+    gbs = bytes_ / (ms * 1e-3) / 1e9
+    pipe_peak = FP32_NOMINAL_TFLOPS if precision == "fp32" else FP64_NOMINAL_TFLOPS
+    rf = {"bound": "hbm", "kernel": dom, "achieved": round(gbs, 2), "peak": pk["hbm_gbs"],
+          "unit": "GB/s", "frac": round(gbs / pk["hbm_gbs"], 4), "traffic": None,
+          "peak_source": pk["source"], "ms_per_launch": round(ms, 4),
+          "bytes_per_launch": bytes_}  # fmt: skip
+    if flops:
+        tf = flops / (ms * 1e-3) / 1e12
+        rf["pipe"] = {"unit": "TFLOP/s", "achieved": round(tf, 3), "peak": round(pipe_peak, 2),
+                      "frac": round(tf / pipe_peak, 4), "peak_source": "nominal",
+                      "precision": precision}  # fmt: skip
+    return rf, dom
+
+
+def run_gpu(args, rank, world):
+    import torch
+
+    from blackhole_nebula_simulator_b200 import _lib, blocks
+    from blackhole_nebula_simulator_b200.device import ctx
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    ic, bc = workload(args.workload, args.n, args.precision, seed_shift=rank)
+    st = blocks.initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=1e12)
+    for _ in range(args.warmup):
+        blocks.advance(st, bc)
+    c = ctx(dev)
+    stream = torch.cuda.current_stream()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    _lib.check(c, _lib.lib().nb_profile(c, 1))
+    steps0 = st.particle_steps
+    launches0 = _lib.lib().nb_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev.index) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            blocks.advance(st, bc)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = _lib.lib().nb_launch_count() - launches0
+    prof = profile_read(c)
+    prof["_launches"] = launches
+    _lib.check(c, _lib.lib().nb_profile(c, 0))
+    ms = e0.elapsed_time(e1)
+    psteps = st.particle_steps - steps0
+    if world > 1:
+        t = torch.tensor([ms, float(psteps)], dtype=torch.float64, device=dev)
+        tmax = t.clone()
+        torch.distributed.all_reduce(tmax[:1], op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(t[1:], op=torch.distributed.ReduceOp.SUM)
+        ms, total = float(tmax[0]), float(t[1])
+    else:
+        total = float(psteps)
+    led = blocks.ledger(st, bc)
+    e2e = run_e2e(args, st, bc, dev)
+    return ms, total, prof, clk.summary(), st, led, e2e
+
+
+def run_e2e(args, st, bc, dev):
+    """Same metric through the public API with host state: every step copies the block state in
+    from pinned host memory and reads the updated state back."""
+    import torch
+
+    from blackhole_nebula_simulator_b200 import blocks
+
+    names = [k for k, v in st.__dict__.items() if isinstance(v, torch.Tensor) and k != "_rows"]
+    host = {k: torch.empty_like(getattr(st, k), device="cpu").pin_memory() for k in names}
+    for k in names:
+        host[k].copy_(getattr(st, k))
+    back = ("x", "p", "u", "h", "level", "n_end")
+    h2d = sum(host[k].numel() * host[k].element_size() for k in names)
+    d2h = sum(host[k].numel() * host[k].element_size() for k in back)
+    steps = max(1, min(args.steps, 3))
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    s0 = st.particle_steps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        for k in names:
+            getattr(st, k).copy_(host[k], non_blocking=True)
+        blocks.advance(st, bc)
+        for k in back:
+            host[k].copy_(getattr(st, k), non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"value": (st.particle_steps - s0) / (ms * 1e-3), "unit": "particle-steps/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": steps}  # fmt: skip
+
+
+def cpu_reference(args, steps, warmup, sample_n=None):
+    """The reference algorithm on the host cores: the CPU oracle's block step (C + OpenMP on all
+    host threads), on a bounded sample of the workload (same generator and physics, fewer
+    particles), so that the run stays within minutes."""
+    from oracle import steps as osteps
+
+    n_full = {"torus": 4_194_304, "streams": 1_048_576, "cloud": 262_144}[args.workload]
+    n = sample_n or min(args.n or n_full, 131_072)
+    ic, bc = workload(args.workload, n, "fp64")
+    st = osteps.blocks_initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=1e12)
+    for _ in range(warmup):
+        osteps.blocks_advance(st, bc)
+    s0 = st.particle_steps
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        osteps.blocks_advance(st, bc)
+    dt = time.perf_counter() - t0
+    cores = os.cpu_count()
+    return {"value": (st.particle_steps - s0) / dt, "unit": "particle-steps/s", "cores": cores,
+            "kind": "port", "sample": f"{args.workload} workload at {n} particles (same generator "
+            f"and physics), {steps} timed system steps after {warmup} warm-up, oracle on "
+            f"{cores} OpenMP threads"}  # fmt: skip
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="torus", choices=["torus", "streams", "cloud"])
+    ap.add_argument("--n", type=int, default=None)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    n_full = args.n or {"torus": 4_194_304, "streams": 1_048_576, "cloud": 262_144}[args.workload]
+    config = {"workload": f"{args.workload}, {n_full} particles, block time steps",
+              "particles": n_full, "precision": args.precision, "l2_flush": "inputs larger than L2",
+              "parallelism": f"replicas x{world}"}  # fmt: skip
+    metric = "particle-steps/s"
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cb = cpu_reference(args, max(1, min(args.steps, 3)), max(1, min(args.warmup, 1)))
+        print(json.dumps({"metric": metric, "value": cb["value"], "unit": "particle-steps/s",
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "higher_is_better": True, "impl": "reference", "dtype": "f64",
+                          "data": "synthetic", "config": config, "cpu_baseline": cb,
+                          "e2e": {"value": cb["value"], "unit": "particle-steps/s",
+                                  "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))  # fmt: skip
+        return
+    if world > 1:
+        import torch
+
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    ms, total, prof, clocks, st, led, e2e = run_gpu(args, rank, world)
+    if rank == 0:
+        pk = peaks()
+        launches = prof.pop("_launches")
+        rf, dom = roofline(prof, args.precision, "torus" == args.workload, pk)
+        out = {
+            "metric": metric, "value": total / (ms * 1e-3), "unit": "particle-steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
+            "data": "synthetic", "config": config, "roofline": rf, "clocks": clocks, "e2e": e2e,
+            "gpu_launches": launches, "kernel_ms": {k: round(v["ms"], 3) for k, v in prof.items()},
+            "mean_active": total / args.steps / max(world, 1),
+            "list_builds": st.builds, "list_reuses": st.reuses,
+            "energy_rel_drift": None,
+        }  # fmt: skip
+        if not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_reference(args, 2, 1)
+        print(json.dumps(out))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

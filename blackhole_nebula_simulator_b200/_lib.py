@@ -60,7 +60,10 @@ _SIGS = {
     "nb_destroy": (None, [_vp]),
     "nb_last_error": (_c.c_char_p, [_vp]),
     "nb_version": (_int, []),
+    "nb_launch_count": (_i64, []),
     "nb_reset_cache": (_int, [_vp]),
+    "nb_profile": (_int, [_vp, _int]),
+    "nb_profile_read": (_int, [_vp, _c.POINTER(_dbl)]),
     "nb_find_neighbours": (_int, [_vp, _i64, _vp, _vp, _vp, _c.POINTER(_i64), _vp]),
     "nb_neighbours_export": (_int, [_vp, _vp, _vp, _vp]),
     "nb_tighten": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),

@@ -11,6 +11,10 @@
 #include "sph.cuh"
 #include "steps.cuh"
 
+namespace nbk {
+unsigned long long g_launch_count = 0;
+}
+
 struct nb_ctx {
   nbk::Engine E;
 };
@@ -96,6 +100,8 @@ extern "C" {
 
 int nb_version(void) { return 1; }
 
+int64_t nb_launch_count(void) { return (int64_t)__atomic_load_n(&nbk::g_launch_count, __ATOMIC_RELAXED); }
+
 nb_ctx* nb_create(int device) {
   nb_ctx* c = new (std::nothrow) nb_ctx();
   if (!c) return nullptr;
@@ -154,7 +160,7 @@ int nb_tighten(nb_ctx* ctx, int64_t n, const double* pos, const double* h, const
   Engine& E = ctx->E;
   if (!out_off) NB_CUDA(cudaMemsetAsync(counts, 0, sizeof(int64_t) * n, S(stream)));
   if (nrows > 0)
-    k_tighten<<<nbk::grid_for(nrows), NB_THREADS, 0, S(stream)>>>(nrows, rows, pos, h, offset,
+    nbk::count_launch(), k_tighten<<<nbk::grid_for(nrows), NB_THREADS, 0, S(stream)>>>(nrows, rows, pos, h, offset,
                                                                   index, counts, out_off, out_idx);
   NB_CUDA(cudaGetLastError());
   return nbk::check_device_error(E, S(stream));
@@ -173,7 +179,7 @@ int nb_density(nb_ctx* ctx, int64_t n, const double* pos, const double* mass,
   nbk::DensityParams dp{kernel_id, cnorm_of(kernel_id), eta, tol, h_max};
   nbk::launch_density64<int64_t>(rows ? nrows : n, rows, E.ws.pk0, mass, h_start, h_search,
                                  offset, index, dp, nullptr, h_out, rho, omega, iters, flags,
-                                 S(stream));
+                                 nullptr, S(stream));
   NB_CUDA(cudaGetLastError());
   return nbk::check_device_error(E, S(stream));
 }
@@ -290,7 +296,7 @@ int nb_beta_cool(nb_ctx* ctx, int64_t n, const double* u, const double* u_floor,
                  const double* t_cool, double* out, void* stream) {
   NB_TRY(begin(ctx));
   Engine& E = ctx->E;
-  if (n > 0) k_beta<<<nbk::grid_for(n), NB_THREADS, 0, S(stream)>>>(n, u, u_floor, dt, t_cool, out);
+  if (n > 0) nbk::count_launch(), k_beta<<<nbk::grid_for(n), NB_THREADS, 0, S(stream)>>>(n, u, u_floor, dt, t_cool, out);
   NB_CUDA(cudaGetLastError());
   return 0;
 }
@@ -301,7 +307,7 @@ int nb_brems_cool(nb_ctx* ctx, int64_t n, const double* u, const double* rho, co
   Engine& E = ctx->E;
   if (!prm) return nbk::set_host_error(E, "params missing"), NB_ERR_INPUT;
   if (n > 0)
-    k_brems<<<nbk::grid_for(n), NB_THREADS, 0, S(stream)>>>(n, u, rho, dt, dt_scalar,
+    nbk::count_launch(), k_brems<<<nbk::grid_for(n), NB_THREADS, 0, S(stream)>>>(n, u, rho, dt, dt_scalar,
                                                             brems_params(prm), out);
   NB_CUDA(cudaGetLastError());
   return 0;
@@ -356,6 +362,31 @@ int nb_block_land(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* stream)
   NB_TRY(begin(ctx));
   NB_TRY(check_params(ctx->E, prm));
   return nbk::block_land(ctx->E, st, prm, S(stream));
+}
+
+int nb_profile(nb_ctx* ctx, int on) {
+  NB_TRY(begin(ctx));
+  nbk::Prof& P = ctx->E.prof;
+  P.on = on != 0;
+  for (int c = 0; c < nbk::PROF_NCAT; ++c) {
+    P.ms[c] = 0;
+    P.launches[c] = 0;
+    P.units[c] = 0;
+    P.pairs[c] = 0;
+  }
+  return 0;
+}
+
+int nb_profile_read(nb_ctx* ctx, double* out) {
+  NB_TRY(begin(ctx));
+  nbk::Prof& P = ctx->E.prof;
+  for (int c = 0; c < nbk::PROF_NCAT; ++c) {
+    out[4 * c + 0] = P.ms[c];
+    out[4 * c + 1] = (double)P.launches[c];
+    out[4 * c + 2] = P.units[c];
+    out[4 * c + 3] = P.pairs[c];
+  }
+  return 0;
 }
 
 }  // extern "C"

@@ -73,6 +73,13 @@ struct Kahan {
   }
 };
 
+// Launches of this library's own kernels (read through nb_launch_count).
+extern unsigned long long g_launch_count;
+inline int count_launch() {
+  __atomic_add_fetch(&g_launch_count, 1ull, __ATOMIC_RELAXED);
+  return 0;
+}
+
 inline unsigned grid_for(int64_t n, int threads = NB_THREADS) {
   int64_t b = (n + threads - 1) / threads;
   return (unsigned)(b > 0 ? b : 1);

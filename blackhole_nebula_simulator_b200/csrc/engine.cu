@@ -50,6 +50,8 @@ int Engine::ensure_n(int64_t n) {
     NB_CUDA(cudaMallocHost((void**)&h_err, sizeof(int) * 4));
     NB_CUDA(cudaMalloc((void**)&bbox, sizeof(double) * 8));
     NB_CUDA(cudaMallocHost((void**)&h_red, sizeof(double) * 64));
+    NB_CUDA(cudaEventCreate(&prof.a));
+    NB_CUDA(cudaEventCreate(&prof.b));
   }
   if (n <= cap_n && keys_a) return 0;
   int64_t c = std::max<int64_t>(n + n / 4, 1024);
@@ -420,6 +422,28 @@ void Workspace::release() {
   *this = Workspace{cache};
 }
 
+__global__ void k_gather_rows_i64(int64_t nrows, const int64_t* __restrict__ rows,
+                                  const int64_t* __restrict__ a, int64_t* __restrict__ out) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q < nrows) out[q] = a[rows[q]];
+}
+
+// sum of a[rows] into E.ws.h_i64[0] (profiling only)
+static int sum_rows_i64(Engine& E, int64_t nrows, const int64_t* rows, const int64_t* a,
+                        cudaStream_t st) {
+  Workspace& W = E.ws;
+  if (nrows <= 0) {
+    W.h_i64[0] = 0;
+    return 0;
+  }
+  count_launch(), k_gather_rows_i64<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, a, W.i_tmp);
+  size_t tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceReduce::Sum(E.cub_tmp, tmp, W.i_tmp, W.d_i64, (int)nrows, st));
+  NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  return 0;
+}
+
 static int read_int(Engine& E, int* d, int* out, cudaStream_t st) {
   NB_CUDA(cudaMemcpyAsync(E.ws.h_int, d, sizeof(int), cudaMemcpyDeviceToHost, st));
   NB_CUDA(cudaStreamSynchronize(st));
@@ -436,10 +460,10 @@ static int density_on_lists(Engine& E, int64_t n, const double* x, const double*
   Workspace& W = E.ws;
   Lists& L = E.lists;
   if (nrows == 0) return 0;
-  k_rows_to_sorted<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.inv_perm, W.rows_s);
-  k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, mass, W.d_a);
-  k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, h_start, W.d_b);
-  k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, h_search, W.d_c);
+  count_launch(), k_rows_to_sorted<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.inv_perm, W.rows_s);
+  count_launch(), k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, mass, W.d_a);
+  count_launch(), k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, h_start, W.d_b);
+  count_launch(), k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, h_search, W.d_c);
   DensityParams dp{prm->kernel_id, prm->cnorm, prm->eta, prm->tol, prm->h_max};
   if (prm->precision == 1) {
     double span = 0;
@@ -447,13 +471,24 @@ static int density_on_lists(Engine& E, int64_t n, const double* x, const double*
     NB_CUDA(cudaStreamSynchronize(st));
     for (int a = 0; a < 3; ++a) span = std::max(span, W.h_dbl[3 + a] - W.h_dbl[a]);
     double cell = std::max(span / 1000.0, 1e-30);
-    k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, E.bbox, cell, W.pk32);
+    count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, E.bbox, cell, W.pk32);
+    E.prof.begin(st);
     launch_density32<int32_t>(nrows, W.rows_s, W.pk32, (float)cell, W.d_a, W.d_b, W.d_c, L.off,
-                              L.idx, dp, L.perm, h_out, rho, omega, W.iters, W.flags, st);
+                              L.idx, dp, L.perm, h_out, rho, omega, W.iters, W.flags,
+                              E.prof.on ? W.pairs : nullptr, st);
   } else {
-    k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, nullptr, W.pk0);
+    count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, nullptr, W.pk0);
+    E.prof.begin(st);
     launch_density64<int32_t>(nrows, W.rows_s, W.pk0, W.d_a, W.d_b, W.d_c, L.off, L.idx, dp,
-                              L.perm, h_out, rho, omega, W.iters, W.flags, st);
+                              L.perm, h_out, rho, omega, W.iters, W.flags,
+                              E.prof.on ? W.pairs : nullptr, st);
+  }
+  if (E.prof.on) {
+    // kernel evaluations inside the support (pair evaluations summed over every Newton sum)
+    E.prof.end(PROF_DENSITY, st, (double)nrows, 0.0);
+    NB_CUDA(cudaMemsetAsync(W.d_i64, 0, sizeof(int64_t), st));
+    NB_TRY(sum_rows_i64(E, nrows, rows, W.pairs, st));
+    E.prof.pairs[PROF_DENSITY] += (double)W.h_i64[0];
   }
   NB_CUDA(cudaGetLastError());
   return 0;
@@ -466,7 +501,7 @@ static int reuse_limits(Engine& E, int64_t n, const double* x, const double* hg,
   Workspace& W = E.ws;
   Cache& C = W.cache;
   *ok = 0;
-  k_disp<<<grid_for(n), NB_THREADS, 0, st>>>(n, x, C.x_ref, W.d_disp, W.i32a);
+  count_launch(), k_disp<<<grid_for(n), NB_THREADS, 0, st>>>(n, x, C.x_ref, W.d_disp, W.i32a);
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceRadixSort::SortPairsDescending(E.cub_tmp, tmp, W.d_disp, W.dk_b, W.i32a,
                                                     W.i32b, (int)n, 0, 64, st));
@@ -478,7 +513,7 @@ static int reuse_limits(Engine& E, int64_t n, const double* x, const double* hg,
     if (nf >= top) break;
     double d_rest = W.h_dbl[nf];
     NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
-    k_reuse_test<<<grid_for(n), NB_THREADS, 0, st>>>(n, C.hs, W.d_disp, d_rest, hg, W.m_rows,
+    count_launch(), k_reuse_test<<<grid_for(n), NB_THREADS, 0, st>>>(n, C.hs, W.d_disp, d_rest, hg, W.m_rows,
                                                      W.d_heff, W.d_hlim, W.d_int);
     int fail = 0;
     NB_TRY(read_int(E, W.d_int, &fail, st));
@@ -488,7 +523,7 @@ static int reuse_limits(Engine& E, int64_t n, const double* x, const double* hg,
       return 0;
     }
     NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
-    k_fast_complete<<<nf, NB_THREADS, 0, st>>>(n, nf, W.i32b, x, W.d_hlim, E.lists.inv_perm,
+    count_launch(), k_fast_complete<<<nf, NB_THREADS, 0, st>>>(n, nf, W.i32b, x, W.d_hlim, E.lists.inv_perm,
                                                E.lists.off, E.lists.idx, W.d_int);
     NB_TRY(read_int(E, W.d_int, &fail, st));
     if (!fail) {
@@ -510,7 +545,7 @@ int compute_density(Engine& E, int64_t n, const double* x, const double* mass, d
   Cache& C = W.cache;
   NB_TRY(W.ensure(E, n));
   NB_CUDA(cudaMemsetAsync(W.m_rows, 0, n, st));
-  k_mask_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, n, W.m_rows, E.d_err);
+  count_launch(), k_mask_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, n, W.m_rows, E.d_err);
   NB_CUDA(cudaMemcpyAsync(W.d_hg, h, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   if (C.valid && C.n == n && n > 0 && E.lists.n == n) {
     int ok = 0;
@@ -518,23 +553,23 @@ int compute_density(Engine& E, int64_t n, const double* x, const double* mass, d
     if (ok) {
       NB_TRY(density_on_lists(E, n, x, mass, W.d_hg, W.d_heff, nrows, rows, prm, h, rho, omega, st));
       NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
-      k_count_flag2<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, W.flags, W.d_int);
+      count_launch(), k_count_flag2<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, W.flags, W.d_int);
       int grow_n = 0;
       NB_TRY(read_int(E, W.d_int, &grow_n, st));
       if (grow_n == 0) {
         *reuses += 1;
         return check_device_error(E, st);
       }
-      k_max_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, h, W.d_hg);
+      count_launch(), k_max_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, h, W.d_hg);
     }
   }
-  k_hsearch<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.d_hg, prm->h_max, prm->skin, W.d_hs);
+  count_launch(), k_hsearch<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.d_hg, prm->h_max, prm->skin, W.d_hs);
   for (int round = 0; round < 12; ++round) {
     NB_TRY(build_lists(E, n, x, W.d_hs, st));
     *builds += 1;
     NB_TRY(density_on_lists(E, n, x, mass, W.d_hg, W.d_hs, nrows, rows, prm, h, rho, omega, st));
     NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
-    k_grow<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, W.flags, h, W.d_hs, W.d_hg, W.d_int);
+    count_launch(), k_grow<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, W.flags, h, W.d_hs, W.d_hg, W.d_int);
     int grow_n = 0;
     NB_TRY(read_int(E, W.d_int, &grow_n, st));
     if (grow_n == 0) {
@@ -554,22 +589,22 @@ void mark_rows(Engine& E, int64_t nrows, const int64_t* rows, int tight, const d
                const double* h, uint8_t* mark, cudaStream_t st) {
   if (nrows <= 0) return;
   Lists& L = E.lists;
-  k_mark<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.perm, L.inv_perm, L.off, L.idx,
+  count_launch(), k_mark<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.perm, L.inv_perm, L.off, L.idx,
                                                  tight, x, h, mark);
 }
 
 void mask_and_not(int64_t n, const uint8_t* a, const uint8_t* b, uint8_t* out, cudaStream_t st) {
-  if (n > 0) k_mask_and_not<<<grid_for(n), NB_THREADS, 0, st>>>(n, a, b, out);
+  if (n > 0) count_launch(), k_mask_and_not<<<grid_for(n), NB_THREADS, 0, st>>>(n, a, b, out);
 }
 
 void mask_or(int64_t n, const uint8_t* a, uint8_t* b, cudaStream_t st) {
-  if (n > 0) k_mask_or<<<grid_for(n), NB_THREADS, 0, st>>>(n, a, b);
+  if (n > 0) count_launch(), k_mask_or<<<grid_for(n), NB_THREADS, 0, st>>>(n, a, b);
 }
 
 int select_mask(Engine& E, int64_t n, const uint8_t* mask, int64_t* out, int64_t* count,
                 cudaStream_t st) {
   Workspace& W = E.ws;
-  k_iota64<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.i_tmp);
+  count_launch(), k_iota64<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.i_tmp);
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceSelect::Flagged(E.cub_tmp, tmp, W.i_tmp, mask, out, W.d_i64, (int)n, st));
   NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
@@ -586,12 +621,12 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   Workspace& W = E.ws;
   Lists& L = E.lists;
   int64_t n = s->n;
-  k_eos<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->rho, u, prm->gamma, W.d_P, W.d_cs, E.d_err);
+  count_launch(), k_eos<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->rho, u, prm->gamma, W.d_P, W.d_cs, E.d_err);
   if (nrows == 0) return check_device_error(E, st);
-  k_rows_to_sorted<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.inv_perm, W.rows_s);
-  k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, vel, s->mass, W.pk1);
-  k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->h, s->rho, s->omega, W.d_P, W.pk2);
-  k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, W.pk3);
+  count_launch(), k_rows_to_sorted<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.inv_perm, W.rows_s);
+  count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, vel, s->mass, W.pk1);
+  count_launch(), k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->h, s->rho, s->omega, W.d_P, W.pk2);
+  count_launch(), k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, W.pk3);
   ForceParams fp{};
   fp.kid = prm->kernel_id;
   fp.cnorm = prm->cnorm;
@@ -619,15 +654,23 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
     for (int a = 0; a < 3; ++a) span = std::max(span, W.h_dbl[3 + a] - W.h_dbl[a]);
     // the grid must cover the current positions: recompute the box when particles moved
     double cell = std::max(span / 1000.0, 1e-30);
-    k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, E.bbox, cell, W.pk32);
+    count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, E.bbox, cell, W.pk32);
+    E.prof.begin(st);
     launch_forces32<int32_t>(nrows, W.rows_s, W.pk32, (float)cell, W.pk1, W.pk2, W.pk3, L.off,
                              L.idx, fp, L.perm, fo, st);
   } else {
-    k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, nullptr, W.pk0);
+    count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, nullptr, W.pk0);
+    E.prof.begin(st);
     launch_forces64<int32_t>(nrows, W.rows_s, W.pk0, W.pk1, W.pk2, W.pk3, L.off, L.idx, fp,
                              L.perm, fo, st);
   }
-  k_combine_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(
+  if (E.prof.on) {
+    E.prof.end(PROF_FORCES, st, (double)nrows, 0.0);
+    // interacting pairs of the rows (written per row by the kernel)
+    NB_TRY(sum_rows_i64(E, nrows, rows, W.pairs, st));
+    E.prof.pairs[PROF_FORCES] += (double)W.h_i64[0];
+  }
+  count_launch(), k_combine_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(
       nrows, rows, prm->viscosity, prm->disc_alpha_av, W.v_dacc, W.d_ddudt, W.d_cs, s->h,
       W.d_vsig, s->a_hydro, s->dudt, s->vsig_max, s->nu);
   NB_CUDA(cudaGetLastError());

@@ -63,8 +63,34 @@ struct Workspace {
   void release();
 };
 
+// Live timing of the main kernels with CUDA events on the launching stream (off by default).
+enum ProfCat { PROF_LISTS = 0, PROF_DENSITY = 1, PROF_FORCES = 2, PROF_FLOW = 3, PROF_NCAT = 4 };
+struct Prof {
+  bool on = false;
+  cudaEvent_t a = nullptr, b = nullptr;
+  double ms[PROF_NCAT] = {0};
+  int64_t launches[PROF_NCAT] = {0};
+  double units[PROF_NCAT] = {0};   // rows (density, forces, flow) or particles (lists)
+  double pairs[PROF_NCAT] = {0};   // list entries read (lists: entries written)
+  void begin(cudaStream_t st) {
+    if (on) cudaEventRecord(a, st);
+  }
+  void end(int cat, cudaStream_t st, double u, double pr) {
+    if (!on) return;
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    ms[cat] += t;
+    launches[cat] += 1;
+    units[cat] += u;
+    pairs[cat] += pr;
+  }
+};
+
 struct Engine {
   int device = 0;
+  Prof prof;
   int* d_err = nullptr;
   int* h_err = nullptr;  // pinned
   char last_error[512] = {0};

@@ -102,15 +102,15 @@ __global__ void k_sum_partials(int nb, int terms, const double* __restrict__ par
 void launch_glf(int64_t n, const double* x, const double* p, const double* dt, double dt_scalar,
                 double* xo, double* po, int64_t* iters, cudaStream_t st) {
   if (n > 0)
-    k_glf_many<<<grid_for(n, 128), 128, 0, st>>>(n, x, p, dt, dt_scalar, xo, po, iters);
+    count_launch(), k_glf_many<<<grid_for(n, 128), 128, 0, st>>>(n, x, p, dt, dt_scalar, xo, po, iters);
 }
 
 void launch_v_from_p(int64_t n, const double* x, const double* p, double* v, cudaStream_t st) {
-  if (n > 0) k_v_from_p<<<grid_for(n), NB_THREADS, 0, st>>>(n, x, p, v);
+  if (n > 0) count_launch(), k_v_from_p<<<grid_for(n), NB_THREADS, 0, st>>>(n, x, p, v);
 }
 
 void launch_p_from_v(int64_t n, const double* x, const double* v, double* p, cudaStream_t st) {
-  if (n > 0) k_p_from_v<<<grid_for(n), NB_THREADS, 0, st>>>(n, x, v, p);
+  if (n > 0) count_launch(), k_p_from_v<<<grid_for(n), NB_THREADS, 0, st>>>(n, x, v, p);
 }
 
 int ledger_blocks(int64_t n) { return (int)std::min<int64_t>(grid_for(n), 592); }
@@ -118,8 +118,8 @@ int ledger_blocks(int64_t n) { return (int)std::min<int64_t>(grid_for(n), 592); 
 void launch_ledger(int64_t n, const double* x, const double* p, const double* u, const double* m,
                    double* part, double* out, cudaStream_t st) {
   int nb = ledger_blocks(n);
-  k_ledger_partial<<<nb, NB_THREADS, 0, st>>>(n, x, p, u, m, part);
-  k_sum_partials<<<1, 32, 0, st>>>(nb, LEDGER_TERMS, part, out);
+  count_launch(), k_ledger_partial<<<nb, NB_THREADS, 0, st>>>(n, x, p, u, m, part);
+  count_launch(), k_sum_partials<<<1, 32, 0, st>>>(nb, LEDGER_TERMS, part, out);
 }
 
 }  // namespace nbk

@@ -274,15 +274,16 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
     return 0;
   }
   Lists& L = E.lists;
+  E.prof.begin(st);
   // bounding box and Morton keys
   int nbb = (int)std::min<int64_t>(grid_for(n), 1184);
-  k_bbox_partial<<<nbb, NB_THREADS, 0, st>>>(n, pos, E.bbox_part);
-  k_bbox_final<<<1, 32, 0, st>>>(nbb, E.bbox_part, E.bbox);
-  k_morton<<<grid_for(n), NB_THREADS, 0, st>>>(n, pos, E.bbox, E.keys_a, E.vals_a);
+  count_launch(), k_bbox_partial<<<nbb, NB_THREADS, 0, st>>>(n, pos, E.bbox_part);
+  count_launch(), k_bbox_final<<<1, 32, 0, st>>>(nbb, E.bbox_part, E.bbox);
+  count_launch(), k_morton<<<grid_for(n), NB_THREADS, 0, st>>>(n, pos, E.bbox, E.keys_a, E.vals_a);
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceRadixSort::SortPairs(E.cub_tmp, tmp, E.keys_a, E.keys_b, E.vals_a, L.perm,
                                           (int)n, 0, 63, st));
-  k_gather_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, pos, hs, L.spos, L.inv_perm);
+  count_launch(), k_gather_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, pos, hs, L.spos, L.inv_perm);
   // tree
   int64_t nleaf = (n + LEAF - 1) / LEAF;
   TreeView tv;
@@ -300,16 +301,16 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
   tv.nlevels = nl;
   if (tv.level_size[nl - 1] != 1) return set_host_error(E, "tree deeper than MAX_LEVELS");
   NB_TRY(E.ensure_nodes(offs));
-  k_leaf_boxes<<<grid_for(nleaf), NB_THREADS, 0, st>>>(n, nleaf, L.spos, E.node_lo, E.node_hi);
+  count_launch(), k_leaf_boxes<<<grid_for(nleaf), NB_THREADS, 0, st>>>(n, nleaf, L.spos, E.node_lo, E.node_hi);
   for (int l = 1; l < nl; ++l)
-    k_level_up<<<grid_for(tv.level_size[l]), NB_THREADS, 0, st>>>(
+    count_launch(), k_level_up<<<grid_for(tv.level_size[l]), NB_THREADS, 0, st>>>(
         tv.level_size[l - 1], tv.level_size[l], E.node_lo + tv.level_off[l - 1],
         E.node_hi + tv.level_off[l - 1], E.node_lo + tv.level_off[l], E.node_hi + tv.level_off[l]);
   tv.lo = E.node_lo;
   tv.hi = E.node_hi;
   // count, scan, fill
   unsigned gb = grid_for(nleaf * 32);
-  k_lists<0><<<gb, NB_THREADS, 0, st>>>(n, nleaf, tv, L.spos, E.counts, nullptr, nullptr, E.d_err);
+  count_launch(), k_lists<0><<<gb, NB_THREADS, 0, st>>>(n, nleaf, tv, L.spos, E.counts, nullptr, nullptr, E.d_err);
   NB_CUDA(cudaMemsetAsync(L.off, 0, sizeof(int64_t), st));
   tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, E.counts, L.off + 1, (int)n, st));
@@ -317,7 +318,8 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
   NB_CUDA(cudaMemcpyAsync(&total, L.off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   NB_CUDA(cudaStreamSynchronize(st));
   NB_TRY(E.ensure_list_capacity(total));
-  k_lists<1><<<gb, NB_THREADS, 0, st>>>(n, nleaf, tv, L.spos, nullptr, L.off, L.idx, E.d_err);
+  count_launch(), k_lists<1><<<gb, NB_THREADS, 0, st>>>(n, nleaf, tv, L.spos, nullptr, L.off, L.idx, E.d_err);
+  E.prof.end(PROF_LISTS, st, (double)n, (double)total);
   L.n = n;
   L.total = total;
   return check_device_error(E, st);
@@ -329,7 +331,7 @@ int export_lists_offsets(Engine& E, int64_t* off_out, cudaStream_t st) {
   int64_t n = L.n;
   NB_CUDA(cudaMemsetAsync(off_out, 0, sizeof(int64_t), st));
   if (n == 0) return 0;
-  k_export_counts<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.inv_perm, L.off, E.counts);
+  count_launch(), k_export_counts<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.inv_perm, L.off, E.counts);
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, E.counts, off_out + 1, (int)n, st));
   return check_device_error(E, st);
@@ -342,7 +344,7 @@ int export_lists(Engine& E, int64_t* off_out, int64_t* idx_out, cudaStream_t st)
   int64_t n = L.n;
   if (n == 0) return 0;
   size_t tmp = E.cub_bytes;
-  k_export_fill<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, L.off, L.idx, off_out, idx_out);
+  count_launch(), k_export_fill<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, L.off, L.idx, off_out, idx_out);
   if (L.total > 0) {
     NB_TRY(E.ensure_sort_keys(L.total));
     NB_CUDA(cudaMemcpyAsync(E.sort_keys, idx_out, sizeof(int64_t) * L.total,

@@ -38,13 +38,14 @@ template <typename I>
 void launch_density64(int64_t nrows, const int64_t* rows, const double4* pos, const double* mass,
                       const double* h_start, const double* h_search, const int64_t* off,
                       const I* idx, DensityParams prm, const int32_t* out_map, double* h_out,
-                      double* rho, double* omega, int64_t* iters, int64_t* flags, cudaStream_t st);
+                      double* rho, double* omega, int64_t* iters, int64_t* flags, int64_t* work,
+                      cudaStream_t st);
 template <typename I>
 void launch_density32(int64_t nrows, const int64_t* rows, const float4* pos, float cell,
                       const double* mass, const double* h_start, const double* h_search,
                       const int64_t* off, const I* idx, DensityParams prm, const int32_t* out_map,
                       double* h_out, double* rho, double* omega, int64_t* iters, int64_t* flags,
-                      cudaStream_t st);
+                      int64_t* work, cudaStream_t st);
 template <typename I>
 void launch_forces64(int64_t nrows, const int64_t* rows, const double4* pos, const double4* vm,
                      const double4* hydro, const double4* aux, const int64_t* off, const I* idx,

@@ -9,12 +9,12 @@ void launch_density32(int64_t nrows, const int64_t* rows, const float4* pos, flo
                       const double* mass, const double* h_start, const double* h_search,
                       const int64_t* off, const I* idx, DensityParams prm, const int32_t* out_map,
                       double* h_out, double* rho, double* omega, int64_t* iters, int64_t* flags,
-                      cudaStream_t st) {
+                      int64_t* work, cudaStream_t st) {
   if (nrows <= 0) return;
   Pos32 geo{pos, cell};
-  k_density<float, Pos32, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+  count_launch(), k_density<float, Pos32, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
       nrows, rows, geo, mass, h_start, h_search, off, idx, prm, out_map, h_out, rho, omega, iters,
-      flags);
+      flags, work);
 }
 
 template <typename I>
@@ -24,7 +24,7 @@ void launch_forces32(int64_t nrows, const int64_t* rows, const float4* pos, floa
                      ForceOut out, cudaStream_t st) {
   if (nrows <= 0) return;
   Pos32 geo{pos, cell};
-  k_forces<float, Pos32, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+  count_launch(), k_forces<float, Pos32, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
       nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
 }
 
@@ -33,7 +33,7 @@ template void launch_density32<int32_t>(int64_t, const int64_t*, const float4*, 
                                         const double*, const double*, const double*,
                                         const int64_t*, const int32_t*, DensityParams,
                                         const int32_t*, double*, double*, double*, int64_t*,
-                                        int64_t*, cudaStream_t);
+                                        int64_t*, int64_t*, cudaStream_t);
 template void launch_forces32<int32_t>(int64_t, const int64_t*, const float4*, float,
                                        const double4*, const double4*, const double4*,
                                        const int64_t*, const int32_t*, ForceParams,

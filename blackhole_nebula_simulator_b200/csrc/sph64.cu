@@ -8,12 +8,13 @@ template <typename I>
 void launch_density64(int64_t nrows, const int64_t* rows, const double4* pos, const double* mass,
                       const double* h_start, const double* h_search, const int64_t* off,
                       const I* idx, DensityParams prm, const int32_t* out_map, double* h_out,
-                      double* rho, double* omega, int64_t* iters, int64_t* flags, cudaStream_t st) {
+                      double* rho, double* omega, int64_t* iters, int64_t* flags, int64_t* work,
+                      cudaStream_t st) {
   if (nrows <= 0) return;
   Pos64 geo{pos};
-  k_density<double, Pos64, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+  count_launch(), k_density<double, Pos64, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
       nrows, rows, geo, mass, h_start, h_search, off, idx, prm, out_map, h_out, rho, omega, iters,
-      flags);
+      flags, work);
 }
 
 template <typename I>
@@ -22,18 +23,20 @@ void launch_forces64(int64_t nrows, const int64_t* rows, const double4* pos, con
                      ForceParams prm, const int32_t* out_map, ForceOut out, cudaStream_t st) {
   if (nrows <= 0) return;
   Pos64 geo{pos};
-  k_forces<double, Pos64, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+  count_launch(), k_forces<double, Pos64, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
       nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
 }
 
 template void launch_density64<int64_t>(int64_t, const int64_t*, const double4*, const double*,
                                         const double*, const double*, const int64_t*,
                                         const int64_t*, DensityParams, const int32_t*, double*,
-                                        double*, double*, int64_t*, int64_t*, cudaStream_t);
+                                        double*, double*, int64_t*, int64_t*, int64_t*,
+                                        cudaStream_t);
 template void launch_density64<int32_t>(int64_t, const int64_t*, const double4*, const double*,
                                         const double*, const double*, const int64_t*,
                                         const int32_t*, DensityParams, const int32_t*, double*,
-                                        double*, double*, int64_t*, int64_t*, cudaStream_t);
+                                        double*, double*, int64_t*, int64_t*, int64_t*,
+                                        cudaStream_t);
 template void launch_forces64<int64_t>(int64_t, const int64_t*, const double4*, const double4*,
                                        const double4*, const double4*, const int64_t*,
                                        const int64_t*, ForceParams, const int32_t*, ForceOut,
@@ -68,14 +71,14 @@ __global__ void k_pack_vm(int64_t n, const double* __restrict__ vel, const doubl
 
 
 void pack_pos(int64_t n, const double* pos, const double* w, double4* out, cudaStream_t st) {
-  if (n > 0) k_pack_pos<<<grid_for(n), NB_THREADS, 0, st>>>(n, pos, w, out);
+  if (n > 0) count_launch(), k_pack_pos<<<grid_for(n), NB_THREADS, 0, st>>>(n, pos, w, out);
 }
 void pack4(int64_t n, const double* a, const double* b, const double* c, const double* d,
            double4* out, cudaStream_t st) {
-  if (n > 0) k_pack4<<<grid_for(n), NB_THREADS, 0, st>>>(n, a, b, c, d, out);
+  if (n > 0) count_launch(), k_pack4<<<grid_for(n), NB_THREADS, 0, st>>>(n, a, b, c, d, out);
 }
 void pack_vm(int64_t n, const double* vel, const double* m, double4* out, cudaStream_t st) {
-  if (n > 0) k_pack_vm<<<grid_for(n), NB_THREADS, 0, st>>>(n, vel, m, out);
+  if (n > 0) count_launch(), k_pack_vm<<<grid_for(n), NB_THREADS, 0, st>>>(n, vel, m, out);
 }
 
 }  // namespace nbk

@@ -72,7 +72,7 @@ struct Acc<float> {
 template <typename R, typename PosT, typename I>
 __device__ void density_sums(const PosT& geo, int64_t i, const int64_t* off, const I* idx,
                              const double* mass, R r2max, R h, int kid, R cnorm, double& rs_out,
-                             double& dws_out) {
+                             double& dws_out, int64_t& work) {
   Acc<R> rs, dws;
   R inv_h = R(1) / h;
   R ih2 = inv_h * inv_h;
@@ -86,6 +86,7 @@ __device__ void density_sums(const PosT& geo, int64_t i, const int64_t* off, con
     if (!(d2 < r2max)) continue;
     R q = sqrt(d2) * inv_h;
     if (q < R(2)) {
+      work += 1;
       R fq = kernel_f<R>(q, kid);
       R m = (R)mass[j];
       rs.add(m * cnorm * ih3 * fq);
@@ -103,7 +104,7 @@ __global__ void __launch_bounds__(NB_THREADS)
               const double* __restrict__ h_search, const int64_t* __restrict__ off,
               const I* __restrict__ idx, DensityParams prm, const int32_t* __restrict__ out_map,
               double* __restrict__ h_out, double* __restrict__ rho, double* __restrict__ omega,
-              int64_t* __restrict__ iters, int64_t* __restrict__ flags) {
+              int64_t* __restrict__ iters, int64_t* __restrict__ flags, int64_t* __restrict__ work) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= nrows) return;
   int64_t i = rows ? rows[q] : q;
@@ -119,10 +120,11 @@ __global__ void __launch_bounds__(NB_THREADS)
   const double eta = prm.eta, e3 = eta * eta * eta;
   const int kid = prm.kid;
   const R cn = (R)prm.cnorm;
+  int64_t evals = 0;
   while (it < 50) {
     it += 1;
     double rs, dws;
-    density_sums<R>(geo, i, off, idx, mass, r2max, (R)h, kid, cn, rs, dws);
+    density_sums<R>(geo, i, off, idx, mass, r2max, (R)h, kid, cn, rs, dws, evals);
     double t = eta / h;
     double f = rs - m_i * (t * t * t);
     double h2 = h * h;
@@ -142,7 +144,7 @@ __global__ void __launch_bounds__(NB_THREADS)
   }
   if (h >= hs * (1 - 1e-3)) {
     double rs_lim, dummy;
-    density_sums<R>(geo, i, off, idx, mass, r2max, (R)hs, kid, cn, rs_lim, dummy);
+    density_sums<R>(geo, i, off, idx, mass, r2max, (R)hs, kid, cn, rs_lim, dummy, evals);
     double t = eta / hs;
     if (rs_lim - m_i * (t * t * t) < 0) {
       h = hs;
@@ -150,12 +152,13 @@ __global__ void __launch_bounds__(NB_THREADS)
     }
   }
   double rs, dws;
-  density_sums<R>(geo, i, off, idx, mass, r2max, (R)h, kid, cn, rs, dws);
+  density_sums<R>(geo, i, off, idx, mass, r2max, (R)h, kid, cn, rs, dws, evals);
   h_out[o] = h;
   rho[o] = rs;
   omega[o] = flag == 1 ? 1.0 : 1.0 + h / (3.0 * rs) * dws;
   if (iters) iters[o] = it;
   if (flags) flags[o] = flag;
+  if (work) work[o] = evals;
 }
 
 // ---------------------------------------------------------------- forces
@@ -245,14 +248,19 @@ __global__ void __launch_bounds__(NB_THREADS)
       work.add(m_b * vdotr * fa);
     }
     if (prm.use_disc) {
+      // the reference's disc kernel forms its terms in its own order (sim/sph.py:1097-1114)
       const double4 xb = aux[b];
-      R qa = -rho_a * h_a / (R(2) * r) * aav * cs_a * vdotr * inv_orr_a;
-      R qb = -rho_b * h_b / (R(2) * r) * aav * (R)xb.y * vdotr * inv_orr_b;
+      R ex = -ddx, ey = -ddy, ez = -ddz;  // x_a - x_b
+      R vdr = ((R)va.x - (R)vb.x) * ex / r;
+      vdr = vdr + ((R)va.y - (R)vb.y) * ey / r;
+      vdr = vdr + ((R)va.z - (R)vb.z) * ez / r;
+      R qa = -rho_a * h_a / (R(2) * r) * aav * cs_a * vdr * (R(1) / (om_a * rho_a * rho_a));
+      R qb = -rho_b * h_b / (R(2) * r) * aav * (R)xb.y * vdr / (om_b * rho_b * rho_b);
       R f = m_b * (qa * fa + qb * fb);
-      dax.add(-f * rx);
-      day.add(-f * ry);
-      daz.add(-f * rz);
-      dheat.add(m_b * qa * vdotr * fa);
+      dax.add(-(f * ex / r));
+      day.add(-(f * ey / r));
+      daz.add(-(f * ez / r));
+      dheat.add(m_b * qa * vdr * fa);
     }
   }
   if (prm.use_sph) {

@@ -51,11 +51,11 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
   Workspace& W = E.ws;
   int64_t n = s->n;
   NB_TRY(W.ensure(E, n));
-  k_any_nonpositive<<<grid_for(n), NB_THREADS, 0, st>>>(n, u, E.d_err);
+  count_launch(), k_any_nonpositive<<<grid_for(n), NB_THREADS, 0, st>>>(n, u, E.d_err);
   NB_TRY(check_device_error(E, st));
   // todo = every particle without a cache, else rows and their cached-list neighbours
   if (!W.cache.valid || W.cache.n != n || E.lists.n != n) {
-    k_fill_u8<<<grid_for(n), NB_THREADS, 0, st>>>(n, 1, W.m_need);
+    count_launch(), k_fill_u8<<<grid_for(n), NB_THREADS, 0, st>>>(n, 1, W.m_need);
   } else {
     NB_CUDA(cudaMemsetAsync(W.m_need, 0, n, st));
     mark_rows(E, nrows, rows, 0, s->x, s->h, W.m_need, st);
@@ -87,7 +87,7 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
     }
   }
   if (prm->viscosity)
-    k_set_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, prm->alpha_const, s->alpha);
+    count_launch(), k_set_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, prm->alpha_const, s->alpha);
   return engine_forces(E, s, vel, u, nrows, rows, prm, st);
 }
 
@@ -173,7 +173,7 @@ int coupled_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_
   int64_t n = s->n;
   NB_TRY(W.ensure(E, n));
   W.cache.valid = false;
-  k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
+  count_launch(), k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
   launch_v_from_p(n, s->x, s->p, W.v_eval, st);
   NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st));
   return 0;
@@ -186,12 +186,14 @@ int coupled_step(Engine& E, nb_state* s, const nb_params* prm, double dt, cudaSt
   double half = 0.5 * dt;
   // p_half, u_half; gravity flow over dt
   double* u_half = W.d_uh;
-  k_kick_half<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->p, s->a_hydro, s->u, s->dudt, half,
+  count_launch(), k_kick_half<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->p, s->a_hydro, s->u, s->dudt, half,
                                                   W.v_tmp, u_half);
+  E.prof.begin(st);
   launch_glf(n, s->x, W.v_tmp, nullptr, dt, W.v_pred, W.v_flow, W.iters, st);
+  E.prof.end(PROF_FLOW, st, (double)n, 0.0);
   NB_TRY(glf_status(E, n, W.iters, st));
   if (prm->cooling == 1 || prm->cooling == 2) {
-    k_cool_shared<<<grid_for(n), NB_THREADS, 0, st>>>(n, prm->cooling, s->x, W.v_pred, s->rho,
+    count_launch(), k_cool_shared<<<grid_for(n), NB_THREADS, 0, st>>>(n, prm->cooling, s->x, W.v_pred, s->rho,
                                                       s->mass, dt, prm->cooling_beta,
                                                       prm->u_floor, brems_of(prm), u_half, W.d_dm);
     double de = 0;
@@ -200,13 +202,13 @@ int coupled_step(Engine& E, nb_state* s, const nb_params* prm, double dt, cudaSt
   }
   // predicted state: x1, p_flow, u_half + dt/2 dudt; predictor momentum for velocities
   NB_CUDA(cudaMemcpyAsync(s->x, W.v_pred, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, st));
-  k_pred_shared<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.v_flow, s->a_hydro, u_half, s->dudt,
+  count_launch(), k_pred_shared<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.v_flow, s->a_hydro, u_half, s->dudt,
                                                     half, W.v_tmp, s->u);
   launch_v_from_p(n, s->x, W.v_tmp, W.v_eval, st);
-  k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
+  count_launch(), k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
   NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st));
   // closing kick with the new forces
-  k_pred_shared<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.v_flow, s->a_hydro, u_half, s->dudt,
+  count_launch(), k_pred_shared<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.v_flow, s->a_hydro, u_half, s->dudt,
                                                     half, s->p, s->u);
   s->particle_steps += n;
   s->last_active = n;
@@ -235,7 +237,7 @@ int coupled_stable_dt(Engine& E, nb_state* s, const nb_params* prm, double* dt, 
   Workspace& W = E.ws;
   int64_t n = s->n;
   NB_TRY(W.ensure(E, n));
-  k_stable_dt<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->h, s->vsig_max, s->a_hydro,
+  count_launch(), k_stable_dt<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->h, s->vsig_max, s->a_hydro,
                                                   prm->disc_alpha_av > 0 ? s->nu : nullptr, s->x,
                                                   prm->courant, prm->c_force, prm->eta_orb, W.d_b);
   size_t tmp = E.cub_bytes;
@@ -487,7 +489,7 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
   Lists& L = E.lists;
   int64_t n = s->n;
   if (nrows == 0) return 0;
-  k_wanted_levels<<<grid_for(nrows), NB_THREADS, 0, st>>>(
+  count_launch(), k_wanted_levels<<<grid_for(nrows), NB_THREADS, 0, st>>>(
       nrows, rows, s->tick_n, prm->dt_max, s->h, s->vsig_max, s->a_hydro,
       prm->disc_alpha_av > 0 ? s->nu : nullptr, s->x, prm->courant, prm->c_force, prm->eta_orb,
       s->level_offset, s->level, E.d_err);
@@ -496,7 +498,7 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
     bool settled = false;
     for (int sweep = 0; sweep < 4096; ++sweep) {
       NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
-      k_limit_sweep<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.perm, L.inv_perm, L.off,
+      count_launch(), k_limit_sweep<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.perm, L.inv_perm, L.off,
                                                             L.idx, s->x, s->h, prm->max_gap,
                                                             s->level, W.d_int);
       NB_CUDA(cudaMemcpyAsync(W.h_int, W.d_int, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -508,22 +510,22 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
     }
     if (!settled) return set_host_error(E, "level limiter did not settle");
   }
-  k_land<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, s->tick_n, s->n_stop, s->level, E.d_err);
+  count_launch(), k_land<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, s->tick_n, s->n_stop, s->level, E.d_err);
   NB_TRY(check_device_error(E, st));
   if (prm->limiter) {
-    k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, -1, W.need);
-    k_wake_need<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.perm, L.inv_perm, L.off,
+    count_launch(), k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, -1, W.need);
+    count_launch(), k_wake_need<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.perm, L.inv_perm, L.off,
                                                         L.idx, s->x, s->h, s->level, prm->max_gap,
                                                         W.need);
     NB_CUDA(cudaMemsetAsync(W.d_i64, 0, sizeof(int64_t), st));
-    k_cut_steps<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->tick_n, s->tick, W.need, s->a_hydro,
+    count_launch(), k_cut_steps<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->tick_n, s->tick, W.need, s->a_hydro,
                                                     s->dudt, s->level, s->n_end, s->p_half,
                                                     s->u_half, (unsigned long long*)W.d_i64);
     NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     NB_CUDA(cudaStreamSynchronize(st));
     s->woken += W.h_i64[0];
   }
-  k_open<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, s->tick_n, s->tick, s->level, s->x,
+  count_launch(), k_open<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, s->tick_n, s->tick, s->level, s->x,
                                                  s->p, s->u, s->a_hydro, s->dudt, s->n_beg,
                                                  s->n_end, s->x_beg, s->p_half, s->u_half);
   NB_CUDA(cudaGetLastError());
@@ -537,10 +539,10 @@ int block_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t 
   int64_t n = s->n;
   NB_TRY(W.ensure(E, n));
   W.cache.valid = false;
-  k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
+  count_launch(), k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
   launch_v_from_p(n, s->x, s->p, W.v_eval, st);
   NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st));
-  k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, 0, s->level);
+  count_launch(), k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, 0, s->level);
   return choose_levels_and_open(E, s, prm, n, W.rows, st);
 }
 
@@ -557,13 +559,15 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   NB_CUDA(cudaStreamSynchronize(st));
   int64_t n_next = W.h_i64[0];
   // flow of every particle from its step start; predictor momenta; active flags
-  k_block_flow<<<grid_for(n, 128), 128, 0, st>>>(n, n_next, s->tick, s->x_beg, s->p_half, s->n_beg,
+  E.prof.begin(st);
+  count_launch(), k_block_flow<<<grid_for(n, 128), 128, 0, st>>>(n, n_next, s->tick, s->x_beg, s->p_half, s->n_beg,
                                                  s->n_end, s->a_hydro, s->x, W.v_flow, W.v_pred,
                                                  W.iters, W.m_rows);
+  E.prof.end(PROF_FLOW, st, (double)n, 0.0);
   NB_TRY(glf_status(E, n, W.iters, st));
   int64_t nrows = 0;
   NB_TRY(select_mask(E, n, W.m_rows, W.rows, &nrows, st));
-  k_block_cool<<<grid_for(n), NB_THREADS, 0, st>>>(
+  count_launch(), k_block_cool<<<grid_for(n), NB_THREADS, 0, st>>>(
       n, prm->cooling == 1 ? 1 : (prm->cooling >= 2 ? 2 : 0), n_next, s->tick, s->n_beg,
       s->n_end, s->x_beg, s->x, s->rho, s->mass, s->dudt, prm->cooling_beta, prm->u_floor,
       brems_of(prm), s->u_half, s->u, s->luminosity, W.d_dm);
@@ -575,7 +579,7 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   s->tick_n = n_next;
   launch_v_from_p(n, s->x, W.v_pred, W.v_eval, st);
   NB_TRY(hydro_rows(E, s, prm, nrows, W.rows, W.v_eval, s->u, st));
-  k_block_close<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, W.rows, s->tick, s->n_beg, s->n_end,
+  count_launch(), k_block_close<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, W.rows, s->tick, s->n_beg, s->n_end,
                                                        W.v_flow, s->a_hydro, s->u_half, s->dudt,
                                                        W.v_pred, s->u);
   NB_CUDA(cudaMemcpyAsync(s->p, W.v_pred, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, st));
@@ -621,13 +625,13 @@ int block_land(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st) {
   Workspace& W = E.ws;
   int64_t n = s->n;
   NB_TRY(W.ensure(E, n));
-  k_fresh<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->tick_n, s->n_stop, s->n_beg, s->n_end, W.m_tmp);
+  count_launch(), k_fresh<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->tick_n, s->n_stop, s->n_beg, s->n_end, W.m_tmp);
   int64_t nf = 0;
   NB_TRY(select_mask(E, n, W.m_tmp, W.rows2, &nf, st));
   if (nf == 0) return 0;
-  k_land<<<grid_for(nf), NB_THREADS, 0, st>>>(nf, W.rows2, s->tick_n, s->n_stop, s->level, E.d_err);
+  count_launch(), k_land<<<grid_for(nf), NB_THREADS, 0, st>>>(nf, W.rows2, s->tick_n, s->n_stop, s->level, E.d_err);
   NB_TRY(check_device_error(E, st));
-  k_open_only<<<grid_for(nf), NB_THREADS, 0, st>>>(nf, W.rows2, s->tick_n, s->tick, s->level, s->x,
+  count_launch(), k_open_only<<<grid_for(nf), NB_THREADS, 0, st>>>(nf, W.rows2, s->tick_n, s->tick, s->level, s->x,
                                                    s->p, s->u, s->a_hydro, s->dudt, s->n_beg,
                                                    s->n_end, s->x_beg, s->p_half, s->u_half);
   NB_CUDA(cudaGetLastError());

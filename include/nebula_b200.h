@@ -80,6 +80,8 @@ NB_API nb_ctx* nb_create(int device);
 NB_API void nb_destroy(nb_ctx* ctx);
 NB_API const char* nb_last_error(nb_ctx* ctx);
 NB_API int nb_version(void);
+/* Number of this library's own kernels launched so far by this process (all contexts). */
+NB_API int64_t nb_launch_count(void);
 
 /* ---------------------------------------------------------------- operators
  * One-for-one replacements of the reference's inner functions (sim/neighbours.py, sim/sph.py,
@@ -156,6 +158,12 @@ NB_API int nb_block_advance(nb_ctx* ctx, nb_state* st, const nb_params* prm, int
                      void* stream);
 /* Re-open the steps just opened so they land on n_stop (sim/blocks.py:722-734, run's prologue). */
 NB_API int nb_block_land(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* stream);
+
+/* Live kernel timing with CUDA events on the launching stream: nb_profile(ctx, 1) resets and
+ * starts, nb_profile_read fills out[16] = for each of {list build, density, forces, gravity
+ * flow}: (milliseconds, launches, rows or particles processed, pair evaluations). */
+NB_API int nb_profile(nb_ctx* ctx, int on);
+NB_API int nb_profile_read(nb_ctx* ctx, double* out);
 
 /* Drop the cached neighbour lists (the next density call rebuilds them). */
 NB_API int nb_reset_cache(nb_ctx* ctx);
