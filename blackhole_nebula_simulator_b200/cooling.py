@@ -62,11 +62,13 @@ def brems_cool(u, rho, dt, consts: BremsConstants) -> torch.Tensor:
     prm.u_floor, prm.brems_t_floor = consts.u_floor, consts.t_floor
     out = torch.empty_like(u)
     c = ctx()
+    rho_t = dev_f64(rho, (n,))
     if isinstance(dt, (int, float)):
-        st = _lib.lib().nb_brems_cool(c, n, ptr(u), ptr(dev_f64(rho, (n,))), None, float(dt),
-                                      prm, ptr(out), stream())  # fmt: skip
+        st = _lib.lib().nb_brems_cool(c, n, ptr(u), ptr(rho_t), None, float(dt), prm, ptr(out),
+                                      stream())  # fmt: skip
     else:
-        st = _lib.lib().nb_brems_cool(c, n, ptr(u), ptr(dev_f64(rho, (n,))),
-                                      ptr(dev_f64(dt, (n,))), 0.0, prm, ptr(out), stream())
+        dt_t = dev_f64(dt, (n,))
+        st = _lib.lib().nb_brems_cool(c, n, ptr(u), ptr(rho_t), ptr(dt_t), 0.0, prm, ptr(out),
+                                      stream())  # fmt: skip
     _lib.check(c, st)
     return out

@@ -213,7 +213,10 @@ __global__ void __launch_bounds__(NB_THREADS)
     R rx = -ddx / r, ry = -ddy / r, rz = -ddz / r;  // r_hat of x_a - x_b
     R fa = dwdr<R>(r, h_a, kid, cn);
     R fb = dwdr<R>(r, h_b, kid, cn);
-    R vdotr = ((R)va.x - (R)vb.x) * rx + ((R)va.y - (R)vb.y) * ry + ((R)va.z - (R)vb.z) * rz;
+    // velocity differences are formed in double before rounding, so a large common (orbital)
+    // velocity costs the FP32 path no precision
+    const R dvx = (R)(va.x - vb.x), dvy = (R)(va.y - vb.y), dvz = (R)(va.z - vb.z);
+    R vdotr = dvx * rx + dvy * ry + dvz * rz;
     R num_a = P_a, num_b = P_b;
     R inv_orr_b = R(1) / (om_b * rho_b * rho_b);
     if (prm.use_sph) {
@@ -235,7 +238,7 @@ __global__ void __launch_bounds__(NB_THREADS)
             vu = sqrt(fabs(P_a - P_b) / (R(0.5) * (rho_a + rho_b)));
           else
             vu = fabs(vdotr);
-          R dc = m_b * alpha_u * vu * (u_a - (R)xb.x) * R(0.5) *
+          R dc = m_b * alpha_u * vu * (R)(xa.x - xb.x) * R(0.5) *
                  (fa * inv_or_a + fb / (om_b * rho_b));
           heat.add(dc);
           cheat.add(dc);
@@ -251,9 +254,9 @@ __global__ void __launch_bounds__(NB_THREADS)
       // the reference's disc kernel forms its terms in its own order (sim/sph.py:1097-1114)
       const double4 xb = aux[b];
       R ex = -ddx, ey = -ddy, ez = -ddz;  // x_a - x_b
-      R vdr = ((R)va.x - (R)vb.x) * ex / r;
-      vdr = vdr + ((R)va.y - (R)vb.y) * ey / r;
-      vdr = vdr + ((R)va.z - (R)vb.z) * ez / r;
+      R vdr = dvx * ex / r;
+      vdr = vdr + dvy * ey / r;
+      vdr = vdr + dvz * ez / r;
       R qa = -rho_a * h_a / (R(2) * r) * aav * cs_a * vdr * (R(1) / (om_a * rho_a * rho_a));
       R qb = -rho_b * h_b / (R(2) * r) * aav * (R)xb.y * vdr / (om_b * rho_b * rho_b);
       R f = m_b * (qa * fa + qb * fb);

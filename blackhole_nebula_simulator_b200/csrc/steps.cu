@@ -42,6 +42,16 @@ __global__ void k_iota(int64_t n, int64_t* __restrict__ out) {
   if (i < n) out[i] = i;
 }
 
+static BremsParams brems_of(const nb_params* prm) {
+  BremsParams b;
+  b.tfac = prm->brems_tfac;
+  b.b = prm->brems_b;
+  b.kappa = prm->brems_kappa;
+  b.u_floor = prm->u_floor;
+  b.t_floor = prm->brems_t_floor;
+  return b;
+}
+
 // ---------------------------------------------------------------- hydro of the active rows
 // sim/blocks.py:217-239 (_density_touched) and 242-315 (_hydro_rows): density for the rows and
 // every neighbour in the cached lists, widened until every interacting neighbour is fresh; then
@@ -131,15 +141,6 @@ __global__ void k_pred_shared(int64_t n, const double* __restrict__ p_flow,
   u_pred[i] = u_half[i] + half * dudt[i];
 }
 
-static BremsParams brems_of(const nb_params* prm) {
-  BremsParams b;
-  b.tfac = prm->brems_tfac;
-  b.b = prm->brems_b;
-  b.kappa = prm->brems_kappa;
-  b.u_floor = prm->u_floor;
-  b.t_floor = prm->brems_t_floor;
-  return b;
-}
 
 static int glf_status(Engine& E, int64_t n, const int64_t* iters, cudaStream_t st) {
   size_t tmp = E.cub_bytes;
@@ -218,10 +219,21 @@ int coupled_step(Engine& E, nb_state* s, const nb_params* prm, double dt, cudaSt
 
 // sim/coupled.py:213-226: min over particles of C_cour h / v_sig, C_force sqrt(h / |a|),
 // viscous 0.25 h^2 / nu and eta_orb r^(3/2).
+// Bremsstrahlung time-step limit (this project's criterion; the reference's beta-cooling is
+// exact at any step): C_cool u / |du/dt| for gas above the floor temperature, else inf.
+constexpr double C_COOL = 0.25;
+__device__ __forceinline__ double cooling_dt(int law, double u, double rho, const BremsParams& bp) {
+  if (law != 2 || !(bp.tfac * u > bp.t_floor)) return INFINITY;
+  double rate = fabs(brems_rate(u, rho, bp));
+  return rate > 0 ? C_COOL * u / rate : INFINITY;
+}
+
 __global__ void k_stable_dt(int64_t n, const double* __restrict__ h, const double* __restrict__ vsig,
                             const double* __restrict__ a, const double* __restrict__ nu,
                             const double* __restrict__ x, double courant, double c_force,
-                            double eta_orb, double* __restrict__ out) {
+                            double eta_orb, int law, const double* __restrict__ u,
+                            const double* __restrict__ rho, BremsParams bp,
+                            double* __restrict__ out) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   double dt = courant * (h[i] / vsig[i]);
@@ -230,7 +242,7 @@ __global__ void k_stable_dt(int64_t n, const double* __restrict__ h, const doubl
   if (nu && nu[i] > 0) dt = fmin(dt, 0.25 * h[i] * h[i] / nu[i]);
   double r = norm3(x + 3 * i);
   dt = fmin(dt, eta_orb * pow(r, 1.5));
-  out[i] = dt;
+  out[i] = fmin(dt, cooling_dt(law, u[i], rho[i], bp));
 }
 
 int coupled_stable_dt(Engine& E, nb_state* s, const nb_params* prm, double* dt, cudaStream_t st) {
@@ -239,7 +251,8 @@ int coupled_stable_dt(Engine& E, nb_state* s, const nb_params* prm, double* dt, 
   NB_TRY(W.ensure(E, n));
   count_launch(), k_stable_dt<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->h, s->vsig_max, s->a_hydro,
                                                   prm->disc_alpha_av > 0 ? s->nu : nullptr, s->x,
-                                                  prm->courant, prm->c_force, prm->eta_orb, W.d_b);
+                                                  prm->courant, prm->c_force, prm->eta_orb,
+                                                  prm->cooling, s->u, s->rho, brems_of(prm), W.d_b);
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceReduce::Min(E.cub_tmp, tmp, W.d_b, W.d_tmp, (int)n, st));
   NB_CUDA(cudaMemcpyAsync(W.h_dbl, W.d_tmp, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -328,9 +341,10 @@ __global__ void k_wanted_levels(int64_t nrows, const int64_t* __restrict__ rows,
                                 double dt_max, const double* __restrict__ h,
                                 const double* __restrict__ vsig, const double* __restrict__ a,
                                 const double* __restrict__ nu, const double* __restrict__ x,
-                                double courant, double c_force, double eta_orb,
-                                const int64_t* __restrict__ offset, int64_t* __restrict__ level,
-                                int* err) {
+                                double courant, double c_force, double eta_orb, int law,
+                                const double* __restrict__ u, const double* __restrict__ rho,
+                                BremsParams bp, const int64_t* __restrict__ offset,
+                                int64_t* __restrict__ level, int* err) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= nrows) return;
   int64_t i = rows[q];
@@ -340,6 +354,7 @@ __global__ void k_wanted_levels(int64_t nrows, const int64_t* __restrict__ rows,
   if (amag > 0) dt = fmin(dt, c_force * sqrt(hi / amag));
   if (nu && nu[i] > 0) dt = fmin(dt, 0.25 * (hi * hi) / nu[i]);
   dt = fmin(dt, eta_orb * pow(norm3(x + 3 * i), 1.5));
+  dt = fmin(dt, cooling_dt(law, u[i], rho[i], bp));
   if (!(dt > 0)) {
     set_error(err, ERR_DT);
     return;
@@ -492,7 +507,7 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
   count_launch(), k_wanted_levels<<<grid_for(nrows), NB_THREADS, 0, st>>>(
       nrows, rows, s->tick_n, prm->dt_max, s->h, s->vsig_max, s->a_hydro,
       prm->disc_alpha_av > 0 ? s->nu : nullptr, s->x, prm->courant, prm->c_force, prm->eta_orb,
-      s->level_offset, s->level, E.d_err);
+      prm->cooling, s->u, s->rho, brems_of(prm), s->level_offset, s->level, E.d_err);
   NB_TRY(check_device_error(E, st));
   if (prm->limiter) {
     bool settled = false;

@@ -118,7 +118,7 @@ def gn_circular_speed(r):
 
 
 def torus(n: int = 4_194_304, r_major: float = 100.0, a_minor: float = 40.0,
-          sigma: float = 15.0, total_mass: float = 1.0, t_kelvin: float = 1.0e9,
+          sigma: float = 15.0, total_mass: float = 0.01, t_kelvin: float = 1.0e9,
           noise: float = 0.01, kernel: str = "cubic", seed: int = 4) -> InitialConditions:  # fmt: skip
     """Torus about the z axis (major radius r_major, minor radius a_minor) with a Gaussian density
     profile exp(-s^2 / 2 sigma^2) in the minor radius s, random seeded positions, circular GN

@@ -155,10 +155,11 @@ def disc_forces_numba(pos, vel, mass, h, rho, omega, c_s, alpha_av, nb: Neighbou
     acc = torch.empty((m, 3), dtype=torch.float64, device=pos.device)
     dudt = torch.empty(m, dtype=torch.float64, device=pos.device)
     off, idx = dev_i64(nb.offset), dev_i64(nb.index)
-    _call("nb_disc_forces", n, ptr(pos), ptr(dev_f64(vel)), ptr(dev_f64(mass, (n,))),
-          ptr(dev_f64(h)), ptr(dev_f64(rho)), ptr(dev_f64(omega)), ptr(dev_f64(c_s)),
-          float(alpha_av), ptr(off), ptr(idx), m, ptr(rows_t), KERNEL_IDS[kernel_name], ptr(acc),
-          ptr(dudt), stream())  # fmt: skip
+    # every converted input stays referenced until the call returns
+    ins = [dev_f64(vel), dev_f64(mass, (n,)), dev_f64(h), dev_f64(rho), dev_f64(omega),
+           dev_f64(c_s)]  # fmt: skip
+    _call("nb_disc_forces", n, ptr(pos), *[ptr(a) for a in ins], float(alpha_av), ptr(off),
+          ptr(idx), m, ptr(rows_t), KERNEL_IDS[kernel_name], ptr(acc), ptr(dudt), stream())
     return acc, dudt
 
 
@@ -170,9 +171,10 @@ def glf_step_many(x, p, dt):
     n = len(x)
     x1, p1 = torch.empty_like(x), torch.empty_like(p)
     it = torch.empty(n, dtype=torch.int64, device=x.device)
-    if isinstance(dt, (int, float)):
+    if isinstance(dt, (int, float)) or (hasattr(dt, "ndim") and dt.ndim == 0):
         _call("nb_glf_step_many", n, ptr(x), ptr(p), None, float(dt), ptr(x1), ptr(p1), ptr(it),
               stream())  # fmt: skip
+        return x1, p1, it
     else:
         dtt = dev_f64(dt, (n,))
         _call("nb_glf_step_many", n, ptr(x), ptr(p), ptr(dtt), 0.0, ptr(x1), ptr(p1), ptr(it),
@@ -183,16 +185,18 @@ def glf_step_many(x, p, dt):
 def gn_v_from_p(x, p):
     """sim/fastphys.py:35-42: v = A p + C (p.x) x."""
     x = dev_f64(x)
+    p = dev_f64(p)
     v = torch.empty_like(x)
-    _call("nb_gn_v_from_p", len(x), ptr(x), ptr(dev_f64(p)), ptr(v), stream())
+    _call("nb_gn_v_from_p", len(x), ptr(x), ptr(p), ptr(v), stream())
     return v
 
 
 def gn_p_from_v(x, v):
     """physics/gravity.py:66-77: p = f v + g rdot x/r."""
     x = dev_f64(x)
+    v = dev_f64(v)
     p = torch.empty_like(x)
-    _call("nb_gn_p_from_v", len(x), ptr(x), ptr(dev_f64(v)), ptr(p), stream())
+    _call("nb_gn_p_from_v", len(x), ptr(x), ptr(v), ptr(p), stream())
     return p
 
 
@@ -201,17 +205,16 @@ def beta_cool(u, u_floor, dt, t_cool):
     u = dev_f64(u)
     n = len(u)
     out = torch.empty_like(u)
-    _call("nb_beta_cool", n, ptr(u), ptr(dev_f64(u_floor, (n,))), ptr(dev_f64(dt, (n,))),
-          ptr(dev_f64(t_cool, (n,))), ptr(out), stream())  # fmt: skip
+    uf, dtt, tc = dev_f64(u_floor, (n,)), dev_f64(dt, (n,)), dev_f64(t_cool, (n,))
+    _call("nb_beta_cool", n, ptr(u), ptr(uf), ptr(dtt), ptr(tc), ptr(out), stream())
     return out
 
 
 def ledger_sums(x, p, u, mass) -> dict:
     """sim/coupled.py:261-270 sums on the device: energy sum m (H + u) (without radiated energy),
     sum m |H|, angular momentum, momentum, mass."""
-    x = dev_f64(x)
+    x, p, u, mass = dev_f64(x), dev_f64(p), dev_f64(u), dev_f64(mass)
     out = (ctypes.c_double * 9)()
-    _call("nb_ledger", len(x), ptr(x), ptr(dev_f64(p)), ptr(dev_f64(u)), ptr(dev_f64(mass)), out,
-          stream())  # fmt: skip
+    _call("nb_ledger", len(x), ptr(x), ptr(p), ptr(u), ptr(mass), out, stream())
     v = list(out)
     return {"energy": v[0], "abs_h": v[1], "angmom": v[2:5], "momentum": v[5:8], "mass": v[8]}

@@ -25,6 +25,7 @@ from .sph import C_NORM, KERNEL_IDS, compute_density
 
 K_MAX = 40
 C_VISC = 0.25
+C_COOL = 0.25  # bremsstrahlung time-step factor: dt <= C_COOL u / |du/dt_cool| (own criterion)
 
 
 # --------------------------------------------------------------------------- GN helpers
@@ -157,7 +158,7 @@ def coupled_stable_dt(st: GasState, cc) -> float:
             dt = min(dt, float(np.min(np.where(st.nu > 0, C_VISC * st.h**2 / st.nu, np.inf))))
     r = np.linalg.norm(st.x, axis=1)
     dt = min(dt, cc.eta_orb * np.min(r**1.5))
-    return float(dt)
+    return float(min(dt, float(np.min(cooling_dt(cc, st.u, st.rho)))))
 
 
 def coupled_step(st: GasState, cc, dt: float, reuse=True) -> GasState:
@@ -315,7 +316,19 @@ def wanted_dt(st: BlockState, bc, rows):
         nu = st.nu[rows]
         dt = np.minimum(dt, np.where(nu > 0, C_VISC * h**2 / nu, np.inf))
     dt = np.minimum(dt, cc.eta_orb * np.linalg.norm(st.x[rows], axis=1) ** 1.5)
-    return dt
+    return np.minimum(dt, cooling_dt(cc, st.u[rows], st.rho[rows]))
+
+
+def cooling_dt(cc, u, rho):
+    """Bremsstrahlung time-step limit C_COOL u / |du/dt| for gas above the floor (inf elsewhere;
+    beta-cooling is exact at any step and needs none, as in the reference)."""
+    if cc.cooling != "brems":
+        return np.full(len(u), np.inf)
+    consts = ocool.brems_constants(cc.hydro.gamma, t_floor=cc.t_floor)
+    rate = np.abs(ocool.brems_rate(u, rho, consts))
+    hot = (consts[0] * u > consts[4]) & (rate > 0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.where(hot, C_COOL * u / rate, np.inf)
 
 
 def _land(st: BlockState, k):
