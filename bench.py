@@ -91,7 +91,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)  # fmt: skip
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -185,6 +185,7 @@ def run_gpu(args, rank, world):
         blocks.advance(st, bc)
     c = ctx(dev)
     stream = torch.cuda.current_stream()
+    snap = snapshot_state(st)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -213,41 +214,62 @@ def run_gpu(args, rank, world):
     else:
         total = float(psteps)
     led = blocks.ledger(st, bc)
-    e2e = run_e2e(args, st, bc, dev)
+    e2e = run_e2e(args, st, bc, snap)
     return ms, total, prof, clk.summary(), st, led, e2e
 
 
-def run_e2e(args, st, bc, dev):
-    """Same metric through the public API with host state: every step copies the block state in
-    from pinned host memory and reads the updated state back."""
+def _tensor_fields(st):
+    import torch
+
+    return [k for k, v in st.__dict__.items() if isinstance(v, torch.Tensor) and k != "_rows"]
+
+
+def snapshot_state(st):
+    """Pinned host copy of the block state and its host-side counters (before the timed steps)."""
+    import copy
+
+    host = {k: getattr(st, k).detach().to("cpu").pin_memory() for k in _tensor_fields(st)}
+    scal = {k: copy.copy(v) for k, v in st.__dict__.items() if k not in host and k != "_rows"
+            and not k.startswith("_")}  # fmt: skip
+    return host, scal
+
+
+def run_e2e(args, st, bc, snap):
+    """The same K system steps again, through the public API with the state in host memory:
+    each step copies the whole block state in from pinned host memory and the updated state back
+    out, timed with CUDA events around copies and steps."""
     import torch
 
     from blackhole_nebula_simulator_b200 import blocks
 
-    names = [k for k, v in st.__dict__.items() if isinstance(v, torch.Tensor) and k != "_rows"]
-    host = {k: torch.empty_like(getattr(st, k), device="cpu").pin_memory() for k in names}
-    for k in names:
-        host[k].copy_(getattr(st, k))
-    back = ("x", "p", "u", "h", "level", "n_end")
-    h2d = sum(host[k].numel() * host[k].element_size() for k in names)
-    d2h = sum(host[k].numel() * host[k].element_size() for k in back)
-    steps = max(1, min(args.steps, 3))
+    host, scal = snap
+    for k, v in scal.items():
+        setattr(st, k, v)
+    names = list(host)
+    nbytes = sum(host[k].numel() * host[k].element_size() for k in names)
     stream = torch.cuda.current_stream()
     torch.cuda.synchronize()
     s0 = st.particle_steps
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(steps):
+    for _ in range(args.steps):
         for k in names:
             getattr(st, k).copy_(host[k], non_blocking=True)
         blocks.advance(st, bc)
-        for k in back:
+        for k in names:
             host[k].copy_(getattr(st, k), non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     return {"value": (st.particle_steps - s0) / (ms * 1e-3), "unit": "particle-steps/s",
-            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": steps}  # fmt: skip
+            "h2d_bytes_per_step": int(nbytes), "d2h_bytes_per_step": int(nbytes),
+            "steps": args.steps, "ms_per_step": ms / args.steps}  # fmt: skip
+
+
+def h_stats(st):
+    h = st.h.detach().cpu().numpy()
+    q = np.percentile(h, [0, 50, 99, 100])
+    return {"min": float(q[0]), "median": float(q[1]), "p99": float(q[2]), "max": float(q[3])}
 
 
 def cpu_reference(args, steps, warmup, sample_n=None):
@@ -257,7 +279,7 @@ def cpu_reference(args, steps, warmup, sample_n=None):
     from oracle import steps as osteps
 
     n_full = {"torus": 4_194_304, "streams": 1_048_576, "cloud": 262_144}[args.workload]
-    n = sample_n or min(args.n or n_full, 131_072)
+    n = sample_n or min(args.n or n_full, 32_768)
     ic, bc = workload(args.workload, n, "fp64")
     st = osteps.blocks_initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=1e12)
     for _ in range(warmup):
@@ -321,6 +343,11 @@ def main():
             "gpu_launches": launches, "kernel_ms": {k: round(v["ms"], 3) for k, v in prof.items()},
             "mean_active": total / args.steps / max(world, 1),
             "list_builds": st.builds, "list_reuses": st.reuses,
+            "mean_list_entries": (prof["lists"]["pairs"] / prof["lists"]["units"]
+                                  if prof["lists"]["units"] else None),
+            "pairs_per_force_row": (prof["forces"]["pairs"] / prof["forces"]["units"]
+                                    if prof["forces"]["units"] else None),
+            "h_stats": h_stats(st),
             "energy_rel_drift": None,
         }  # fmt: skip
         if not args.no_cpu_baseline:

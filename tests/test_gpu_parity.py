@@ -149,8 +149,9 @@ def test_cooling_laws(nb):
     from oracle import cooling as ocool
 
     g = golden("cooling.npz")
+    # exp() of CUDA and of the host C library may differ by an ulp: a few ulps of tolerance
     check("beta_cool", g["u_new"], _np(ops.beta_cool(g["u"], g["u_floor"], g["dt"], g["t_cool"])),
-          rtol=1e-15)  # fmt: skip
+          rtol=4e-15)  # fmt: skip
     rng = np.random.default_rng(5)
     consts = cooling.brems_constants()
     oc = ocool.brems_constants()
