@@ -86,6 +86,9 @@ _SIGS = {
     "nb_block_initialise": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams), _vp]),
     "nb_block_advance": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams), _vp, _vp]),
     "nb_block_land": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams), _vp]),
+    "nb_density_noalloc": (_int, [_i64, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _int, _dbl,
+                                  _dbl, _dbl, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "nb_noalloc_last_error": (_c.c_char_p, []),
 }  # fmt: skip
 
 EXPORTED = tuple(_SIGS)

@@ -29,6 +29,7 @@ SOURCES = {
     "engine.cu": False,
     "steps.cu": False,
     "capi.cu": False,
+    "noalloc.cu": False,
 }
 
 

@@ -159,6 +159,24 @@ NB_API int nb_block_advance(nb_ctx* ctx, nb_state* st, const nb_params* prm, int
 /* Re-open the steps just opened so they land on n_stop (sim/blocks.py:722-734, run's prologue). */
 NB_API int nb_block_land(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* stream);
 
+/* ---------------------------------------------------------------- allocation-free variant
+ * No counterpart in the reference.  nb_density_noalloc is nb_density for callers that cannot
+ * allocate device memory (a host framework that owns the device allocator, or a run that must
+ * not allocate once planned): it takes no context and allocates nothing.  Its scratch (the packed
+ * positions) is a fixed device array of NB_NOALLOC_MAX_N particles, 8 MiB, held by every GPU
+ * that loads the library until exit; larger n returns NB_ERR_INPUT.  The first call on a device
+ * looks up that array's device address (cudaGetSymbolAddress), so make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  Messages of failed calls: nb_noalloc_last_error (per host thread). */
+#define NB_NOALLOC_MAX_N 262144
+NB_API int nb_density_noalloc(int64_t n, const double* pos, const double* mass,
+                              const double* h_start, const double* h_search,
+                              const int64_t* offset, const int64_t* index, int64_t nrows,
+                              const int64_t* rows, int kernel_id, double eta, double tol,
+                              double h_max, double* h_out, double* rho, double* omega,
+                              int64_t* iters, int64_t* flags, void* stream);
+NB_API const char* nb_noalloc_last_error(void);
+
 /* Live kernel timing with CUDA events on the launching stream: nb_profile(ctx, 1) resets and
  * starts, nb_profile_read fills out[16] = for each of {list build, density, forces, gravity
  * flow}: (milliseconds, launches, rows or particles processed, pair evaluations). */
