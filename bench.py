@@ -49,7 +49,22 @@ def peaks():
     return {**PEAKS_FALLBACK, "source": "fallback"}
 
 
-def workload(name: str, n: int | None, precision: str, seed_shift: int = 0):
+WEIGHTS = os.path.join(ROOT, "blackhole_nebula_simulator_b200", "data", "cooling_mlp.npy")
+
+
+def cooling_network():
+    """The trained cooling network (weights trained on the GPU by the library's kernels and
+    saved by `python -m blackhole_nebula_simulator_b200.cooling`); trained here if absent."""
+    from blackhole_nebula_simulator_b200 import cooling
+
+    if os.path.exists(WEIGHTS):
+        return cooling.load_network(WEIGHTS, cooling.mlp_params(judge=64))
+    net = cooling.train_network()
+    net.params = cooling.mlp_params(judge=64)
+    return net
+
+
+def workload(name: str, n: int | None, precision: str, seed_shift: int = 0, mlp=None):
     from blackhole_nebula_simulator_b200 import ics
     from blackhole_nebula_simulator_b200.config import BlockConfig, CoupledConfig, HydroConfig
 
@@ -60,12 +75,13 @@ def workload(name: str, n: int | None, precision: str, seed_shift: int = 0):
         ic = ics.torus(n, seed=4 + seed_shift)
         alpha_av = 10.0 * 0.1 * 15.0 / float(np.mean(ic.h))  # alpha_SS = 0.1, H = sigma = 15
         hc = HydroConfig(disc_alpha_av=alpha_av, **common)
-        bc = BlockConfig(coupled=CoupledConfig(hydro=hc, cooling="brems"), dt_max=256.0)
+        bc = BlockConfig(coupled=CoupledConfig(hydro=hc, cooling="brems", cooling_mlp=mlp),
+                         dt_max=256.0)  # fmt: skip
     elif name == "streams":
         n = n or 1_048_576
         ic = ics.streams(n, seed=3 + seed_shift)
-        bc = BlockConfig(coupled=CoupledConfig(hydro=HydroConfig(**common), cooling="brems"),
-                         dt_max=4096.0)  # fmt: skip
+        bc = BlockConfig(coupled=CoupledConfig(hydro=HydroConfig(**common), cooling="brems",
+                                               cooling_mlp=mlp), dt_max=4096.0)  # fmt: skip
     elif name == "cloud":
         n = n or 262_144
         ic = ics.cloud(n, seed=1 + seed_shift)
@@ -171,15 +187,18 @@ def roofline(prof, precision, disc, pk):
     return rf, dom
 
 
-def run_gpu(args, rank, world):
+def run_gpu(args, rank, world, precision=None, use_mlp=None, e2e=True):
     import torch
 
-    from blackhole_nebula_simulator_b200 import _lib, blocks
+    from blackhole_nebula_simulator_b200 import _lib, blocks, cooling
     from blackhole_nebula_simulator_b200.device import ctx
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    ic, bc = workload(args.workload, args.n, args.precision, seed_shift=rank)
+    precision = precision or args.precision
+    use_mlp = (precision == "fp32") if use_mlp is None else use_mlp
+    net = cooling_network() if use_mlp else None
+    ic, bc = workload(args.workload, args.n, precision, seed_shift=rank, mlp=net)
     st = blocks.initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=1e12)
     for _ in range(args.warmup):
         blocks.advance(st, bc)
@@ -214,8 +233,9 @@ def run_gpu(args, rank, world):
     else:
         total = float(psteps)
     led = blocks.ledger(st, bc)
-    e2e = run_e2e(args, st, bc, snap)
-    return ms, total, prof, clk.summary(), st, led, e2e
+    mlp = cooling.mlp_stats(reset=True) if use_mlp else None
+    e2e_out = run_e2e(args, st, bc, snap) if e2e else None
+    return ms, total, prof, clk.summary(), st, led, e2e_out, mlp
 
 
 def _tensor_fields(st):
@@ -306,6 +326,7 @@ def main():
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain comparison form")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -329,7 +350,16 @@ def main():
         import torch
 
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    ms, total, prof, clocks, st, led, e2e = run_gpu(args, rank, world)
+    ms, total, prof, clocks, st, led, e2e, mlp = run_gpu(args, rank, world)
+    plain = None
+    if args.precision == "fp32" and not args.no_plain:
+        # the comparison form of the metric: FP64 pair arithmetic with the exact integrator
+        p_ms, p_total, p_prof, p_clk, p_st, _, _, _ = run_gpu(args, rank, world, "fp64", False,
+                                                              e2e=False)  # fmt: skip
+        plain = {"value": p_total / (p_ms * 1e-3), "unit": "particle-steps/s",
+                 "ms_per_step": p_ms / args.steps, "dtype": "f64", "cooling": "exact integrator",
+                 "kernel_ms": {k: round(v["ms"], 3) for k, v in p_prof.items()
+                               if not k.startswith("_")}}  # fmt: skip
     if rank == 0:
         pk = peaks()
         launches = prof.pop("_launches")
@@ -348,7 +378,11 @@ def main():
             "pairs_per_force_row": (prof["forces"]["pairs"] / prof["forces"]["units"]
                                     if prof["forces"]["units"] else None),
             "h_stats": h_stats(st),
-            "energy_rel_drift": None,
+            "cooling": ("network (BF16 tensor cores, exact fallback)" if mlp is not None
+                        else "exact integrator"),
+            "cooling_network": mlp,
+            "fp64_plain": plain,
+            "speedup_vs_fp64_plain": (total / (ms * 1e-3)) / plain["value"] if plain else None,
         }  # fmt: skip
         if not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_reference(args, 2, 1)

@@ -29,6 +29,15 @@ class NebulaCudaError(RuntimeError):
     """A CUDA or host-side failure inside libnebula_b200.so."""
 
 
+class NbMlpParams(_c.Structure):
+    _fields_ = [
+        ("tfac", _dbl), ("b", _dbl), ("kappa", _dbl), ("u_floor", _dbl), ("t_floor", _dbl),
+        ("rho_unit_cgs", _dbl), ("t_unit_s", _dbl), ("lrho_lo", _dbl), ("lrho_hi", _dbl),
+        ("lt_lo", _dbl), ("lt_hi", _dbl), ("ldt_lo", _dbl), ("ldt_hi", _dbl), ("check_tol", _dbl),
+        ("judge", _int),
+    ]  # fmt: skip
+
+
 class NbParams(_c.Structure):
     _fields_ = [
         ("kernel_id", _int), ("cnorm", _dbl), ("eta", _dbl), ("tol", _dbl), ("h_max", _dbl),
@@ -37,7 +46,7 @@ class NbParams(_c.Structure):
         ("disc_alpha_av", _dbl), ("courant", _dbl), ("c_force", _dbl), ("eta_orb", _dbl),
         ("precision", _int), ("cooling", _int), ("cooling_beta", _dbl), ("u_floor", _dbl),
         ("brems_tfac", _dbl), ("brems_b", _dbl), ("brems_kappa", _dbl), ("brems_t_floor", _dbl),
-        ("dt_max", _dbl), ("limiter", _int), ("max_gap", _int),
+        ("dt_max", _dbl), ("limiter", _int), ("max_gap", _int), ("mlp", NbMlpParams),
     ]  # fmt: skip
 
 
@@ -86,6 +95,13 @@ _SIGS = {
     "nb_block_initialise": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams), _vp]),
     "nb_block_advance": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams), _vp, _vp]),
     "nb_block_land": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams), _vp]),
+    "nb_mlp_data": (_int, [_vp, _i64, _c.c_uint64, _c.POINTER(NbMlpParams), _vp, _vp, _vp, _vp]),
+    "nb_mlp_grad": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _c.POINTER(_dbl), _vp]),
+    "nb_mlp_train": (_int, [_vp, _c.POINTER(NbMlpParams), _i64, _i64, _int, _dbl, _c.c_uint64,
+                            _vp, _vp]),
+    "nb_mlp_weights": (_int, [_vp, _vp, _vp, _vp]),
+    "nb_mlp_cool": (_int, [_vp, _i64, _vp, _vp, _vp, _dbl, _c.POINTER(NbMlpParams), _vp, _vp, _vp]),
+    "nb_mlp_stats": (_int, [_vp, _c.POINTER(_dbl), _int]),
     "nb_density_noalloc": (_int, [_i64, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _int, _dbl,
                                   _dbl, _dbl, _vp, _vp, _vp, _vp, _vp, _vp]),
     "nb_noalloc_last_error": (_c.c_char_p, []),

@@ -30,6 +30,7 @@ SOURCES = {
     "steps.cu": False,
     "capi.cu": False,
     "noalloc.cu": False,
+    "mlp.cu": True,
 }
 
 

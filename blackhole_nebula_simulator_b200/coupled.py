@@ -37,6 +37,10 @@ def make_params(cc: CoupledConfig, dt_max: float = 4096.0, limiter: bool = True,
     if cc.cooling == "brems":
         bcst = brems_constants(hc.gamma, hc.gas_units, cc.t_floor)
         p.cooling = 2
+        if cc.cooling_mlp is not None:  # the learned step, exact fallback inside
+            p.cooling = 3
+            p.mlp = cc.cooling_mlp.params
+            cc.cooling_mlp.install()
         p.brems_tfac, p.brems_b, p.brems_kappa, p.brems_t_floor = bcst.tfac, bcst.b, bcst.kappa, bcst.t_floor
         p.u_floor = bcst.u_floor
     elif math.isfinite(cc.cooling_beta):

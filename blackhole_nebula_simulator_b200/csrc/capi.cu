@@ -15,10 +15,6 @@ namespace nbk {
 unsigned long long g_launch_count = 0;
 }
 
-struct nb_ctx {
-  nbk::Engine E;
-};
-
 using nbk::Engine;
 
 namespace {

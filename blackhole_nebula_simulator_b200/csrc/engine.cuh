@@ -9,6 +9,7 @@
 #include <cstring>
 
 #include "common.cuh"
+#include "../../include/nebula_b200.h"
 
 namespace nbk {
 
@@ -121,6 +122,11 @@ struct Engine {
 };
 
 size_t cub_bytes_needed(int64_t n, int64_t m);
+struct MlpHull;
+// learned cooling (mlp.cu): u_out = cooled u of n particles (dt per particle or dt_scalar)
+int mlp_cool(Engine& E, int64_t n, const double* u, const double* rho, const double* dt,
+             double dt_scalar, const struct ::nb_mlp_params* mp, double* u_out, int8_t* mode,
+             cudaStream_t st);
 int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaStream_t st);
 int export_lists_offsets(Engine& E, int64_t* off_out, cudaStream_t st);
 int export_lists(Engine& E, int64_t* off_out, int64_t* idx_out, cudaStream_t st);
@@ -133,6 +139,10 @@ inline int set_host_error(Engine& E, const char* msg) {
 int check_device_error(Engine& E, cudaStream_t st);
 
 }  // namespace nbk
+
+struct nb_ctx {
+  nbk::Engine E;
+};
 
 #define NB_CUDA(call)                                                                        \
   do {                                                                                       \

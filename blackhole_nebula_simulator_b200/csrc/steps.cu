@@ -131,6 +131,15 @@ __global__ void k_cool_shared(int64_t n, int law, const double* __restrict__ x0,
   u_half[i] = un;
 }
 
+// dm = m (u_half - u_cooled); u_half <- u_cooled
+__global__ void k_dm_shared(int64_t n, const double* __restrict__ m, const double* __restrict__ uc,
+                            double* __restrict__ u_half, double* __restrict__ dm) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  dm[i] = m[i] * (u_half[i] - uc[i]);
+  u_half[i] = uc[i];
+}
+
 __global__ void k_pred_shared(int64_t n, const double* __restrict__ p_flow,
                               const double* __restrict__ a, const double* __restrict__ u_half,
                               const double* __restrict__ dudt, double half,
@@ -223,7 +232,7 @@ int coupled_step(Engine& E, nb_state* s, const nb_params* prm, double dt, cudaSt
 // exact at any step): C_cool u / |du/dt| for gas above the floor temperature, else inf.
 constexpr double C_COOL = 0.25;
 __device__ __forceinline__ double cooling_dt(int law, double u, double rho, const BremsParams& bp) {
-  if (law != 2 || !(bp.tfac * u > bp.t_floor)) return INFINITY;
+  if ((law != 2 && law != 3) || !(bp.tfac * u > bp.t_floor)) return INFINITY;
   double rate = fabs(brems_rate(u, rho, bp));
   return rate > 0 ? C_COOL * u / rate : INFINITY;
 }
@@ -294,7 +303,8 @@ __global__ void k_block_cool(int64_t n, int law, int64_t n_next, double tick,
                              const double* __restrict__ x_beg, const double* __restrict__ x,
                              const double* __restrict__ rho, const double* __restrict__ m,
                              const double* __restrict__ dudt, double beta, double u_floor,
-                             BremsParams bp, double* __restrict__ u_half, double* __restrict__ u,
+                             BremsParams bp, const double* __restrict__ uc_in,
+                             double* __restrict__ u_half, double* __restrict__ u,
                              double* __restrict__ lum, double* __restrict__ dm) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -309,6 +319,8 @@ __global__ void k_block_cool(int64_t n, int law, int64_t n_next, double tick,
     uc = beta_cool_one(uh, u_floor, s, t_cool);
   } else if (law == 2) {
     uc = brems_cool_one(uh, rho[i], s, bp);
+  } else if (law == 3) {
+    uc = uc_in[i];
   }
   if (law != 0) {
     double d = act ? m[i] * (uh - uc) : 0.0;
@@ -319,6 +331,12 @@ __global__ void k_block_cool(int64_t n, int law, int64_t n_next, double tick,
     }
   }
   u[i] = uc + (s - half_len) * dudt[i];
+}
+
+__global__ void k_elapsed(int64_t n, int64_t n_next, double tick, const int64_t* __restrict__ n_beg,
+                          double* __restrict__ s) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) s[i] = (double)(n_next - n_beg[i]) * tick;
 }
 
 // closing kicks of the rows (sim/blocks.py:544-547)
@@ -582,10 +600,15 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   NB_TRY(glf_status(E, n, W.iters, st));
   int64_t nrows = 0;
   NB_TRY(select_mask(E, n, W.m_rows, W.rows, &nrows, st));
+  if (prm->cooling == 3) {
+    // every particle's elapsed time, then the network's cooled u_half (exact fallback inside)
+    count_launch(), k_elapsed<<<grid_for(n), NB_THREADS, 0, st>>>(n, n_next, s->tick, s->n_beg, W.d_b);
+    NB_TRY(mlp_cool(E, n, s->u_half, s->rho, W.d_b, 0.0, &prm->mlp, W.d_c, nullptr, st));
+  }
   count_launch(), k_block_cool<<<grid_for(n), NB_THREADS, 0, st>>>(
-      n, prm->cooling == 1 ? 1 : (prm->cooling >= 2 ? 2 : 0), n_next, s->tick, s->n_beg,
-      s->n_end, s->x_beg, s->x, s->rho, s->mass, s->dudt, prm->cooling_beta, prm->u_floor,
-      brems_of(prm), s->u_half, s->u, s->luminosity, W.d_dm);
+      n, prm->cooling, n_next, s->tick, s->n_beg, s->n_end, s->x_beg, s->x, s->rho, s->mass,
+      s->dudt, prm->cooling_beta, prm->u_floor, brems_of(prm), W.d_c, s->u_half, s->u,
+      s->luminosity, W.d_dm);
   if (prm->cooling != 0) {
     double de = 0;
     NB_TRY(sum_doubles(E, n, W.d_dm, &de, st));

@@ -40,6 +40,18 @@ extern "C" {
 
 typedef struct nb_ctx nb_ctx;
 
+/* The learned cooling step (no reference counterpart): the bremsstrahlung law, the unit
+ * conversions of the network's inputs and its training hull (log10 rho [g/cm^3], log10 T [K],
+ * log10 dt [s]), the tolerance of the a-posteriori check (a fraction of u) and the stride of
+ * the exact-integrator comparison ("judge", 0: off). */
+typedef struct nb_mlp_params {
+  double tfac, b, kappa, u_floor, t_floor;
+  double rho_unit_cgs, t_unit_s;
+  double lrho_lo, lrho_hi, lt_lo, lt_hi, ldt_lo, ldt_hi;
+  double check_tol;
+  int judge;
+} nb_mlp_params;
+
 /* Physics and numerics of one run: the fields of the reference's HydroConfig, CoupledConfig and
  * BlockConfig that the CUDA path implements (sim/hydro.py:53-98, sim/coupled.py:62-75,
  * sim/blocks.py:83-100). */
@@ -58,6 +70,7 @@ typedef struct nb_params {
   double brems_tfac, brems_b, brems_kappa, brems_t_floor;
   double dt_max;          /* block steps: level-0 step */
   int limiter, max_gap;
+  nb_mlp_params mlp;      /* cooling 3: the network (weights set by nb_mlp_train / nb_mlp_weights) */
 } nb_params;
 
 /* Device state of a run (the fields of the reference's GasState / BlockState that the step
@@ -145,6 +158,34 @@ NB_API int nb_brems_cool(nb_ctx* ctx, int64_t n, const double* u, const double* 
  * angular momentum (3), momentum (3), mass. */
 NB_API int nb_ledger(nb_ctx* ctx, int64_t n, const double* x, const double* p, const double* u,
               const double* mass, double* out, void* stream);
+
+/* ---------------------------------------------------------------- learned cooling
+ * MLP 3 -> 64 -> 64 -> 64 (SiLU) -> 1 predicting the fraction of u - u_floor one step removes.
+ * Weights: a flat float32 vector of NB_MLP_NPARAM (W1 64x3, b1, W2 64x64, b2, W3 64x64, b3,
+ * W4 1x64, b4), held per device by the library. */
+#define NB_MLP_NPARAM 8641
+/* n training samples, log-uniform over the hull, labelled by the exact integrator: X (n, 3)
+ * scaled inputs, Y (n) labels, U (n, 3) code-unit (u, rho, dt) or NULL. */
+NB_API int nb_mlp_data(nb_ctx* ctx, int64_t n, uint64_t seed, const nb_mlp_params* mp, float* X,
+                       float* Y, double* U, void* stream);
+/* Mean squared error of one batch and its gradient (device g, NB_MLP_NPARAM) at weights w,
+ * with the forward pass rounding the weights to BF16 as inference does. */
+NB_API int nb_mlp_grad(nb_ctx* ctx, int64_t batch, const float* X, const float* Y, const float* w,
+                       float* g, double* loss, void* stream);
+/* Train the device's network from scratch: n_samples fresh samples, Adam, cosine-decayed
+ * learning rate; loss_hist (host, epochs) gets each epoch's last-batch loss (may be NULL). */
+NB_API int nb_mlp_train(nb_ctx* ctx, const nb_mlp_params* mp, int64_t n_samples, int64_t batch,
+                        int epochs, double lr, uint64_t seed, float* loss_hist, void* stream);
+/* Copy the device's weights out (w_out, device) and/or replace them (w_in, device). */
+NB_API int nb_mlp_weights(nb_ctx* ctx, float* w_out, const float* w_in, void* stream);
+/* Cooling of n particles by the network with exact fallback (dt NULL: dt_scalar for all);
+ * mode (optional, int8): 0 exact/no cooling, 1 network, 2 fallback. */
+NB_API int nb_mlp_cool(nb_ctx* ctx, int64_t n, const double* u, const double* rho, const double* dt,
+                       double dt_scalar, const nb_mlp_params* mp, double* u_out, int8_t* mode,
+                       void* stream);
+/* out[5] = max and rms of |du_net - du_exact| / u over the judged samples, judged count,
+ * network results, fallbacks (accumulated since the last reset; reset != 0 clears). */
+NB_API int nb_mlp_stats(nb_ctx* ctx, double* out, int reset);
 
 /* ---------------------------------------------------------------- step runtime
  * The reference's step entry points (sim/coupled.py:198-258, sim/blocks.py:455-563) on device
