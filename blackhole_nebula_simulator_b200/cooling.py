@@ -89,10 +89,11 @@ class Hull:
 
 
 def mlp_params(gamma: float = 5.0 / 3.0, gas_units: units.GasUnits = units.GasUnits(),
-               t_floor: float = 1.0e4, hull: Hull = Hull(), check_tol: float = 1.0e-3,
+               t_floor: float = 1.0e4, hull: Hull = Hull(), check_tol: float = 5.0e-4,
                judge: int = 0) -> _lib.NbMlpParams:  # fmt: skip
     """The network's parameter block: the bremsstrahlung law, the unit conversions of its inputs,
-    the hull, the a-posteriori tolerance (fraction of u) and the judge stride (0: off)."""
+    the hull, the a-posteriori tolerance tol (fraction of u; an accepted step is within 2 tol of
+    the exact integrator) and the judge stride (0: off)."""
     c = brems_constants(gamma, gas_units, t_floor)
     p = _lib.NbMlpParams()
     p.tfac, p.b, p.kappa, p.u_floor, p.t_floor = c.tfac, c.b, c.kappa, c.u_floor, c.t_floor
@@ -119,7 +120,7 @@ class CoolingNetwork:
         _lib.check(c, _lib.lib().nb_mlp_weights(c, None, ptr(self.weights), stream()))
 
 
-def train_network(n_samples: int = 16 * 2**20, batch: int = 65536, epochs: int = 30,
+def train_network(n_samples: int = 16 * 2**20, batch: int = 32768, epochs: int = 40,
                   lr: float = 3.0e-3, seed: int = 2026, params=None) -> CoolingNetwork:  # fmt: skip
     """Train the cooling network on the GPU with the library's own kernels: n_samples
     log-uniform samples labelled by the exact integrator, Adam with a cosine learning rate."""
@@ -181,7 +182,7 @@ def main(argv=None) -> None:
     args = sys.argv[1:] if argv is None else argv
     out = args[0]
     n = int(args[1]) if len(args) > 1 else 16 * 2**20
-    epochs = int(args[2]) if len(args) > 2 else 30
+    epochs = int(args[2]) if len(args) > 2 else 40
     net = train_network(n_samples=n, epochs=epochs)
     np.save(out, net.weights.cpu().numpy())
     print(f"trained on {n} samples, {epochs} epochs; last-batch loss per epoch: "

@@ -147,6 +147,28 @@ __global__ void k_mask_rows(int64_t nrows, const int64_t* __restrict__ rows, int
   mask[i] = 1;
 }
 
+// mask in sorted order from a caller-order mask
+__global__ void k_sorted_mask(int64_t n, const int32_t* __restrict__ perm, const uint8_t* __restrict__ m,
+                              uint8_t* __restrict__ ms) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < n) ms[k] = m[perm[k]];
+}
+
+__global__ void k_pack_sorted_f4(int64_t n, const int32_t* __restrict__ perm,
+                                 const double* __restrict__ a, const double* __restrict__ b,
+                                 const double* __restrict__ c, const double* __restrict__ d,
+                                 int vec3, float4* __restrict__ out) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int64_t i = perm[k];
+  if (vec3)  // a: (n, 3) vector, b: scalar
+    out[k] = make_float4((float)a[3 * i], (float)a[3 * i + 1], (float)a[3 * i + 2],
+                         b ? (float)b[i] : 0.f);
+  else
+    out[k] = make_float4(a ? (float)a[i] : 0.f, b ? (float)b[i] : 0.f, c ? (float)c[i] : 0.f,
+                         d ? (float)d[i] : 0.f);
+}
+
 __global__ void k_rows_to_sorted(int64_t nrows, const int64_t* __restrict__ rows,
                                  const int32_t* __restrict__ inv_perm, int64_t* __restrict__ out) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -377,9 +399,11 @@ int Workspace::ensure(Engine& E, int64_t n) {
   double4** d4[] = {&pk0, &pk1, &pk2, &pk3};
   for (double4** p : d4) NB_CUDA(cudaMalloc((void**)p, sizeof(double4) * c));
   NB_CUDA(cudaMalloc((void**)&pk32, sizeof(float4) * c));
+  float4** f4s[] = {&pf1, &pf2, &pf3};
+  for (float4** p : f4s) NB_CUDA(cudaMalloc((void**)p, sizeof(float4) * c));
   int64_t** i8[] = {&rows, &rows_s, &rows2, &iters, &flags, &need, &i_tmp, &pairs};
   for (int64_t** p : i8) NB_CUDA(cudaMalloc((void**)p, sizeof(int64_t) * (c + 1)));
-  uint8_t** u1[] = {&m_rows, &m_done, &m_need, &m_tmp};
+  uint8_t** u1[] = {&m_rows, &m_done, &m_need, &m_tmp, &m_x, &m_sorted};
   for (uint8_t** p : u1) NB_CUDA(cudaMalloc((void**)p, c));
   NB_CUDA(cudaMalloc((void**)&i32a, sizeof(int32_t) * c));
   NB_CUDA(cudaMalloc((void**)&i32b, sizeof(int32_t) * c));
@@ -412,6 +436,7 @@ int Workspace::ensure(Engine& E, int64_t n) {
 void Workspace::release() {
   void* ps[] = {d_a, d_b, d_c, d_hg, d_hs, d_heff, d_hlim, d_disp, d_P, d_cs, d_vsig, d_ddudt,
                 d_dm, d_tmp, d_uh, v_flow, v_pred, v_eval, v_dacc, v_tmp, pk0, pk1, pk2, pk3, pk32,
+                pf1, pf2, pf3, m_x, m_sorted,
                 rows, rows_s, rows2, iters, flags, need, i_tmp, pairs, m_rows, m_done, m_need,
                 m_tmp, i32a, i32b, dk_b, d_int, d_i64};
   for (void* p : ps)
@@ -444,6 +469,17 @@ static int sum_rows_i64(Engine& E, int64_t nrows, const int64_t* rows, const int
   return 0;
 }
 
+// The rows (caller order) as sorted positions in ascending Morton order, into W.rows_s; the
+// pair passes then walk neighbouring particles in neighbouring threads.
+static int rows_sorted(Engine& E, int64_t n, int64_t nrows, const int64_t* rows, int64_t* count,
+                       cudaStream_t st) {
+  Workspace& W = E.ws;
+  NB_CUDA(cudaMemsetAsync(W.m_x, 0, n, st));
+  count_launch(), k_mask_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, n, W.m_x, E.d_err);
+  count_launch(), k_sorted_mask<<<grid_for(n), NB_THREADS, 0, st>>>(n, E.lists.perm, W.m_x, W.m_sorted);
+  return select_mask(E, n, W.m_sorted, W.rows_s, count, st);
+}
+
 static int read_int(Engine& E, int* d, int* out, cudaStream_t st) {
   NB_CUDA(cudaMemcpyAsync(E.ws.h_int, d, sizeof(int), cudaMemcpyDeviceToHost, st));
   NB_CUDA(cudaStreamSynchronize(st));
@@ -460,7 +496,8 @@ static int density_on_lists(Engine& E, int64_t n, const double* x, const double*
   Workspace& W = E.ws;
   Lists& L = E.lists;
   if (nrows == 0) return 0;
-  count_launch(), k_rows_to_sorted<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.inv_perm, W.rows_s);
+  int64_t ns = 0;
+  NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));
   count_launch(), k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, mass, W.d_a);
   count_launch(), k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, h_start, W.d_b);
   count_launch(), k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, h_search, W.d_c);
@@ -623,10 +660,17 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   int64_t n = s->n;
   count_launch(), k_eos<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->rho, u, prm->gamma, W.d_P, W.d_cs, E.d_err);
   if (nrows == 0) return check_device_error(E, st);
-  count_launch(), k_rows_to_sorted<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.inv_perm, W.rows_s);
-  count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, vel, s->mass, W.pk1);
-  count_launch(), k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->h, s->rho, s->omega, W.d_P, W.pk2);
-  count_launch(), k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, W.pk3);
+  int64_t ns = 0;
+  NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));
+  if (prm->precision == 1) {
+    count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, vel, s->mass, nullptr, nullptr, 1, W.pf1);
+    count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->h, s->rho, s->omega, W.d_P, 0, W.pf2);
+    count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, 0, W.pf3);
+  } else {
+    count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, vel, s->mass, W.pk1);
+    count_launch(), k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->h, s->rho, s->omega, W.d_P, W.pk2);
+    count_launch(), k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, W.pk3);
+  }
   ForceParams fp{};
   fp.kid = prm->kernel_id;
   fp.cnorm = prm->cnorm;
@@ -656,7 +700,7 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
     double cell = std::max(span / 1000.0, 1e-30);
     count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, E.bbox, cell, W.pk32);
     E.prof.begin(st);
-    launch_forces32<int32_t>(nrows, W.rows_s, W.pk32, (float)cell, W.pk1, W.pk2, W.pk3, L.off,
+    launch_forces32<int32_t>(nrows, W.rows_s, W.pk32, (float)cell, W.pf1, W.pf2, W.pf3, L.off,
                              L.idx, fp, L.perm, fo, st);
   } else {
     count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, nullptr, W.pk0);

@@ -50,9 +50,11 @@ struct Workspace {
          *v_tmp = nullptr;  // (n, 3)
   double4 *pk0 = nullptr, *pk1 = nullptr, *pk2 = nullptr, *pk3 = nullptr;  // sorted packs
   float4* pk32 = nullptr;
+  float4 *pf1 = nullptr, *pf2 = nullptr, *pf3 = nullptr;  // FP32 packs of the force pass
   int64_t *rows = nullptr, *rows_s = nullptr, *rows2 = nullptr, *iters = nullptr,
           *flags = nullptr, *need = nullptr, *i_tmp = nullptr, *pairs = nullptr;
-  uint8_t *m_rows = nullptr, *m_done = nullptr, *m_need = nullptr, *m_tmp = nullptr;
+  uint8_t *m_rows = nullptr, *m_done = nullptr, *m_need = nullptr, *m_tmp = nullptr,
+          *m_x = nullptr, *m_sorted = nullptr;
   int32_t *i32a = nullptr, *i32b = nullptr;
   double* dk_b = nullptr;
   int* d_int = nullptr;

@@ -83,16 +83,17 @@ __global__ void k_fwd(int64_t B, int in, int out, const float* __restrict__ A, c
   float z = b[o];
   for (int i = 0; i < in; ++i) z = fmaf(bf16r(W[o * in + i]), A[s * in + i], z);
   Z[t] = z;
-  Aout[t] = act ? silu(z) : z;
+  Aout[t] = act == 1 ? silu(z) : (act == 2 ? 1.0f / (1.0f + __expf(-z)) : z);
 }
 
-// dY = 2 (y - label) / B; per-sample squared error for the loss
+// the output is f = sigmoid(z4); loss = mean (f - label)^2: dZ4 = 2 (f - label) f (1 - f) / B
 __global__ void k_loss(int64_t B, const float* __restrict__ y, const float* __restrict__ lab,
-                       float* __restrict__ dy, float* __restrict__ se) {
+                       float* __restrict__ dz, float* __restrict__ se) {
   int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= B) return;
-  float d = y[s] - lab[s];
-  dy[s] = 2.0f * d / (float)B;
+  float f = y[s];
+  float d = f - lab[s];
+  dz[s] = 2.0f * d * f * (1.0f - f) / (float)B;
   se[s] = d * d;
 }
 
@@ -209,7 +210,7 @@ static int mlp_grad(Engine& E, MlpBuffers& M, int64_t B, const float* X, const f
   count_launch(), k_fwd<<<G(B * MLP_H), T, 0, st>>>(B, MLP_IN, MLP_H, X, w + MLP_W1, w + MLP_B1, M.Z1, M.A1, 1);
   count_launch(), k_fwd<<<G(B * MLP_H), T, 0, st>>>(B, MLP_H, MLP_H, M.A1, w + MLP_W2, w + MLP_B2, M.Z2, M.A2, 1);
   count_launch(), k_fwd<<<G(B * MLP_H), T, 0, st>>>(B, MLP_H, MLP_H, M.A2, w + MLP_W3, w + MLP_B3, M.Z3, M.A3, 1);
-  count_launch(), k_fwd<<<G(B), T, 0, st>>>(B, MLP_H, 1, M.A3, w + MLP_W4, w + MLP_B4, M.Yd, M.Y, 0);
+  count_launch(), k_fwd<<<G(B), T, 0, st>>>(B, MLP_H, 1, M.A3, w + MLP_W4, w + MLP_B4, M.Yd, M.Y, 2);
   count_launch(), k_loss<<<G(B), T, 0, st>>>(B, M.Y, lab, M.dZ4, M.se);
   int nchunk = (int)((B + WG_CHUNK - 1) / WG_CHUNK);
   // layer 4
@@ -411,17 +412,26 @@ __global__ void __launch_bounds__(128) k_mlp_cool(int64_t n, const double* __res
         un = u;
       } else {
         bool ok = inside;
-        double ff = fmin(fmax((double)f, 0.0), 1.0);
+        double ff = 1.0 / (1.0 + exp(-(double)f));  // the network predicts logit f
         double um = u - ff * (u - bp.u_floor);
         if (ok) {
-          // a-posteriori bracket: the cooling rate grows with T, so the exact step lies between
-          // dt |rate(u_new)| and dt |rate(u)|; accept within check_tol u of that bracket
+          // a-posteriori acceptance: the cooling rate r(u) grows with T, so the exact step du_e
+          // satisfies dt r(u_e) <= du_e <= dt r(u).  If du_m lies within tol of
+          // [dt r(u_m), dt r(u)], then |du_m - du_e| <= dt (r(u) - r(u_m)) + tol; accept only
+          // when that bound is <= 2 tol.  A prediction at the floor is accepted only when even
+          // the floor's rate dt r(u_floor) removes all of u - u_floor (then the exact step ends
+          // at the floor too).
           double du = u - um;
-          double lo = d * fabs(brems_rate(um, r, bp)), hi = d * fabs(brems_rate(u, r, bp));
           double tol = hl.check_tol * u;
-          bool at_floor = um <= bp.u_floor * (1.0 + 1e-12);
-          if (at_floor) ok = hi >= du - tol;  // reaching the floor needs enough cooling
-          else ok = du >= fmin(lo, hi) - tol && du <= hi + tol;
+          double r_hi = d * fabs(brems_rate(u, r, bp));
+          if (ff >= 1.0 - 1e-6) {
+            double r_f = d * fabs(brems_rate(bp.u_floor * (1.0 + 1e-12), r, bp));
+            ok = r_f >= u - bp.u_floor;
+            um = bp.u_floor;
+          } else {
+            double r_lo = d * fabs(brems_rate(um, r, bp));
+            ok = du >= r_lo - tol && du <= r_hi + tol && (r_hi - r_lo) <= tol;
+          }
         }
         if (ok) {
           un = um;

@@ -52,7 +52,7 @@ void launch_forces64(int64_t nrows, const int64_t* rows, const double4* pos, con
                      ForceParams prm, const int32_t* out_map, ForceOut out, cudaStream_t st);
 template <typename I>
 void launch_forces32(int64_t nrows, const int64_t* rows, const float4* pos, float cell,
-                     const double4* vm, const double4* hydro, const double4* aux,
+                     const float4* vm, const float4* hydro, const float4* aux,
                      const int64_t* off, const I* idx, ForceParams prm, const int32_t* out_map,
                      ForceOut out, cudaStream_t st);
 

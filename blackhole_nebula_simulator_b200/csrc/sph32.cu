@@ -19,12 +19,12 @@ void launch_density32(int64_t nrows, const int64_t* rows, const float4* pos, flo
 
 template <typename I>
 void launch_forces32(int64_t nrows, const int64_t* rows, const float4* pos, float cell,
-                     const double4* vm, const double4* hydro, const double4* aux,
+                     const float4* vm, const float4* hydro, const float4* aux,
                      const int64_t* off, const I* idx, ForceParams prm, const int32_t* out_map,
                      ForceOut out, cudaStream_t st) {
   if (nrows <= 0) return;
   Pos32 geo{pos, cell};
-  count_launch(), k_forces<float, Pos32, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+  count_launch(), k_forces<float, Pos32, I, float4><<<grid_for(nrows), NB_THREADS, 0, st>>>(
       nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
 }
 
@@ -35,7 +35,7 @@ template void launch_density32<int32_t>(int64_t, const int64_t*, const float4*, 
                                         const int32_t*, double*, double*, double*, int64_t*,
                                         int64_t*, int64_t*, cudaStream_t);
 template void launch_forces32<int32_t>(int64_t, const int64_t*, const float4*, float,
-                                       const double4*, const double4*, const double4*,
+                                       const float4*, const float4*, const float4*,
                                        const int64_t*, const int32_t*, ForceParams,
                                        const int32_t*, ForceOut, cudaStream_t);
 

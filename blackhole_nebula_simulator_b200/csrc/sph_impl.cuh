@@ -97,6 +97,33 @@ __device__ void density_sums(const PosT& geo, int64_t i, const int64_t* off, con
   dws_out = dws.get();
 }
 
+// Sums over the cached in-range entries (r, m) of one row.
+template <typename R>
+__device__ __forceinline__ void cached_sums(const R* rr, const R* mm, int cnt, R h, int kid,
+                                            R cnorm, double& rs_out, double& dws_out,
+                                            int64_t& work) {
+  Acc<R> rs, dws;
+  R inv_h = R(1) / h;
+  R ih2 = inv_h * inv_h;
+  R ih3 = ih2 * inv_h;
+  R ih4 = ih2 * ih2;
+  for (int k = 0; k < cnt; ++k) {
+    R q = rr[k] * inv_h;
+    if (q < R(2)) {
+      work += 1;
+      R fq = kernel_f<R>(q, kid);
+      R m = mm[k];
+      rs.add(m * cnorm * ih3 * fq);
+      dws.add(m * (-cnorm * ih4 * (R(3) * fq + q * kernel_df<R>(q, kid))));
+    }
+  }
+  rs_out = rs.get();
+  dws_out = dws.get();
+}
+
+// In-range entries a row may cache in its thread's local array; longer rows re-walk the list.
+constexpr int DENSITY_CACHE = 192;
+
 template <typename R, typename PosT, typename I>
 __global__ void __launch_bounds__(NB_THREADS)
     k_density(int64_t nrows, const int64_t* __restrict__ rows, PosT geo,
@@ -113,18 +140,42 @@ __global__ void __launch_bounds__(NB_THREADS)
   double hs = fmin(h_search[i], prm.h_max);
   double r_max = 2.0 * hs;
   R r2max = (R)(r_max * r_max);
+  const int kid = prm.kid;
+  const R cn = (R)prm.cnorm;
+  int64_t evals = 0;
+  // distances and masses of the entries inside r_max, computed once (sim/sph.py:231-248)
+  R rr[DENSITY_CACHE], mm[DENSITY_CACHE];
+  int cnt = 0;
+  bool cached = true;
+  for (int64_t e = off[i]; e < off[i + 1]; ++e) {
+    int64_t j = (int64_t)idx[e];
+    R dx, dy, dz;
+    geo.diff(i, j, dx, dy, dz);
+    R d2 = sqdist(dx, dy, dz);
+    if (!(d2 < r2max)) continue;
+    if (cnt < DENSITY_CACHE) {
+      rr[cnt] = sqrt(d2);
+      mm[cnt] = (R)mass[j];
+    } else {
+      cached = false;
+    }
+    cnt += 1;
+  }
+  auto sums = [&](R h, double& rs, double& dws) {
+    if (cached)
+      cached_sums<R>(rr, mm, cnt, h, kid, cn, rs, dws, evals);
+    else
+      density_sums<R>(geo, i, off, idx, mass, r2max, h, kid, cn, rs, dws, evals);
+  };
   double lo = 0.0, hi = hs;
   double h = fmin(h_start[i], hi);
   double h0 = h;
   int flag = 3, it = 0;
   const double eta = prm.eta, e3 = eta * eta * eta;
-  const int kid = prm.kid;
-  const R cn = (R)prm.cnorm;
-  int64_t evals = 0;
   while (it < 50) {
     it += 1;
     double rs, dws;
-    density_sums<R>(geo, i, off, idx, mass, r2max, (R)h, kid, cn, rs, dws, evals);
+    sums((R)h, rs, dws);
     double t = eta / h;
     double f = rs - m_i * (t * t * t);
     double h2 = h * h;
@@ -144,7 +195,7 @@ __global__ void __launch_bounds__(NB_THREADS)
   }
   if (h >= hs * (1 - 1e-3)) {
     double rs_lim, dummy;
-    density_sums<R>(geo, i, off, idx, mass, r2max, (R)hs, kid, cn, rs_lim, dummy, evals);
+    sums((R)hs, rs_lim, dummy);
     double t = eta / hs;
     if (rs_lim - m_i * (t * t * t) < 0) {
       h = hs;
@@ -152,7 +203,7 @@ __global__ void __launch_bounds__(NB_THREADS)
     }
   }
   double rs, dws;
-  density_sums<R>(geo, i, off, idx, mass, r2max, (R)h, kid, cn, rs, dws, evals);
+  sums((R)h, rs, dws);
   h_out[o] = h;
   rho[o] = rs;
   omega[o] = flag == 1 ? 1.0 : 1.0 + h / (3.0 * rs) * dws;
@@ -170,19 +221,19 @@ __device__ __forceinline__ R dwdr(R r, R h, int kid, R cnorm) {
   return cnorm / (h2 * h2) * kernel_df<R>(r / h, kid);
 }
 
-template <typename R, typename PosT, typename I>
-__global__ void __launch_bounds__(NB_THREADS)
+template <typename R, typename PosT, typename I, typename V4>
+__global__ void __launch_bounds__(NB_THREADS, 2)
     k_forces(int64_t nrows, const int64_t* __restrict__ rows, PosT geo,
-             const double4* __restrict__ vm,    // (vx, vy, vz, mass)
-             const double4* __restrict__ hydro, // (h, rho, omega, P)
-             const double4* __restrict__ aux,   // (u, c_s, alpha, unused)
+             const V4* __restrict__ vm,    // (vx, vy, vz, mass)
+             const V4* __restrict__ hydro, // (h, rho, omega, P)
+             const V4* __restrict__ aux,   // (u, c_s, alpha, unused)
              const int64_t* __restrict__ off, const I* __restrict__ idx, ForceParams prm,
              const int32_t* __restrict__ out_map, ForceOut out) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= nrows) return;
   int64_t a = rows ? rows[q] : q;
   int64_t o = out_map ? (int64_t)out_map[a] : q;
-  const double4 va = vm[a], ha = hydro[a], xa = aux[a];
+  const V4 va = vm[a], ha = hydro[a], xa = aux[a];
   const R h_a = (R)ha.x, rho_a = (R)ha.y, om_a = (R)ha.z, P_a = (R)ha.w;
   const R inv_or_a = R(1) / (om_a * rho_a);
   const R inv_orr_a = R(1) / (om_a * rho_a * rho_a);
@@ -198,7 +249,7 @@ __global__ void __launch_bounds__(NB_THREADS)
     if (b == a) continue;
     R ddx, ddy, ddz;
     geo.diff(a, b, ddx, ddy, ddz);  // x_b - x_a
-    const double4 hb4 = hydro[b];
+    const V4 hb4 = hydro[b];
     const R h_b = (R)hb4.x;
     R d2 = sqdist(ddx, ddy, ddz);
     if (prm.tighten) {
@@ -206,7 +257,7 @@ __global__ void __launch_bounds__(NB_THREADS)
       if (!(d2 < rr * rr)) continue;
     }
     npairs += 1;
-    const double4 vb = vm[b];
+    const V4 vb = vm[b];
     const R rho_b = (R)hb4.y, om_b = (R)hb4.z, P_b = (R)hb4.w;
     const R m_b = (R)vb.w;
     R r = sqrt(d2);
@@ -221,7 +272,7 @@ __global__ void __launch_bounds__(NB_THREADS)
     R inv_orr_b = R(1) / (om_b * rho_b * rho_b);
     if (prm.use_sph) {
       if (prm.use_visc) {
-        const double4 xb = aux[b];
+        const V4 xb = aux[b];
         R vsig_a = al_a * cs_a + beta * fabs(vdotr);
         R vsig_b = (R)xb.z * (R)xb.y + beta * fabs(vdotr);
         if (vsig_a > vmax) vmax = vsig_a;
@@ -252,7 +303,7 @@ __global__ void __launch_bounds__(NB_THREADS)
     }
     if (prm.use_disc) {
       // the reference's disc kernel forms its terms in its own order (sim/sph.py:1097-1114)
-      const double4 xb = aux[b];
+      const V4 xb = aux[b];
       R ex = -ddx, ey = -ddy, ez = -ddz;  // x_a - x_b
       R vdr = dvx * ex / r;
       vdr = vdr + dvy * ey / r;

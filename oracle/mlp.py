@@ -3,7 +3,8 @@
 The network (3 -> 64 -> 64 -> 64 SiLU -> 1) and its training loss have no counterpart in the
 reference; this NumPy restatement checks the GPU kernels' gradients: forward with the weights
 rounded to BF16 (round to nearest even, as the inference kernel stores them), mean squared error,
-and the straight-through backward pass in float64.
+a sigmoid output (the network predicts logit f), and the straight-through backward pass in
+float64.
 """
 
 from __future__ import annotations
@@ -55,11 +56,11 @@ def loss_and_grad(w, X, Y):
     a2 = silu(z2)
     z3 = a2 @ Wq["W3"].T + Wq["b3"]
     a3 = silu(z3)
-    y = a3 @ Wq["W4"].T + Wq["b4"]
+    y = 1.0 / (1.0 + np.exp(-(a3 @ Wq["W4"].T + Wq["b4"])))  # f = sigmoid(z4)
     d = y[:, 0] - np.asarray(Y, np.float64)
     B = len(X)
     loss = float(np.mean(d * d))
-    dy = (2.0 * d / B)[:, None]
+    dy = (2.0 * d * y[:, 0] * (1.0 - y[:, 0]) / B)[:, None]
     g = {"W4": dy.T @ a3, "b4": dy.sum(0)}
     dz3 = (dy @ Wq["W4"]) * dsilu(z3)
     g["W3"], g["b3"] = dz3.T @ a2, dz3.sum(0)
@@ -77,7 +78,7 @@ def predict(w, X):
     a = np.asarray(X, np.float64)
     for i in (1, 2, 3):
         a = silu(a @ Wq[f"W{i}"].T + Wq[f"b{i}"])
-    return (a @ Wq["W4"].T + Wq["b4"])[:, 0]
+    return 1.0 / (1.0 + np.exp(-(a @ Wq["W4"].T + Wq["b4"])[:, 0]))
 
 
 def label(u, rho, dt, consts):
