@@ -121,8 +121,9 @@ __device__ __forceinline__ void cached_sums(const R* rr, const R* mm, int cnt, R
   dws_out = dws.get();
 }
 
-// In-range entries a row may cache in its thread's local array; longer rows re-walk the list.
-constexpr int DENSITY_CACHE = 192;
+// In-range entries a row may cache in its thread's local array (0: every sum walks the list; a
+// per-thread cache in local memory measured slower than re-walking the Morton-local list).
+constexpr int DENSITY_CACHE = 0;
 
 template <typename R, typename PosT, typename I>
 __global__ void __launch_bounds__(NB_THREADS)
@@ -143,23 +144,27 @@ __global__ void __launch_bounds__(NB_THREADS)
   const int kid = prm.kid;
   const R cn = (R)prm.cnorm;
   int64_t evals = 0;
-  // distances and masses of the entries inside r_max, computed once (sim/sph.py:231-248)
-  R rr[DENSITY_CACHE], mm[DENSITY_CACHE];
+  // distances and masses of the entries inside r_max (sim/sph.py:231-248): cached when
+  // DENSITY_CACHE > 0, else recomputed from the list by every sum
+  constexpr int CAP = DENSITY_CACHE > 0 ? DENSITY_CACHE : 1;
+  R rr[CAP], mm[CAP];
   int cnt = 0;
-  bool cached = true;
-  for (int64_t e = off[i]; e < off[i + 1]; ++e) {
-    int64_t j = (int64_t)idx[e];
-    R dx, dy, dz;
-    geo.diff(i, j, dx, dy, dz);
-    R d2 = sqdist(dx, dy, dz);
-    if (!(d2 < r2max)) continue;
-    if (cnt < DENSITY_CACHE) {
-      rr[cnt] = sqrt(d2);
-      mm[cnt] = (R)mass[j];
-    } else {
-      cached = false;
+  bool cached = DENSITY_CACHE > 0;
+  if (DENSITY_CACHE > 0) {
+    for (int64_t e = off[i]; e < off[i + 1]; ++e) {
+      int64_t j = (int64_t)idx[e];
+      R dx, dy, dz;
+      geo.diff(i, j, dx, dy, dz);
+      R d2 = sqdist(dx, dy, dz);
+      if (!(d2 < r2max)) continue;
+      if (cnt < DENSITY_CACHE) {
+        rr[cnt] = sqrt(d2);
+        mm[cnt] = (R)mass[j];
+      } else {
+        cached = false;
+      }
+      cnt += 1;
     }
-    cnt += 1;
   }
   auto sums = [&](R h, double& rs, double& dws) {
     if (cached)
