@@ -89,6 +89,18 @@ int Engine::grow2(int64_t m) {
   return 0;
 }
 
+int Engine::ensure_sub(int64_t m) {
+  Engine& E = *this;
+  if (m <= cap_sub && sub_lo) return 0;
+  int64_t c = std::max<int64_t>(m + m / 4, 256);
+  if (sub_lo) cudaFree(sub_lo);
+  if (sub_hi) cudaFree(sub_hi);
+  NB_CUDA(cudaMalloc((void**)&sub_lo, sizeof(double4) * c));
+  NB_CUDA(cudaMalloc((void**)&sub_hi, sizeof(double4) * c));
+  cap_sub = c;
+  return 0;
+}
+
 int Engine::ensure_list_capacity(int64_t m) {
   Engine& E = *this;
   NB_TRY(grow(E, lists.idx, cap_list, std::max<int64_t>(m, 1)));
@@ -102,7 +114,7 @@ int Engine::ensure_sort_keys(int64_t m) {
 }
 
 void Engine::release() {
-  void* ps[] = {d_err, bbox, bbox_part, keys_a, keys_b, vals_a, counts, node_lo, node_hi,
+  void* ps[] = {d_err, bbox, bbox_part, keys_a, keys_b, vals_a, counts, node_lo, node_hi, sub_lo, sub_hi,
                 cub_tmp, sort_keys, red, lists.perm, lists.inv_perm, lists.spos, lists.off,
                 lists.idx};
   for (void* p : ps)

@@ -106,6 +106,9 @@ struct Engine {
   int64_t* counts = nullptr;
   double4* node_lo = nullptr;
   double4* node_hi = nullptr;
+  double4* sub_lo = nullptr;  // sub-leaf boxes
+  double4* sub_hi = nullptr;
+  int64_t cap_sub = 0;
   void* cub_tmp = nullptr;
   size_t cub_bytes = 0;
   int64_t* sort_keys = nullptr;
@@ -117,6 +120,7 @@ struct Engine {
   int ensure_n(int64_t n);
   int ensure_nodes(int64_t m);
   int grow2(int64_t m);
+  int ensure_sub(int64_t m);
   int ensure_list_capacity(int64_t m);
   int ensure_sort_keys(int64_t m);
   int ensure_cub(size_t bytes);

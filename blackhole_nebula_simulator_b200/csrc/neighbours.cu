@@ -19,8 +19,10 @@
 namespace nbk {
 
 static constexpr int LEAF = 32;
+static constexpr int SUB = 8;  // sub-leaf: the unit each lane tests its own sphere against
 static constexpr int FAN = 8;
 static constexpr int STACK = 96;
+static constexpr int QCAP = 24;  // sub-leaves a lane queues before the warp flushes
 
 // ---------------------------------------------------------------- bounding box
 __global__ void k_bbox_partial(int64_t n, const double* __restrict__ pos, double* __restrict__ part) {
@@ -120,6 +122,27 @@ __global__ void k_leaf_boxes(int64_t n, int64_t nleaf, const double4* __restrict
   hi[l] = mx;
 }
 
+// Boxes (and largest h) of the sub-leaves of SUB consecutive sorted particles.
+__global__ void k_sub_boxes(int64_t n, int64_t nsub, const double4* __restrict__ spos,
+                            double4* __restrict__ lo, double4* __restrict__ hi) {
+  int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (l >= nsub) return;
+  int64_t a = l * SUB, b = min(a + SUB, n);
+  double4 mn = make_double4(1e308, 1e308, 1e308, 0.0), mx = make_double4(-1e308, -1e308, -1e308, 0.0);
+  for (int64_t k = a; k < b; ++k) {
+    double4 p = spos[k];
+    mn.x = fmin(mn.x, p.x);
+    mn.y = fmin(mn.y, p.y);
+    mn.z = fmin(mn.z, p.z);
+    mx.x = fmax(mx.x, p.x);
+    mx.y = fmax(mx.y, p.y);
+    mx.z = fmax(mx.z, p.z);
+    mn.w = fmax(mn.w, p.w);
+  }
+  lo[l] = mn;
+  hi[l] = mx;
+}
+
 __global__ void k_level_up(int64_t nchild, int64_t nparent, const double4* __restrict__ clo,
                            const double4* __restrict__ chi, double4* __restrict__ plo,
                            double4* __restrict__ phi) {
@@ -153,6 +176,124 @@ __device__ __forceinline__ double box_gap2(double4 alo, double4 ahi, double4 blo
   double gy = fmax(fmax(blo.y - ahi.y, alo.y - bhi.y), 0.0);
   double gz = fmax(fmax(blo.z - ahi.z, alo.z - bhi.z), 0.0);
   return gx * gx + gy * gy + gz * gz;
+}
+
+__device__ __forceinline__ double point_gap2(double x, double y, double z, double4 blo, double4 bhi) {
+  double gx = fmax(fmax(blo.x - x, x - bhi.x), 0.0);
+  double gy = fmax(fmax(blo.y - y, y - bhi.y), 0.0);
+  double gz = fmax(fmax(blo.z - z, z - bhi.z), 0.0);
+  return gx * gx + gy * gy + gz * gz;
+}
+
+// Warp per query leaf, as k_lists, but at each candidate leaf every lane tests its own search
+// sphere against the leaf's sub-leaves and queues the ones it reaches (shared memory, per lane,
+// in ascending order); the warp flushes the queues in lockstep, each lane walking its own
+// sub-leaves' particles.  Rows come out sorted as with k_lists.
+template <int PASS>
+__global__ void __launch_bounds__(NB_THREADS) k_lists_sub(int64_t n, int64_t nleaf, TreeView tv,
+                                                          const double4* __restrict__ slo,
+                                                          const double4* __restrict__ shi,
+                                                          const double4* __restrict__ spos,
+                                                          int64_t* __restrict__ counts,
+                                                          const int64_t* __restrict__ off,
+                                                          int32_t* __restrict__ idx, int* err) {
+  __shared__ int64_t stack_s[NB_THREADS / 32][STACK];
+  __shared__ int32_t queue_s[NB_THREADS / 32][QCAP][32];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int64_t leaf = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (leaf >= nleaf) return;  // warp-uniform
+  int64_t* stack = stack_s[wib];
+  int32_t(*queue)[32] = queue_s[wib];
+  int64_t k = leaf * LEAF + lane;
+  bool valid = k < n;
+  double4 me = valid ? spos[k] : make_double4(0, 0, 0, 0);
+  double ri = 2.0 * me.w;
+  double r2i = __dmul_rn(ri, ri);
+  const double4 qlo = tv.lo[leaf], qhi = tv.hi[leaf];
+  const double qh = qlo.w;
+  int64_t m = 0, base = 0, cap = 0;
+  if (PASS == 1 && valid) {
+    base = off[k];
+    cap = off[k + 1] - base;
+  }
+  int qn = 0;  // this lane's queued sub-leaves
+  auto flush = [&]() {
+    int qmax = qn;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) qmax = max(qmax, __shfl_xor_sync(0xffffffffu, qmax, o));
+    for (int t = 0; t < qmax; ++t) {
+      if (t < qn) {
+        int64_t sb = (int64_t)queue[t][lane] * SUB;
+        int64_t se = min(sb + SUB, n);
+        for (int64_t j = sb; j < se; ++j) {
+          double4 c = spos[j];
+          double d2 = d2_exact(c.x - me.x, c.y - me.y, c.z - me.z);
+          double rj = 2.0 * c.w;
+          if (d2 < r2i || d2 < __dmul_rn(rj, rj)) {
+            if (PASS == 1) {
+              if (m < cap)
+                idx[base + m] = (int32_t)j;
+              else
+                set_error(err, ERR_LIST_OVERFLOW);
+            }
+            m += 1;
+          }
+        }
+      }
+    }
+    __syncwarp();
+    qn = 0;
+  };
+  int sp = 0;
+  if (lane == 0) stack[0] = ((int64_t)(tv.nlevels - 1) << 40);
+  sp = 1;
+  __syncwarp();
+  while (sp > 0) {
+    int64_t e = stack[sp - 1];
+    __syncwarp();
+    sp -= 1;
+    int lvl = (int)(e >> 40);
+    int64_t node = e & ((1ll << 40) - 1);
+    if (lvl == 0) {
+      // candidate leaf: queue the sub-leaves this lane's sphere reaches
+      int64_t s0 = node * (LEAF / SUB);
+      int64_t s1 = min(s0 + LEAF / SUB, (n + SUB - 1) / SUB);
+      if (valid) {
+        for (int64_t sidx = s0; sidx < s1; ++sidx) {
+          double4 blo = slo[sidx], bhi = shi[sidx];
+          double reach = 2.0 * fmax(me.w, blo.w);
+          if (point_gap2(me.x, me.y, me.z, blo, bhi) < reach * reach * (1.0 + 1e-12))
+            queue[qn++][lane] = (int32_t)sidx;
+        }
+      }
+      if (__any_sync(0xffffffffu, qn > QCAP - LEAF / SUB)) flush();
+      continue;
+    }
+    int64_t c0 = node * FAN;
+    int64_t csize = tv.level_size[lvl - 1];
+    int64_t child = c0 + lane;
+    bool hit = false;
+    if (lane < FAN && child < csize) {
+      int64_t g = tv.level_off[lvl - 1] + child;
+      double4 blo = tv.lo[g], bhi = tv.hi[g];
+      double reach = 2.0 * fmax(qh, blo.w);
+      hit = box_gap2(qlo, qhi, blo, bhi) < reach * reach * (1.0 + 1e-12);
+    }
+    unsigned mask = __ballot_sync(0xffffffffu, hit);
+    int nh = __popc(mask);
+    if (sp + nh > STACK) {
+      set_error(err, ERR_TRAVERSAL_STACK);
+      break;
+    }
+    if (hit) {
+      int above = __popc(mask & ~((2u << lane) - 1u));
+      stack[sp + above] = ((int64_t)(lvl - 1) << 40) | child;
+    }
+    __syncwarp();
+    sp += nh;
+  }
+  flush();
+  if (PASS == 0 && valid) counts[k] = m;
 }
 
 // Warp per query leaf.  pass 0 counts each row's entries, pass 1 writes them.  Node entries on
@@ -308,9 +449,12 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
         E.node_hi + tv.level_off[l - 1], E.node_lo + tv.level_off[l], E.node_hi + tv.level_off[l]);
   tv.lo = E.node_lo;
   tv.hi = E.node_hi;
+  int64_t nsub = (n + SUB - 1) / SUB;
+  NB_TRY(E.ensure_sub(nsub));
+  count_launch(), k_sub_boxes<<<grid_for(nsub), NB_THREADS, 0, st>>>(n, nsub, L.spos, E.sub_lo, E.sub_hi);
   // count, scan, fill
   unsigned gb = grid_for(nleaf * 32);
-  count_launch(), k_lists<0><<<gb, NB_THREADS, 0, st>>>(n, nleaf, tv, L.spos, E.counts, nullptr, nullptr, E.d_err);
+  count_launch(), k_lists_sub<0><<<gb, NB_THREADS, 0, st>>>(n, nleaf, tv, E.sub_lo, E.sub_hi, L.spos, E.counts, nullptr, nullptr, E.d_err);
   NB_CUDA(cudaMemsetAsync(L.off, 0, sizeof(int64_t), st));
   tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, E.counts, L.off + 1, (int)n, st));
@@ -318,7 +462,7 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
   NB_CUDA(cudaMemcpyAsync(&total, L.off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   NB_CUDA(cudaStreamSynchronize(st));
   NB_TRY(E.ensure_list_capacity(total));
-  count_launch(), k_lists<1><<<gb, NB_THREADS, 0, st>>>(n, nleaf, tv, L.spos, nullptr, L.off, L.idx, E.d_err);
+  count_launch(), k_lists_sub<1><<<gb, NB_THREADS, 0, st>>>(n, nleaf, tv, E.sub_lo, E.sub_hi, L.spos, nullptr, L.off, L.idx, E.d_err);
   E.prof.end(PROF_LISTS, st, (double)n, (double)total);
   L.n = n;
   L.total = total;
