@@ -327,6 +327,29 @@ __global__ void k_combine_rows(int64_t nrows, const int64_t* __restrict__ rows, 
   vsig[i] = use_visc ? vsig_f[i] : cs[i];
 }
 
+// touched sets over Morton-ordered rows: pk holds sorted (x, y, z, h) of the current state; marks
+// go to the caller-order mask
+__global__ void k_mark_s(int64_t nrows, const int64_t* __restrict__ rows_s,
+                         const int32_t* __restrict__ perm, const int64_t* __restrict__ off,
+                         const int32_t* __restrict__ idx, int tight, const double4* __restrict__ pk,
+                         uint8_t* __restrict__ mark) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t k = rows_s[q];
+  mark[perm[k]] = 1;
+  double4 me = pk[k];
+  for (int64_t e = off[k]; e < off[k + 1]; ++e) {
+    int32_t js = idx[e];
+    if (tight) {
+      double4 o = pk[js];
+      double d2 = d2_exact(o.x - me.x, o.y - me.y, o.z - me.z);
+      double rr = 2.0 * fmax(me.w, o.w);
+      if (!(d2 < rr * rr)) continue;
+    }
+    mark[perm[js]] = 1;
+  }
+}
+
 // touched sets: mark the rows and their list entries (optionally only interacting pairs)
 __global__ void k_mark(int64_t nrows, const int64_t* __restrict__ rows,
                        const int32_t* __restrict__ perm, const int32_t* __restrict__ inv_perm,
@@ -413,7 +436,7 @@ int Workspace::ensure(Engine& E, int64_t n) {
   NB_CUDA(cudaMalloc((void**)&pk32, sizeof(float4) * c));
   float4** f4s[] = {&pf1, &pf2, &pf3};
   for (float4** p : f4s) NB_CUDA(cudaMalloc((void**)p, sizeof(float4) * c));
-  int64_t** i8[] = {&rows, &rows_s, &rows2, &iters, &flags, &need, &i_tmp, &pairs};
+  int64_t** i8[] = {&rows, &rows_s, &rows2, &iters, &flags, &need, &i_tmp, &pairs, &i_lvl, &i_tmp2};
   for (int64_t** p : i8) NB_CUDA(cudaMalloc((void**)p, sizeof(int64_t) * (c + 1)));
   uint8_t** u1[] = {&m_rows, &m_done, &m_need, &m_tmp, &m_x, &m_sorted};
   for (uint8_t** p : u1) NB_CUDA(cudaMalloc((void**)p, c));
@@ -449,7 +472,7 @@ void Workspace::release() {
   void* ps[] = {d_a, d_b, d_c, d_hg, d_hs, d_heff, d_hlim, d_disp, d_P, d_cs, d_vsig, d_ddudt,
                 d_dm, d_tmp, d_uh, v_flow, v_pred, v_eval, v_dacc, v_tmp, pk0, pk1, pk2, pk3, pk32,
                 pf1, pf2, pf3, m_x, m_sorted,
-                rows, rows_s, rows2, iters, flags, need, i_tmp, pairs, m_rows, m_done, m_need,
+                rows, rows_s, rows2, iters, flags, need, i_tmp, pairs, i_lvl, i_tmp2, m_rows, m_done, m_need,
                 m_tmp, i32a, i32b, dk_b, d_int, d_i64};
   for (void* p : ps)
     if (p) cudaFree(p);
@@ -634,12 +657,27 @@ int compute_density(Engine& E, int64_t n, const double* x, const double* mass, d
   return NB_ERR_SEARCH;
 }
 
-void mark_rows(Engine& E, int64_t nrows, const int64_t* rows, int tight, const double* x,
-               const double* h, uint8_t* mark, cudaStream_t st) {
-  if (nrows <= 0) return;
+int mark_rows(Engine& E, int64_t nrows, const int64_t* rows, int tight, const double* x,
+              const double* h, uint8_t* mark, cudaStream_t st) {
+  if (nrows <= 0) return 0;
   Lists& L = E.lists;
-  count_launch(), k_mark<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.perm, L.inv_perm, L.off, L.idx,
-                                                 tight, x, h, mark);
+  Workspace& W = E.ws;
+  int64_t n = L.n, ns = 0;
+  NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));
+  count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, h, W.pk0);
+  count_launch(), k_mark_s<<<grid_for(ns), NB_THREADS, 0, st>>>(ns, W.rows_s, L.perm, L.off, L.idx,
+                                                               tight, W.pk0, mark);
+  return 0;
+}
+
+int sorted_rows_and_pack(Engine& E, int64_t nrows, const int64_t* rows, const double* x,
+                         const double* h, int64_t* ns, cudaStream_t st) {
+  Lists& L = E.lists;
+  Workspace& W = E.ws;
+  int64_t n = L.n;
+  NB_TRY(rows_sorted(E, n, nrows, rows, ns, st));
+  count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, h, W.pk0);
+  return 0;
 }
 
 void mask_and_not(int64_t n, const uint8_t* a, const uint8_t* b, uint8_t* out, cudaStream_t st) {

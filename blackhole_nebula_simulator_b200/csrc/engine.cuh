@@ -52,7 +52,8 @@ struct Workspace {
   float4* pk32 = nullptr;
   float4 *pf1 = nullptr, *pf2 = nullptr, *pf3 = nullptr;  // FP32 packs of the force pass
   int64_t *rows = nullptr, *rows_s = nullptr, *rows2 = nullptr, *iters = nullptr,
-          *flags = nullptr, *need = nullptr, *i_tmp = nullptr, *pairs = nullptr;
+          *flags = nullptr, *need = nullptr, *i_tmp = nullptr, *pairs = nullptr,
+          *i_lvl = nullptr, *i_tmp2 = nullptr;
   uint8_t *m_rows = nullptr, *m_done = nullptr, *m_need = nullptr, *m_tmp = nullptr,
           *m_x = nullptr, *m_sorted = nullptr;
   int32_t *i32a = nullptr, *i32b = nullptr;

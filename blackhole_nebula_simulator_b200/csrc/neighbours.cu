@@ -54,14 +54,25 @@ __global__ void k_bbox_partial(int64_t n, const double* __restrict__ pos, double
 }
 
 __global__ void k_bbox_final(int nb, const double* __restrict__ part, double* __restrict__ box6) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  __shared__ double s[6][NB_THREADS];
   double r[6] = {1e308, 1e308, 1e308, -1e308, -1e308, -1e308};
-  for (int b = 0; b < nb; ++b)
+  for (int b = threadIdx.x; b < nb; b += blockDim.x)
     for (int c = 0; c < 3; ++c) {
       r[c] = fmin(r[c], part[6 * b + c]);
       r[3 + c] = fmax(r[3 + c], part[6 * b + 3 + c]);
     }
-  for (int c = 0; c < 6; ++c) box6[c] = r[c];
+  for (int c = 0; c < 6; ++c) s[c][threadIdx.x] = r[c];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int c = 0; c < 3; ++c) {
+        s[c][threadIdx.x] = fmin(s[c][threadIdx.x], s[c][threadIdx.x + w]);
+        s[3 + c][threadIdx.x] = fmax(s[3 + c][threadIdx.x], s[3 + c][threadIdx.x + w]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < 6; ++c) box6[c] = s[c][0];
 }
 
 // ---------------------------------------------------------------- Morton keys
@@ -419,7 +430,7 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
   // bounding box and Morton keys
   int nbb = (int)std::min<int64_t>(grid_for(n), 1184);
   count_launch(), k_bbox_partial<<<nbb, NB_THREADS, 0, st>>>(n, pos, E.bbox_part);
-  count_launch(), k_bbox_final<<<1, 32, 0, st>>>(nbb, E.bbox_part, E.bbox);
+  count_launch(), k_bbox_final<<<1, NB_THREADS, 0, st>>>(nbb, E.bbox_part, E.bbox);
   count_launch(), k_morton<<<grid_for(n), NB_THREADS, 0, st>>>(n, pos, E.bbox, E.keys_a, E.vals_a);
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceRadixSort::SortPairs(E.cub_tmp, tmp, E.keys_a, E.keys_b, E.vals_a, L.perm,

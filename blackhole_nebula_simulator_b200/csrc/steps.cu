@@ -68,7 +68,7 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
     count_launch(), k_fill_u8<<<grid_for(n), NB_THREADS, 0, st>>>(n, 1, W.m_need);
   } else {
     NB_CUDA(cudaMemsetAsync(W.m_need, 0, n, st));
-    mark_rows(E, nrows, rows, 0, s->x, s->h, W.m_need, st);
+    NB_TRY(mark_rows(E, nrows, rows, 0, s->x, s->h, W.m_need, st));
   }
   NB_CUDA(cudaMemsetAsync(W.m_done, 0, n, st));
   bool settled = false;
@@ -84,7 +84,7 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
     mask_or(n, W.m_need, W.m_done, st);
     // interacting neighbours of the rows at the current h
     NB_CUDA(cudaMemsetAsync(W.m_tmp, 0, n, st));
-    mark_rows(E, nrows, rows, 1, s->x, s->h, W.m_tmp, st);
+    NB_TRY(mark_rows(E, nrows, rows, 1, s->x, s->h, W.m_tmp, st));
     mask_and_not(n, W.m_tmp, W.m_done, W.m_need, st);
   }
   if (!settled) {
@@ -399,31 +399,52 @@ __global__ void k_wanted_levels(int64_t nrows, const int64_t* __restrict__ rows,
   level[i] = nw;
 }
 
-// one sweep of the level limiter over the rows' interacting pairs (sim/blocks.py:337-353); the
-// least fixed point above the start is unique, so in-place sweeps reach the reference's levels
-__global__ void k_limit_sweep(int64_t nrows, const int64_t* __restrict__ rows,
-                              const int32_t* __restrict__ perm, const int32_t* __restrict__ inv_perm,
+// one sweep of the level limiter over the rows' interacting pairs (sim/blocks.py:337-353), on
+// Morton-ordered rows with sorted (x, h) and a sorted copy of the levels; the least fixed point
+// above the start is unique, so in-place sweeps reach the reference's levels
+__global__ void k_limit_sweep(int64_t nrows, const int64_t* __restrict__ rows_s,
                               const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
-                              const double* __restrict__ x, const double* __restrict__ h,
-                              int64_t max_gap, int64_t* level, int* changed) {
+                              const double4* __restrict__ pk, int64_t max_gap, int64_t* level_s,
+                              int* changed) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= nrows) return;
-  int64_t i = rows[q];
-  int64_t k = inv_perm[i];
-  double xi0 = x[3 * i], xi1 = x[3 * i + 1], xi2 = x[3 * i + 2], hi = h[i];
-  int64_t need = ((volatile int64_t*)level)[i];
+  int64_t k = rows_s[q];
+  double4 me = pk[k];
+  int64_t need = ((volatile int64_t*)level_s)[k];
   for (int64_t e = off[k]; e < off[k + 1]; ++e) {
-    int64_t j = perm[idx[e]];
-    double d2 = d2_exact(x[3 * j] - xi0, x[3 * j + 1] - xi1, x[3 * j + 2] - xi2);
-    double rr = 2.0 * fmax(hi, h[j]);
+    int32_t js = idx[e];
+    double4 o = pk[js];
+    double d2 = d2_exact(o.x - me.x, o.y - me.y, o.z - me.z);
+    double rr = 2.0 * fmax(me.w, o.w);
     if (!(d2 < rr * rr)) continue;
-    int64_t lj = ((volatile int64_t*)level)[j];
+    int64_t lj = ((volatile int64_t*)level_s)[js];
     if (lj - max_gap > need) need = lj - max_gap;
   }
-  if (need > ((volatile int64_t*)level)[i]) {
-    atomicMax((long long*)&level[i], (long long)need);
+  if (need > ((volatile int64_t*)level_s)[k]) {
+    atomicMax((long long*)&level_s[k], (long long)need);
     *changed = 1;
   }
+}
+
+__global__ void k_gather_i64(int64_t n, const int32_t* __restrict__ perm, const int64_t* __restrict__ a,
+                             int64_t* __restrict__ out) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < n) out[k] = a[perm[k]];
+}
+
+__global__ void k_scatter_rows_i64(int64_t nrows, const int64_t* __restrict__ rows_s,
+                                   const int32_t* __restrict__ perm, const int64_t* __restrict__ a_s,
+                                   int64_t* __restrict__ a) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t k = rows_s[q];
+  a[perm[k]] = a_s[k];
+}
+
+__global__ void k_scatter_i64(int64_t n, const int32_t* __restrict__ perm, const int64_t* __restrict__ a_s,
+                              int64_t* __restrict__ a) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < n) a[perm[k]] = a_s[k];
 }
 
 // _land (sim/blocks.py:383-393) and the K_MAX check of _choose_levels
@@ -444,25 +465,24 @@ __global__ void k_land(int64_t nrows, const int64_t* __restrict__ rows, int64_t 
   level[i] = k;
 }
 
-// _wake_targets (sim/blocks.py:356-364): need[j] = max over active i of level_i - max_gap
-__global__ void k_wake_need(int64_t nrows, const int64_t* __restrict__ rows,
-                            const int32_t* __restrict__ perm, const int32_t* __restrict__ inv_perm,
+// _wake_targets (sim/blocks.py:356-364): need[j] = max over active i of level_i - max_gap, on
+// Morton-ordered rows into a sorted need array
+__global__ void k_wake_need(int64_t nrows, const int64_t* __restrict__ rows_s,
                             const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
-                            const double* __restrict__ x, const double* __restrict__ h,
-                            const int64_t* __restrict__ level, int64_t max_gap,
-                            int64_t* __restrict__ need) {
+                            const double4* __restrict__ pk, const int64_t* __restrict__ level_s,
+                            int64_t max_gap, int64_t* __restrict__ need_s) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= nrows) return;
-  int64_t i = rows[q];
-  int64_t k = inv_perm[i];
-  double xi0 = x[3 * i], xi1 = x[3 * i + 1], xi2 = x[3 * i + 2], hi = h[i];
-  long long v = (long long)(level[i] - max_gap);
+  int64_t k = rows_s[q];
+  double4 me = pk[k];
+  long long v = (long long)(level_s[k] - max_gap);
   for (int64_t e = off[k]; e < off[k + 1]; ++e) {
-    int64_t j = perm[idx[e]];
-    double d2 = d2_exact(x[3 * j] - xi0, x[3 * j + 1] - xi1, x[3 * j + 2] - xi2);
-    double rr = 2.0 * fmax(hi, h[j]);
+    int32_t js = idx[e];
+    double4 o = pk[js];
+    double d2 = d2_exact(o.x - me.x, o.y - me.y, o.z - me.z);
+    double rr = 2.0 * fmax(me.w, o.w);
     if (!(d2 < rr * rr)) continue;
-    atomicMax((long long*)&need[j], v);
+    atomicMax((long long*)&need_s[js], v);
   }
 }
 
@@ -527,13 +547,16 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
       prm->disc_alpha_av > 0 ? s->nu : nullptr, s->x, prm->courant, prm->c_force, prm->eta_orb,
       prm->cooling, s->u, s->rho, brems_of(prm), s->level_offset, s->level, E.d_err);
   NB_TRY(check_device_error(E, st));
+  int64_t ns = 0;
   if (prm->limiter) {
+    // Morton-ordered rows, sorted (x, h) and a sorted copy of the levels
+    NB_TRY(sorted_rows_and_pack(E, nrows, rows, s->x, s->h, &ns, st));
+    count_launch(), k_gather_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, W.i_lvl);
     bool settled = false;
     for (int sweep = 0; sweep < 4096; ++sweep) {
       NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
-      count_launch(), k_limit_sweep<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.perm, L.inv_perm, L.off,
-                                                            L.idx, s->x, s->h, prm->max_gap,
-                                                            s->level, W.d_int);
+      count_launch(), k_limit_sweep<<<grid_for(ns), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,
+                                                                         prm->max_gap, W.i_lvl, W.d_int);
       NB_CUDA(cudaMemcpyAsync(W.h_int, W.d_int, sizeof(int), cudaMemcpyDeviceToHost, st));
       NB_CUDA(cudaStreamSynchronize(st));
       if (W.h_int[0] == 0) {
@@ -542,14 +565,17 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
       }
     }
     if (!settled) return set_host_error(E, "level limiter did not settle");
+    count_launch(), k_scatter_rows_i64<<<grid_for(ns), NB_THREADS, 0, st>>>(ns, W.rows_s, L.perm, W.i_lvl, s->level);
   }
   count_launch(), k_land<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, s->tick_n, s->n_stop, s->level, E.d_err);
   NB_TRY(check_device_error(E, st));
   if (prm->limiter) {
-    count_launch(), k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, -1, W.need);
-    count_launch(), k_wake_need<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, L.perm, L.inv_perm, L.off,
-                                                        L.idx, s->x, s->h, s->level, prm->max_gap,
-                                                        W.need);
+    // levels after _land, sorted; need in sorted order, then back to the caller's order
+    count_launch(), k_gather_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, W.i_lvl);
+    count_launch(), k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, -1, W.i_tmp2);
+    count_launch(), k_wake_need<<<grid_for(ns), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,
+                                                                   W.i_lvl, prm->max_gap, W.i_tmp2);
+    count_launch(), k_scatter_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, W.i_tmp2, W.need);
     NB_CUDA(cudaMemsetAsync(W.d_i64, 0, sizeof(int64_t), st));
     count_launch(), k_cut_steps<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->tick_n, s->tick, W.need, s->a_hydro,
                                                     s->dudt, s->level, s->n_end, s->p_half,

@@ -29,8 +29,11 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
 int block_land(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st);
 
 // launchers of engine.cu kernels used by steps.cu
-void mark_rows(Engine& E, int64_t nrows, const int64_t* rows, int tight, const double* x,
-               const double* h, uint8_t* mark, cudaStream_t st);
+int mark_rows(Engine& E, int64_t nrows, const int64_t* rows, int tight, const double* x,
+              const double* h, uint8_t* mark, cudaStream_t st);
+// rows as ascending sorted positions in E.ws.rows_s (count ns) and E.ws.pk0 = sorted (x, h)
+int sorted_rows_and_pack(Engine& E, int64_t nrows, const int64_t* rows, const double* x,
+                         const double* h, int64_t* ns, cudaStream_t st);
 void mask_and_not(int64_t n, const uint8_t* a, const uint8_t* b, uint8_t* out, cudaStream_t st);
 void mask_or(int64_t n, const uint8_t* a, uint8_t* b, cudaStream_t st);
 
