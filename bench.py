@@ -205,6 +205,7 @@ def run_gpu(args, rank, world, precision=None, use_mlp=None, e2e=True):
     c = ctx(dev)
     stream = torch.cuda.current_stream()
     snap = snapshot_state(st)
+    led0 = blocks.ledger(st, bc)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -233,6 +234,7 @@ def run_gpu(args, rank, world, precision=None, use_mlp=None, e2e=True):
     else:
         total = float(psteps)
     led = blocks.ledger(st, bc)
+    led["drift"] = (led["energy"] - led0["energy"]) / led0["abs_h"]
     mlp = cooling.mlp_stats(reset=True) if use_mlp else None
     e2e_out = run_e2e(args, st, bc, snap) if e2e else None
     return ms, total, prof, clk.summary(), st, led, e2e_out, mlp
@@ -332,7 +334,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     n_full = args.n or {"torus": 4_194_304, "streams": 1_048_576, "cloud": 262_144}[args.workload]
     config = {"workload": f"{args.workload}, {n_full} particles, block time steps",
-              "particles": n_full, "precision": args.precision, "l2_flush": "inputs larger than L2",
+              "particles": n_full,
+              "precision": args.precision if args.impl == "ours" else "fp64 (CPU oracle)",
+              "l2_flush": "inputs larger than L2",
               "parallelism": f"replicas x{world}"}  # fmt: skip
     metric = "particle-steps/s"
     if args.impl == "reference":
@@ -354,10 +358,11 @@ def main():
     plain = None
     if args.precision == "fp32" and not args.no_plain:
         # the comparison form of the metric: FP64 pair arithmetic with the exact integrator
-        p_ms, p_total, p_prof, p_clk, p_st, _, _, _ = run_gpu(args, rank, world, "fp64", False,
-                                                              e2e=False)  # fmt: skip
+        p_ms, p_total, p_prof, p_clk, p_st, p_led, _, _ = run_gpu(args, rank, world, "fp64", False,
+                                                                  e2e=False)  # fmt: skip
         plain = {"value": p_total / (p_ms * 1e-3), "unit": "particle-steps/s",
                  "ms_per_step": p_ms / args.steps, "dtype": "f64", "cooling": "exact integrator",
+                 "energy_rel_drift_timed": p_led["drift"],
                  "kernel_ms": {k: round(v["ms"], 3) for k, v in p_prof.items()
                                if not k.startswith("_")}}  # fmt: skip
     if rank == 0:
@@ -381,6 +386,7 @@ def main():
             "cooling": ("network (BF16 tensor cores, exact fallback)" if mlp is not None
                         else "exact integrator"),
             "cooling_network": mlp,
+            "energy_rel_drift_timed": led["drift"],
             "fp64_plain": plain,
             "speedup_vs_fp64_plain": (total / (ms * 1e-3)) / plain["value"] if plain else None,
         }  # fmt: skip

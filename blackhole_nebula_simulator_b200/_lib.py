@@ -83,6 +83,7 @@ _SIGS = {
     "nb_disc_forces": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _dbl, _vp, _vp,
                               _i64, _vp, _int, _vp, _vp, _vp]),
     "nb_glf_step_many": (_int, [_vp, _i64, _vp, _vp, _vp, _dbl, _vp, _vp, _vp, _vp]),
+    "nb_integrate_orbit": (_int, [_vp, _int, _vp, _dbl, _dbl, _i64, _i64, _vp, _vp, _vp, _vp, _vp]),
     "nb_gn_v_from_p": (_int, [_vp, _i64, _vp, _vp, _vp, _vp]),
     "nb_gn_p_from_v": (_int, [_vp, _i64, _vp, _vp, _vp, _vp]),
     "nb_beta_cool": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -272,6 +272,18 @@ int nb_glf_step_many(nb_ctx* ctx, int64_t n, const double* x, const double* p, c
   return w == -1 ? NB_ERR_GLF_P_HALF : w == -2 ? NB_ERR_GLF_X1 : NB_ERR_GLF_RADIUS;
 }
 
+int nb_integrate_orbit(nb_ctx* ctx, int norb, const double* state0, double dt_max, double eta,
+                       int64_t n_end, int64_t max_records, double* t_out, double* s_out,
+                       int64_t* it_out, int64_t* nrec, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  nbk::launch_integrate_orbit(norb, state0, dt_max, eta, n_end, max_records, t_out, s_out, it_out,
+                              nrec, S(stream));
+  NB_CUDA(cudaGetLastError());
+  NB_CUDA(cudaStreamSynchronize(S(stream)));
+  return 0;
+}
+
 int nb_gn_v_from_p(nb_ctx* ctx, int64_t n, const double* x, const double* p, double* v, void* stream) {
   NB_TRY(begin(ctx));
   Engine& E = ctx->E;

@@ -99,6 +99,85 @@ __global__ void k_sum_partials(int nb, int terms, const double* __restrict__ par
   out[t] = s;
 }
 
+// Orbit level (sim/integrator.py:201-210): smallest k with dt_max / 2^k <= eta r^1.5 (K_MAX + 1
+// when none), halving dt_max like the reference so the same k comes out.
+__device__ __forceinline__ int orbit_level(double r, double eta, double dt_max) {
+  double target = eta * pow(r, 1.5);
+  double dt = dt_max;
+  int k = 0;
+  while (dt > target && k <= 40) {
+    dt *= 0.5;
+    k += 1;
+  }
+  return k;
+}
+
+// One orbit per thread on the integer tick timeline (tick = dt_max / 2^40) until tick n_end,
+// recording every step (sim/integrator.py:220-253).  eta > 0: quantized adaptive steps; else
+// fixed dt_max.  nrec[o] = records, or a negative failure code (-1/-2/-3 GLF, -4 level, -5 full).
+__global__ void k_integrate_orbit(int norb, const double* __restrict__ state0, double dt_max,
+                                  double eta, int64_t n_end, int64_t max_records,
+                                  double* __restrict__ t_out, double* __restrict__ s_out,
+                                  int64_t* __restrict__ it_out, int64_t* __restrict__ nrec) {
+  int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= norb) return;
+  const double tick = dt_max / 1099511627776.0;  // 2^40
+  double x[3] = {state0[6 * o], state0[6 * o + 1], state0[6 * o + 2]};
+  double p[3] = {state0[6 * o + 3], state0[6 * o + 4], state0[6 * o + 5]};
+  double* T = t_out + (int64_t)o * max_records;
+  double* S = s_out + (int64_t)o * max_records * 6;
+  int64_t* I = it_out + (int64_t)o * max_records;
+  int64_t n = 0, m = 0;
+  T[0] = 0.0;
+  for (int c = 0; c < 3; ++c) {
+    S[c] = x[c];
+    S[3 + c] = p[c];
+  }
+  I[0] = 0;
+  while (n < n_end) {
+    if (m + 1 >= max_records) {
+      nrec[o] = -5;
+      return;
+    }
+    int k = 0;
+    if (eta > 0.0) k = orbit_level(sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]), eta, dt_max);
+    while (k <= 40 && ((int64_t)1 << (40 - k)) > n_end - n) k += 1;  // never past the end
+    if (k > 40) {
+      nrec[o] = -4;
+      return;
+    }
+    int64_t steps = (int64_t)1 << (40 - k);
+    double xo[3], po[3];
+    int it = glf_one(x, p, dt_max / (double)((int64_t)1 << k), xo, po);
+    if (it < 0) {
+      nrec[o] = it;
+      return;
+    }
+    for (int c = 0; c < 3; ++c) {
+      x[c] = xo[c];
+      p[c] = po[c];
+    }
+    n += steps;
+    m += 1;
+    T[m] = (double)n * tick;
+    for (int c = 0; c < 3; ++c) {
+      S[6 * m + c] = x[c];
+      S[6 * m + 3 + c] = p[c];
+    }
+    I[m] = it;
+  }
+  nrec[o] = m + 1;
+}
+
+void launch_integrate_orbit(int norb, const double* state0, double dt_max, double eta,
+                            int64_t n_end, int64_t max_records, double* t_out, double* s_out,
+                            int64_t* it_out, int64_t* nrec, cudaStream_t st) {
+  if (norb > 0)
+    count_launch(), k_integrate_orbit<<<(norb + 63) / 64, 64, 0, st>>>(norb, state0, dt_max, eta, n_end,
+                                                                     max_records, t_out, s_out,
+                                                                     it_out, nrec);
+}
+
 void launch_glf(int64_t n, const double* x, const double* p, const double* dt, double dt_scalar,
                 double* xo, double* po, int64_t* iters, cudaStream_t st) {
   if (n > 0)

@@ -86,6 +86,9 @@ __device__ __forceinline__ int glf_one(const double x[3], const double p[3], dou
 
 void launch_glf(int64_t n, const double* x, const double* p, const double* dt, double dt_scalar,
                 double* xo, double* po, int64_t* iters, cudaStream_t st);
+void launch_integrate_orbit(int norb, const double* state0, double dt_max, double eta,
+                            int64_t n_end, int64_t max_records, double* t_out, double* s_out,
+                            int64_t* it_out, int64_t* nrec, cudaStream_t st);
 void launch_v_from_p(int64_t n, const double* x, const double* p, double* v, cudaStream_t st);
 void launch_p_from_v(int64_t n, const double* x, const double* v, double* p, cudaStream_t st);
 int ledger_blocks(int64_t n);

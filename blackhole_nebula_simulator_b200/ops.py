@@ -182,6 +182,49 @@ def glf_step_many(x, p, dt):
     return x1, p1, it
 
 
+@dataclass
+class Orbit:
+    """A recorded orbit (sim/integrator.py:256-264): times, positions, momenta, iterations."""
+
+    t: object
+    x: object
+    p: object
+    iterations: object
+
+
+def integrate_orbit(x0, p0, t_end, *, eta=None, dt=None, dt_max=4096.0, max_records=5_000_000):
+    """sim/integrator.py:267-298: one particle from t = 0 to t_end with the generalized leapfrog
+    on the integer tick timeline (adaptive quantized steps with eta, or fixed dt).  Returns NumPy
+    arrays like the reference; raises GLFConvergenceError / ValueError like it."""
+    import numpy as np
+
+    if (eta is None) == (dt is None):
+        raise ValueError("give exactly one of eta (adaptive) or dt (fixed)")
+    if dt is not None:
+        dt_max, eta = float(dt), 0.0
+    tick = dt_max / 2.0**40
+    n_end = int(round(t_end / tick))
+    s0 = dev_f64(np.concatenate([np.asarray(x0, float), np.asarray(p0, float)]))
+    d = s0.device
+    t = torch.empty(max_records, dtype=torch.float64, device=d)
+    s = torch.empty((max_records, 6), dtype=torch.float64, device=d)
+    it = torch.empty(max_records, dtype=torch.int64, device=d)
+    nrec = torch.empty(1, dtype=torch.int64, device=d)
+    _call("nb_integrate_orbit", 1, ptr(s0), float(dt_max), float(eta), n_end, int(max_records),
+          ptr(t), ptr(s), ptr(it), ptr(nrec), stream())  # fmt: skip
+    m = int(nrec.item())
+    if m == -5:
+        raise ValueError(f"more than max_records={max_records} steps; raise max_records")
+    if m < 0:
+        msg = {-1: "stage 1 (p_half) did not converge in 10 iterations: time step too large",
+               -2: "stage 2 (x1) did not converge in 10 iterations: time step too large",
+               -3: "particle inside r = 2.5",
+               -4: "time step would need more than 40 halvings of dt_max"}[m]  # fmt: skip
+        raise GLFConvergenceError(msg)
+    s = s[:m].cpu().numpy()
+    return Orbit(t[:m].cpu().numpy(), s[:, :3].copy(), s[:, 3:].copy(), it[:m].cpu().numpy())
+
+
 def gn_v_from_p(x, p):
     """sim/fastphys.py:35-42: v = A p + C (p.x) x."""
     x = dev_f64(x)

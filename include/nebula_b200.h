@@ -141,6 +141,15 @@ NB_API int nb_disc_forces(nb_ctx* ctx, int64_t n, const double* pos, const doubl
 NB_API int nb_glf_step_many(nb_ctx* ctx, int64_t n, const double* x, const double* p, const double* dt,
                      double dt_scalar, double* x1, double* p1, int64_t* iters, void* stream);
 
+/* integrate_orbit (sim/integrator.py:220-298): norb test-particle orbits (state0: norb x 6 = x, p)
+ * on the tick timeline (tick = dt_max / 2^40) to tick n_end, one GLF step per record; eta > 0:
+ * quantized adaptive steps eta r^1.5, else fixed dt_max.  Outputs per orbit o at offset
+ * o * max_records: t_out, s_out (x 6), it_out; nrec[o] = records or a negative code (-1/-2/-3 GLF
+ * failures, -4 level beyond K_MAX, -5 max_records too small). */
+NB_API int nb_integrate_orbit(nb_ctx* ctx, int norb, const double* state0, double dt_max, double eta,
+                              int64_t n_end, int64_t max_records, double* t_out, double* s_out,
+                              int64_t* it_out, int64_t* nrec, void* stream);
+
 /* gn_v_from_p_nb (sim/fastphys.py:35-42) and gn_p_from_v (physics/gravity.py:66-77). */
 NB_API int nb_gn_v_from_p(nb_ctx* ctx, int64_t n, const double* x, const double* p, double* v, void* stream);
 NB_API int nb_gn_p_from_v(nb_ctx* ctx, int64_t n, const double* x, const double* v, double* p, void* stream);

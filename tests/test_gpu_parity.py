@@ -237,3 +237,42 @@ def test_fp32_pair_arithmetic_within_stated_tolerance(nb):
     check("fp32 acc", _np(a.a_hydro) / amax, _np(b.a_hydro) / amax, atol=1e-3, per_vector=True)
     scale = np.abs(_np(a.dudt)).max()
     check("fp32 dudt", _np(a.dudt) / scale, _np(b.dudt) / scale, atol=1e-3)
+
+
+def _pericentres(t, x):
+    """Pericentre passages refined by parabolas through the three samples around each minimum
+    of r (the method of the reference's analysis/orbit_metrics.py:12-30)."""
+    r = np.linalg.norm(x, axis=1)
+    phi = np.unwrap(np.arctan2(x[:, 1], x[:, 0]))
+    idx = np.where((r[1:-1] < r[:-2]) & (r[1:-1] <= r[2:]))[0] + 1
+    times, angles = [], []
+    for i in idx:
+        sl = slice(i - 1, i + 2)
+        c = np.polyfit(t[sl], r[sl], 2)
+        tp = -c[1] / (2 * c[0])
+        times.append(tp)
+        angles.append(np.polyval(np.polyfit(t[sl] - tp, phi[sl], 2), 0.0))
+    return np.array(times), np.array(angles)
+
+
+def test_gn_orbit_precession_and_conservation(nb):
+    """The reference's orbit test (tests/sim/test_integrator.py:95-122, expected values of
+    reference/expected-values.md): cloud orbit r_p = 25, r_a = 5,000, eta = 0.00125, 3 radial
+    periods; first pericentre 396,223.627 and period 792,447.254 (rtol 1e-5), precession
+    24.0398 deg per orbit (atol 0.01 deg), |dH/H| < 1e-4, |dL/L| < 1e-12."""
+    ops = nb[0]
+    from blackhole_nebula_simulator_b200 import ics
+    from oracle import steps as osteps
+
+    x0, v0, p0 = ics.apocentre_state(25.0, 5000.0)
+    orb = ops.integrate_orbit(x0, p0, 3 * 792_447.254, eta=0.00125)
+    tp, phi = _pericentres(orb.t, orb.x)
+    check("pericentres found", 3, len(tp))
+    check("first pericentre time", 396_223.627, tp[0], rtol=1e-5)
+    check("radial periods", np.full(2, 792_447.254), np.diff(tp), rtol=1e-5)
+    check("precession per orbit (deg)", np.full(2, 24.0398), np.degrees(np.diff(phi) - 2 * np.pi),
+          atol=0.01)  # fmt: skip
+    H = osteps.gn_hamiltonian(orb.x, orb.p)
+    L = np.linalg.norm(np.cross(orb.x, orb.p), axis=1)
+    check("max |dH/H|", 0.0, np.max(np.abs(H / H[0] - 1)), atol=1e-4)
+    check("max |dL/L|", 0.0, np.max(np.abs(L / L[0] - 1)), atol=1e-12)
