@@ -248,8 +248,8 @@ def _pericentres(t, x):
     times, angles = [], []
     for i in idx:
         sl = slice(i - 1, i + 2)
-        c = np.polyfit(t[sl], r[sl], 2)
-        tp = -c[1] / (2 * c[0])
+        a, b, _ = np.polyfit(t[sl] - t[i], r[sl], 2)
+        tp = t[i] - b / (2.0 * a)
         times.append(tp)
         angles.append(np.polyval(np.polyfit(t[sl] - tp, phi[sl], 2), 0.0))
     return np.array(times), np.array(angles)
