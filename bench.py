@@ -49,6 +49,13 @@ def peaks():
     return {**PEAKS_FALLBACK, "source": "fallback"}
 
 
+# Disc viscosity of the torus: alpha_AV = 1, the value of the reference's own disc-viscosity block
+# test.  It gives alpha_SS = alpha_AV <h> / (10 H) (physics/disc_viscosity.py:56-58) with H = 15 M;
+# alpha_SS = 0.1 would need alpha_AV = 10 alpha_SS H / <h> ~ 16 at 4,194,304 particles
+# (<h> ~ 0.93 M), where a few particles heat without bound within ten system steps in FP64 and
+# FP32 alike under the reference's viscous step limit 0.25 h^2 / nu.
+TORUS_ALPHA_AV = 1.0
+TORUS_SCALE_HEIGHT = 15.0
 WEIGHTS = os.path.join(ROOT, "blackhole_nebula_simulator_b200", "data", "cooling_mlp.npy")
 
 
@@ -73,8 +80,7 @@ def workload(name: str, n: int | None, precision: str, seed_shift: int = 0, mlp=
     if name == "torus":
         n = n or 4_194_304
         ic = ics.torus(n, seed=4 + seed_shift)
-        alpha_av = 10.0 * 0.1 * 15.0 / float(np.mean(ic.h))  # alpha_SS = 0.1, H = sigma = 15
-        hc = HydroConfig(disc_alpha_av=alpha_av, **common)
+        hc = HydroConfig(disc_alpha_av=TORUS_ALPHA_AV, **common)
         bc = BlockConfig(coupled=CoupledConfig(hydro=hc, cooling="brems", cooling_mlp=mlp),
                          dt_max=256.0)  # fmt: skip
     elif name == "streams":
@@ -199,7 +205,7 @@ def run_gpu(args, rank, world, precision=None, use_mlp=None, e2e=True):
     use_mlp = (precision == "fp32") if use_mlp is None else use_mlp
     net = cooling_network() if use_mlp else None
     ic, bc = workload(args.workload, args.n, precision, seed_shift=rank, mlp=net)
-    st = blocks.initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=1e12)
+    st = blocks.initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=bc.dt_max * 2.0**20)
     led_init = blocks.ledger(st, bc)  # every particle is at a step boundary here
     for _ in range(args.warmup):
         blocks.advance(st, bc)
@@ -312,7 +318,7 @@ def cpu_reference(args, steps, warmup, sample_n=None):
     n_full = {"torus": 4_194_304, "streams": 1_048_576, "cloud": 262_144}[args.workload]
     n = sample_n or min(args.n or n_full, 32_768)
     ic, bc = workload(args.workload, n, "fp64")
-    st = osteps.blocks_initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=1e12)
+    st = osteps.blocks_initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=bc.dt_max * 2.0**20)
     for _ in range(warmup):
         osteps.blocks_advance(st, bc)
     s0 = st.particle_steps
@@ -347,6 +353,9 @@ def main():
               "precision": args.precision if args.impl == "ours" else "fp64 (CPU oracle)",
               "l2_flush": "inputs larger than L2",
               "parallelism": f"replicas x{world}"}  # fmt: skip
+    if args.workload == "torus":
+        config["disc_alpha_av"] = TORUS_ALPHA_AV
+        config["scale_height"] = TORUS_SCALE_HEIGHT
     metric = "particle-steps/s"
     if args.impl == "reference":
         if rank != 0:
@@ -392,6 +401,8 @@ def main():
             "pairs_per_force_row": (prof["forces"]["pairs"] / prof["forces"]["units"]
                                     if prof["forces"]["units"] else None),
             "h_stats": h_stats(st),
+            "disc_alpha_ss": (TORUS_ALPHA_AV * float(st.h.mean()) / (10.0 * TORUS_SCALE_HEIGHT)
+                              if args.workload == "torus" else None),
             "cooling": ("network (BF16 tensor cores, exact fallback)" if mlp is not None
                         else "exact integrator"),
             "cooling_network": mlp,

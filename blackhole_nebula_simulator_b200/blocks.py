@@ -124,6 +124,8 @@ def initialise(x, v, u, mass, h_guess, cfg: BlockConfig, t_stop: float, t0: floa
     p = ops.gn_p_from_v(x, dev_f64(v))
     u = dev_f64(u, (n,)).clone()
     tick = cfg.dt_max / 2.0**K_MAX
+    if (t_stop - t0) / tick >= 2.0**62:
+        raise ValueError("t_stop - t0 exceeds 2^62 ticks of dt_max / 2^40 (int64 tick timeline)")
     st = BlockState(
         n=0, t0=t0, tick=tick, level=zi(), n_beg=zi(), n_end=zi(), x_beg=x.clone(),
         p_half=p.clone(), u_half=u.clone(), x=x.clone(), p=p, u=u,

@@ -50,6 +50,8 @@ int Engine::ensure_n(int64_t n) {
     NB_CUDA(cudaMallocHost((void**)&h_err, sizeof(int) * 4));
     NB_CUDA(cudaMalloc((void**)&bbox, sizeof(double) * 8));
     NB_CUDA(cudaMallocHost((void**)&h_red, sizeof(double) * 64));
+    NB_CUDA(cudaMalloc((void**)&d_rowmax, 2 * sizeof(unsigned long long)));
+    NB_CUDA(cudaMallocHost((void**)&h_build, sizeof(int64_t) * 2));
     NB_CUDA(cudaEventCreate(&prof.a));
     NB_CUDA(cudaEventCreate(&prof.b));
   }
@@ -107,6 +109,11 @@ int Engine::ensure_list_capacity(int64_t m) {
   return 0;
 }
 
+int Engine::ensure_ell(int64_t m) {
+  Engine& E = *this;
+  return grow(E, ell, cap_ell, m);
+}
+
 int Engine::ensure_sort_keys(int64_t m) {
   Engine& E = *this;
   NB_TRY(grow(E, sort_keys, cap_sort, m));
@@ -116,10 +123,11 @@ int Engine::ensure_sort_keys(int64_t m) {
 void Engine::release() {
   void* ps[] = {d_err, bbox, bbox_part, keys_a, keys_b, vals_a, counts, node_lo, node_hi, sub_lo, sub_hi,
                 cub_tmp, sort_keys, red, lists.perm, lists.inv_perm, lists.spos, lists.off,
-                lists.idx};
+                lists.idx, ell, d_rowmax};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (h_err) cudaFreeHost(h_err);
+  if (h_build) cudaFreeHost(h_build);
   if (h_red) cudaFreeHost(h_red);
   ws.release();
 }

@@ -113,6 +113,11 @@ struct Engine {
   void* cub_tmp = nullptr;
   size_t cub_bytes = 0;
   int64_t* sort_keys = nullptr;
+  // one-pass list build: rows written to fixed-width slots (row_cap entries each), then packed
+  int32_t* ell = nullptr;
+  int64_t cap_ell = 0, row_cap = 256;
+  unsigned long long* d_rowmax = nullptr;
+  int64_t* h_build = nullptr;  // pinned: total entries and longest row of the last build
   double* red = nullptr;      // reduction partials (doubles)
   double* h_red = nullptr;    // pinned host copy of small reductions
   Lists lists;
@@ -124,6 +129,7 @@ struct Engine {
   int ensure_sub(int64_t m);
   int ensure_list_capacity(int64_t m);
   int ensure_sort_keys(int64_t m);
+  int ensure_ell(int64_t m);
   int ensure_cub(size_t bytes);
   void release();
 };

@@ -23,6 +23,9 @@ static constexpr int SUB = 8;  // sub-leaf: the unit each lane tests its own sph
 static constexpr int FAN = 8;
 static constexpr int STACK = 96;
 static constexpr int QCAP = 24;  // sub-leaves a lane queues before the warp flushes
+// entries of the fixed-width row scratch of the one-pass build (int32, 16 GiB); larger builds
+// count first and fill second
+static constexpr double ELL_MAX_ENTRIES = 4.0 * 1024 * 1024 * 1024;
 
 // ---------------------------------------------------------------- bounding box
 __global__ void k_bbox_partial(int64_t n, const double* __restrict__ pos, double* __restrict__ part) {
@@ -196,23 +199,33 @@ __device__ __forceinline__ double point_gap2(double x, double y, double z, doubl
   return gx * gx + gy * gy + gz * gz;
 }
 
-// Warp per query leaf, as k_lists, but at each candidate leaf every lane tests its own search
-// sphere against the leaf's sub-leaves and queues the ones it reaches (shared memory, per lane,
-// in ascending order); the warp flushes the queues in lockstep, each lane walking its own
-// sub-leaves' particles.  Rows come out sorted as with k_lists.
+// Warp per query leaf.  The warp walks the tree of boxes with an explicit stack in shared memory
+// (entries (level << 40) | index; children pushed highest first, so candidate leaves are reached
+// in ascending order).  At each candidate leaf every lane tests its own search sphere against the
+// leaf's sub-leaves and queues the ones it reaches (shared memory, per lane, in ascending order);
+// the warp flushes the queues in lockstep, each lane walking its own sub-leaves' particles, so
+// every row comes out sorted.
+// PASS 0 counts each row's entries; PASS 1 writes them at off[k]; PASS 2 writes them into a
+// fixed-width slot of row_cap entries at k * row_cap, counts them, and records the longest row.
 template <int PASS>
-__global__ void __launch_bounds__(NB_THREADS) k_lists_sub(int64_t n, int64_t nleaf, TreeView tv,
+__global__ void __launch_bounds__(NB_THREADS) k_lists_sub(int64_t n, int64_t nwork,
+                                                          const uint64_t* __restrict__ leaves,
+                                                          TreeView tv,
                                                           const double4* __restrict__ slo,
                                                           const double4* __restrict__ shi,
                                                           const double4* __restrict__ spos,
                                                           int64_t* __restrict__ counts,
                                                           const int64_t* __restrict__ off,
-                                                          int32_t* __restrict__ idx, int* err) {
+                                                          int32_t* __restrict__ idx,
+                                                          int64_t row_cap,
+                                                          unsigned long long* __restrict__ rowmax,
+                                                          int* err) {
   __shared__ int64_t stack_s[NB_THREADS / 32][STACK];
   __shared__ int32_t queue_s[NB_THREADS / 32][QCAP][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  int64_t leaf = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  if (leaf >= nleaf) return;  // warp-uniform
+  int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (w >= nwork) return;  // warp-uniform
+  int64_t leaf = leaves ? (int64_t)leaves[w] : w;  // all leaves, or the listed ones
   int64_t* stack = stack_s[wib];
   int32_t(*queue)[32] = queue_s[wib];
   int64_t k = leaf * LEAF + lane;
@@ -226,6 +239,10 @@ __global__ void __launch_bounds__(NB_THREADS) k_lists_sub(int64_t n, int64_t nle
   if (PASS == 1 && valid) {
     base = off[k];
     cap = off[k + 1] - base;
+  }
+  if (PASS == 2) {
+    base = k * row_cap;
+    cap = row_cap;
   }
   int qn = 0;  // this lane's queued sub-leaves
   auto flush = [&]() {
@@ -246,6 +263,8 @@ __global__ void __launch_bounds__(NB_THREADS) k_lists_sub(int64_t n, int64_t nle
                 idx[base + m] = (int32_t)j;
               else
                 set_error(err, ERR_LIST_OVERFLOW);
+            } else if (PASS == 2) {
+              if (m < cap) idx[base + m] = (int32_t)j;  // longer rows are redone wider
             }
             m += 1;
           }
@@ -304,97 +323,35 @@ __global__ void __launch_bounds__(NB_THREADS) k_lists_sub(int64_t n, int64_t nle
     sp += nh;
   }
   flush();
-  if (PASS == 0 && valid) counts[k] = m;
+  if (PASS != 1 && valid) counts[k] = m;
+  if (PASS == 2) {
+    unsigned mx = __reduce_max_sync(0xffffffffu, valid ? (unsigned)m : 0u);
+    if (lane == 0) atomicMax(rowmax, (unsigned long long)mx);
+  }
 }
 
-// Warp per query leaf.  pass 0 counts each row's entries, pass 1 writes them.  Node entries on
-// the stack are (level << 40) | index; children are pushed highest first so leaves are reached in
-// ascending order, which keeps every row sorted.
-template <int PASS>
-__global__ void __launch_bounds__(NB_THREADS) k_lists(int64_t n, int64_t nleaf, TreeView tv,
-                                                      const double4* __restrict__ spos,
-                                                      int64_t* __restrict__ counts,
-                                                      const int64_t* __restrict__ off,
-                                                      int32_t* __restrict__ idx, int* err) {
-  __shared__ int64_t stack_s[NB_THREADS / 32][STACK];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  int64_t leaf = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  if (leaf >= nleaf) return;  // warp-uniform
-  int64_t* stack = stack_s[wib];
-  int64_t k = leaf * LEAF + lane;
-  bool valid = k < n;
-  double4 me = valid ? spos[k] : make_double4(0, 0, 0, 0);
-  double ri = 2.0 * me.w;
-  double r2i = __dmul_rn(ri, ri);
-  const double4 qlo = tv.lo[leaf], qhi = tv.hi[leaf];
-  const double qh = qlo.w;
-  int64_t m = 0, base = 0, cap = 0;
-  if (PASS == 1 && valid) {
-    base = off[k];
-    cap = off[k + 1] - base;
-  }
-  int sp = 0;
-  if (lane == 0) stack[0] = ((int64_t)(tv.nlevels - 1) << 40);
-  sp = 1;
-  __syncwarp();
-  while (sp > 0) {
-    int64_t e = stack[sp - 1];
-    __syncwarp();
-    sp -= 1;
-    int lvl = (int)(e >> 40);
-    int64_t node = e & ((1ll << 40) - 1);
-    if (lvl == 0) {
-      // candidate leaf: lanes load its particles, every query lane tests all of them
-      int64_t cb = node * LEAF;
-      int64_t kk = cb + lane;
-      double4 c = kk < n ? spos[kk] : make_double4(0, 0, 0, 0);
-      int cnt = (int)min((int64_t)LEAF, n - cb);
-      for (int t = 0; t < cnt; ++t) {
-        double cx = __shfl_sync(0xffffffffu, c.x, t);
-        double cy = __shfl_sync(0xffffffffu, c.y, t);
-        double cz = __shfl_sync(0xffffffffu, c.z, t);
-        double ch = __shfl_sync(0xffffffffu, c.w, t);
-        if (!valid) continue;
-        double d2 = d2_exact(cx - me.x, cy - me.y, cz - me.z);
-        double rj = 2.0 * ch;
-        if (d2 < r2i || d2 < __dmul_rn(rj, rj)) {
-          if (PASS == 1) {
-            if (m < cap)
-              idx[base + m] = (int32_t)(cb + t);
-            else
-              set_error(err, ERR_LIST_OVERFLOW);
-          }
-          m += 1;
-        }
-      }
-      continue;
-    }
-    // internal node: lanes 0..FAN-1 test one child each against the query leaf's box
-    int64_t c0 = node * FAN;
-    int64_t csize = tv.level_size[lvl - 1];
-    int64_t child = c0 + lane;
-    bool hit = false;
-    if (lane < FAN && child < csize) {
-      int64_t g = tv.level_off[lvl - 1] + child;
-      double4 blo = tv.lo[g], bhi = tv.hi[g];
-      double reach = 2.0 * fmax(qh, blo.w);
-      hit = box_gap2(qlo, qhi, blo, bhi) < reach * reach * (1.0 + 1e-12);
-    }
-    unsigned mask = __ballot_sync(0xffffffffu, hit);
-    int nh = __popc(mask);
-    if (sp + nh > STACK) {
-      set_error(err, ERR_TRAVERSAL_STACK);
-      break;
-    }
-    if (hit) {
-      // highest child first on the stack: its position counts the set bits above this lane
-      int above = __popc(mask & ~((2u << lane) - 1u));
-      stack[sp + above] = ((int64_t)(lvl - 1) << 40) | child;
-    }
-    __syncwarp();
-    sp += nh;
-  }
-  if (PASS == 0 && valid) counts[k] = m;
+// Pack the fixed-width rows into CSR: warp per row, coalesced on both sides.  Rows longer than
+// the width are left to the CSR pass over their leaves.
+__global__ void k_pack_rows(int64_t n, int64_t row_cap, const int32_t* __restrict__ ell,
+                            const int64_t* __restrict__ off, int32_t* __restrict__ idx) {
+  int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (k >= n) return;
+  int64_t b = off[k], cnt = off[k + 1] - b;
+  if (cnt > row_cap) return;
+  const int32_t* src = ell + k * row_cap;
+  for (int64_t t = lane; t < cnt; t += 32) idx[b + t] = src[t];
+}
+
+// Leaves holding a row longer than the width (unordered list; each is redone on its own).
+__global__ void k_long_leaves(int64_t n, int64_t nleaf, const int64_t* __restrict__ counts,
+                              int64_t row_cap, uint64_t* __restrict__ out,
+                              unsigned long long* __restrict__ nout) {
+  int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (l >= nleaf) return;
+  bool longer = false;
+  for (int64_t k = l * LEAF; k < min((l + 1) * LEAF, n); ++k) longer |= counts[k] > row_cap;
+  if (longer) out[atomicAdd(nout, 1ull)] = (uint64_t)l;
 }
 
 // ---------------------------------------------------------------- export to original order
@@ -463,17 +420,47 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
   int64_t nsub = (n + SUB - 1) / SUB;
   NB_TRY(E.ensure_sub(nsub));
   count_launch(), k_sub_boxes<<<grid_for(nsub), NB_THREADS, 0, st>>>(n, nsub, L.spos, E.sub_lo, E.sub_hi);
-  // count, scan, fill
   unsigned gb = grid_for(nleaf * 32);
-  count_launch(), k_lists_sub<0><<<gb, NB_THREADS, 0, st>>>(n, nleaf, tv, E.sub_lo, E.sub_hi, L.spos, E.counts, nullptr, nullptr, E.d_err);
-  NB_CUDA(cudaMemsetAsync(L.off, 0, sizeof(int64_t), st));
-  tmp = E.cub_bytes;
-  NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, E.counts, L.off + 1, (int)n, st));
   int64_t total = 0;
-  NB_CUDA(cudaMemcpyAsync(&total, L.off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
-  NB_TRY(E.ensure_list_capacity(total));
-  count_launch(), k_lists_sub<1><<<gb, NB_THREADS, 0, st>>>(n, nleaf, tv, E.sub_lo, E.sub_hi, L.spos, nullptr, L.off, L.idx, E.d_err);
+  if ((double)n * (double)E.row_cap <= ELL_MAX_ENTRIES) {
+    // one traversal into fixed-width rows, scan, pack; the few rows longer than the width are
+    // written straight into CSR by a second traversal over their leaves only
+    NB_TRY(E.ensure_ell(n * E.row_cap));
+    NB_CUDA(cudaMemsetAsync(E.d_rowmax, 0, 2 * sizeof(unsigned long long), st));
+    count_launch(), k_lists_sub<2><<<gb, NB_THREADS, 0, st>>>(n, nleaf, nullptr, tv, E.sub_lo, E.sub_hi, L.spos, E.counts, nullptr, E.ell, E.row_cap, E.d_rowmax, E.d_err);
+    NB_CUDA(cudaMemsetAsync(L.off, 0, sizeof(int64_t), st));
+    tmp = E.cub_bytes;
+    NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, E.counts, L.off + 1, (int)n, st));
+    NB_CUDA(cudaMemcpyAsync(E.h_build, L.off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    NB_CUDA(cudaMemcpyAsync(E.h_build + 1, E.d_rowmax, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    NB_CUDA(cudaStreamSynchronize(st));
+    total = E.h_build[0];
+    int64_t longest = E.h_build[1];
+    NB_TRY(E.ensure_list_capacity(total));
+    count_launch(), k_pack_rows<<<grid_for(n * 32), NB_THREADS, 0, st>>>(n, E.row_cap, E.ell, L.off, L.idx);
+    if (longest > E.row_cap) {
+      uint64_t* leaves = E.keys_b;  // free after the sort
+      count_launch(), k_long_leaves<<<grid_for(nleaf), NB_THREADS, 0, st>>>(n, nleaf, E.counts, E.row_cap, leaves, E.d_rowmax + 1);
+      NB_CUDA(cudaMemcpyAsync(E.h_build + 1, E.d_rowmax + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+      NB_CUDA(cudaStreamSynchronize(st));
+      int64_t nlong = E.h_build[1];
+      count_launch(), k_lists_sub<1><<<grid_for(nlong * 32), NB_THREADS, 0, st>>>(n, nlong, leaves, tv, E.sub_lo, E.sub_hi, L.spos, nullptr, L.off, L.idx, 0, nullptr, E.d_err);
+    }
+    // width for the next build: the mean row with room to spare
+    int64_t mean = total / n;
+    E.row_cap = std::min<int64_t>(std::max<int64_t>((mean + mean / 2 + 32 + 31) / 32 * 32, 64), 1024);
+  } else {
+    // count, scan, fill
+    count_launch(), k_lists_sub<0><<<gb, NB_THREADS, 0, st>>>(n, nleaf, nullptr, tv, E.sub_lo, E.sub_hi, L.spos, E.counts, nullptr, nullptr, 0, nullptr, E.d_err);
+    NB_CUDA(cudaMemsetAsync(L.off, 0, sizeof(int64_t), st));
+    tmp = E.cub_bytes;
+    NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, E.counts, L.off + 1, (int)n, st));
+    NB_CUDA(cudaMemcpyAsync(E.h_build, L.off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    NB_CUDA(cudaStreamSynchronize(st));
+    total = E.h_build[0];
+    NB_TRY(E.ensure_list_capacity(total));
+    count_launch(), k_lists_sub<1><<<gb, NB_THREADS, 0, st>>>(n, nleaf, nullptr, tv, E.sub_lo, E.sub_hi, L.spos, nullptr, L.off, L.idx, 0, nullptr, E.d_err);
+  }
   E.prof.end(PROF_LISTS, st, (double)n, (double)total);
   L.n = n;
   L.total = total;

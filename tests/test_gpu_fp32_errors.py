@@ -18,7 +18,7 @@ TOL = {"h": 1e-5, "rho": 1e-5, "x": 1e-9, "p": 1e-6, "u": 1e-4, "a_hydro": 1e-4,
 def _run(ic, bc, steps):
     from blackhole_nebula_simulator_b200 import blocks
 
-    st = blocks.initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=1e12)
+    st = blocks.initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=bc.dt_max * 2.0**20)
     for _ in range(steps):
         blocks.advance(st, bc)
     return st

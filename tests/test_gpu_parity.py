@@ -56,6 +56,25 @@ def test_cloud_lists_and_tighten_bit_exact(nb):
     check("tight indices", g["tight_index"].astype(np.int64), _np(t.index))
 
 
+def test_long_and_short_rows_bit_exact(nb):
+    """Rows far longer than the one-pass build's slot width (a few particles with 8x the search
+    radius) beside ordinary rows, twice in a row so the second build runs with the width the first
+    one chose: exact equality with the oracle's lists."""
+    from oracle import native
+
+    ops = nb[0]
+    rng = np.random.default_rng(21)
+    pos = rng.uniform(0.0, 1.0, (40000, 3))
+    h = np.full(len(pos), 0.02) * rng.uniform(0.8, 1.25, len(pos))
+    h[rng.choice(len(pos), 40, replace=False)] *= 8.0
+    ref = native.find_neighbours(pos, h)
+    assert np.diff(ref.offset).max() > 1024
+    for attempt in range(2):
+        lists = ops.find_neighbours(pos, h)
+        check(f"offsets ({attempt})", ref.offset, _np(lists.offset))
+        check(f"indices ({attempt})", ref.index.astype(np.int64), _np(lists.index))
+
+
 def test_single_particle_lists_itself(nb):
     ops = nb[0]
     lists = ops.find_neighbours(np.array([[0.3, 0.2, 0.1]]), np.array([0.1]))
@@ -202,7 +221,8 @@ def test_block_steps_match_reference(nb):
     _, _, blocks, _ = nb
     g = golden("blocks.npz")
     bc = BlockConfig(coupled=_cfg(cooling_beta=230.0), dt_max=64.0)
-    st = blocks.initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc, t_stop=1e9,
+    # the fixture's t_stop (1e9) lies beyond the int64 tick range; no step lands on either
+    st = blocks.initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc, t_stop=1e6,
                            level_offset=g["level_offset"])  # fmt: skip
     check("init levels", g["init_level"], _np(st.level))
     check("init n_end", g["init_n_end"], _np(st.n_end))
