@@ -50,7 +50,7 @@ int Engine::ensure_n(int64_t n) {
     NB_CUDA(cudaMallocHost((void**)&h_err, sizeof(int) * 4));
     NB_CUDA(cudaMalloc((void**)&bbox, sizeof(double) * 8));
     NB_CUDA(cudaMallocHost((void**)&h_red, sizeof(double) * 64));
-    NB_CUDA(cudaMalloc((void**)&d_rowmax, 2 * sizeof(unsigned long long)));
+    NB_CUDA(cudaMalloc((void**)&d_rowmax, 4 * sizeof(unsigned long long)));
     NB_CUDA(cudaMallocHost((void**)&h_build, sizeof(int64_t) * 2));
     NB_CUDA(cudaEventCreate(&prof.a));
     NB_CUDA(cudaEventCreate(&prof.b));

@@ -116,6 +116,7 @@ struct Engine {
   // one-pass list build: rows written to fixed-width slots (row_cap entries each), then packed
   int32_t* ell = nullptr;
   int64_t cap_ell = 0, row_cap = 256;
+  int64_t list_slots = 0;  // resident blocks of the persistent list kernel
   unsigned long long* d_rowmax = nullptr;
   int64_t* h_build = nullptr;  // pinned: total entries and longest row of the last build
   double* red = nullptr;      // reduction partials (doubles)

@@ -199,35 +199,25 @@ __device__ __forceinline__ double point_gap2(double x, double y, double z, doubl
   return gx * gx + gy * gy + gz * gz;
 }
 
-// Warp per query leaf.  The warp walks the tree of boxes with an explicit stack in shared memory
-// (entries (level << 40) | index; children pushed highest first, so candidate leaves are reached
-// in ascending order).  At each candidate leaf every lane tests its own search sphere against the
-// leaf's sub-leaves and queues the ones it reaches (shared memory, per lane, in ascending order);
-// the warp flushes the queues in lockstep, each lane walking its own sub-leaves' particles, so
-// every row comes out sorted.
+// The rows of one query leaf of LEAF consecutive sorted particles, one lane per particle.  The
+// warp walks the tree of boxes with an explicit stack in shared memory (entries (level << 40) |
+// index; children pushed highest first, so candidate leaves are reached in ascending order).  At
+// each candidate leaf every lane tests its own search sphere against the leaf's sub-leaves and
+// queues the ones it reaches (shared memory, per lane, in ascending order); the warp flushes the
+// queues in lockstep, each lane walking its own sub-leaves' particles, so every row comes out
+// sorted.
 // PASS 0 counts each row's entries; PASS 1 writes them at off[k]; PASS 2 writes them into a
-// fixed-width slot of row_cap entries at k * row_cap, counts them, and records the longest row.
+// fixed-width slot of row_cap entries at k * row_cap and counts them.  Returns the row length.
 template <int PASS>
-__global__ void __launch_bounds__(NB_THREADS) k_lists_sub(int64_t n, int64_t nwork,
-                                                          const uint64_t* __restrict__ leaves,
-                                                          TreeView tv,
-                                                          const double4* __restrict__ slo,
-                                                          const double4* __restrict__ shi,
-                                                          const double4* __restrict__ spos,
-                                                          int64_t* __restrict__ counts,
-                                                          const int64_t* __restrict__ off,
-                                                          int32_t* __restrict__ idx,
-                                                          int64_t row_cap,
-                                                          unsigned long long* __restrict__ rowmax,
-                                                          int* err) {
-  __shared__ int64_t stack_s[NB_THREADS / 32][STACK];
-  __shared__ int32_t queue_s[NB_THREADS / 32][QCAP][32];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  if (w >= nwork) return;  // warp-uniform
-  int64_t leaf = leaves ? (int64_t)leaves[w] : w;  // all leaves, or the listed ones
-  int64_t* stack = stack_s[wib];
-  int32_t(*queue)[32] = queue_s[wib];
+__device__ __forceinline__ int64_t leaf_rows(int64_t leaf, int64_t n, const TreeView& tv,
+                                             const double4* __restrict__ slo,
+                                             const double4* __restrict__ shi,
+                                             const double4* __restrict__ spos,
+                                             int64_t* __restrict__ counts,
+                                             const int64_t* __restrict__ off,
+                                             int32_t* __restrict__ idx, int64_t row_cap,
+                                             int64_t* stack, int32_t (*queue)[32], int lane,
+                                             int* err) {
   int64_t k = leaf * LEAF + lane;
   bool valid = k < n;
   double4 me = valid ? spos[k] : make_double4(0, 0, 0, 0);
@@ -264,7 +254,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_lists_sub(int64_t n, int64_t nwo
               else
                 set_error(err, ERR_LIST_OVERFLOW);
             } else if (PASS == 2) {
-              if (m < cap) idx[base + m] = (int32_t)j;  // longer rows are redone wider
+              if (m < cap) idx[base + m] = (int32_t)j;  // longer rows are redone in CSR
             }
             m += 1;
           }
@@ -275,6 +265,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_lists_sub(int64_t n, int64_t nwo
     qn = 0;
   };
   int sp = 0;
+  __syncwarp();
   if (lane == 0) stack[0] = ((int64_t)(tv.nlevels - 1) << 40);
   sp = 1;
   __syncwarp();
@@ -324,10 +315,61 @@ __global__ void __launch_bounds__(NB_THREADS) k_lists_sub(int64_t n, int64_t nwo
   }
   flush();
   if (PASS != 1 && valid) counts[k] = m;
+  return valid ? m : 0;
+}
+
+// Persistent list kernel: each warp takes the next query leaf from `order` (heaviest first) until
+// none is left, so a few slow leaves (sparse regions whose 32 Morton-consecutive particles spread
+// far) overlap with the rest instead of holding whole blocks.  PASS 2 also records the longest
+// row in *rowmax.
+template <int PASS>
+__global__ void __launch_bounds__(NB_THREADS) k_lists_sub(int64_t n, int64_t nwork,
+                                                          const int32_t* __restrict__ order,
+                                                          unsigned long long* __restrict__ next,
+                                                          TreeView tv,
+                                                          const double4* __restrict__ slo,
+                                                          const double4* __restrict__ shi,
+                                                          const double4* __restrict__ spos,
+                                                          int64_t* __restrict__ counts,
+                                                          const int64_t* __restrict__ off,
+                                                          int32_t* __restrict__ idx,
+                                                          int64_t row_cap,
+                                                          unsigned long long* __restrict__ rowmax,
+                                                          int* err) {
+  __shared__ int64_t stack_s[NB_THREADS / 32][STACK];
+  __shared__ int32_t queue_s[NB_THREADS / 32][QCAP][32];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int64_t* stack = stack_s[wib];
+  int32_t(*queue)[32] = queue_s[wib];
+  unsigned longest = 0;
+  while (true) {
+    unsigned long long w = 0;
+    if (lane == 0) w = atomicAdd(next, 1ull);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if (w >= (unsigned long long)nwork) break;  // warp-uniform
+    int64_t leaf = order[w];
+    int64_t m = leaf_rows<PASS>(leaf, n, tv, slo, shi, spos, counts, off, idx, row_cap, stack,
+                                queue, lane, err);
+    longest = max(longest, (unsigned)m);
+  }
   if (PASS == 2) {
-    unsigned mx = __reduce_max_sync(0xffffffffu, valid ? (unsigned)m : 0u);
+    unsigned mx = __reduce_max_sync(0xffffffffu, longest);
     if (lane == 0) atomicMax(rowmax, (unsigned long long)mx);
   }
+}
+
+// Cost key of each query leaf for the heaviest-first order: the linear size of the region its
+// traversal covers (box extent plus twice the largest search diameter), as descending-order bits.
+__global__ void k_leaf_cost(int64_t nleaf, const double4* __restrict__ lo,
+                            const double4* __restrict__ hi, uint32_t* __restrict__ key,
+                            int32_t* __restrict__ id) {
+  int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (l >= nleaf) return;
+  double4 a = lo[l], b = hi[l];
+  double ext = fmax(fmax(b.x - a.x, b.y - a.y), b.z - a.z);
+  float c = (float)(ext + 4.0 * a.w);
+  key[l] = ~__float_as_uint(c);  // non-negative floats order like their bits
+  id[l] = (int32_t)l;
 }
 
 // Pack the fixed-width rows into CSR: warp per row, coalesced on both sides.  Rows longer than
@@ -345,13 +387,13 @@ __global__ void k_pack_rows(int64_t n, int64_t row_cap, const int32_t* __restric
 
 // Leaves holding a row longer than the width (unordered list; each is redone on its own).
 __global__ void k_long_leaves(int64_t n, int64_t nleaf, const int64_t* __restrict__ counts,
-                              int64_t row_cap, uint64_t* __restrict__ out,
+                              int64_t row_cap, int32_t* __restrict__ out,
                               unsigned long long* __restrict__ nout) {
   int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (l >= nleaf) return;
   bool longer = false;
   for (int64_t k = l * LEAF; k < min((l + 1) * LEAF, n); ++k) longer |= counts[k] > row_cap;
-  if (longer) out[atomicAdd(nout, 1ull)] = (uint64_t)l;
+  if (longer) out[atomicAdd(nout, 1ull)] = (int32_t)l;
 }
 
 // ---------------------------------------------------------------- export to original order
@@ -374,6 +416,17 @@ __global__ void k_export_fill(int64_t n, const int32_t* __restrict__ perm,
 }
 
 // ---------------------------------------------------------------- host orchestration
+// Resident blocks of the persistent list kernel over the whole device (fewest of its variants).
+static int list_kernel_slots(Engine& E) {
+  if (E.list_slots > 0) return 0;
+  int sms = 0, b0 = 0, b1 = 0, b2 = 0;
+  NB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E.device));
+  NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_lists_sub<0>, NB_THREADS, 0));
+  NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_lists_sub<1>, NB_THREADS, 0));
+  NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_lists_sub<2>, NB_THREADS, 0));
+  E.list_slots = (int64_t)sms * std::max(1, std::min(b0, std::min(b1, b2)));
+  return 0;
+}
 int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaStream_t st) {
   NB_TRY(E.ensure_n(n));
   if (n == 0) {
@@ -420,14 +473,27 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
   int64_t nsub = (n + SUB - 1) / SUB;
   NB_TRY(E.ensure_sub(nsub));
   count_launch(), k_sub_boxes<<<grid_for(nsub), NB_THREADS, 0, st>>>(n, nsub, L.spos, E.sub_lo, E.sub_hi);
-  unsigned gb = grid_for(nleaf * 32);
+  // query leaves heaviest first, for the persistent list kernel
+  uint32_t* cost = reinterpret_cast<uint32_t*>(E.keys_a);
+  uint32_t* cost_sorted = reinterpret_cast<uint32_t*>(E.keys_b);
+  int32_t* order = reinterpret_cast<int32_t*>(E.keys_b) + E.cap_n;  // second half of keys_b
+  count_launch(), k_leaf_cost<<<grid_for(nleaf), NB_THREADS, 0, st>>>(nleaf, E.node_lo, E.node_hi, cost, E.vals_a);
+  tmp = 0;
+  NB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, cost, cost_sorted, E.vals_a, order, (int)nleaf, 0, 32, st));
+  NB_TRY(E.ensure_cub(tmp));
+  tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceRadixSort::SortPairs(E.cub_tmp, tmp, cost, cost_sorted, E.vals_a, order, (int)nleaf, 0, 32, st));
+  NB_CUDA(cudaMemsetAsync(E.d_rowmax, 0, 4 * sizeof(unsigned long long), st));
+  NB_TRY(list_kernel_slots(E));
+  auto grid = [&](int64_t nwork) {
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((nwork * 32 + NB_THREADS - 1) / NB_THREADS, E.list_slots));
+  };
   int64_t total = 0;
   if ((double)n * (double)E.row_cap <= ELL_MAX_ENTRIES) {
     // one traversal into fixed-width rows, scan, pack; the few rows longer than the width are
     // written straight into CSR by a second traversal over their leaves only
     NB_TRY(E.ensure_ell(n * E.row_cap));
-    NB_CUDA(cudaMemsetAsync(E.d_rowmax, 0, 2 * sizeof(unsigned long long), st));
-    count_launch(), k_lists_sub<2><<<gb, NB_THREADS, 0, st>>>(n, nleaf, nullptr, tv, E.sub_lo, E.sub_hi, L.spos, E.counts, nullptr, E.ell, E.row_cap, E.d_rowmax, E.d_err);
+    count_launch(), k_lists_sub<2><<<grid(nleaf), NB_THREADS, 0, st>>>(n, nleaf, order, E.d_rowmax + 2, tv, E.sub_lo, E.sub_hi, L.spos, E.counts, nullptr, E.ell, E.row_cap, E.d_rowmax, E.d_err);
     NB_CUDA(cudaMemsetAsync(L.off, 0, sizeof(int64_t), st));
     tmp = E.cub_bytes;
     NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, E.counts, L.off + 1, (int)n, st));
@@ -439,19 +505,19 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
     NB_TRY(E.ensure_list_capacity(total));
     count_launch(), k_pack_rows<<<grid_for(n * 32), NB_THREADS, 0, st>>>(n, E.row_cap, E.ell, L.off, L.idx);
     if (longest > E.row_cap) {
-      uint64_t* leaves = E.keys_b;  // free after the sort
+      int32_t* leaves = reinterpret_cast<int32_t*>(E.keys_a);  // free after the order sort
       count_launch(), k_long_leaves<<<grid_for(nleaf), NB_THREADS, 0, st>>>(n, nleaf, E.counts, E.row_cap, leaves, E.d_rowmax + 1);
       NB_CUDA(cudaMemcpyAsync(E.h_build + 1, E.d_rowmax + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
       NB_CUDA(cudaStreamSynchronize(st));
       int64_t nlong = E.h_build[1];
-      count_launch(), k_lists_sub<1><<<grid_for(nlong * 32), NB_THREADS, 0, st>>>(n, nlong, leaves, tv, E.sub_lo, E.sub_hi, L.spos, nullptr, L.off, L.idx, 0, nullptr, E.d_err);
+      count_launch(), k_lists_sub<1><<<grid(nlong), NB_THREADS, 0, st>>>(n, nlong, leaves, E.d_rowmax + 3, tv, E.sub_lo, E.sub_hi, L.spos, nullptr, L.off, L.idx, 0, nullptr, E.d_err);
     }
     // width for the next build: the mean row with room to spare
     int64_t mean = total / n;
     E.row_cap = std::min<int64_t>(std::max<int64_t>((mean + mean / 2 + 32 + 31) / 32 * 32, 64), 1024);
   } else {
     // count, scan, fill
-    count_launch(), k_lists_sub<0><<<gb, NB_THREADS, 0, st>>>(n, nleaf, nullptr, tv, E.sub_lo, E.sub_hi, L.spos, E.counts, nullptr, nullptr, 0, nullptr, E.d_err);
+    count_launch(), k_lists_sub<0><<<grid(nleaf), NB_THREADS, 0, st>>>(n, nleaf, order, E.d_rowmax + 2, tv, E.sub_lo, E.sub_hi, L.spos, E.counts, nullptr, nullptr, 0, nullptr, E.d_err);
     NB_CUDA(cudaMemsetAsync(L.off, 0, sizeof(int64_t), st));
     tmp = E.cub_bytes;
     NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, E.counts, L.off + 1, (int)n, st));
@@ -459,7 +525,7 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
     NB_CUDA(cudaStreamSynchronize(st));
     total = E.h_build[0];
     NB_TRY(E.ensure_list_capacity(total));
-    count_launch(), k_lists_sub<1><<<gb, NB_THREADS, 0, st>>>(n, nleaf, nullptr, tv, E.sub_lo, E.sub_hi, L.spos, nullptr, L.off, L.idx, 0, nullptr, E.d_err);
+    count_launch(), k_lists_sub<1><<<grid(nleaf), NB_THREADS, 0, st>>>(n, nleaf, order, E.d_rowmax + 3, tv, E.sub_lo, E.sub_hi, L.spos, nullptr, L.off, L.idx, 0, nullptr, E.d_err);
   }
   E.prof.end(PROF_LISTS, st, (double)n, (double)total);
   L.n = n;
