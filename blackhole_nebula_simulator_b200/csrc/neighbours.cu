@@ -512,9 +512,10 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
       int64_t nlong = E.h_build[1];
       count_launch(), k_lists_sub<1><<<grid(nlong), NB_THREADS, 0, st>>>(n, nlong, leaves, E.d_rowmax + 3, tv, E.sub_lo, E.sub_hi, L.spos, nullptr, L.off, L.idx, 0, nullptr, E.d_err);
     }
-    // width for the next build: the mean row with room to spare
-    int64_t mean = total / n;
-    E.row_cap = std::min<int64_t>(std::max<int64_t>((mean + mean / 2 + 32 + 31) / 32 * 32, 64), 1024);
+    // width for the next build: this build's longest row with room to spare, within the
+    // scratch bound (rows beyond it take the CSR redo above)
+    int64_t widest = std::min<int64_t>(1024, (int64_t)(ELL_MAX_ENTRIES / (double)n) / 32 * 32);
+    E.row_cap = std::min<int64_t>(std::max<int64_t>((longest + longest / 8 + 31) / 32 * 32, 64), std::max<int64_t>(widest, 64));
   } else {
     // count, scan, fill
     count_launch(), k_lists_sub<0><<<grid(nleaf), NB_THREADS, 0, st>>>(n, nleaf, order, E.d_rowmax + 2, tv, E.sub_lo, E.sub_hi, L.spos, E.counts, nullptr, nullptr, 0, nullptr, E.d_err);

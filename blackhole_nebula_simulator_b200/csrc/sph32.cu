@@ -12,7 +12,7 @@ void launch_density32(int64_t nrows, const int64_t* rows, const float4* pos, flo
                       int64_t* work, cudaStream_t st) {
   if (nrows <= 0) return;
   Pos32 geo{pos, cell};
-  count_launch(), k_density<float, Pos32, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+  count_launch(), k_density<float, Pos32, I><<<grid_for((nrows + 3) / 4 * 32, DENSITY_THREADS), DENSITY_THREADS, 0, st>>>(
       nrows, rows, geo, mass, h_start, h_search, off, idx, prm, out_map, h_out, rho, omega, iters,
       flags, work);
 }

@@ -12,7 +12,7 @@ void launch_density64(int64_t nrows, const int64_t* rows, const double4* pos, co
                       cudaStream_t st) {
   if (nrows <= 0) return;
   Pos64 geo{pos};
-  count_launch(), k_density<double, Pos64, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+  count_launch(), k_density_thread<double, Pos64, I><<<grid_for(nrows), NB_THREADS, 0, st>>>(
       nrows, rows, geo, mass, h_start, h_search, off, idx, prm, out_map, h_out, rho, omega, iters,
       flags, work);
 }

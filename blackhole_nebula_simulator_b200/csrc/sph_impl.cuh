@@ -1,7 +1,8 @@
 // SPH pair passes on neighbour lists (implementation, included by sph64.cu and sph32.cu): the h-rho Newton solve and the fused pressure + artificial
 // viscosity (+ conductivity, + disc viscosity) force and du/dt pass.
 //
-// Both run one thread per row over CSR lists.  They are templated on the list index type so the
+// The density solve runs eight lanes per row with a shared-memory cache of the in-range entries
+// (FP32) or one thread per row (FP64); the force pass one thread per row.  Both walk CSR lists.  They are templated on the list index type so the
 // same code serves the caller-order int64 lists of the operator API and the engine's sorted int32
 // lists, and on the arithmetic: FP64 (every pair term in double) or FP32 (positions as float
 // offsets from cell centres, float pair terms, Kahan-compensated sums, the Newton update and all
@@ -125,9 +126,12 @@ __device__ __forceinline__ void cached_sums(const R* rr, const R* mm, int cnt, R
 // per-thread cache in local memory measured slower than re-walking the Morton-local list).
 constexpr int DENSITY_CACHE = 0;
 
+// One thread per row (the FP64 form: its shared-memory cache of (r, m) in double would hold
+// occupancy too low for the row-group kernel below to pay off).
+
 template <typename R, typename PosT, typename I>
 __global__ void __launch_bounds__(NB_THREADS)
-    k_density(int64_t nrows, const int64_t* __restrict__ rows, PosT geo,
+    k_density_thread(int64_t nrows, const int64_t* __restrict__ rows, PosT geo,
               const double* __restrict__ mass, const double* __restrict__ h_start,
               const double* __restrict__ h_search, const int64_t* __restrict__ off,
               const I* __restrict__ idx, DensityParams prm, const int32_t* __restrict__ out_map,
@@ -215,6 +219,202 @@ __global__ void __launch_bounds__(NB_THREADS)
   if (iters) iters[o] = it;
   if (flags) flags[o] = flag;
   if (work) work[o] = evals;
+}
+
+// Sums over the 8 lanes of a row group (lanes 8g .. 8g+7 of a warp).  Every lane of the group ends
+// with the same value (each butterfly step adds the same two operands on both lanes).  FP64: plain
+// sums.  FP32: each lane's Kahan partial (s, -c) is combined pairwise with an exact two-sum, the
+// rounding errors and the lanes' compensations carried in a second float.
+__device__ __forceinline__ double group_total(double v) {
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double group_total(const Acc<double>& a) { return group_total(a.s); }
+__device__ __forceinline__ double group_total(const Acc<float>& a) {
+  float s = a.k.s, k = -a.k.c;
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) {
+    float s2 = __shfl_xor_sync(0xffffffffu, s, o);
+    float k2 = __shfl_xor_sync(0xffffffffu, k, o);
+    float t = __fadd_rn(s, s2);
+    float bp = __fsub_rn(t, s);
+    float e = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bp)), __fsub_rn(s2, bp));
+    s = t;
+    k = __fadd_rn(__fadd_rn(k, k2), e);
+  }
+  return (double)s + (double)k;
+}
+
+template <typename R>
+struct DensityEntry;
+template <>
+struct DensityEntry<float> {
+  using T = float2;
+  static constexpr int CAP = 256;  // in-range entries a row keeps in shared memory
+};
+template <>
+struct DensityEntry<double> {
+  using T = double2;
+  static constexpr int CAP = 192;
+};
+constexpr int DENSITY_THREADS = 128;  // 16 rows per block
+
+// Eight lanes per row, four rows per warp.  The lanes of a row split its list (entry e to lane
+// e mod 8, coalesced index loads) and store the distance and mass of every entry inside the search
+// radius in shared memory, in list order; each Newton iteration then sums the kernel terms over
+// that cache and reduces across the eight lanes, so the lanes of a row take the same Newton steps.
+// Rows with more in-range entries than the cache holds re-walk their list in every sum.
+template <typename R, typename PosT, typename I>
+__global__ void __launch_bounds__(DENSITY_THREADS)
+    k_density(int64_t nrows, const int64_t* __restrict__ rows, PosT geo,
+              const double* __restrict__ mass, const double* __restrict__ h_start,
+              const double* __restrict__ h_search, const int64_t* __restrict__ off,
+              const I* __restrict__ idx, DensityParams prm, const int32_t* __restrict__ out_map,
+              double* __restrict__ h_out, double* __restrict__ rho, double* __restrict__ omega,
+              int64_t* __restrict__ iters, int64_t* __restrict__ flags, int64_t* __restrict__ work) {
+  using E2 = typename DensityEntry<R>::T;
+  constexpr int CAP = DensityEntry<R>::CAP;
+  __shared__ E2 cache_s[DENSITY_THREADS / 8][CAP];
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, gl = lane & 7, g = lane >> 3;
+  const int64_t q = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 4 + g;
+  const bool live = q < nrows;
+  if (!__any_sync(FULL, live)) return;  // warp-uniform
+  E2* cache = cache_s[threadIdx.x >> 3];
+  int64_t i = 0, o = 0, e0 = 0, e1 = 0;
+  double m_i = 1.0, hs = 1.0;
+  if (live) {
+    i = rows ? rows[q] : q;
+    o = out_map ? (int64_t)out_map[i] : q;
+    m_i = mass[i];
+    hs = fmin(h_search[i], prm.h_max);
+    e0 = off[i];
+    e1 = off[i + 1];
+  }
+  const double r_max = 2.0 * hs;
+  const R r2max = (R)(r_max * r_max);
+  const int kid = prm.kid;
+  const R cn = (R)prm.cnorm;
+  // distances and masses of the entries inside r_max (sim/sph.py:231-248), in list order
+  const unsigned len = (unsigned)(e1 - e0);
+  const unsigned maxlen = __reduce_max_sync(FULL, len);
+  int cnt = 0;
+  for (unsigned b = 0; b < maxlen; b += 8) {
+    bool inr = false;
+    R r = R(0), m = R(0);
+    if (b + gl < len) {
+      int64_t j = (int64_t)idx[e0 + b + gl];
+      R dx, dy, dz;
+      geo.diff(i, j, dx, dy, dz);
+      R d2 = sqdist(dx, dy, dz);
+      if (d2 < r2max) {
+        inr = true;
+        r = sqrt(d2);
+        m = (R)mass[j];
+      }
+    }
+    unsigned seg = (__ballot_sync(FULL, inr) >> (8 * g)) & 0xffu;
+    int pos = cnt + __popc(seg & ((1u << gl) - 1u));
+    if (inr && pos < CAP) {
+      E2 v;
+      v.x = r;
+      v.y = m;
+      cache[pos] = v;
+    }
+    cnt += __popc(seg);
+  }
+  __syncwarp();
+  const bool cached = cnt <= CAP;
+  int64_t evals = 0;
+  // kernel sums at h of the rows whose `active` is set; every lane takes part in the reductions
+  auto sums = [&](R h, bool active, double& rs_out, double& dws_out) {
+    Acc<R> rs, dws;
+    if (active) {
+      R inv_h = R(1) / h;
+      R ih2 = inv_h * inv_h;
+      R ih3 = ih2 * inv_h;
+      R ih4 = ih2 * ih2;
+      auto term = [&](R rj, R mj) {
+        R qq = rj * inv_h;
+        if (qq < R(2)) {
+          evals += 1;
+          R fq = kernel_f<R>(qq, kid);
+          rs.add(mj * cn * ih3 * fq);
+          dws.add(mj * (-cn * ih4 * (R(3) * fq + qq * kernel_df<R>(qq, kid))));
+        }
+      };
+      if (cached) {
+        for (int t = gl; t < cnt; t += 8) {
+          E2 v = cache[t];
+          term(v.x, v.y);
+        }
+      } else {
+        for (int64_t e = e0 + gl; e < e1; e += 8) {
+          int64_t j = (int64_t)idx[e];
+          R dx, dy, dz;
+          geo.diff(i, j, dx, dy, dz);
+          R d2 = sqdist(dx, dy, dz);
+          if (!(d2 < r2max)) continue;
+          term(sqrt(d2), (R)mass[j]);
+        }
+      }
+    }
+    rs_out = group_total(rs);
+    dws_out = group_total(dws);
+  };
+  double lo = 0.0, hi = hs;
+  double h = live ? fmin(h_start[i], hi) : 1.0;
+  double h0 = h;
+  int flag = 3, it = 0;
+  bool done = !live;
+  const double eta = prm.eta, e3 = eta * eta * eta;
+  while (__any_sync(FULL, !done)) {
+    double rs, dws;
+    sums((R)h, !done, rs, dws);
+    if (!done) {
+      it += 1;
+      double t = eta / h;
+      double f = rs - m_i * (t * t * t);
+      double h2 = h * h;
+      double df = dws + 3.0 * m_i * e3 / (h2 * h2);
+      if (f > 0)
+        hi = h;
+      else
+        lo = h;
+      double h_new = df > 0 ? h - f / df : 0.5 * (lo + hi);
+      if (!(lo <= h_new && h_new <= hi)) h_new = 0.5 * (lo + hi);
+      if (fabs(h_new - h) < prm.tol * h0) {
+        flag = 0;
+        done = true;
+      } else if (it >= 50) {
+        done = true;
+      }
+      h = h_new;
+    }
+  }
+  const bool cap_test = live && h >= hs * (1 - 1e-3);
+  if (__any_sync(FULL, cap_test)) {
+    double rs_lim, dummy;
+    sums((R)hs, cap_test, rs_lim, dummy);
+    double t = eta / hs;
+    if (cap_test && rs_lim - m_i * (t * t * t) < 0) {
+      h = hs;
+      flag = hs >= prm.h_max ? 1 : 2;
+    }
+  }
+  double rs, dws;
+  sums((R)h, live, rs, dws);
+#pragma unroll
+  for (int of = 4; of > 0; of >>= 1) evals += __shfl_xor_sync(FULL, evals, of);
+  if (live && gl == 0) {
+    h_out[o] = h;
+    rho[o] = rs;
+    omega[o] = flag == 1 ? 1.0 : 1.0 + h / (3.0 * rs) * dws;
+    if (iters) iters[o] = it;
+    if (flags) flags[o] = flag;
+    if (work) work[o] = evals;
+  }
 }
 
 // ---------------------------------------------------------------- forces
