@@ -24,7 +24,7 @@ void launch_forces32(int64_t nrows, const int64_t* rows, const float4* pos, floa
                      ForceOut out, cudaStream_t st) {
   if (nrows <= 0) return;
   Pos32 geo{pos, cell};
-  count_launch(), k_forces<float, Pos32, I, float4><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+  count_launch(), k_forces_g<float, Pos32, I, float4><<<grid_for(nrows * 8), NB_THREADS, 0, st>>>(
       nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
 }
 

@@ -23,7 +23,7 @@ void launch_forces64(int64_t nrows, const int64_t* rows, const double4* pos, con
                      ForceParams prm, const int32_t* out_map, ForceOut out, cudaStream_t st) {
   if (nrows <= 0) return;
   Pos64 geo{pos};
-  count_launch(), k_forces<double, Pos64, I, double4><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+  count_launch(), k_forces_g<double, Pos64, I, double4><<<grid_for(nrows * 8), NB_THREADS, 0, st>>>(
       nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
 }
 

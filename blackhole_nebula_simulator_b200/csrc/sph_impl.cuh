@@ -2,7 +2,7 @@
 // viscosity (+ conductivity, + disc viscosity) force and du/dt pass.
 //
 // The density solve runs eight lanes per row with a shared-memory cache of the in-range entries
-// (FP32) or one thread per row (FP64); the force pass one thread per row.  Both walk CSR lists.  They are templated on the list index type so the
+// (FP32) or one thread per row (FP64); the force pass eight lanes per row.  Both walk CSR lists.  They are templated on the list index type so the
 // same code serves the caller-order int64 lists of the operator API and the engine's sorted int32
 // lists, and on the arithmetic: FP64 (every pair term in double) or FP32 (positions as float
 // offsets from cell centres, float pair terms, Kahan-compensated sums, the Newton update and all
@@ -426,18 +426,28 @@ __device__ __forceinline__ R dwdr(R r, R h, int kid, R cnorm) {
   return cnorm / (h2 * h2) * kernel_df<R>(r / h, kid);
 }
 
+// Fused pressure + artificial viscosity (+ conductivity) + P dV (+ disc viscosity) pass.  Eight
+// lanes per row (lanes 8g .. 8g+7 of a warp), each taking every eighth list entry; the pair terms
+// are summed per lane and then over the row's lanes.
 template <typename R, typename PosT, typename I, typename V4>
 __global__ void __launch_bounds__(NB_THREADS, 2)
-    k_forces(int64_t nrows, const int64_t* __restrict__ rows, PosT geo,
+    k_forces_g(int64_t nrows, const int64_t* __restrict__ rows, PosT geo,
              const V4* __restrict__ vm,    // (vx, vy, vz, mass)
              const V4* __restrict__ hydro, // (h, rho, omega, P)
              const V4* __restrict__ aux,   // (u, c_s, alpha, unused)
              const int64_t* __restrict__ off, const I* __restrict__ idx, ForceParams prm,
              const int32_t* __restrict__ out_map, ForceOut out) {
-  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= nrows) return;
-  int64_t a = rows ? rows[q] : q;
-  int64_t o = out_map ? (int64_t)out_map[a] : q;
+  const unsigned FULL = 0xffffffffu;
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t q = t >> 3;
+  const int gl = (int)(t & 7);
+  const bool live = q < nrows;
+  if (!__any_sync(FULL, live)) return;  // warp-uniform
+  int64_t a = 0, o = 0;
+  if (live) {
+    a = rows ? rows[q] : q;
+    o = out_map ? (int64_t)out_map[a] : q;
+  }
   const V4 va = vm[a], ha = hydro[a], xa = aux[a];
   const R h_a = (R)ha.x, rho_a = (R)ha.y, om_a = (R)ha.z, P_a = (R)ha.w;
   const R inv_or_a = R(1) / (om_a * rho_a);
@@ -449,7 +459,8 @@ __global__ void __launch_bounds__(NB_THREADS, 2)
   Acc<R> ax, ay, az, work, heat, vheat, cheat, dax, day, daz, dheat;
   R vmax = prm.use_visc ? cs_a : R(0);
   int64_t npairs = 0;
-  for (int64_t e = off[a]; e < off[a + 1]; ++e) {
+  const int64_t e_end = live ? off[a + 1] : 0;
+  for (int64_t e = (live ? off[a] : 0) + gl; e < e_end; e += 8) {
     int64_t b = (int64_t)idx[e];
     if (b == a) continue;
     R ddx, ddy, ddz;
@@ -522,25 +533,50 @@ __global__ void __launch_bounds__(NB_THREADS, 2)
       dheat.add(m_b * qa * vdr * fa);
     }
   }
+  // sums over the row's eight lanes (uniform flags: every lane takes part in every reduction)
+  double s_ax = 0, s_ay = 0, s_az = 0, s_work = 0, s_heat = 0, s_vheat = 0, s_cheat = 0;
+  double s_dax = 0, s_day = 0, s_daz = 0, s_dheat = 0;
   if (prm.use_sph) {
-    double du = (double)P_a * (double)inv_or_a / (double)rho_a * work.get() + heat.get();
+    s_ax = group_total(ax);
+    s_ay = group_total(ay);
+    s_az = group_total(az);
+    s_work = group_total(work);
+    s_heat = group_total(heat);
+    s_vheat = group_total(vheat);
+    s_cheat = group_total(cheat);
+  }
+  if (prm.use_disc) {
+    s_dax = group_total(dax);
+    s_day = group_total(day);
+    s_daz = group_total(daz);
+    s_dheat = group_total(dheat);
+  }
+#pragma unroll
+  for (int of = 4; of > 0; of >>= 1) {
+    R vo = __shfl_xor_sync(FULL, vmax, of);
+    vmax = vo > vmax ? vo : vmax;
+    npairs += __shfl_xor_sync(FULL, npairs, of);
+  }
+  if (!live || gl != 0) return;
+  if (prm.use_sph) {
+    double du = (double)P_a * (double)inv_or_a / (double)rho_a * s_work + s_heat;
     if (out.acc) {
-      out.acc[3 * o + 0] = ax.get();
-      out.acc[3 * o + 1] = ay.get();
-      out.acc[3 * o + 2] = az.get();
+      out.acc[3 * o + 0] = s_ax;
+      out.acc[3 * o + 1] = s_ay;
+      out.acc[3 * o + 2] = s_az;
     }
     if (out.dudt) out.dudt[o] = du;
     if (out.vsig) out.vsig[o] = (double)vmax;
-    if (out.vheat) out.vheat[o] = vheat.get();
-    if (out.cheat) out.cheat[o] = cheat.get();
+    if (out.vheat) out.vheat[o] = s_vheat;
+    if (out.cheat) out.cheat[o] = s_cheat;
   }
   if (prm.use_disc) {
     if (out.dacc) {
-      out.dacc[3 * o + 0] = dax.get();
-      out.dacc[3 * o + 1] = day.get();
-      out.dacc[3 * o + 2] = daz.get();
+      out.dacc[3 * o + 0] = s_dax;
+      out.dacc[3 * o + 1] = s_day;
+      out.dacc[3 * o + 2] = s_daz;
     }
-    if (out.ddudt) out.ddudt[o] = dheat.get();
+    if (out.ddudt) out.ddudt[o] = s_dheat;
   }
   if (out.pairs) out.pairs[o] = npairs;
 }

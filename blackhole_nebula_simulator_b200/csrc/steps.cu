@@ -406,21 +406,32 @@ __global__ void k_limit_sweep(int64_t nrows, const int64_t* __restrict__ rows_s,
                               const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
                               const double4* __restrict__ pk, int64_t max_gap, int64_t* level_s,
                               int* changed) {
-  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= nrows) return;
-  int64_t k = rows_s[q];
-  double4 me = pk[k];
-  int64_t need = ((volatile int64_t*)level_s)[k];
-  for (int64_t e = off[k]; e < off[k + 1]; ++e) {
-    int32_t js = idx[e];
-    double4 o = pk[js];
-    double d2 = d2_exact(o.x - me.x, o.y - me.y, o.z - me.z);
-    double rr = 2.0 * fmax(me.w, o.w);
-    if (!(d2 < rr * rr)) continue;
-    int64_t lj = ((volatile int64_t*)level_s)[js];
-    if (lj - max_gap > need) need = lj - max_gap;
+  // eight lanes per row (lanes 8g .. 8g+7 of a warp), each taking every eighth list entry
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t q = t >> 3;
+  const int gl = (int)(t & 7);
+  const bool live = q < nrows;
+  int64_t k = 0, need = INT64_MIN;
+  if (live) {
+    k = rows_s[q];
+    double4 me = pk[k];
+    need = ((volatile int64_t*)level_s)[k];
+    for (int64_t e = off[k] + gl; e < off[k + 1]; e += 8) {
+      int32_t js = idx[e];
+      double4 o = pk[js];
+      double d2 = d2_exact(o.x - me.x, o.y - me.y, o.z - me.z);
+      double rr = 2.0 * fmax(me.w, o.w);
+      if (!(d2 < rr * rr)) continue;
+      int64_t lj = ((volatile int64_t*)level_s)[js];
+      if (lj - max_gap > need) need = lj - max_gap;
+    }
   }
-  if (need > ((volatile int64_t*)level_s)[k]) {
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) {
+    int64_t other = __shfl_xor_sync(0xffffffffu, need, o);
+    need = other > need ? other : need;
+  }
+  if (live && gl == 0 && need > ((volatile int64_t*)level_s)[k]) {
     atomicMax((long long*)&level_s[k], (long long)need);
     *changed = 1;
   }
@@ -471,12 +482,15 @@ __global__ void k_wake_need(int64_t nrows, const int64_t* __restrict__ rows_s,
                             const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
                             const double4* __restrict__ pk, const int64_t* __restrict__ level_s,
                             int64_t max_gap, int64_t* __restrict__ need_s) {
-  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  // eight lanes per row, each taking every eighth list entry
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t q = t >> 3;
+  const int gl = (int)(t & 7);
   if (q >= nrows) return;
   int64_t k = rows_s[q];
   double4 me = pk[k];
   long long v = (long long)(level_s[k] - max_gap);
-  for (int64_t e = off[k]; e < off[k + 1]; ++e) {
+  for (int64_t e = off[k] + gl; e < off[k + 1]; e += 8) {
     int32_t js = idx[e];
     double4 o = pk[js];
     double d2 = d2_exact(o.x - me.x, o.y - me.y, o.z - me.z);
@@ -555,7 +569,7 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
     bool settled = false;
     for (int sweep = 0; sweep < 4096; ++sweep) {
       NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
-      count_launch(), k_limit_sweep<<<grid_for(ns), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,
+      count_launch(), k_limit_sweep<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,
                                                                          prm->max_gap, W.i_lvl, W.d_int);
       NB_CUDA(cudaMemcpyAsync(W.h_int, W.d_int, sizeof(int), cudaMemcpyDeviceToHost, st));
       NB_CUDA(cudaStreamSynchronize(st));
@@ -573,7 +587,7 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
     // levels after _land, sorted; need in sorted order, then back to the caller's order
     count_launch(), k_gather_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, W.i_lvl);
     count_launch(), k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, -1, W.i_tmp2);
-    count_launch(), k_wake_need<<<grid_for(ns), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,
+    count_launch(), k_wake_need<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,
                                                                    W.i_lvl, prm->max_gap, W.i_tmp2);
     count_launch(), k_scatter_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, W.i_tmp2, W.need);
     NB_CUDA(cudaMemsetAsync(W.d_i64, 0, sizeof(int64_t), st));
