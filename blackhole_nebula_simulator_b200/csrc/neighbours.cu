@@ -23,9 +23,9 @@ static constexpr int SUB = 8;  // sub-leaf: the unit each lane tests its own sph
 static constexpr int FAN = 8;
 static constexpr int STACK = 96;
 static constexpr int QCAP = 24;  // sub-leaves a lane queues before the warp flushes
-// entries of the fixed-width row scratch of the one-pass build (int32, 16 GiB); larger builds
+// entries of the fixed-width row scratch of the one-pass build (int32, 24 GiB); larger builds
 // count first and fill second
-static constexpr double ELL_MAX_ENTRIES = 4.0 * 1024 * 1024 * 1024;
+static constexpr double ELL_MAX_ENTRIES = 6.0 * 1024 * 1024 * 1024;
 
 // ---------------------------------------------------------------- bounding box
 __global__ void k_bbox_partial(int64_t n, const double* __restrict__ pos, double* __restrict__ part) {
@@ -512,10 +512,11 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
       int64_t nlong = E.h_build[1];
       count_launch(), k_lists_sub<1><<<grid(nlong), NB_THREADS, 0, st>>>(n, nlong, leaves, E.d_rowmax + 3, tv, E.sub_lo, E.sub_hi, L.spos, nullptr, L.off, L.idx, 0, nullptr, E.d_err);
     }
-    // width for the next build: this build's longest row with room to spare, within the
-    // scratch bound (rows beyond it take the CSR redo above)
+    // width for the next build: half as much again as this build's longest row (a redo of the
+    // longest leaves costs far more than idle slots, which are never read), within the scratch
+    // bound (rows beyond it take the CSR redo above)
     int64_t widest = std::min<int64_t>(1024, (int64_t)(ELL_MAX_ENTRIES / (double)n) / 32 * 32);
-    E.row_cap = std::min<int64_t>(std::max<int64_t>((longest + longest / 8 + 31) / 32 * 32, 64), std::max<int64_t>(widest, 64));
+    E.row_cap = std::min<int64_t>(std::max<int64_t>((longest + longest / 2 + 31) / 32 * 32, 256), std::max<int64_t>(widest, 64));
   } else {
     // count, scan, fill
     count_launch(), k_lists_sub<0><<<grid(nleaf), NB_THREADS, 0, st>>>(n, nleaf, order, E.d_rowmax + 2, tv, E.sub_lo, E.sub_hi, L.spos, E.counts, nullptr, nullptr, 0, nullptr, E.d_err);

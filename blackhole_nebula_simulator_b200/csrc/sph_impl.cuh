@@ -426,6 +426,8 @@ __device__ __forceinline__ R dwdr(R r, R h, int kid, R cnorm) {
   return cnorm / (h2 * h2) * kernel_df<R>(r / h, kid);
 }
 
+constexpr int FORCE_QUEUE = 64;  // interacting entries a row queues before its lanes drain them
+
 // Fused pressure + artificial viscosity (+ conductivity) + P dV (+ disc viscosity) pass.  Eight
 // lanes per row (lanes 8g .. 8g+7 of a warp), each taking every eighth list entry; the pair terms
 // are summed per lane and then over the row's lanes.
@@ -459,19 +461,22 @@ __global__ void __launch_bounds__(NB_THREADS, 2)
   Acc<R> ax, ay, az, work, heat, vheat, cheat, dax, day, daz, dheat;
   R vmax = prm.use_visc ? cs_a : R(0);
   int64_t npairs = 0;
-  const int64_t e_end = live ? off[a + 1] : 0;
-  for (int64_t e = (live ? off[a] : 0) + gl; e < e_end; e += 8) {
-    int64_t b = (int64_t)idx[e];
-    if (b == a) continue;
+  // the row's list in rounds of eight entries: lanes test their entry, the interacting ones are
+  // queued in shared memory in list order, and full queues are drained with all eight lanes
+  // busy on pair terms
+  __shared__ int32_t queue_s[NB_THREADS / 8][FORCE_QUEUE + 8];
+  int32_t* pq = queue_s[threadIdx.x >> 3];
+  const int g = (threadIdx.x & 31) >> 3;
+  const int64_t e_beg = live ? off[a] : 0, e_end = live ? off[a + 1] : 0;
+  const unsigned len = (unsigned)(e_end - e_beg);
+  const unsigned maxlen = __reduce_max_sync(FULL, len);
+  int pc = 0;
+  auto pair = [&](int64_t b) {
     R ddx, ddy, ddz;
     geo.diff(a, b, ddx, ddy, ddz);  // x_b - x_a
     const V4 hb4 = hydro[b];
     const R h_b = (R)hb4.x;
     R d2 = sqdist(ddx, ddy, ddz);
-    if (prm.tighten) {
-      R rr = R(2) * (h_a > h_b ? h_a : h_b);
-      if (!(d2 < rr * rr)) continue;
-    }
     npairs += 1;
     const V4 vb = vm[b];
     const R rho_b = (R)hb4.y, om_b = (R)hb4.z, P_b = (R)hb4.w;
@@ -532,7 +537,34 @@ __global__ void __launch_bounds__(NB_THREADS, 2)
       daz.add(-(f * ez / r));
       dheat.add(m_b * qa * vdr * fa);
     }
+    };
+  auto drain = [&]() {
+    for (int k2 = gl; k2 < pc; k2 += 8) pair((int64_t)pq[k2]);
+    __syncwarp();
+    pc = 0;
+  };
+  for (unsigned base = 0; base < maxlen; base += 8) {
+    bool take = false;
+    int64_t b = 0;
+    if (base + gl < len) {
+      b = (int64_t)idx[e_beg + base + gl];
+      if (b != a) {
+        take = true;
+        if (prm.tighten) {
+          R ddx, ddy, ddz;
+          geo.diff(a, b, ddx, ddy, ddz);
+          const R h_b = (R)hydro[b].x;
+          R rr = R(2) * (h_a > h_b ? h_a : h_b);
+          take = sqdist(ddx, ddy, ddz) < rr * rr;
+        }
+      }
+    }
+    unsigned seg = (__ballot_sync(FULL, take) >> (8 * g)) & 0xffu;
+    if (take) pq[pc + __popc(seg & ((1u << gl) - 1u))] = (int32_t)b;
+    pc += __popc(seg);
+    if (__any_sync(FULL, pc > FORCE_QUEUE - 8)) drain();
   }
+  drain();
   // sums over the row's eight lanes (uniform flags: every lane takes part in every reduction)
   double s_ax = 0, s_ay = 0, s_az = 0, s_work = 0, s_heat = 0, s_vheat = 0, s_cheat = 0;
   double s_dax = 0, s_day = 0, s_daz = 0, s_dheat = 0;
