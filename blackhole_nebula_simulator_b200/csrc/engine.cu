@@ -2,7 +2,7 @@
 // search-doubling loop, the fused EOS + force pass, and the shared-step and block-step drivers.
 //
 // State arrays stay in the caller's particle order.  Each list build sorts the particles in
-// Morton order; the pair passes read packed copies in that order (coalesced, cache-friendly) and
+// Hilbert-curve order; the pair passes read packed copies in that order (coalesced, cache-friendly) and
 // scatter their results back to the caller's order.
 #include <cub/cub.cuh>
 
@@ -335,7 +335,7 @@ __global__ void k_combine_rows(int64_t nrows, const int64_t* __restrict__ rows, 
   vsig[i] = use_visc ? vsig_f[i] : cs[i];
 }
 
-// touched sets over Morton-ordered rows: pk holds sorted (x, y, z, h) of the current state; marks
+// touched sets over curve-ordered rows: pk holds sorted (x, y, z, h) of the current state; marks
 // go to the caller-order mask.  Eight lanes per row, each taking every eighth list entry.
 __global__ void k_mark_s(int64_t nrows, const int64_t* __restrict__ rows_s,
                          const int32_t* __restrict__ perm, const int64_t* __restrict__ off,
@@ -514,7 +514,7 @@ static int sum_rows_i64(Engine& E, int64_t nrows, const int64_t* rows, const int
   return 0;
 }
 
-// The rows (caller order) as sorted positions in ascending Morton order, into W.rows_s; the
+// The rows (caller order) as sorted positions in ascending curve order, into W.rows_s; the
 // pair passes then walk neighbouring particles in neighbouring threads.
 static int rows_sorted(Engine& E, int64_t n, int64_t nrows, const int64_t* rows, int64_t* count,
                        cudaStream_t st) {

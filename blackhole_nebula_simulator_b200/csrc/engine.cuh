@@ -15,7 +15,7 @@ namespace nbk {
 
 constexpr int MAX_LEVELS = 16;
 
-// Symmetric lists of the last build, in sorted (Morton) order: row k belongs to the particle
+// Symmetric lists of the last build, in sorted (Hilbert-curve) order: row k belongs to the particle
 // perm[k] of the caller's order; entries are sorted positions.
 struct Lists {
   int64_t n = 0, total = 0;

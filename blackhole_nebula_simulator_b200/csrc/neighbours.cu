@@ -1,4 +1,4 @@
-// Neighbour lists on the GPU: Morton-sorted particles, an implicit 8-ary tree of boxes over
+// Neighbour lists on the GPU: particles sorted along a Hilbert curve, an implicit 8-ary tree of boxes over
 // leaves of 32 consecutive sorted particles, and a warp-per-leaf traversal that writes exact
 // symmetric lists.
 //
@@ -10,7 +10,7 @@
 // least 2 max(h_query_max, h_node_max) (with a 1e-12 relative margin on the safe side), which
 // can never drop a pair the test above accepts.
 //
-// Rows come out in sorted (Morton) order with each row's entries in ascending sorted index.
+// Rows come out in sorted (curve) order with each row's entries in ascending sorted index.
 #include <cub/cub.cuh>
 
 #include "common.cuh"
@@ -78,7 +78,7 @@ __global__ void k_bbox_final(int nb, const double* __restrict__ part, double* __
     for (int c = 0; c < 6; ++c) box6[c] = s[c][0];
 }
 
-// ---------------------------------------------------------------- Morton keys
+// ---------------------------------------------------------------- curve keys
 __device__ __forceinline__ uint64_t spread21(uint64_t v) {
   v &= 0x1fffffull;
   v = (v | (v << 32)) & 0x1f00000000ffffull;
@@ -89,19 +89,52 @@ __device__ __forceinline__ uint64_t spread21(uint64_t v) {
   return v;
 }
 
-__global__ void k_morton(int64_t n, const double* __restrict__ pos, const double* __restrict__ box6,
-                         uint64_t* __restrict__ keys, int32_t* __restrict__ vals) {
+// Hilbert index of a point on the 2^21 grid over the bounding box: J. Skilling's transform
+// ("Programming the Hilbert curve", AIP Conf. Proc. 707, 2004) from axes to the transposed
+// index, then the three coordinates' bits interleaved (first axis most significant).  Runs of
+// consecutive particles along the Hilbert curve have tighter boxes than Morton runs (fewer jumps
+// between distant octants), so leaves and sub-leaves prune better.
+__device__ __forceinline__ uint64_t hilbert_key(uint32_t x0, uint32_t x1, uint32_t x2) {
+  uint32_t X[3] = {x0, x1, x2};
+  const uint32_t M = 1u << 20;
+  for (uint32_t Q = M; Q > 1; Q >>= 1) {
+    const uint32_t P = Q - 1;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (X[i] & Q) {
+        X[0] ^= P;  // invert the low bits of the first axis
+      } else {
+        uint32_t t = (X[0] ^ X[i]) & P;  // exchange the low bits of axes 0 and i
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  X[1] ^= X[0];  // Gray encode
+  X[2] ^= X[1];
+  uint32_t t = 0;
+  for (uint32_t Q = M; Q > 1; Q >>= 1)
+    if (X[2] & Q) t ^= Q - 1;
+  X[0] ^= t;
+  X[1] ^= t;
+  X[2] ^= t;
+  return (spread21(X[0]) << 2) | (spread21(X[1]) << 1) | spread21(X[2]);
+}
+
+__global__ void k_curve_keys(int64_t n, const double* __restrict__ pos,
+                             const double* __restrict__ box6, uint64_t* __restrict__ keys,
+                             int32_t* __restrict__ vals) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   double span = fmax(fmax(box6[3] - box6[0], box6[4] - box6[1]), box6[5] - box6[2]);
   double scale = span > 0 ? 2097151.0 / span : 0.0;
-  uint64_t q[3];
+  uint32_t q[3];
   for (int c = 0; c < 3; ++c) {
     double t = (pos[3 * i + c] - box6[c]) * scale;
     t = fmin(fmax(t, 0.0), 2097151.0);
-    q[c] = (uint64_t)t;
+    q[c] = (uint32_t)t;
   }
-  keys[i] = (spread21(q[0]) << 2) | (spread21(q[1]) << 1) | spread21(q[2]);
+  keys[i] = hilbert_key(q[0], q[1], q[2]);
   vals[i] = (int32_t)i;
 }
 
@@ -319,7 +352,7 @@ __device__ __forceinline__ int64_t leaf_rows(int64_t leaf, int64_t n, const Tree
 }
 
 // Persistent list kernel: each warp takes the next query leaf from `order` (heaviest first) until
-// none is left, so a few slow leaves (sparse regions whose 32 Morton-consecutive particles spread
+// none is left, so a few slow leaves (sparse regions whose 32 curve-consecutive particles spread
 // far) overlap with the rest instead of holding whole blocks.  PASS 2 also records the longest
 // row in *rowmax.
 template <int PASS>
@@ -437,11 +470,11 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
   }
   Lists& L = E.lists;
   E.prof.begin(st);
-  // bounding box and Morton keys
+  // bounding box and Hilbert keys
   int nbb = (int)std::min<int64_t>(grid_for(n), 1184);
   count_launch(), k_bbox_partial<<<nbb, NB_THREADS, 0, st>>>(n, pos, E.bbox_part);
   count_launch(), k_bbox_final<<<1, NB_THREADS, 0, st>>>(nbb, E.bbox_part, E.bbox);
-  count_launch(), k_morton<<<grid_for(n), NB_THREADS, 0, st>>>(n, pos, E.bbox, E.keys_a, E.vals_a);
+  count_launch(), k_curve_keys<<<grid_for(n), NB_THREADS, 0, st>>>(n, pos, E.bbox, E.keys_a, E.vals_a);
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceRadixSort::SortPairs(E.cub_tmp, tmp, E.keys_a, E.keys_b, E.vals_a, L.perm,
                                           (int)n, 0, 63, st));

@@ -123,7 +123,7 @@ __device__ __forceinline__ void cached_sums(const R* rr, const R* mm, int cnt, R
 }
 
 // In-range entries a row may cache in its thread's local array (0: every sum walks the list; a
-// per-thread cache in local memory measured slower than re-walking the Morton-local list).
+// per-thread cache in local memory measured slower than re-walking the curve-local list).
 constexpr int DENSITY_CACHE = 0;
 
 // One thread per row (the FP64 form: its shared-memory cache of (r, m) in double would hold

@@ -400,7 +400,7 @@ __global__ void k_wanted_levels(int64_t nrows, const int64_t* __restrict__ rows,
 }
 
 // one sweep of the level limiter over the rows' interacting pairs (sim/blocks.py:337-353), on
-// Morton-ordered rows with sorted (x, h) and a sorted copy of the levels; the least fixed point
+// curve-ordered rows with sorted (x, h) and a sorted copy of the levels; the least fixed point
 // above the start is unique, so in-place sweeps reach the reference's levels
 __global__ void k_limit_sweep(int64_t nrows, const int64_t* __restrict__ rows_s,
                               const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
@@ -477,7 +477,7 @@ __global__ void k_land(int64_t nrows, const int64_t* __restrict__ rows, int64_t 
 }
 
 // _wake_targets (sim/blocks.py:356-364): need[j] = max over active i of level_i - max_gap, on
-// Morton-ordered rows into a sorted need array
+// curve-ordered rows into a sorted need array
 __global__ void k_wake_need(int64_t nrows, const int64_t* __restrict__ rows_s,
                             const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
                             const double4* __restrict__ pk, const int64_t* __restrict__ level_s,
@@ -563,7 +563,7 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
   NB_TRY(check_device_error(E, st));
   int64_t ns = 0;
   if (prm->limiter) {
-    // Morton-ordered rows, sorted (x, h) and a sorted copy of the levels
+    // curve-ordered rows, sorted (x, h) and a sorted copy of the levels
     NB_TRY(sorted_rows_and_pack(E, nrows, rows, s->x, s->h, &ns, st));
     count_launch(), k_gather_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, W.i_lvl);
     bool settled = false;

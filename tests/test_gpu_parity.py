@@ -2,7 +2,7 @@
 
 Tolerances: neighbour lists, cells, levels and tick counters exactly; FP64 single-call kernels
 at rtol 1e-12 (the reference's own Numba-vs-readable tolerance); the GN flow bit for bit; whole
-FP64 steps at the tolerances of the oracle's own pinning (sums run in Morton order on the GPU,
+FP64 steps at the tolerances of the oracle's own pinning (sums run in Hilbert-curve order on the GPU,
 so they differ from the reference's list order by rounding only).
 """
 
