@@ -375,12 +375,19 @@ int nb_block_land(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* stream)
 int nb_profile(nb_ctx* ctx, int on) {
   NB_TRY(begin(ctx));
   nbk::Prof& P = ctx->E.prof;
+  nbk::Engine& E = ctx->E;
+  P.flush();
   P.on = on != 0;
+  P.open = false;
   for (int c = 0; c < nbk::PROF_NCAT; ++c) {
     P.ms[c] = 0;
     P.launches[c] = 0;
     P.units[c] = 0;
     P.pairs[c] = 0;
+  }
+  if (P.on) {
+    if (P.ensure() != 0) return nbk::set_host_error(E, "profile events could not be created");
+    NB_CUDA(cudaMemset(P.d_pairs, 0, sizeof(unsigned long long) * nbk::PROF_NCAT));
   }
   return 0;
 }
@@ -388,11 +395,15 @@ int nb_profile(nb_ctx* ctx, int on) {
 int nb_profile_read(nb_ctx* ctx, double* out) {
   NB_TRY(begin(ctx));
   nbk::Prof& P = ctx->E.prof;
+  nbk::Engine& E = ctx->E;
+  P.flush();
+  unsigned long long dev[nbk::PROF_NCAT] = {0};
+  if (P.d_pairs) NB_CUDA(cudaMemcpy(dev, P.d_pairs, sizeof(dev), cudaMemcpyDeviceToHost));
   for (int c = 0; c < nbk::PROF_NCAT; ++c) {
+    out[4 * c + 3] = P.pairs[c] + (double)dev[c];
     out[4 * c + 0] = P.ms[c];
     out[4 * c + 1] = (double)P.launches[c];
     out[4 * c + 2] = P.units[c];
-    out[4 * c + 3] = P.pairs[c];
   }
   return 0;
 }

@@ -52,8 +52,6 @@ int Engine::ensure_n(int64_t n) {
     NB_CUDA(cudaMallocHost((void**)&h_red, sizeof(double) * 64));
     NB_CUDA(cudaMalloc((void**)&d_rowmax, 4 * sizeof(unsigned long long)));
     NB_CUDA(cudaMallocHost((void**)&h_build, sizeof(int64_t) * 2));
-    NB_CUDA(cudaEventCreate(&prof.a));
-    NB_CUDA(cudaEventCreate(&prof.b));
   }
   if (n <= cap_n && keys_a) return 0;
   int64_t c = std::max<int64_t>(n + n / 4, 1024);
@@ -75,6 +73,15 @@ int Engine::ensure_n(int64_t n) {
   cap_n = c;
   lists.n = 0;
   return ensure_cub(cub_bytes_needed(c, 0));
+}
+
+int Prof::ensure() {
+  if (ev[0]) return 0;
+  for (int k = 0; k < 2 * POOL; ++k)
+    if (cudaEventCreate(&ev[k]) != cudaSuccess) return -2;
+  if (cudaMalloc((void**)&d_pairs, sizeof(unsigned long long) * PROF_NCAT) != cudaSuccess) return -2;
+  if (cudaMemset(d_pairs, 0, sizeof(unsigned long long) * PROF_NCAT) != cudaSuccess) return -2;
+  return 0;
 }
 
 int Engine::ensure_nodes(int64_t m) { return grow2(m); }
@@ -128,6 +135,7 @@ void Engine::release() {
     if (p) cudaFree(p);
   if (h_err) cudaFreeHost(h_err);
   if (h_build) cudaFreeHost(h_build);
+  prof.release();
   if (h_red) cudaFreeHost(h_red);
   ws.release();
 }
@@ -289,9 +297,11 @@ __global__ void k_pack_sorted4(int64_t n, const int32_t* __restrict__ perm, cons
 // packed 10 bits per axis, and the float offset from the cell centre.
 __global__ void k_pack_sorted32(int64_t n, const int32_t* __restrict__ perm,
                                 const double* __restrict__ x, const double* __restrict__ box6,
-                                double cell, float4* __restrict__ out) {
+                                float4* __restrict__ out) {
   int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (k >= n) return;
+  double span = fmax(fmax(box6[3] - box6[0], box6[4] - box6[1]), box6[5] - box6[2]);
+  const double cell = fmax(span / 1000.0, 1e-30);
   int64_t i = perm[k];
   int c[3];
   float o[3];
@@ -499,19 +509,27 @@ __global__ void k_gather_rows_i64(int64_t nrows, const int64_t* __restrict__ row
 }
 
 // sum of a[rows] into E.ws.h_i64[0] (profiling only)
-static int sum_rows_i64(Engine& E, int64_t nrows, const int64_t* rows, const int64_t* a,
-                        cudaStream_t st) {
-  Workspace& W = E.ws;
-  if (nrows <= 0) {
-    W.h_i64[0] = 0;
-    return 0;
+// profile: add a[rows] into the device counter of category `cat` (no host synchronisation)
+__global__ void k_prof_sum_rows(int64_t nrows, const int64_t* __restrict__ rows,
+                                const int64_t* __restrict__ a, unsigned long long* __restrict__ acc) {
+  __shared__ unsigned long long s[NB_THREADS / 32];
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  unsigned long long v = q < nrows ? (unsigned long long)a[rows[q]] : 0ull;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int w = 0; w < NB_THREADS / 32; ++w) t += s[w];
+    atomicAdd(acc, t);
   }
-  count_launch(), k_gather_rows_i64<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, a, W.i_tmp);
-  size_t tmp = E.cub_bytes;
-  NB_CUDA(cub::DeviceReduce::Sum(E.cub_tmp, tmp, W.i_tmp, W.d_i64, (int)nrows, st));
-  NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
-  return 0;
+}
+
+static void prof_pairs(Engine& E, int cat, int64_t nrows, const int64_t* rows, const int64_t* a,
+                       cudaStream_t st) {
+  if (nrows <= 0 || E.prof.ensure() != 0) return;
+  count_launch(), k_prof_sum_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, a, E.prof.d_pairs + cat);
 }
 
 // The rows (caller order) as sorted positions in ascending curve order, into W.rows_s; the
@@ -548,14 +566,11 @@ static int density_on_lists(Engine& E, int64_t n, const double* x, const double*
   count_launch(), k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, h_search, W.d_c);
   DensityParams dp{prm->kernel_id, prm->cnorm, prm->eta, prm->tol, prm->h_max};
   if (prm->precision == 1) {
-    double span = 0;
-    NB_CUDA(cudaMemcpyAsync(W.h_dbl, E.bbox, sizeof(double) * 6, cudaMemcpyDeviceToHost, st));
-    NB_CUDA(cudaStreamSynchronize(st));
-    for (int a = 0; a < 3; ++a) span = std::max(span, W.h_dbl[3 + a] - W.h_dbl[a]);
-    double cell = std::max(span / 1000.0, 1e-30);
-    count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, E.bbox, cell, W.pk32);
+    // grid over the box of the last list build (cells clamp to it; the edge is derived on the
+    // device, so no host round trip)
+    count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, E.bbox, W.pk32);
     E.prof.begin(st);
-    launch_density32<int32_t>(nrows, W.rows_s, W.pk32, (float)cell, W.d_a, W.d_b, W.d_c, L.off,
+    launch_density32<int32_t>(nrows, W.rows_s, W.pk32, E.bbox, W.d_a, W.d_b, W.d_c, L.off,
                               L.idx, dp, L.perm, h_out, rho, omega, W.iters, W.flags,
                               E.prof.on ? W.pairs : nullptr, st);
   } else {
@@ -568,9 +583,7 @@ static int density_on_lists(Engine& E, int64_t n, const double* x, const double*
   if (E.prof.on) {
     // kernel evaluations inside the support (pair evaluations summed over every Newton sum)
     E.prof.end(PROF_DENSITY, st, (double)nrows, 0.0);
-    NB_CUDA(cudaMemsetAsync(W.d_i64, 0, sizeof(int64_t), st));
-    NB_TRY(sum_rows_i64(E, nrows, rows, W.pairs, st));
-    E.prof.pairs[PROF_DENSITY] += (double)W.h_i64[0];
+    prof_pairs(E, PROF_DENSITY, nrows, rows, W.pairs, st);
   }
   NB_CUDA(cudaGetLastError());
   return 0;
@@ -752,15 +765,9 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   fo.ddudt = W.d_ddudt;
   fo.pairs = W.pairs;
   if (prm->precision == 1) {
-    NB_CUDA(cudaMemcpyAsync(W.h_dbl, E.bbox, sizeof(double) * 6, cudaMemcpyDeviceToHost, st));
-    NB_CUDA(cudaStreamSynchronize(st));
-    double span = 0;
-    for (int a = 0; a < 3; ++a) span = std::max(span, W.h_dbl[3 + a] - W.h_dbl[a]);
-    // the grid must cover the current positions: recompute the box when particles moved
-    double cell = std::max(span / 1000.0, 1e-30);
-    count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, E.bbox, cell, W.pk32);
+    count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, E.bbox, W.pk32);
     E.prof.begin(st);
-    launch_forces32<int32_t>(nrows, W.rows_s, W.pk32, (float)cell, W.pf1, W.pf2, W.pf3, L.off,
+    launch_forces32<int32_t>(nrows, W.rows_s, W.pk32, E.bbox, W.pf1, W.pf2, W.pf3, L.off,
                              L.idx, fp, L.perm, fo, st);
   } else {
     count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, nullptr, W.pk0);
@@ -771,8 +778,7 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   if (E.prof.on) {
     E.prof.end(PROF_FORCES, st, (double)nrows, 0.0);
     // interacting pairs of the rows (written per row by the kernel)
-    NB_TRY(sum_rows_i64(E, nrows, rows, W.pairs, st));
-    E.prof.pairs[PROF_FORCES] += (double)W.h_i64[0];
+    prof_pairs(E, PROF_FORCES, nrows, rows, W.pairs, st);
   }
   count_launch(), k_combine_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(
       nrows, rows, prm->viscosity, prm->disc_alpha_av, W.v_dacc, W.d_ddudt, W.d_cs, s->h,

@@ -68,27 +68,54 @@ struct Workspace {
 };
 
 // Live timing of the main kernels with CUDA events on the launching stream (off by default).
+// Event pairs are recorded into a pool and read only when the profile is read (or the pool is
+// full), and pair counts are summed on the device, so profiling adds no host synchronisation to
+// the steps it times.
 enum ProfCat { PROF_LISTS = 0, PROF_DENSITY = 1, PROF_FORCES = 2, PROF_FLOW = 3, PROF_NCAT = 4 };
 struct Prof {
+  static constexpr int POOL = 1024;
   bool on = false;
-  cudaEvent_t a = nullptr, b = nullptr;
+  cudaEvent_t ev[2 * POOL] = {};
+  int cat[POOL] = {};
+  int used = 0;        // event pairs recorded and not yet read
+  bool open = false;   // a begin() without its end()
   double ms[PROF_NCAT] = {0};
   int64_t launches[PROF_NCAT] = {0};
   double units[PROF_NCAT] = {0};   // rows (density, forces, flow) or particles (lists)
-  double pairs[PROF_NCAT] = {0};   // list entries read (lists: entries written)
+  double pairs[PROF_NCAT] = {0};   // host-known counts (lists: entries written)
+  unsigned long long* d_pairs = nullptr;  // device-summed counts (density, forces)
+  int ensure();
   void begin(cudaStream_t st) {
-    if (on) cudaEventRecord(a, st);
-  }
-  void end(int cat, cudaStream_t st, double u, double pr) {
     if (!on) return;
-    cudaEventRecord(b, st);
-    cudaEventSynchronize(b);
-    float t = 0.f;
-    cudaEventElapsedTime(&t, a, b);
-    ms[cat] += t;
-    launches[cat] += 1;
-    units[cat] += u;
-    pairs[cat] += pr;
+    if (used == POOL) flush();
+    if (ensure() != 0) return;
+    cudaEventRecord(ev[2 * used], st);
+    open = true;
+  }
+  void end(int c, cudaStream_t st, double u, double pr) {
+    if (!on || !open) return;
+    cudaEventRecord(ev[2 * used + 1], st);
+    cat[used] = c;
+    used += 1;
+    open = false;
+    launches[c] += 1;
+    units[c] += u;
+    pairs[c] += pr;
+  }
+  // waits for the recorded pairs and adds their times
+  void flush() {
+    for (int k = 0; k < used; ++k) {
+      float t = 0.f;
+      cudaEventSynchronize(ev[2 * k + 1]);
+      cudaEventElapsedTime(&t, ev[2 * k], ev[2 * k + 1]);
+      ms[cat[k]] += t;
+    }
+    used = 0;
+  }
+  void release() {
+    for (int k = 0; k < 2 * POOL; ++k)
+      if (ev[k]) cudaEventDestroy(ev[k]);
+    if (d_pairs) cudaFree(d_pairs);
   }
 };
 

@@ -41,7 +41,7 @@ void launch_density64(int64_t nrows, const int64_t* rows, const double4* pos, co
                       double* rho, double* omega, int64_t* iters, int64_t* flags, int64_t* work,
                       cudaStream_t st);
 template <typename I>
-void launch_density32(int64_t nrows, const int64_t* rows, const float4* pos, float cell,
+void launch_density32(int64_t nrows, const int64_t* rows, const float4* pos, const double* box6,
                       const double* mass, const double* h_start, const double* h_search,
                       const int64_t* off, const I* idx, DensityParams prm, const int32_t* out_map,
                       double* h_out, double* rho, double* omega, int64_t* iters, int64_t* flags,
@@ -51,7 +51,7 @@ void launch_forces64(int64_t nrows, const int64_t* rows, const double4* pos, con
                      const double4* hydro, const double4* aux, const int64_t* off, const I* idx,
                      ForceParams prm, const int32_t* out_map, ForceOut out, cudaStream_t st);
 template <typename I>
-void launch_forces32(int64_t nrows, const int64_t* rows, const float4* pos, float cell,
+void launch_forces32(int64_t nrows, const int64_t* rows, const float4* pos, const double* box6,
                      const float4* vm, const float4* hydro, const float4* aux,
                      const int64_t* off, const I* idx, ForceParams prm, const int32_t* out_map,
                      ForceOut out, cudaStream_t st);

@@ -18,6 +18,7 @@ namespace nbk {
 // FP64: packed (x, y, z, w) doubles.  dx = x_j - x_i as the reference forms it.
 struct Pos64 {
   const double4* p;
+  __device__ __forceinline__ void ready() {}
   __device__ __forceinline__ void diff(int64_t i, int64_t j, double& dx, double& dy,
                                        double& dz) const {
     double4 a = p[i], b = p[j];
@@ -33,6 +34,14 @@ struct Pos64 {
 struct Pos32 {
   const float4* p;  // (ox, oy, oz, packed cell: 10 bits per axis)
   float cell;
+  const double* box6 = nullptr;  // grid corner and far corner; the edge is derived on the device
+  // edge of the grid cells: the largest side of the box over 1000, as the packing kernel uses
+  __device__ __forceinline__ void ready() {
+    if (box6) {
+      double span = fmax(fmax(box6[3] - box6[0], box6[4] - box6[1]), box6[5] - box6[2]);
+      cell = (float)fmax(span / 1000.0, 1e-30);
+    }
+  }
   __device__ __forceinline__ void diff(int64_t i, int64_t j, float& dx, float& dy,
                                        float& dz) const {
     float4 a = p[i], b = p[j];
@@ -131,12 +140,14 @@ constexpr int DENSITY_CACHE = 0;
 
 template <typename R, typename PosT, typename I>
 __global__ void __launch_bounds__(NB_THREADS)
-    k_density_thread(int64_t nrows, const int64_t* __restrict__ rows, PosT geo,
+    k_density_thread(int64_t nrows, const int64_t* __restrict__ rows, PosT geo_in,
               const double* __restrict__ mass, const double* __restrict__ h_start,
               const double* __restrict__ h_search, const int64_t* __restrict__ off,
               const I* __restrict__ idx, DensityParams prm, const int32_t* __restrict__ out_map,
               double* __restrict__ h_out, double* __restrict__ rho, double* __restrict__ omega,
               int64_t* __restrict__ iters, int64_t* __restrict__ flags, int64_t* __restrict__ work) {
+  PosT geo = geo_in;
+  geo.ready();
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= nrows) return;
   int64_t i = rows ? rows[q] : q;
@@ -267,12 +278,14 @@ constexpr int DENSITY_THREADS = 128;  // 16 rows per block
 // Rows with more in-range entries than the cache holds re-walk their list in every sum.
 template <typename R, typename PosT, typename I>
 __global__ void __launch_bounds__(DENSITY_THREADS)
-    k_density(int64_t nrows, const int64_t* __restrict__ rows, PosT geo,
+    k_density(int64_t nrows, const int64_t* __restrict__ rows, PosT geo_in,
               const double* __restrict__ mass, const double* __restrict__ h_start,
               const double* __restrict__ h_search, const int64_t* __restrict__ off,
               const I* __restrict__ idx, DensityParams prm, const int32_t* __restrict__ out_map,
               double* __restrict__ h_out, double* __restrict__ rho, double* __restrict__ omega,
               int64_t* __restrict__ iters, int64_t* __restrict__ flags, int64_t* __restrict__ work) {
+  PosT geo = geo_in;
+  geo.ready();
   using E2 = typename DensityEntry<R>::T;
   constexpr int CAP = DensityEntry<R>::CAP;
   __shared__ E2 cache_s[DENSITY_THREADS / 8][CAP];
@@ -433,12 +446,14 @@ constexpr int FORCE_QUEUE = 64;  // interacting entries a row queues before its 
 // are summed per lane and then over the row's lanes.
 template <typename R, typename PosT, typename I, typename V4>
 __global__ void __launch_bounds__(NB_THREADS, 2)
-    k_forces_g(int64_t nrows, const int64_t* __restrict__ rows, PosT geo,
+    k_forces_g(int64_t nrows, const int64_t* __restrict__ rows, PosT geo_in,
              const V4* __restrict__ vm,    // (vx, vy, vz, mass)
              const V4* __restrict__ hydro, // (h, rho, omega, P)
              const V4* __restrict__ aux,   // (u, c_s, alpha, unused)
              const int64_t* __restrict__ off, const I* __restrict__ idx, ForceParams prm,
              const int32_t* __restrict__ out_map, ForceOut out) {
+  PosT geo = geo_in;
+  geo.ready();
   const unsigned FULL = 0xffffffffu;
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t q = t >> 3;
