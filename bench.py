@@ -394,6 +394,10 @@ def main():
             "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
             "data": "synthetic", "config": config, "roofline": rf, "clocks": clocks, "e2e": e2e,
             "gpu_launches": launches, "kernel_ms": {k: round(v["ms"], 3) for k, v in prof.items()},
+            "kernel_detail": {k: {"launches": v["launches"], "units_per_launch":
+                                  round(v["units"] / max(v["launches"], 1)),
+                                  "pairs_per_launch": round(v["pairs"] / max(v["launches"], 1))}
+                              for k, v in prof.items()},
             "mean_active": total / args.steps / max(world, 1),
             "list_builds": st.builds, "list_reuses": st.reuses,
             "mean_list_entries": (prof["lists"]["pairs"] / prof["lists"]["units"]

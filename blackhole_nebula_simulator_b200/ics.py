@@ -80,15 +80,21 @@ def cloud(n: int = 4096, radius: float = 100.0, total_mass: float = 2.3e-8,
 
 def streams(n: int = 1_048_576, radius: float = 20.0, length: float = 400.0,
             r_collide: float = 1664.0, v_rel: float = 0.056, rho_cgs: float = 1.0e-10,
-            t_kelvin: float = 1.0e4, gap: float = 4.0, kernel: str = "cubic",
+            t_kelvin: float = 1.0e4, gap: float | None = None, kernel: str = "cubic",
             seed: int = 3) -> InitialConditions:  # fmt: skip
     """Two opposing cylinders (radius, length) along y meeting head-on at (r_collide, 0, 0),
     each moving at v_rel/2 toward the other, filled from seeded jittered lattices (n/2 points
-    nearest each axis), uniform density rho_cgs (g/cm^3) and temperature t_kelvin."""
+    nearest each axis), uniform density rho_cgs (g/cm^3) and temperature t_kelvin.
+
+    The streams start `gap` apart (default: one lattice spacing), inside each other's kernel
+    support, so the first step's signal speeds already see the collision; a gap wider than the
+    support lets the first (longest) step run through the onset of the shock unresolved."""
     rng = np.random.default_rng(seed)
     half = n // 2
     vol = math.pi * radius**2 * length
     spacing = (vol / half) ** (1.0 / 3.0)
+    if gap is None:
+        gap = spacing
     pts = _jittered_lattice(rng, spacing, (-radius - spacing, 0.0, -radius - spacing),
                             (radius + spacing, length, radius + spacing))  # fmt: skip
     rc = np.hypot(pts[:, 0], pts[:, 2])
