@@ -193,6 +193,17 @@ def roofline(prof, precision, disc, pk):
     return rf, dom
 
 
+def combine_ranks(ms, psteps, device):
+    """Replicas: the job's time is the slowest rank's, its work the sum over ranks."""
+    import torch
+
+    t = torch.tensor([ms, float(psteps)], dtype=torch.float64, device=device)
+    tmax = t.clone()
+    torch.distributed.all_reduce(tmax, op=torch.distributed.ReduceOp.MAX)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+    return float(tmax[0]), float(t[1])
+
+
 def run_gpu(args, rank, world, precision=None, use_mlp=None, e2e=True):
     import torch
 
@@ -233,11 +244,7 @@ def run_gpu(args, rank, world, precision=None, use_mlp=None, e2e=True):
     ms = e0.elapsed_time(e1)
     psteps = st.particle_steps - steps0
     if world > 1:
-        t = torch.tensor([ms, float(psteps)], dtype=torch.float64, device=dev)
-        tmax = t.clone()
-        torch.distributed.all_reduce(tmax[:1], op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(t[1:], op=torch.distributed.ReduceOp.SUM)
-        ms, total = float(tmax[0]), float(t[1])
+        ms, total = combine_ranks(ms, psteps, dev)
     else:
         total = float(psteps)
     mlp = cooling.mlp_stats(reset=True) if use_mlp else None
