@@ -61,6 +61,16 @@ __device__ __forceinline__ double d2_exact(double dx, double dy, double dz) {
   return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
 }
 
+// List entries are read once per pass: load them with the streaming hint (evict first), so they
+// do not push the gathered neighbour records out of L2.
+template <typename I>
+__device__ __forceinline__ I ld_stream(const I* p) {
+  if constexpr (sizeof(I) == 4)
+    return (I)__ldcs(reinterpret_cast<const int*>(p));
+  else
+    return (I)__ldcs(reinterpret_cast<const long long*>(p));
+}
+
 // Kahan-compensated accumulator for the FP32 pair sums.
 struct Kahan {
   float s, c;

@@ -359,7 +359,7 @@ __global__ void k_mark_s(int64_t nrows, const int64_t* __restrict__ rows_s,
   if (gl == 0) mark[perm[k]] = 1;
   double4 me = pk[k];
   for (int64_t e = off[k] + gl; e < off[k + 1]; e += 8) {
-    int32_t js = idx[e];
+    int32_t js = ld_stream(idx + e);
     if (tight) {
       double4 o = pk[js];
       double d2 = d2_exact(o.x - me.x, o.y - me.y, o.z - me.z);

@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(DENSITY_THREADS)
     bool inr = false;
     R r = R(0), m = R(0);
     if (b + gl < len) {
-      int64_t j = (int64_t)idx[e0 + b + gl];
+      int64_t j = (int64_t)ld_stream(idx + e0 + b + gl);
       R dx, dy, dz;
       geo.diff(i, j, dx, dy, dz);
       R d2 = sqdist(dx, dy, dz);
@@ -440,12 +440,15 @@ __device__ __forceinline__ R dwdr(R r, R h, int kid, R cnorm) {
 }
 
 constexpr int FORCE_QUEUE = 64;  // interacting entries a row queues before its lanes drain them
+// resident blocks per SM the FP32 force pass is compiled for (registers: 65536 / (256 * 3) = 85;
+// the FP64 form keeps 2, its doubles would spill)
+constexpr int FORCE_BLOCKS_PER_SM_FP32 = 3;
 
 // Fused pressure + artificial viscosity (+ conductivity) + P dV (+ disc viscosity) pass.  Eight
 // lanes per row (lanes 8g .. 8g+7 of a warp), each taking every eighth list entry; the pair terms
 // are summed per lane and then over the row's lanes.
 template <typename R, typename PosT, typename I, typename V4>
-__global__ void __launch_bounds__(NB_THREADS, 2)
+__global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? FORCE_BLOCKS_PER_SM_FP32 : 2)
     k_forces_g(int64_t nrows, const int64_t* __restrict__ rows, PosT geo_in,
              const V4* __restrict__ vm,    // (vx, vy, vz, mass)
              const V4* __restrict__ hydro, // (h, rho, omega, P)
@@ -562,7 +565,7 @@ __global__ void __launch_bounds__(NB_THREADS, 2)
     bool take = false;
     int64_t b = 0;
     if (base + gl < len) {
-      b = (int64_t)idx[e_beg + base + gl];
+      b = (int64_t)ld_stream(idx + e_beg + base + gl);
       if (b != a) {
         take = true;
         if (prm.tighten) {

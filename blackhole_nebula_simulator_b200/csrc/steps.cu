@@ -417,7 +417,7 @@ __global__ void k_limit_sweep(int64_t nrows, const int64_t* __restrict__ rows_s,
     double4 me = pk[k];
     need = ((volatile int64_t*)level_s)[k];
     for (int64_t e = off[k] + gl; e < off[k + 1]; e += 8) {
-      int32_t js = idx[e];
+      int32_t js = ld_stream(idx + e);
       double4 o = pk[js];
       double d2 = d2_exact(o.x - me.x, o.y - me.y, o.z - me.z);
       double rr = 2.0 * fmax(me.w, o.w);
@@ -491,7 +491,7 @@ __global__ void k_wake_need(int64_t nrows, const int64_t* __restrict__ rows_s,
   double4 me = pk[k];
   long long v = (long long)(level_s[k] - max_gap);
   for (int64_t e = off[k] + gl; e < off[k + 1]; e += 8) {
-    int32_t js = idx[e];
+    int32_t js = ld_stream(idx + e);
     double4 o = pk[js];
     double d2 = d2_exact(o.x - me.x, o.y - me.y, o.z - me.z);
     double rr = 2.0 * fmax(me.w, o.w);
