@@ -19,6 +19,10 @@
 
 namespace nbk {
 
+// the reuse test looks at the TOPK = 65 largest displacements (its fast sets hold at most 64)
+constexpr int TOPK = 65;
+constexpr int TOPK_CHUNK = 2048;
+
 // ---------------------------------------------------------------- workspace
 template <typename T>
 static int grow(Engine& E, T*& p, int64_t& cap, int64_t want) {
@@ -213,12 +217,59 @@ __global__ void k_hsearch(int64_t n, const double* __restrict__ hg, double h_max
 }
 
 __global__ void k_disp(int64_t n, const double* __restrict__ x, const double* __restrict__ xr,
-                       double* __restrict__ disp, int32_t* __restrict__ iota) {
+                       double* __restrict__ disp) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   double dx = x[3 * i] - xr[3 * i], dy = x[3 * i + 1] - xr[3 * i + 1], dz = x[3 * i + 2] - xr[3 * i + 2];
   disp[i] = sqrt(dx * dx + dy * dy + dz * dz);
-  iota[i] = (int32_t)i;
+}
+
+// The TOPK largest displacements with their indices, in descending order and, among equal values,
+// ascending index (the order of a stable descending sort).  Each block sorts a chunk of
+// TOPK_CHUNK candidates (cub::BlockRadixSort, stable) and keeps its first TOPK; passes repeat
+// over the kept candidates until one block remains.  Keys are the displacement's bits + 1
+// (non-negative doubles order like their bits), 0 marks padding, which sorts after every value.
+template <bool FIRST>
+__global__ void __launch_bounds__(256) k_topk(int64_t count, const double* __restrict__ disp,
+                                              const unsigned long long* __restrict__ key_in,
+                                              const int32_t* __restrict__ idx_in,
+                                              unsigned long long* __restrict__ key_out,
+                                              int32_t* __restrict__ idx_out) {
+  using Sort = cub::BlockRadixSort<unsigned long long, 256, TOPK_CHUNK / 256, int32_t>;
+  __shared__ typename Sort::TempStorage tmp;
+  constexpr int ITEMS = TOPK_CHUNK / 256;
+  unsigned long long k[ITEMS];
+  int32_t v[ITEMS];
+  const int64_t base = (int64_t)blockIdx.x * TOPK_CHUNK + (int64_t)threadIdx.x * ITEMS;
+#pragma unroll
+  for (int t = 0; t < ITEMS; ++t) {
+    int64_t g = base + t;
+    if (g < count) {
+      k[t] = FIRST ? (unsigned long long)__double_as_longlong(disp[g]) + 1ull : key_in[g];
+      v[t] = FIRST ? (int32_t)g : idx_in[g];
+    } else {
+      k[t] = 0ull;
+      v[t] = -1;
+    }
+  }
+  Sort(tmp).SortDescending(k, v);
+#pragma unroll
+  for (int t = 0; t < ITEMS; ++t) {
+    int r = threadIdx.x * ITEMS + t;
+    if (r < TOPK) {
+      key_out[(int64_t)blockIdx.x * TOPK + r] = k[t];
+      idx_out[(int64_t)blockIdx.x * TOPK + r] = v[t];
+    }
+  }
+}
+
+__global__ void k_topk_out(int top, const unsigned long long* __restrict__ key,
+                           const int32_t* __restrict__ idx, double* __restrict__ val_out,
+                           int32_t* __restrict__ idx_out) {
+  int r = threadIdx.x;
+  if (r >= top) return;
+  val_out[r] = __longlong_as_double((long long)(key[r] - 1ull));
+  idx_out[r] = idx[r];
 }
 
 // h_eff = hs - (disp + d_rest)/2; fail if a row has h_eff <= h_guess/2 or another particle
@@ -463,6 +514,11 @@ int Workspace::ensure(Engine& E, int64_t n) {
   NB_CUDA(cudaMalloc((void**)&i32a, sizeof(int32_t) * c));
   NB_CUDA(cudaMalloc((void**)&i32b, sizeof(int32_t) * c));
   NB_CUDA(cudaMalloc((void**)&dk_b, sizeof(double) * c));
+  const int64_t tk = (c / TOPK_CHUNK + 2) * TOPK;
+  NB_CUDA(cudaMalloc((void**)&tk_key0, sizeof(unsigned long long) * tk));
+  NB_CUDA(cudaMalloc((void**)&tk_key1, sizeof(unsigned long long) * tk));
+  NB_CUDA(cudaMalloc((void**)&tk_idx0, sizeof(int32_t) * tk));
+  NB_CUDA(cudaMalloc((void**)&tk_idx1, sizeof(int32_t) * tk));
   NB_CUDA(cudaMalloc((void**)&d_int, sizeof(int) * 16));
   NB_CUDA(cudaMalloc((void**)&d_i64, sizeof(int64_t) * 16));
   NB_CUDA(cudaMallocHost((void**)&h_int, sizeof(int) * 16));
@@ -493,7 +549,7 @@ void Workspace::release() {
                 d_dm, d_tmp, d_uh, v_flow, v_pred, v_eval, v_dacc, v_tmp, pk0, pk1, pk2, pk3, pk32,
                 pf1, pf2, pf3, m_x, m_sorted,
                 rows, rows_s, rows2, iters, flags, need, i_tmp, pairs, i_lvl, i_tmp2, m_rows, m_done, m_need,
-                m_tmp, i32a, i32b, dk_b, d_int, d_i64};
+                m_tmp, i32a, i32b, dk_b, d_int, d_i64, tk_key0, tk_key1, tk_idx0, tk_idx1};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (h_int) cudaFreeHost(h_int);
@@ -596,11 +652,30 @@ static int reuse_limits(Engine& E, int64_t n, const double* x, const double* hg,
   Workspace& W = E.ws;
   Cache& C = W.cache;
   *ok = 0;
-  count_launch(), k_disp<<<grid_for(n), NB_THREADS, 0, st>>>(n, x, C.x_ref, W.d_disp, W.i32a);
-  size_t tmp = E.cub_bytes;
-  NB_CUDA(cub::DeviceRadixSort::SortPairsDescending(E.cub_tmp, tmp, W.d_disp, W.dk_b, W.i32a,
-                                                    W.i32b, (int)n, 0, 64, st));
-  int top = (int)std::min<int64_t>(n, 65);
+  count_launch(), k_disp<<<grid_for(n), NB_THREADS, 0, st>>>(n, x, C.x_ref, W.d_disp);
+  // the largest displacements (descending; ties by index) into W.dk_b / W.i32b
+  {
+    int64_t count = n;
+    unsigned long long *kin = nullptr, *kout = W.tk_key0;
+    int32_t *iin = nullptr, *iout = W.tk_idx0;
+    bool first = true;
+    while (true) {
+      int64_t nb = (count + TOPK_CHUNK - 1) / TOPK_CHUNK;
+      if (first)
+        count_launch(), k_topk<true><<<(unsigned)nb, 256, 0, st>>>(count, W.d_disp, nullptr, nullptr, kout, iout);
+      else
+        count_launch(), k_topk<false><<<(unsigned)nb, 256, 0, st>>>(count, nullptr, kin, iin, kout, iout);
+      first = false;
+      count = nb * TOPK;
+      if (nb == 1) break;
+      kin = kout;
+      iin = iout;
+      kout = (kout == W.tk_key0) ? W.tk_key1 : W.tk_key0;
+      iout = (iout == W.tk_idx0) ? W.tk_idx1 : W.tk_idx0;
+    }
+    count_launch(), k_topk_out<<<1, 128, 0, st>>>((int)std::min<int64_t>(n, TOPK), kout, iout, W.dk_b, W.i32b);
+  }
+  int top = (int)std::min<int64_t>(n, TOPK);
   NB_CUDA(cudaMemcpyAsync(W.h_dbl, W.dk_b, sizeof(double) * top, cudaMemcpyDeviceToHost, st));
   NB_CUDA(cudaStreamSynchronize(st));
   static const int FAST[] = {0, 1, 2, 4, 8, 16, 32, 64};

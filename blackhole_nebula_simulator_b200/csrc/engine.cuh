@@ -58,6 +58,8 @@ struct Workspace {
           *m_x = nullptr, *m_sorted = nullptr;
   int32_t *i32a = nullptr, *i32b = nullptr;
   double* dk_b = nullptr;
+  unsigned long long *tk_key0 = nullptr, *tk_key1 = nullptr;  // top-k candidates (reuse test)
+  int32_t *tk_idx0 = nullptr, *tk_idx1 = nullptr;
   int* d_int = nullptr;
   int64_t* d_i64 = nullptr;
   int* h_int = nullptr;

@@ -262,12 +262,14 @@ struct DensityEntry;
 template <>
 struct DensityEntry<float> {
   using T = float2;
-  static constexpr int CAP = 256;  // in-range entries a row keeps in shared memory
+  static constexpr int CAP = 240;     // in-range entries a row keeps in shared memory
+  static constexpr int BLOCKS = 7;    // resident blocks per SM: 7 x (30 KiB + 1 KiB) of shared
 };
 template <>
 struct DensityEntry<double> {
   using T = double2;
   static constexpr int CAP = 192;
+  static constexpr int BLOCKS = 4;
 };
 constexpr int DENSITY_THREADS = 128;  // 16 rows per block
 
@@ -277,7 +279,7 @@ constexpr int DENSITY_THREADS = 128;  // 16 rows per block
 // that cache and reduces across the eight lanes, so the lanes of a row take the same Newton steps.
 // Rows with more in-range entries than the cache holds re-walk their list in every sum.
 template <typename R, typename PosT, typename I>
-__global__ void __launch_bounds__(DENSITY_THREADS)
+__global__ void __launch_bounds__(DENSITY_THREADS, DensityEntry<R>::BLOCKS)
     k_density(int64_t nrows, const int64_t* __restrict__ rows, PosT geo_in,
               const double* __restrict__ mass, const double* __restrict__ h_start,
               const double* __restrict__ h_search, const int64_t* __restrict__ off,
