@@ -320,7 +320,9 @@ __global__ void k_block_cool(int64_t n, int law, int64_t n_next, double tick,
   } else if (law == 2) {
     uc = brems_cool_one(uh, rho[i], s, bp);
   } else if (law == 3) {
-    uc = uc_in[i];
+    // the network's result closes the step; the provisional prediction of a particle in mid-step
+    // takes the exact integrator (cheaper than the network, and replaced when the step closes)
+    uc = act ? uc_in[i] : brems_cool_one(uh, rho[i], s, bp);
   }
   if (law != 0) {
     double d = act ? m[i] * (uh - uc) : 0.0;
@@ -333,10 +335,24 @@ __global__ void k_block_cool(int64_t n, int law, int64_t n_next, double tick,
   u[i] = uc + (s - half_len) * dudt[i];
 }
 
-__global__ void k_elapsed(int64_t n, int64_t n_next, double tick, const int64_t* __restrict__ n_beg,
-                          double* __restrict__ s) {
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) s[i] = (double)(n_next - n_beg[i]) * tick;
+// inputs of the network for the rows: u_half, rho and the elapsed time of each row's step
+__global__ void k_gather_cool_rows(int64_t nrows, const int64_t* __restrict__ rows, int64_t n_next,
+                                   double tick, const int64_t* __restrict__ n_beg,
+                                   const double* __restrict__ u_half, const double* __restrict__ rho,
+                                   double* __restrict__ ug, double* __restrict__ rg,
+                                   double* __restrict__ sg) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  int64_t i = rows[q];
+  ug[q] = u_half[i];
+  rg[q] = rho[i];
+  sg[q] = (double)(n_next - n_beg[i]) * tick;
+}
+
+__global__ void k_scatter_rows_d(int64_t nrows, const int64_t* __restrict__ rows,
+                                 const double* __restrict__ v, double* __restrict__ out) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q < nrows) out[rows[q]] = v[q];
 }
 
 // closing kicks of the rows (sim/blocks.py:544-547)
@@ -640,10 +656,12 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   NB_TRY(glf_status(E, n, W.iters, st));
   int64_t nrows = 0;
   NB_TRY(select_mask(E, n, W.m_rows, W.rows, &nrows, st));
-  if (prm->cooling == 3) {
-    // every particle's elapsed time, then the network's cooled u_half (exact fallback inside)
-    count_launch(), k_elapsed<<<grid_for(n), NB_THREADS, 0, st>>>(n, n_next, s->tick, s->n_beg, W.d_b);
-    NB_TRY(mlp_cool(E, n, s->u_half, s->rho, W.d_b, 0.0, &prm->mlp, W.d_c, nullptr, st));
+  if (prm->cooling == 3 && nrows > 0) {
+    // the network's cooled u_half of the particles whose steps close (exact fallback inside)
+    count_launch(), k_gather_cool_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(
+        nrows, W.rows, n_next, s->tick, s->n_beg, s->u_half, s->rho, W.d_a, W.d_b, W.d_hg);
+    NB_TRY(mlp_cool(E, nrows, W.d_a, W.d_b, W.d_hg, 0.0, &prm->mlp, W.d_tmp, nullptr, st));
+    count_launch(), k_scatter_rows_d<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, W.rows, W.d_tmp, W.d_c);
   }
   count_launch(), k_block_cool<<<grid_for(n), NB_THREADS, 0, st>>>(
       n, prm->cooling, n_next, s->tick, s->n_beg, s->n_end, s->x_beg, s->x, s->rho, s->mass,
