@@ -38,6 +38,10 @@ FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes
 FP64_NOMINAL_TFLOPS = FP32_NOMINAL_TFLOPS / 2.0
 FLOP_PER_DENSITY_EVAL = 25.0  # distance + kernel + two sums per pair evaluation
 FLOP_PER_FORCE_PAIR = 75.0  # pressure + viscosity + P dV (+20 with disc viscosity)
+# DRAM bytes (read + write) per row of one launch, from ncu captures of the FP32 kernels on the
+# 1,048,576-particle torus (profiles/k_forces_g_torus1m.md, profiles/k_density_torus1m.md),
+# scaled to a launch by its rows
+DRAM_BYTES_PER_ROW = {"forces": 1203.0, "density": 997.0}
 
 
 def peaks():
@@ -181,8 +185,10 @@ def roofline(prof, precision, disc, pk):
         flops = 0.0
     gbs = bytes_ / (ms * 1e-3) / 1e9
     pipe_peak = FP32_NOMINAL_TFLOPS if precision == "fp32" else FP64_NOMINAL_TFLOPS
+    traffic = (DRAM_BYTES_PER_ROW[dom] * units
+               if precision == "fp32" and dom in DRAM_BYTES_PER_ROW else None)  # fmt: skip
     rf = {"bound": "hbm", "kernel": dom, "achieved": round(gbs, 2), "peak": pk["hbm_gbs"],
-          "unit": "GB/s", "frac": round(gbs / pk["hbm_gbs"], 4), "traffic": None,
+          "unit": "GB/s", "frac": round(gbs / pk["hbm_gbs"], 4), "traffic": traffic,
           "peak_source": pk["source"], "ms_per_launch": round(ms, 4),
           "bytes_per_launch": bytes_}  # fmt: skip
     if flops:

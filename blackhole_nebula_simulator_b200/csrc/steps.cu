@@ -64,6 +64,9 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
   count_launch(), k_any_nonpositive<<<grid_for(n), NB_THREADS, 0, st>>>(n, u, E.d_err);
   NB_TRY(check_device_error(E, st));
   // todo = every particle without a cache, else rows and their cached-list neighbours
+  // (full_marks: the todo set holds every particle or every list entry of the rows on the lists
+  // that are cached now)
+  bool full_marks = true;
   if (!W.cache.valid || W.cache.n != n || E.lists.n != n) {
     count_launch(), k_fill_u8<<<grid_for(n), NB_THREADS, 0, st>>>(n, 1, W.m_need);
   } else {
@@ -79,9 +82,19 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
       settled = true;
       break;
     }
+    const int64_t builds0 = s->builds;
     NB_TRY(compute_density(E, n, s->x, s->mass, s->h, s->rho, s->omega, ntodo, W.rows2, prm,
                            &s->builds, &s->reuses, st));
     mask_or(n, W.m_need, W.m_done, st);
+    // Reused lists are complete for every pair within 2 max(h_i, h_j) at the new h (the reuse
+    // test proves it for the search limits the solve was capped at), so the interacting
+    // neighbours of the rows are list entries of the rows, all of them done already: the
+    // marking pass below would find nothing new.
+    if (full_marks && s->builds == builds0) {
+      settled = true;
+      break;
+    }
+    full_marks = false;
     // interacting neighbours of the rows at the current h
     NB_CUDA(cudaMemsetAsync(W.m_tmp, 0, n, st));
     NB_TRY(mark_rows(E, nrows, rows, 1, s->x, s->h, W.m_tmp, st));
