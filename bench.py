@@ -154,16 +154,16 @@ def profile_read(ctx):
 
     from blackhole_nebula_simulator_b200 import _lib
 
-    out = (ctypes.c_double * 16)()
+    names = ["lists", "density", "forces", "flow", "marks", "levels", "cooling"]
+    out = (ctypes.c_double * (4 * len(names)))()
     _lib.check(ctx, _lib.lib().nb_profile_read(ctx, out))
-    names = ["lists", "density", "forces", "flow"]
     return {names[c]: {"ms": out[4 * c], "launches": int(out[4 * c + 1]), "units": out[4 * c + 2],
-                       "pairs": out[4 * c + 3]} for c in range(4)}  # fmt: skip
+                       "pairs": out[4 * c + 3]} for c in range(len(names))}  # fmt: skip
 
 
 def roofline(prof, precision, disc, pk):
     """Dominant kernel: its algorithmic bytes per launch over its event-timed duration."""
-    dom = max(prof, key=lambda k: prof[k]["ms"])
+    dom = max(("lists", "density", "forces", "flow"), key=lambda k: prof[k]["ms"])
     d = prof[dom]
     if d["launches"] == 0:
         return None, dom

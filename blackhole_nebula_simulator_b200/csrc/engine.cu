@@ -120,6 +120,11 @@ int Engine::ensure_list_capacity(int64_t m) {
   return 0;
 }
 
+int Engine::ensure_tight(int64_t m) {
+  Engine& E = *this;
+  return grow(E, tidx, cap_tidx, std::max<int64_t>(m, 1));
+}
+
 int Engine::ensure_ell(int64_t m) {
   Engine& E = *this;
   return grow(E, ell, cap_ell, m);
@@ -134,7 +139,7 @@ int Engine::ensure_sort_keys(int64_t m) {
 void Engine::release() {
   void* ps[] = {d_err, bbox, bbox_part, keys_a, keys_b, vals_a, counts, node_lo, node_hi, sub_lo, sub_hi,
                 cub_tmp, sort_keys, red, lists.perm, lists.inv_perm, lists.spos, lists.off,
-                lists.idx, ell, d_rowmax};
+                lists.idx, ell, d_rowmax, tidx};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (h_err) cudaFreeHost(h_err);
@@ -396,19 +401,20 @@ __global__ void k_combine_rows(int64_t nrows, const int64_t* __restrict__ rows, 
   vsig[i] = use_visc ? vsig_f[i] : cs[i];
 }
 
-// touched sets over curve-ordered rows: pk holds sorted (x, y, z, h) of the current state; marks
-// go to the caller-order mask.  Eight lanes per row, each taking every eighth list entry.
+// touched sets over curve-ordered rows: pk holds sorted (x, y, z, h) of the current state (read
+// only with `tight`).  Marks go to a mask in sorted order, where a row's neighbours lie close
+// together; k_unsort_marks moves them to the caller's order in one pass.  Eight lanes per row,
+// each taking every eighth list entry.
 __global__ void k_mark_s(int64_t nrows, const int64_t* __restrict__ rows_s,
-                         const int32_t* __restrict__ perm, const int64_t* __restrict__ off,
-                         const int32_t* __restrict__ idx, int tight, const double4* __restrict__ pk,
-                         uint8_t* __restrict__ mark) {
+                         const int64_t* __restrict__ off, const int32_t* __restrict__ idx, int tight,
+                         const double4* __restrict__ pk, uint8_t* __restrict__ mark_s) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   int64_t q = t >> 3;
   const int gl = (int)(t & 7);
   if (q >= nrows) return;
   int64_t k = rows_s[q];
-  if (gl == 0) mark[perm[k]] = 1;
-  double4 me = pk[k];
+  if (gl == 0) mark_s[k] = 1;
+  double4 me = tight ? pk[k] : make_double4(0, 0, 0, 0);
   for (int64_t e = off[k] + gl; e < off[k + 1]; e += 8) {
     int32_t js = ld_stream(idx + e);
     if (tight) {
@@ -417,8 +423,14 @@ __global__ void k_mark_s(int64_t nrows, const int64_t* __restrict__ rows_s,
       double rr = 2.0 * fmax(me.w, o.w);
       if (!(d2 < rr * rr)) continue;
     }
-    mark[perm[js]] = 1;
+    mark_s[js] = 1;
   }
+}
+
+__global__ void k_unsort_marks(int64_t n, const int32_t* __restrict__ perm,
+                               const uint8_t* __restrict__ mark_s, uint8_t* __restrict__ mark) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < n && mark_s[k]) mark[perm[k]] = 1;
 }
 
 // touched sets: mark the rows and their list entries (optionally only interacting pairs)
@@ -509,7 +521,7 @@ int Workspace::ensure(Engine& E, int64_t n) {
   for (float4** p : f4s) NB_CUDA(cudaMalloc((void**)p, sizeof(float4) * c));
   int64_t** i8[] = {&rows, &rows_s, &rows2, &iters, &flags, &need, &i_tmp, &pairs, &i_lvl, &i_tmp2};
   for (int64_t** p : i8) NB_CUDA(cudaMalloc((void**)p, sizeof(int64_t) * (c + 1)));
-  uint8_t** u1[] = {&m_rows, &m_done, &m_need, &m_tmp, &m_x, &m_sorted};
+  uint8_t** u1[] = {&m_rows, &m_done, &m_need, &m_tmp, &m_x, &m_sorted, &m_smark};
   for (uint8_t** p : u1) NB_CUDA(cudaMalloc((void**)p, c));
   NB_CUDA(cudaMalloc((void**)&i32a, sizeof(int32_t) * c));
   NB_CUDA(cudaMalloc((void**)&i32b, sizeof(int32_t) * c));
@@ -547,7 +559,7 @@ int Workspace::ensure(Engine& E, int64_t n) {
 void Workspace::release() {
   void* ps[] = {d_a, d_b, d_c, d_hg, d_hs, d_heff, d_hlim, d_disp, d_P, d_cs, d_vsig, d_ddudt,
                 d_dm, d_tmp, d_uh, v_flow, v_pred, v_eval, v_dacc, v_tmp, pk0, pk1, pk2, pk3, pk32,
-                pf1, pf2, pf3, m_x, m_sorted,
+                pf1, pf2, pf3, m_x, m_sorted, m_smark,
                 rows, rows_s, rows2, iters, flags, need, i_tmp, pairs, i_lvl, i_tmp2, m_rows, m_done, m_need,
                 m_tmp, i32a, i32b, dk_b, d_int, d_i64, tk_key0, tk_key1, tk_idx0, tk_idx1};
   for (void* p : ps)
@@ -762,9 +774,11 @@ int mark_rows(Engine& E, int64_t nrows, const int64_t* rows, int tight, const do
   Workspace& W = E.ws;
   int64_t n = L.n, ns = 0;
   NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));
-  count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, h, W.pk0);
-  count_launch(), k_mark_s<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.perm, L.off, L.idx,
-                                                               tight, W.pk0, mark);
+  if (tight) count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, h, W.pk0);
+  NB_CUDA(cudaMemsetAsync(W.m_smark, 0, n, st));
+  count_launch(), k_mark_s<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, tight,
+                                                               W.pk0, W.m_smark);
+  count_launch(), k_unsort_marks<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, W.m_smark, mark);
   return 0;
 }
 

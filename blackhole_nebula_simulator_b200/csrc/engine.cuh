@@ -55,7 +55,7 @@ struct Workspace {
           *flags = nullptr, *need = nullptr, *i_tmp = nullptr, *pairs = nullptr,
           *i_lvl = nullptr, *i_tmp2 = nullptr;
   uint8_t *m_rows = nullptr, *m_done = nullptr, *m_need = nullptr, *m_tmp = nullptr,
-          *m_x = nullptr, *m_sorted = nullptr;
+          *m_x = nullptr, *m_sorted = nullptr, *m_smark = nullptr;
   int32_t *i32a = nullptr, *i32b = nullptr;
   double* dk_b = nullptr;
   unsigned long long *tk_key0 = nullptr, *tk_key1 = nullptr;  // top-k candidates (reuse test)
@@ -73,7 +73,10 @@ struct Workspace {
 // Event pairs are recorded into a pool and read only when the profile is read (or the pool is
 // full), and pair counts are summed on the device, so profiling adds no host synchronisation to
 // the steps it times.
-enum ProfCat { PROF_LISTS = 0, PROF_DENSITY = 1, PROF_FORCES = 2, PROF_FLOW = 3, PROF_NCAT = 4 };
+enum ProfCat {
+  PROF_LISTS = 0, PROF_DENSITY = 1, PROF_FORCES = 2, PROF_FLOW = 3, PROF_MARKS = 4,
+  PROF_LEVELS = 5, PROF_COOL = 6, PROF_NCAT = 7
+};
 struct Prof {
   static constexpr int POOL = 1024;
   bool on = false;
@@ -146,6 +149,8 @@ struct Engine {
   int32_t* ell = nullptr;
   int64_t cap_ell = 0, row_cap = 256;
   int64_t list_slots = 0;  // resident blocks of the persistent list kernel
+  int32_t* tidx = nullptr;  // interacting entries of the active rows, in the lists' layout
+  int64_t cap_tidx = 0;
   unsigned long long* d_rowmax = nullptr;
   int64_t* h_build = nullptr;  // pinned: total entries and longest row of the last build
   double* red = nullptr;      // reduction partials (doubles)
@@ -160,6 +165,7 @@ struct Engine {
   int ensure_list_capacity(int64_t m);
   int ensure_sort_keys(int64_t m);
   int ensure_ell(int64_t m);
+  int ensure_tight(int64_t m);
   int ensure_cub(size_t bytes);
   void release();
 };

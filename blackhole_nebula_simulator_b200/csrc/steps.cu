@@ -71,7 +71,9 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
     count_launch(), k_fill_u8<<<grid_for(n), NB_THREADS, 0, st>>>(n, 1, W.m_need);
   } else {
     NB_CUDA(cudaMemsetAsync(W.m_need, 0, n, st));
+    E.prof.begin(st);
     NB_TRY(mark_rows(E, nrows, rows, 0, s->x, s->h, W.m_need, st));
+    E.prof.end(PROF_MARKS, st, (double)nrows, 0.0);
   }
   NB_CUDA(cudaMemsetAsync(W.m_done, 0, n, st));
   bool settled = false;
@@ -97,7 +99,9 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
     full_marks = false;
     // interacting neighbours of the rows at the current h
     NB_CUDA(cudaMemsetAsync(W.m_tmp, 0, n, st));
+    E.prof.begin(st);
     NB_TRY(mark_rows(E, nrows, rows, 1, s->x, s->h, W.m_tmp, st));
+    E.prof.end(PROF_MARKS, st, (double)nrows, 0.0);
     mask_and_not(n, W.m_tmp, W.m_done, W.m_need, st);
   }
   if (!settled) {
@@ -428,14 +432,49 @@ __global__ void k_wanted_levels(int64_t nrows, const int64_t* __restrict__ rows,
   level[i] = nw;
 }
 
-// one sweep of the level limiter over the rows' interacting pairs (sim/blocks.py:337-353), on
-// curve-ordered rows with sorted (x, h) and a sorted copy of the levels; the least fixed point
+// The interacting entries (r < 2 max(h_i, h_j), the reference's FP64 test) of the rows, written
+// into the rows' own stretches of the list storage (tidx[off[k] ..], tcnt[q] of them), so the
+// limiter sweeps and the wake-up walk short lists without distance tests.  Eight lanes per row;
+// a group ballot keeps the entries in list order.
+__global__ void k_tight_rows(int64_t nrows, const int64_t* __restrict__ rows_s,
+                             const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
+                             const double4* __restrict__ pk, int32_t* __restrict__ tidx,
+                             int32_t* __restrict__ tcnt) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t q = t >> 3;
+  const int gl = (int)(t & 7), g = (int)((threadIdx.x & 31) >> 3);
+  const bool live = q < nrows;
+  if (!__any_sync(0xffffffffu, live)) return;  // warp-uniform
+  int64_t k = live ? rows_s[q] : 0;
+  const int64_t e0 = live ? off[k] : 0, e1 = live ? off[k + 1] : 0;
+  const unsigned len = (unsigned)(e1 - e0);
+  const unsigned maxlen = __reduce_max_sync(0xffffffffu, len);
+  double4 me = live ? pk[k] : make_double4(0, 0, 0, 0);
+  int m = 0;
+  for (unsigned b = 0; b < maxlen; b += 8) {
+    bool take = false;
+    int32_t js = 0;
+    if (b + gl < len) {
+      js = ld_stream(idx + e0 + b + gl);
+      double4 o = pk[js];
+      double d2 = d2_exact(o.x - me.x, o.y - me.y, o.z - me.z);
+      double rr = 2.0 * fmax(me.w, o.w);
+      take = d2 < rr * rr;
+    }
+    unsigned seg = (__ballot_sync(0xffffffffu, take) >> (8 * g)) & 0xffu;
+    if (take) tidx[e0 + m + __popc(seg & ((1u << gl) - 1u))] = js;
+    m += __popc(seg);
+  }
+  if (live && gl == 0) tcnt[q] = m;
+}
+
+// one sweep of the level limiter (sim/blocks.py:337-353) over the rows' interacting entries, on
+// curve-ordered rows and a sorted copy of the levels (eight lanes per row); the least fixed point
 // above the start is unique, so in-place sweeps reach the reference's levels
-__global__ void k_limit_sweep(int64_t nrows, const int64_t* __restrict__ rows_s,
-                              const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
-                              const double4* __restrict__ pk, int64_t max_gap, int64_t* level_s,
-                              int* changed) {
-  // eight lanes per row (lanes 8g .. 8g+7 of a warp), each taking every eighth list entry
+__global__ void k_limit_sweep_t(int64_t nrows, const int64_t* __restrict__ rows_s,
+                                const int64_t* __restrict__ off, const int32_t* __restrict__ tidx,
+                                const int32_t* __restrict__ tcnt, int64_t max_gap,
+                                int64_t* level_s, int* changed) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   int64_t q = t >> 3;
   const int gl = (int)(t & 7);
@@ -443,15 +482,10 @@ __global__ void k_limit_sweep(int64_t nrows, const int64_t* __restrict__ rows_s,
   int64_t k = 0, need = INT64_MIN;
   if (live) {
     k = rows_s[q];
-    double4 me = pk[k];
     need = ((volatile int64_t*)level_s)[k];
-    for (int64_t e = off[k] + gl; e < off[k + 1]; e += 8) {
-      int32_t js = ld_stream(idx + e);
-      double4 o = pk[js];
-      double d2 = d2_exact(o.x - me.x, o.y - me.y, o.z - me.z);
-      double rr = 2.0 * fmax(me.w, o.w);
-      if (!(d2 < rr * rr)) continue;
-      int64_t lj = ((volatile int64_t*)level_s)[js];
+    const int32_t* tl = tidx + off[k];
+    for (int c = gl; c < tcnt[q]; c += 8) {
+      int64_t lj = ((volatile int64_t*)level_s)[tl[c]];
       if (lj - max_gap > need) need = lj - max_gap;
     }
   }
@@ -464,6 +498,22 @@ __global__ void k_limit_sweep(int64_t nrows, const int64_t* __restrict__ rows_s,
     atomicMax((long long*)&level_s[k], (long long)need);
     *changed = 1;
   }
+}
+
+// _wake_targets (sim/blocks.py:356-364): need[j] = max over active i of level_i - max_gap, over
+// the rows' interacting entries into a sorted need array (eight lanes per row)
+__global__ void k_wake_need_t(int64_t nrows, const int64_t* __restrict__ rows_s,
+                              const int64_t* __restrict__ off, const int32_t* __restrict__ tidx,
+                              const int32_t* __restrict__ tcnt, const int64_t* __restrict__ level_s,
+                              int64_t max_gap, int64_t* __restrict__ need_s) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t q = t >> 3;
+  const int gl = (int)(t & 7);
+  if (q >= nrows) return;
+  int64_t k = rows_s[q];
+  long long v = (long long)(level_s[k] - max_gap);
+  const int32_t* tl = tidx + off[k];
+  for (int c = gl; c < tcnt[q]; c += 8) atomicMax((long long*)&need_s[tl[c]], v);
 }
 
 __global__ void k_gather_i64(int64_t n, const int32_t* __restrict__ perm, const int64_t* __restrict__ a,
@@ -503,30 +553,6 @@ __global__ void k_land(int64_t nrows, const int64_t* __restrict__ rows, int64_t 
   }
   if (k > K_MAX) set_error(err, ERR_LEVEL);
   level[i] = k;
-}
-
-// _wake_targets (sim/blocks.py:356-364): need[j] = max over active i of level_i - max_gap, on
-// curve-ordered rows into a sorted need array
-__global__ void k_wake_need(int64_t nrows, const int64_t* __restrict__ rows_s,
-                            const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
-                            const double4* __restrict__ pk, const int64_t* __restrict__ level_s,
-                            int64_t max_gap, int64_t* __restrict__ need_s) {
-  // eight lanes per row, each taking every eighth list entry
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  int64_t q = t >> 3;
-  const int gl = (int)(t & 7);
-  if (q >= nrows) return;
-  int64_t k = rows_s[q];
-  double4 me = pk[k];
-  long long v = (long long)(level_s[k] - max_gap);
-  for (int64_t e = off[k] + gl; e < off[k + 1]; e += 8) {
-    int32_t js = ld_stream(idx + e);
-    double4 o = pk[js];
-    double d2 = d2_exact(o.x - me.x, o.y - me.y, o.z - me.z);
-    double rr = 2.0 * fmax(me.w, o.w);
-    if (!(d2 < rr * rr)) continue;
-    atomicMax((long long*)&need_s[js], v);
-  }
 }
 
 // _cut_steps / _cut_to (sim/blocks.py:404-431): shorten running steps longer than `need` allows
@@ -595,11 +621,15 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
     // curve-ordered rows, sorted (x, h) and a sorted copy of the levels
     NB_TRY(sorted_rows_and_pack(E, nrows, rows, s->x, s->h, &ns, st));
     count_launch(), k_gather_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, W.i_lvl);
+    // the rows' interacting entries, once for every sweep and the wake-up walk
+    NB_TRY(E.ensure_tight(L.total));
+    count_launch(), k_tight_rows<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,
+                                                                       E.tidx, W.i32a);
     bool settled = false;
     for (int sweep = 0; sweep < 4096; ++sweep) {
       NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
-      count_launch(), k_limit_sweep<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,
-                                                                         prm->max_gap, W.i_lvl, W.d_int);
+      count_launch(), k_limit_sweep_t<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, E.tidx, W.i32a,
+                                                                           prm->max_gap, W.i_lvl, W.d_int);
       NB_CUDA(cudaMemcpyAsync(W.h_int, W.d_int, sizeof(int), cudaMemcpyDeviceToHost, st));
       NB_CUDA(cudaStreamSynchronize(st));
       if (W.h_int[0] == 0) {
@@ -616,8 +646,8 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
     // levels after _land, sorted; need in sorted order, then back to the caller's order
     count_launch(), k_gather_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, W.i_lvl);
     count_launch(), k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, -1, W.i_tmp2);
-    count_launch(), k_wake_need<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,
-                                                                   W.i_lvl, prm->max_gap, W.i_tmp2);
+    count_launch(), k_wake_need_t<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, E.tidx, W.i32a,
+                                                                     W.i_lvl, prm->max_gap, W.i_tmp2);
     count_launch(), k_scatter_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, W.i_tmp2, W.need);
     NB_CUDA(cudaMemsetAsync(W.d_i64, 0, sizeof(int64_t), st));
     count_launch(), k_cut_steps<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->tick_n, s->tick, W.need, s->a_hydro,
@@ -669,6 +699,7 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   NB_TRY(glf_status(E, n, W.iters, st));
   int64_t nrows = 0;
   NB_TRY(select_mask(E, n, W.m_rows, W.rows, &nrows, st));
+  E.prof.begin(st);
   if (prm->cooling == 3 && nrows > 0) {
     // the network's cooled u_half of the particles whose steps close (exact fallback inside)
     count_launch(), k_gather_cool_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(
@@ -680,6 +711,7 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
       n, prm->cooling, n_next, s->tick, s->n_beg, s->n_end, s->x_beg, s->x, s->rho, s->mass,
       s->dudt, prm->cooling_beta, prm->u_floor, brems_of(prm), W.d_c, s->u_half, s->u,
       s->luminosity, W.d_dm);
+  E.prof.end(PROF_COOL, st, (double)nrows, 0.0);
   if (prm->cooling != 0) {
     double de = 0;
     NB_TRY(sum_doubles(E, n, W.d_dm, &de, st));
@@ -692,7 +724,9 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
                                                        W.v_flow, s->a_hydro, s->u_half, s->dudt,
                                                        W.v_pred, s->u);
   NB_CUDA(cudaMemcpyAsync(s->p, W.v_pred, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, st));
+  E.prof.begin(st);
   NB_TRY(choose_levels_and_open(E, s, prm, nrows, W.rows, st));
+  E.prof.end(PROF_LEVELS, st, (double)nrows, 0.0);
   if (rows_out && nrows > 0)
     NB_CUDA(cudaMemcpyAsync(rows_out, W.rows, sizeof(int64_t) * nrows, cudaMemcpyDeviceToDevice, st));
   s->last_active = nrows;
