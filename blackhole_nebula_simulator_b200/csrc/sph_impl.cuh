@@ -558,8 +558,81 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? FORCE_BLOCKS_PER_
       dheat.add(m_b * qa * vdr * fa);
     }
     };
+  // FP32 form: the same terms with one reciprocal square root per pair and reciprocals of the
+  // per-particle denominators instead of divisions (rounding differs from the FP64 form by a few
+  // float ulps, far inside the FP32 tolerances)
+  const R ih_a = R(1) / h_a;
+  const R cn4_a = cn * (ih_a * ih_a) * (ih_a * ih_a);
+  auto pair_fast = [&](int64_t b) {
+    R ddx, ddy, ddz;
+    geo.diff(a, b, ddx, ddy, ddz);  // x_b - x_a
+    const V4 hb4 = hydro[b];
+    const R h_b = (R)hb4.x;
+    const R d2 = sqdist(ddx, ddy, ddz);
+    npairs += 1;
+    const V4 vb = vm[b];
+    const R rho_b = (R)hb4.y, om_b = (R)hb4.z, P_b = (R)hb4.w;
+    const R m_b = (R)vb.w;
+    const R inv_r = rsqrtf(d2);
+    const R r = d2 * inv_r;
+    const R rx = -ddx * inv_r, ry = -ddy * inv_r, rz = -ddz * inv_r;  // r_hat of x_a - x_b
+    const R ih_b = __frcp_rn(h_b);
+    const R fa = cn4_a * kernel_df<R>(r * ih_a, kid);
+    const R fb = cn * (ih_b * ih_b) * (ih_b * ih_b) * kernel_df<R>(r * ih_b, kid);
+    const R dvx = (R)(va.x - vb.x), dvy = (R)(va.y - vb.y), dvz = (R)(va.z - vb.z);
+    const R vdotr = dvx * rx + dvy * ry + dvz * rz;
+    R num_a = P_a, num_b = P_b;
+    const R inv_orr_b = __frcp_rn(om_b * rho_b * rho_b);
+    if (prm.use_sph) {
+      if (prm.use_visc) {
+        const V4 xb = aux[b];
+        R vsig_a = al_a * cs_a + beta * fabs(vdotr);
+        R vsig_b = (R)xb.z * (R)xb.y + beta * fabs(vdotr);
+        if (vsig_a > vmax) vmax = vsig_a;
+        if (vdotr < R(0)) {
+          num_a += R(-0.5) * rho_a * vsig_a * vdotr;
+          num_b += R(-0.5) * rho_b * vsig_b * vdotr;
+          R dh = m_b * vsig_a * R(0.5) * vdotr * vdotr * fa * inv_or_a;
+          heat.add(-dh);
+          vheat.add(-dh);
+        }
+        if (prm.use_cond) {
+          R vu;
+          if (prm.cond_signal == 0)
+            vu = sqrt(fabs(P_a - P_b) * __frcp_rn(R(0.5) * (rho_a + rho_b)));
+          else
+            vu = fabs(vdotr);
+          R dc = m_b * alpha_u * vu * (R)(xa.x - xb.x) * R(0.5) *
+                 (fa * inv_or_a + fb * inv_orr_b * rho_b);
+          heat.add(dc);
+          cheat.add(dc);
+        }
+      }
+      R f = m_b * (num_a * inv_orr_a * fa + num_b * inv_orr_b * fb);
+      ax.add(-f * rx);
+      ay.add(-f * ry);
+      az.add(-f * rz);
+      work.add(m_b * vdotr * fa);
+    }
+    if (prm.use_disc) {
+      const V4 xb = aux[b];
+      const R vdr = vdotr;  // v_ab . (x_a - x_b) / r
+      R qa = -rho_a * h_a * R(0.5) * inv_r * aav * cs_a * vdr * inv_orr_a;
+      R qb = -rho_b * h_b * R(0.5) * inv_r * aav * (R)xb.y * vdr * inv_orr_b;
+      R f = m_b * (qa * fa + qb * fb);
+      dax.add(-(f * rx));
+      day.add(-(f * ry));
+      daz.add(-(f * rz));
+      dheat.add(m_b * qa * vdr * fa);
+    }
+  };
   auto drain = [&]() {
-    for (int k2 = gl; k2 < pc; k2 += 8) pair((int64_t)pq[k2]);
+    for (int k2 = gl; k2 < pc; k2 += 8) {
+      if constexpr (sizeof(R) == 4)
+        pair_fast((int64_t)pq[k2]);
+      else
+        pair((int64_t)pq[k2]);
+    }
     __syncwarp();
     pc = 0;
   };
