@@ -605,10 +605,20 @@ static void prof_pairs(Engine& E, int cat, int64_t nrows, const int64_t* rows, c
 static int rows_sorted(Engine& E, int64_t n, int64_t nrows, const int64_t* rows, int64_t* count,
                        cudaStream_t st) {
   Workspace& W = E.ws;
+  const bool active = rows == W.rows;
+  if (active && W.rs_ver == W.rows_ver && W.rs_gen == E.lists.gen && W.rs_n == nrows) {
+    *count = W.rs_count;  // the active rows, sorted already on these lists
+    return 0;
+  }
   NB_CUDA(cudaMemsetAsync(W.m_x, 0, n, st));
   count_launch(), k_mask_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, n, W.m_x, E.d_err);
   count_launch(), k_sorted_mask<<<grid_for(n), NB_THREADS, 0, st>>>(n, E.lists.perm, W.m_x, W.m_sorted);
-  return select_mask(E, n, W.m_sorted, W.rows_s, count, st);
+  NB_TRY(select_mask(E, n, W.m_sorted, W.rows_s, count, st));
+  W.rs_ver = active ? W.rows_ver : -1;
+  W.rs_gen = E.lists.gen;
+  W.rs_n = nrows;
+  W.rs_count = *count;
+  return 0;
 }
 
 static int read_int(Engine& E, int* d, int* out, cudaStream_t st) {

@@ -19,6 +19,7 @@ constexpr int MAX_LEVELS = 16;
 // perm[k] of the caller's order; entries are sorted positions.
 struct Lists {
   int64_t n = 0, total = 0;
+  int64_t gen = 0;              // builds so far (the sorted order changes with every build)
   int32_t* perm = nullptr;      // sorted position -> caller index
   int32_t* inv_perm = nullptr;  // caller index -> sorted position
   double4* spos = nullptr;      // sorted (x, y, z, h_search)
@@ -65,6 +66,9 @@ struct Workspace {
   int* h_int = nullptr;
   int64_t* h_i64 = nullptr;
   double* h_dbl = nullptr;
+  // W.rows (the active rows of the current step) changes version whenever it is rewritten; the
+  // sorted copy in rows_s is kept while the rows and the lists stay the same
+  int64_t rows_ver = 0, rs_ver = -1, rs_gen = -1, rs_n = -1, rs_count = 0;
   int ensure(Engine& E, int64_t n);
   void release();
 };

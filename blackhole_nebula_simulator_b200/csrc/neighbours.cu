@@ -469,15 +469,18 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
     return 0;
   }
   Lists& L = E.lists;
+  L.gen += 1;
   E.prof.begin(st);
   // bounding box and Hilbert keys
   int nbb = (int)std::min<int64_t>(grid_for(n), 1184);
   count_launch(), k_bbox_partial<<<nbb, NB_THREADS, 0, st>>>(n, pos, E.bbox_part);
   count_launch(), k_bbox_final<<<1, NB_THREADS, 0, st>>>(nbb, E.bbox_part, E.bbox);
   count_launch(), k_curve_keys<<<grid_for(n), NB_THREADS, 0, st>>>(n, pos, E.bbox, E.keys_a, E.vals_a);
+  // the top 48 of the 63 key bits (2^16 cells per axis over the box; within a cell the caller's
+  // order): six radix passes instead of eight, and the leaves stay as compact
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceRadixSort::SortPairs(E.cub_tmp, tmp, E.keys_a, E.keys_b, E.vals_a, L.perm,
-                                          (int)n, 0, 63, st));
+                                          (int)n, 15, 63, st));
   count_launch(), k_gather_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, pos, hs, L.spos, L.inv_perm);
   // tree
   int64_t nleaf = (n + LEAF - 1) / LEAF;

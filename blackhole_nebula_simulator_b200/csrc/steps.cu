@@ -201,6 +201,7 @@ int coupled_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_
   NB_TRY(W.ensure(E, n));
   W.cache.valid = false;
   count_launch(), k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
+  W.rows_ver += 1;
   launch_v_from_p(n, s->x, s->p, W.v_eval, st);
   NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st));
   return 0;
@@ -233,6 +234,7 @@ int coupled_step(Engine& E, nb_state* s, const nb_params* prm, double dt, cudaSt
                                                     half, W.v_tmp, s->u);
   launch_v_from_p(n, s->x, W.v_tmp, W.v_eval, st);
   count_launch(), k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
+  W.rows_ver += 1;
   NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st));
   // closing kick with the new forces
   count_launch(), k_pred_shared<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.v_flow, s->a_hydro, u_half, s->dudt,
@@ -672,6 +674,7 @@ int block_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t 
   NB_TRY(W.ensure(E, n));
   W.cache.valid = false;
   count_launch(), k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
+  W.rows_ver += 1;
   launch_v_from_p(n, s->x, s->p, W.v_eval, st);
   NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st));
   count_launch(), k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, 0, s->level);
@@ -699,6 +702,7 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   NB_TRY(glf_status(E, n, W.iters, st));
   int64_t nrows = 0;
   NB_TRY(select_mask(E, n, W.m_rows, W.rows, &nrows, st));
+  W.rows_ver += 1;
   E.prof.begin(st);
   if (prm->cooling == 3 && nrows > 0) {
     // the network's cooled u_half of the particles whose steps close (exact fallback inside)
