@@ -25,6 +25,9 @@ int begin(nb_ctx* ctx) {
   if (!ctx) return NB_ERR_INPUT;
   Engine& E = ctx->E;
   E.last_error[0] = 0;
+  // checks left pending by a call that failed part-way belong to that call
+  E.ws.pend_err = E.ws.pend_glf = false;
+  E.ws.pend_erad = nullptr;
   NB_CUDA(cudaSetDevice(E.device));
   return 0;
 }

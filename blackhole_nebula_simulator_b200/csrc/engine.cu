@@ -152,6 +152,7 @@ void Engine::release() {
 int check_device_error(Engine& E, cudaStream_t st) {
   NB_CUDA(cudaMemcpyAsync(E.h_err, E.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   NB_CUDA(cudaStreamSynchronize(st));
+  E.ws.pend_err = false;  // this read covers a deferred check of the same word
   NB_CUDA(cudaGetLastError());
   int code = E.h_err[0];
   if (code == 0) return 0;
@@ -280,11 +281,12 @@ __global__ void k_topk_out(int top, const unsigned long long* __restrict__ key,
 // h_eff = hs - (disp + d_rest)/2; fail if a row has h_eff <= h_guess/2 or another particle
 // h_guess > h_eff (sim/sph.py:134-138).  Also fills h_lim (rows: h_eff, others: h_guess).
 __global__ void k_reuse_test(int64_t n, const double* __restrict__ hs, const double* __restrict__ disp,
-                             double d_rest, const double* __restrict__ hg,
+                             const double* __restrict__ d_rest_p, const double* __restrict__ hg,
                              const uint8_t* __restrict__ is_row, double* __restrict__ h_eff,
                              double* __restrict__ h_lim, int* __restrict__ fail) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const double d_rest = *d_rest_p;  // the largest displacement outside the fast set
   double he = hs[i] - 0.5 * (disp[i] + d_rest);
   h_eff[i] = he;
   bool row = is_row[i];
@@ -536,6 +538,8 @@ int Workspace::ensure(Engine& E, int64_t n) {
   NB_CUDA(cudaMallocHost((void**)&h_int, sizeof(int) * 16));
   NB_CUDA(cudaMallocHost((void**)&h_i64, sizeof(int64_t) * 16));
   NB_CUDA(cudaMallocHost((void**)&h_dbl, sizeof(double) * 80));
+  NB_CUDA(cudaMalloc((void**)&d_scal, sizeof(double) * 8));
+  NB_CUDA(cudaMalloc((void**)&d_scal_i, sizeof(int64_t) * 8));
   cap = c;
   if (cache.cap < c) {
     if (cache.x_ref) cudaFree(cache.x_ref);
@@ -561,7 +565,8 @@ void Workspace::release() {
                 d_dm, d_tmp, d_uh, v_flow, v_pred, v_eval, v_dacc, v_tmp, pk0, pk1, pk2, pk3, pk32,
                 pf1, pf2, pf3, m_x, m_sorted, m_smark,
                 rows, rows_s, rows2, iters, flags, need, i_tmp, pairs, i_lvl, i_tmp2, m_rows, m_done, m_need,
-                m_tmp, i32a, i32b, dk_b, d_int, d_i64, tk_key0, tk_key1, tk_idx0, tk_idx1};
+                m_tmp, i32a, i32b, dk_b, d_int, d_i64, tk_key0, tk_key1, tk_idx0, tk_idx1, d_scal,
+                d_scal_i};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (h_int) cudaFreeHost(h_int);
@@ -621,11 +626,58 @@ static int rows_sorted(Engine& E, int64_t n, int64_t nrows, const int64_t* rows,
   return 0;
 }
 
+// Pending checks: copy their device words next to the caller's own read (before its
+// synchronisation), then act on them (after it).
+int pending_enqueue(Engine& E, cudaStream_t st) {
+  Workspace& W = E.ws;
+  if (W.pend_err) NB_CUDA(cudaMemcpyAsync(E.h_err, E.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (W.pend_glf)
+    NB_CUDA(cudaMemcpyAsync(W.h_i64 + 8, W.d_scal_i, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  if (W.pend_erad)
+    NB_CUDA(cudaMemcpyAsync(W.h_dbl + 72, W.d_scal, sizeof(double), cudaMemcpyDeviceToHost, st));
+  return 0;
+}
+
+int pending_finish(Engine& E, cudaStream_t st) {
+  Workspace& W = E.ws;
+  if (W.pend_erad) {
+    *W.pend_erad += W.h_dbl[72];
+    W.pend_erad = nullptr;
+  }
+  if (W.pend_glf) {
+    W.pend_glf = false;
+    int64_t worst = W.h_i64[8];
+    if (worst < 0) {
+      const char* msg = worst == -1   ? "stage 1 (p_half) did not converge in 10 iterations: time step too large"
+                        : worst == -2 ? "stage 2 (x1) did not converge in 10 iterations: time step too large"
+                                      : "particle inside r = 2.5";
+      std::snprintf(E.last_error, sizeof(E.last_error), "%s", msg);
+      W.pend_err = false;
+      return worst == -1 ? NB_ERR_GLF_P_HALF : worst == -2 ? NB_ERR_GLF_X1 : NB_ERR_GLF_RADIUS;
+    }
+  }
+  if (W.pend_err) {
+    W.pend_err = false;
+    if (E.h_err[0] != 0) return check_device_error(E, st);  // maps the code (and clears it)
+  }
+  return 0;
+}
+
+// the pending checks on their own (at the end of a step entry point)
+int pending_flush(Engine& E, cudaStream_t st) {
+  Workspace& W = E.ws;
+  if (!W.pend_err && !W.pend_glf && !W.pend_erad) return 0;
+  NB_TRY(pending_enqueue(E, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  return pending_finish(E, st);
+}
+
 static int read_int(Engine& E, int* d, int* out, cudaStream_t st) {
   NB_CUDA(cudaMemcpyAsync(E.ws.h_int, d, sizeof(int), cudaMemcpyDeviceToHost, st));
+  NB_TRY(pending_enqueue(E, st));
   NB_CUDA(cudaStreamSynchronize(st));
   *out = E.ws.h_int[0];
-  return 0;
+  return pending_finish(E, st);
 }
 
 // Density pass of `rows` on the current lists with the given search radii; results into the
@@ -698,14 +750,11 @@ static int reuse_limits(Engine& E, int64_t n, const double* x, const double* hg,
     count_launch(), k_topk_out<<<1, 128, 0, st>>>((int)std::min<int64_t>(n, TOPK), kout, iout, W.dk_b, W.i32b);
   }
   int top = (int)std::min<int64_t>(n, TOPK);
-  NB_CUDA(cudaMemcpyAsync(W.h_dbl, W.dk_b, sizeof(double) * top, cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
   static const int FAST[] = {0, 1, 2, 4, 8, 16, 32, 64};
   for (int nf : FAST) {
     if (nf >= top) break;
-    double d_rest = W.h_dbl[nf];
     NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
-    count_launch(), k_reuse_test<<<grid_for(n), NB_THREADS, 0, st>>>(n, C.hs, W.d_disp, d_rest, hg, W.m_rows,
+    count_launch(), k_reuse_test<<<grid_for(n), NB_THREADS, 0, st>>>(n, C.hs, W.d_disp, W.dk_b + nf, hg, W.m_rows,
                                                      W.d_heff, W.d_hlim, W.d_int);
     int fail = 0;
     NB_TRY(read_int(E, W.d_int, &fail, st));
@@ -817,9 +866,10 @@ int select_mask(Engine& E, int64_t n, const uint8_t* mask, int64_t* out, int64_t
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceSelect::Flagged(E.cub_tmp, tmp, W.i_tmp, mask, out, W.d_i64, (int)n, st));
   NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  NB_TRY(pending_enqueue(E, st));
   NB_CUDA(cudaStreamSynchronize(st));
   *count = W.h_i64[0];
-  return 0;
+  return pending_finish(E, st);
 }
 
 // Fused EOS + force pass for `rows` (caller order) with interacting pairs only (the tightened

@@ -62,7 +62,7 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
   int64_t n = s->n;
   NB_TRY(W.ensure(E, n));
   count_launch(), k_any_nonpositive<<<grid_for(n), NB_THREADS, 0, st>>>(n, u, E.d_err);
-  NB_TRY(check_device_error(E, st));
+  W.pend_err = true;  // read with the touched set's count, before any state is written
   // todo = every particle without a cache, else rows and their cached-list neighbours
   // (full_marks: the todo set holds every particle or every list entry of the rows on the lists
   // that are cached now)
@@ -204,7 +204,7 @@ int coupled_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_
   W.rows_ver += 1;
   launch_v_from_p(n, s->x, s->p, W.v_eval, st);
   NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st));
-  return 0;
+  return pending_flush(E, st);
 }
 
 int coupled_step(Engine& E, nb_state* s, const nb_params* prm, double dt, cudaStream_t st) {
@@ -242,7 +242,7 @@ int coupled_step(Engine& E, nb_state* s, const nb_params* prm, double dt, cudaSt
   s->particle_steps += n;
   s->last_active = n;
   NB_CUDA(cudaGetLastError());
-  return 0;
+  return pending_flush(E, st);
 }
 
 // sim/coupled.py:213-226: min over particles of C_cour h / v_sig, C_force sqrt(h / |a|),
@@ -617,7 +617,7 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
       nrows, rows, s->tick_n, prm->dt_max, s->h, s->vsig_max, s->a_hydro,
       prm->disc_alpha_av > 0 ? s->nu : nullptr, s->x, prm->courant, prm->c_force, prm->eta_orb,
       prm->cooling, s->u, s->rho, brems_of(prm), s->level_offset, s->level, E.d_err);
-  NB_TRY(check_device_error(E, st));
+  W.pend_err = true;  // read with the first limiter sweep's flag (or by the landing check)
   int64_t ns = 0;
   if (prm->limiter) {
     // curve-ordered rows, sorted (x, h) and a sorted copy of the levels
@@ -633,7 +633,9 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
       count_launch(), k_limit_sweep_t<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, E.tidx, W.i32a,
                                                                            prm->max_gap, W.i_lvl, W.d_int);
       NB_CUDA(cudaMemcpyAsync(W.h_int, W.d_int, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NB_TRY(pending_enqueue(E, st));
       NB_CUDA(cudaStreamSynchronize(st));
+      NB_TRY(pending_finish(E, st));
       if (W.h_int[0] == 0) {
         settled = true;
         break;
@@ -656,7 +658,9 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
                                                     s->dudt, s->level, s->n_end, s->p_half,
                                                     s->u_half, (unsigned long long*)W.d_i64);
     NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    NB_TRY(pending_enqueue(E, st));
     NB_CUDA(cudaStreamSynchronize(st));
+    NB_TRY(pending_finish(E, st));
     s->woken += W.h_i64[0];
   }
   count_launch(), k_open<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, s->tick_n, s->tick, s->level, s->x,
@@ -678,7 +682,8 @@ int block_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t 
   launch_v_from_p(n, s->x, s->p, W.v_eval, st);
   NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st));
   count_launch(), k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, 0, s->level);
-  return choose_levels_and_open(E, s, prm, n, W.rows, st);
+  NB_TRY(choose_levels_and_open(E, s, prm, n, W.rows, st));
+  return pending_flush(E, st);
 }
 
 // sim/blocks.py:502-563 (advance): one system step to the earliest step end.  rows_out (optional,
@@ -699,7 +704,12 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
                                                  s->n_end, s->a_hydro, s->x, W.v_flow, W.v_pred,
                                                  W.iters, W.m_rows);
   E.prof.end(PROF_FLOW, st, (double)n, 0.0);
-  NB_TRY(glf_status(E, n, W.iters, st));
+  {
+    // the flow's worst iteration code, read with the active count just below
+    size_t tmp2 = E.cub_bytes;
+    NB_CUDA(cub::DeviceReduce::Min(E.cub_tmp, tmp2, W.iters, W.d_scal_i, (int)n, st));
+    W.pend_glf = true;
+  }
   int64_t nrows = 0;
   NB_TRY(select_mask(E, n, W.m_rows, W.rows, &nrows, st));
   W.rows_ver += 1;
@@ -717,9 +727,10 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
       s->luminosity, W.d_dm);
   E.prof.end(PROF_COOL, st, (double)nrows, 0.0);
   if (prm->cooling != 0) {
-    double de = 0;
-    NB_TRY(sum_doubles(E, n, W.d_dm, &de, st));
-    s->e_radiated += de;
+    // radiated energy of the closing steps, added to the ledger at the next read
+    size_t tmp2 = E.cub_bytes;
+    NB_CUDA(cub::DeviceReduce::Sum(E.cub_tmp, tmp2, W.d_dm, W.d_scal, (int)n, st));
+    W.pend_erad = &s->e_radiated;
   }
   s->tick_n = n_next;
   launch_v_from_p(n, s->x, W.v_pred, W.v_eval, st);
@@ -731,6 +742,7 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   E.prof.begin(st);
   NB_TRY(choose_levels_and_open(E, s, prm, nrows, W.rows, st));
   E.prof.end(PROF_LEVELS, st, (double)nrows, 0.0);
+  NB_TRY(pending_flush(E, st));
   if (rows_out && nrows > 0)
     NB_CUDA(cudaMemcpyAsync(rows_out, W.rows, sizeof(int64_t) * nrows, cudaMemcpyDeviceToDevice, st));
   s->last_active = nrows;

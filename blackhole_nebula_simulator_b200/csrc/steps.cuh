@@ -34,6 +34,10 @@ int mark_rows(Engine& E, int64_t nrows, const int64_t* rows, int tight, const do
 // rows as ascending sorted positions in E.ws.rows_s (count ns) and E.ws.pk0 = sorted (x, h)
 int sorted_rows_and_pack(Engine& E, int64_t nrows, const int64_t* rows, const double* x,
                          const double* h, int64_t* ns, cudaStream_t st);
+// checks read at the next host synchronisation (see Workspace::pend_*)
+int pending_enqueue(Engine& E, cudaStream_t st);
+int pending_finish(Engine& E, cudaStream_t st);
+int pending_flush(Engine& E, cudaStream_t st);
 void mask_and_not(int64_t n, const uint8_t* a, const uint8_t* b, uint8_t* out, cudaStream_t st);
 void mask_or(int64_t n, const uint8_t* a, uint8_t* b, cudaStream_t st);
 

@@ -241,6 +241,32 @@ def test_block_steps_match_reference(nb):
     check("list reuses", int(g["reuses"]), st.reuses)
 
 
+def test_block_step_errors_raise_and_leave_the_context_usable(nb):
+    """u <= 0 and a particle inside the GN flow's r = 2.5 raise the reference's exceptions from a
+    block step (sim/blocks.py:250, sim/integrator.py:50); a clean state steps afterwards."""
+    from blackhole_nebula_simulator_b200.config import BlockConfig
+
+    _, _, blocks, _ = nb
+    g = golden("blocks.npz")
+    bc = BlockConfig(coupled=_cfg(cooling_beta=230.0), dt_max=64.0)
+
+    def fresh():
+        return blocks.initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc, t_stop=1e6,
+                                 level_offset=g["level_offset"])  # fmt: skip
+
+    st = fresh()
+    st.u_half[7] = -1.0  # the predictor carries it into u
+    with pytest.raises(FloatingPointError):
+        blocks.advance(st, bc)
+    st = fresh()
+    st.x_beg[11] = st.x_beg[11] / st.x_beg[11].norm() * 2.0
+    with pytest.raises(nb[0].GLFConvergenceError, match="inside r"):
+        blocks.advance(st, bc)
+    st = fresh()
+    actives = [len(blocks.advance(st, bc)) for _ in range(4)]
+    check("active counts after the errors", g["active_counts"][:4], np.array(actives))
+
+
 def test_fp32_pair_arithmetic_within_stated_tolerance(nb):
     """FP32 pair passes (cell offsets, Kahan sums) against the FP64 path on the 4,096-particle
     cloud stirred by 1% velocity noise: h and rho to 1e-5 relative, accelerations and du/dt to
