@@ -605,8 +605,21 @@ static void prof_pairs(Engine& E, int cat, int64_t nrows, const int64_t* rows, c
   count_launch(), k_prof_sum_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, a, E.prof.d_pairs + cat);
 }
 
+// The selection's count must equal the number of rows (the rows are distinct indices in
+// [0, n)); otherwise flag an input error and fill the tail with a valid index, so no pass reads
+// past the selected entries.
+__global__ void k_rows_count_check(int64_t nrows, const int64_t* __restrict__ count,
+                                   int64_t* __restrict__ rows_s, int* err) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t c = *count;
+  if (q == 0 && c != nrows) set_error(err, ERR_BAD_INDEX);
+  if (q < nrows && q >= c) rows_s[q] = c > 0 ? rows_s[0] : 0;
+}
+
 // The rows (caller order) as sorted positions in ascending curve order, into W.rows_s; the
-// pair passes then walk neighbouring particles in neighbouring threads.
+// pair passes then walk neighbouring particles in neighbouring threads.  The rows are distinct
+// (they come from a selection or are all particles), so their count is known without reading
+// the selection's back; a mismatch is reported through the device error word.
 static int rows_sorted(Engine& E, int64_t n, int64_t nrows, const int64_t* rows, int64_t* count,
                        cudaStream_t st) {
   Workspace& W = E.ws;
@@ -618,7 +631,12 @@ static int rows_sorted(Engine& E, int64_t n, int64_t nrows, const int64_t* rows,
   NB_CUDA(cudaMemsetAsync(W.m_x, 0, n, st));
   count_launch(), k_mask_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, n, W.m_x, E.d_err);
   count_launch(), k_sorted_mask<<<grid_for(n), NB_THREADS, 0, st>>>(n, E.lists.perm, W.m_x, W.m_sorted);
-  NB_TRY(select_mask(E, n, W.m_sorted, W.rows_s, count, st));
+  count_launch(), k_iota64<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.i_tmp);
+  size_t tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceSelect::Flagged(E.cub_tmp, tmp, W.i_tmp, W.m_sorted, W.rows_s, W.d_i64 + 4, (int)n, st));
+  count_launch(), k_rows_count_check<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, W.d_i64 + 4, W.rows_s, E.d_err);
+  W.pend_err = true;
+  *count = nrows;
   W.rs_ver = active ? W.rows_ver : -1;
   W.rs_gen = E.lists.gen;
   W.rs_n = nrows;
