@@ -814,10 +814,11 @@ int compute_density(Engine& E, int64_t n, const double* x, const double* mass, d
       NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
       count_launch(), k_count_flag2<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, W.flags, W.d_int);
       int grow_n = 0;
+      W.pend_err = true;  // the density's error word comes back with the count
       NB_TRY(read_int(E, W.d_int, &grow_n, st));
       if (grow_n == 0) {
         *reuses += 1;
-        return check_device_error(E, st);
+        return 0;
       }
       count_launch(), k_max_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, h, W.d_hg);
     }
@@ -830,13 +831,14 @@ int compute_density(Engine& E, int64_t n, const double* x, const double* mass, d
     NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
     count_launch(), k_grow<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, W.flags, h, W.d_hs, W.d_hg, W.d_int);
     int grow_n = 0;
+    W.pend_err = true;  // the build's and the density's error word comes back with the count
     NB_TRY(read_int(E, W.d_int, &grow_n, st));
     if (grow_n == 0) {
       NB_CUDA(cudaMemcpyAsync(C.x_ref, x, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, st));
       NB_CUDA(cudaMemcpyAsync(C.hs, W.d_hs, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
       C.valid = true;
       C.n = n;
-      return check_device_error(E, st);
+      return 0;
     }
   }
   std::snprintf(E.last_error, sizeof(E.last_error),

@@ -562,9 +562,9 @@ __global__ void k_cut_steps(int64_t n, int64_t tick_n, double tick, const int64_
                             const double* __restrict__ a, const double* __restrict__ dudt,
                             int64_t* __restrict__ level, int64_t* __restrict__ n_end,
                             double* __restrict__ p_half, double* __restrict__ u_half,
-                            unsigned long long* __restrict__ woken) {
+                            unsigned long long* __restrict__ woken, const int* __restrict__ err) {
   int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (j >= n) return;
+  if (j >= n || *err) return;  // a failed landing leaves the state as it was
   int64_t nd = need[j];
   if (!(n_end[j] > tick_n && nd > level[j])) return;
   int64_t t_new = ticks_of(nd);
@@ -586,9 +586,9 @@ __global__ void k_open(int64_t nrows, const int64_t* __restrict__ rows, int64_t 
                        const double* __restrict__ a, const double* __restrict__ dudt,
                        int64_t* __restrict__ n_beg, int64_t* __restrict__ n_end,
                        double* __restrict__ x_beg, double* __restrict__ p_half,
-                       double* __restrict__ u_half) {
+                       double* __restrict__ u_half, const int* __restrict__ err) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= nrows) return;
+  if (q >= nrows || *err) return;  // a failed landing leaves the state as it was
   int64_t i = rows[q];
   int64_t t = ticks_of(level[i]);
   double length = (double)t * tick;
@@ -645,7 +645,7 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
     count_launch(), k_scatter_rows_i64<<<grid_for(ns), NB_THREADS, 0, st>>>(ns, W.rows_s, L.perm, W.i_lvl, s->level);
   }
   count_launch(), k_land<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, s->tick_n, s->n_stop, s->level, E.d_err);
-  NB_TRY(check_device_error(E, st));
+  W.pend_err = true;  // read with the wake-up count (the kernels below skip their writes on it)
   if (prm->limiter) {
     // levels after _land, sorted; need in sorted order, then back to the caller's order
     count_launch(), k_gather_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, W.i_lvl);
@@ -656,7 +656,7 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
     NB_CUDA(cudaMemsetAsync(W.d_i64, 0, sizeof(int64_t), st));
     count_launch(), k_cut_steps<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->tick_n, s->tick, W.need, s->a_hydro,
                                                     s->dudt, s->level, s->n_end, s->p_half,
-                                                    s->u_half, (unsigned long long*)W.d_i64);
+                                                    s->u_half, (unsigned long long*)W.d_i64, E.d_err);
     NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     NB_TRY(pending_enqueue(E, st));
     NB_CUDA(cudaStreamSynchronize(st));
@@ -665,7 +665,7 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
   }
   count_launch(), k_open<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, s->tick_n, s->tick, s->level, s->x,
                                                  s->p, s->u, s->a_hydro, s->dudt, s->n_beg,
-                                                 s->n_end, s->x_beg, s->p_half, s->u_half);
+                                                 s->n_end, s->x_beg, s->p_half, s->u_half, E.d_err);
   NB_CUDA(cudaGetLastError());
   return 0;
 }
