@@ -429,6 +429,32 @@ __global__ void k_mark_s(int64_t nrows, const int64_t* __restrict__ rows_s,
   }
 }
 
+// The same touched set read the other way round (the lists are symmetric): particle k is touched
+// if it is a row or a row is among its own entries.  Eight lanes per particle scan its list until
+// one of them meets a row, and the mark goes straight to the caller's order.  Cheaper than
+// scattering marks when a large share of the particles are rows.
+__global__ void k_mark_gather(int64_t n, const int64_t* __restrict__ off,
+                              const int32_t* __restrict__ idx, const uint8_t* __restrict__ row_s,
+                              const int32_t* __restrict__ perm, uint8_t* __restrict__ mark) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t k = t >> 3;
+  const int gl = (int)(t & 7), g = (int)((threadIdx.x & 31) >> 3);
+  const bool live = k < n;
+  if (!__any_sync(0xffffffffu, live)) return;  // warp-uniform
+  bool hit = live && row_s[k];
+  const int64_t e0 = live ? off[k] : 0, e1 = live ? off[k + 1] : 0;
+  for (int64_t b = e0; ; b += 8) {
+    unsigned grp = (__ballot_sync(0xffffffffu, hit) >> (8 * g)) & 0xffu;
+    bool more = grp == 0 && b < e1;  // this particle still unresolved
+    if (!__any_sync(0xffffffffu, more)) {
+      hit = grp != 0;
+      break;
+    }
+    if (more && b + gl < e1) hit = hit || row_s[ld_stream(idx + b + gl)];
+  }
+  if (live && gl == 0 && hit) mark[perm[k]] = 1;
+}
+
 __global__ void k_unsort_marks(int64_t n, const int32_t* __restrict__ perm,
                                const uint8_t* __restrict__ mark_s, uint8_t* __restrict__ mark) {
   int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -853,6 +879,11 @@ int mark_rows(Engine& E, int64_t nrows, const int64_t* rows, int tight, const do
   Workspace& W = E.ws;
   int64_t n = L.n, ns = 0;
   NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));
+  if (!tight && nrows * 4 > n) {
+    // most particles are rows: gather (W.m_sorted holds the rows' sorted mask)
+    count_launch(), k_mark_gather<<<grid_for(n * 8), NB_THREADS, 0, st>>>(n, L.off, L.idx, W.m_sorted, L.perm, mark);
+    return 0;
+  }
   if (tight) count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, h, W.pk0);
   NB_CUDA(cudaMemsetAsync(W.m_smark, 0, n, st));
   count_launch(), k_mark_s<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, tight,
