@@ -342,6 +342,11 @@ __global__ void k_pack_sorted(int64_t n, const int32_t* __restrict__ perm,
   out[k] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], w ? w[i] : 0.0);
 }
 
+__global__ void k_to_float(int64_t n, const double* __restrict__ a, float* __restrict__ out) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < n) out[k] = (float)a[k];
+}
+
 __global__ void k_pack_sorted4(int64_t n, const int32_t* __restrict__ perm, const double* __restrict__ a,
                                const double* __restrict__ b, const double* __restrict__ c,
                                const double* __restrict__ d, double4* __restrict__ out) {
@@ -545,6 +550,7 @@ int Workspace::ensure(Engine& E, int64_t n) {
   double4** d4[] = {&pk0, &pk1, &pk2, &pk3};
   for (double4** p : d4) NB_CUDA(cudaMalloc((void**)p, sizeof(double4) * c));
   NB_CUDA(cudaMalloc((void**)&pk32, sizeof(float4) * c));
+  NB_CUDA(cudaMalloc((void**)&f_mass, sizeof(float) * c));
   float4** f4s[] = {&pf1, &pf2, &pf3};
   for (float4** p : f4s) NB_CUDA(cudaMalloc((void**)p, sizeof(float4) * c));
   int64_t** i8[] = {&rows, &rows_s, &rows2, &iters, &flags, &need, &i_tmp, &pairs, &i_lvl, &i_tmp2};
@@ -589,7 +595,7 @@ int Workspace::ensure(Engine& E, int64_t n) {
 void Workspace::release() {
   void* ps[] = {d_a, d_b, d_c, d_hg, d_hs, d_heff, d_hlim, d_disp, d_P, d_cs, d_vsig, d_ddudt,
                 d_dm, d_tmp, d_uh, v_flow, v_pred, v_eval, v_dacc, v_tmp, pk0, pk1, pk2, pk3, pk32,
-                pf1, pf2, pf3, m_x, m_sorted, m_smark,
+                pf1, pf2, pf3, m_x, m_sorted, m_smark, f_mass,
                 rows, rows_s, rows2, iters, flags, need, i_tmp, pairs, i_lvl, i_tmp2, m_rows, m_done, m_need,
                 m_tmp, i32a, i32b, dk_b, d_int, d_i64, tk_key0, tk_key1, tk_idx0, tk_idx1, d_scal,
                 d_scal_i};
@@ -743,6 +749,8 @@ static int density_on_lists(Engine& E, int64_t n, const double* x, const double*
     // grid over the box of the last list build (cells clamp to it; the edge is derived on the
     // device, so no host round trip)
     count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, E.bbox, W.pk32);
+    count_launch(), k_to_float<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.d_a, W.f_mass);
+    dp.massf = W.f_mass;
     E.prof.begin(st);
     launch_density32<int32_t>(nrows, W.rows_s, W.pk32, E.bbox, W.d_a, W.d_b, W.d_c, L.off,
                               L.idx, dp, L.perm, h_out, rho, omega, W.iters, W.flags,

@@ -51,6 +51,7 @@ struct Workspace {
          *v_tmp = nullptr;  // (n, 3)
   double4 *pk0 = nullptr, *pk1 = nullptr, *pk2 = nullptr, *pk3 = nullptr;  // sorted packs
   float4* pk32 = nullptr;
+  float* f_mass = nullptr;  // sorted masses as floats (FP32 density)
   float4 *pf1 = nullptr, *pf2 = nullptr, *pf3 = nullptr;  // FP32 packs of the force pass
   int64_t *rows = nullptr, *rows_s = nullptr, *rows2 = nullptr, *iters = nullptr,
           *flags = nullptr, *need = nullptr, *i_tmp = nullptr, *pairs = nullptr,

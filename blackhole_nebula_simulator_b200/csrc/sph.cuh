@@ -8,6 +8,7 @@ namespace nbk {
 struct DensityParams {
   int kid;
   double cnorm, eta, tol, h_max;
+  const float* massf = nullptr;  // FP32 form: neighbour masses as floats (sorted order), or null
 };
 
 struct ForceParams {

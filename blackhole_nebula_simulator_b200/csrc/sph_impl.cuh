@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(DENSITY_THREADS, DensityEntry<R>::BLOCKS)
       if (d2 < r2max) {
         inr = true;
         r = sqrt(d2);
-        m = (R)mass[j];
+        m = prm.massf ? (R)prm.massf[j] : (R)mass[j];
       }
     }
     unsigned seg = (__ballot_sync(FULL, inr) >> (8 * g)) & 0xffu;
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(DENSITY_THREADS, DensityEntry<R>::BLOCKS)
           geo.diff(i, j, dx, dy, dz);
           R d2 = sqdist(dx, dy, dz);
           if (!(d2 < r2max)) continue;
-          term(sqrt(d2), (R)mass[j]);
+          term(sqrt(d2), prm.massf ? (R)prm.massf[j] : (R)mass[j]);
         }
       }
     }
