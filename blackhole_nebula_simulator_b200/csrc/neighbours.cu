@@ -312,7 +312,14 @@ __device__ __forceinline__ int64_t leaf_rows(int64_t leaf, int64_t n, const Tree
       // candidate leaf: queue the sub-leaves this lane's sphere reaches
       int64_t s0 = node * (LEAF / SUB);
       int64_t s1 = min(s0 + LEAF / SUB, (n + SUB - 1) / SUB);
-      if (valid) {
+      bool near = valid;
+      if (near) {
+        // the leaf's own box first: a lane whose sphere misses it skips the sub-leaf tests
+        const double4 llo = tv.lo[node], lhi = tv.hi[node];
+        const double lreach = 2.0 * fmax(me.w, llo.w);
+        near = point_gap2(me.x, me.y, me.z, llo, lhi) < lreach * lreach * (1.0 + 1e-12);
+      }
+      if (near) {
         for (int64_t sidx = s0; sidx < s1; ++sidx) {
           double4 blo = slo[sidx], bhi = shi[sidx];
           double reach = 2.0 * fmax(me.w, blo.w);
