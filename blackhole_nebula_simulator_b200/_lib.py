@@ -47,6 +47,8 @@ class NbParams(_c.Structure):
         ("precision", _int), ("cooling", _int), ("cooling_beta", _dbl), ("u_floor", _dbl),
         ("brems_tfac", _dbl), ("brems_b", _dbl), ("brems_kappa", _dbl), ("brems_t_floor", _dbl),
         ("dt_max", _dbl), ("limiter", _int), ("max_gap", _int), ("mlp", NbMlpParams),
+        ("eos", _int), ("eos_rho_si", _dbl), ("eos_u_si", _dbl), ("eos_a1", _dbl),
+        ("eos_a_rad", _dbl),
     ]  # fmt: skip
 
 
@@ -89,6 +91,7 @@ _SIGS = {
     "nb_beta_cool": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     "nb_brems_cool": (_int, [_vp, _i64, _vp, _vp, _vp, _dbl, _c.POINTER(NbParams), _vp, _vp]),
     "nb_ledger": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _c.POINTER(_dbl), _vp]),
+    "nb_eos": (_int, [_vp, _i64, _vp, _vp, _c.POINTER(NbParams), _vp, _vp, _vp, _vp, _vp]),
     "nb_coupled_initialise": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams), _vp]),
     "nb_coupled_step": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams), _dbl, _vp]),
     "nb_coupled_stable_dt": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams),
@@ -131,7 +134,7 @@ def lib():
 _ERRORS = {
     11: GLFConvergenceError, 12: GLFConvergenceError, 13: GLFConvergenceError,
     20: RuntimeError, 21: RuntimeError, 22: FloatingPointError, 23: ValueError, 24: ValueError,
-    25: NotImplementedError, 26: ValueError,
+    25: NotImplementedError, 26: ValueError, 27: ValueError, 28: RuntimeError,
 }  # fmt: skip
 
 

@@ -119,6 +119,16 @@ class BlockConfig:
     removal_sync: bool = True
 
 
+# equations of state of sim/hydro.py:121-139 and their ids in nb_params.eos
+EOS_IDS = {"ideal": 0, "gasrad": 1, "radiation": 2}
+
+
+def eos_fields(hc) -> dict:
+    """The nb_params EOS fields of a HydroConfig (gas + radiation in SI inside the T-solve)."""
+    return dict(eos=EOS_IDS[hc.eos], eos_rho_si=hc.gas_units.density_kg_m3, eos_u_si=units.C**2,
+                eos_a1=1.5 * units.K_B / (units.MU * units.M_P), eos_a_rad=units.A_RAD)  # fmt: skip
+
+
 def check_supported(cc: CoupledConfig) -> None:
     """Raise NotImplementedError for reference options outside the CUDA path."""
     hc = cc.hydro
@@ -127,8 +137,11 @@ def check_supported(cc: CoupledConfig) -> None:
         bad.append("periodic box")
     if hc.isothermal_cs is not None:
         bad.append("isothermal equation of state")
-    if hc.eos != "ideal":
-        bad.append(f"eos={hc.eos!r}")
+    if hc.eos not in EOS_IDS:
+        raise ValueError(f"unknown equation of state {hc.eos!r}")
+    cooling_on = cc.cooling == "brems" or math.isfinite(cc.cooling_beta)
+    if hc.eos != "ideal" and cooling_on:
+        bad.append(f"cooling with eos={hc.eos!r} (the floor energy then depends on rho)")
     if hc.viscosity and hc.switch:
         bad.append("Cullen-Dehnen switch (switch=True)")
     if hc.viscosity and hc.reconstruction:

@@ -14,7 +14,7 @@ from dataclasses import dataclass, field
 import torch
 
 from . import _lib
-from .config import C_NORM, KERNEL_IDS, CoupledConfig, check_supported
+from .config import C_NORM, KERNEL_IDS, CoupledConfig, check_supported, eos_fields
 from .cooling import brems_constants, floor_energy
 from .device import ctx, dev_f64, ptr, stream, to_numpy
 from . import ops
@@ -48,6 +48,8 @@ def make_params(cc: CoupledConfig, dt_max: float = 4096.0, limiter: bool = True,
         p.cooling_beta = cc.cooling_beta
         p.u_floor = floor_energy(hc.gamma, cc.t_floor)
     p.dt_max, p.limiter, p.max_gap = dt_max, int(limiter), int(max_gap)
+    for k, v in eos_fields(hc).items():
+        setattr(p, k, v)
     return p
 
 

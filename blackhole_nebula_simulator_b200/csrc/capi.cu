@@ -7,6 +7,7 @@
 #include "common.cuh"
 #include "cooling.cuh"
 #include "engine.cuh"
+#include "eos.cuh"
 #include "gravity.cuh"
 #include "sph.cuh"
 #include "steps.cuh"
@@ -30,6 +31,24 @@ int begin(nb_ctx* ctx) {
   E.ws.pend_erad = nullptr;
   NB_CUDA(cudaSetDevice(E.device));
   return 0;
+}
+
+__global__ void k_eos_op(int64_t n, const double* __restrict__ rho, const double* __restrict__ u,
+                         nbk::EosParams ep, double* __restrict__ P, double* __restrict__ cs,
+                         double* __restrict__ T, double* __restrict__ beta, int* err) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double ui = u[i];
+  if (!(ui > 0.0)) {
+    nbk::set_error(err, nbk::ERR_NONPOSITIVE_U);
+    return;
+  }
+  double p, c, t, b;
+  nbk::eos_point(ep, rho[i], ui, p, c, t, b, err);
+  P[i] = p;
+  cs[i] = c;
+  if (T) T[i] = t;
+  if (beta) beta[i] = b;
 }
 
 __global__ void k_beta(int64_t n, const double* __restrict__ u, const double* __restrict__ uf,
@@ -322,6 +341,20 @@ int nb_brems_cool(nb_ctx* ctx, int64_t n, const double* u, const double* rho, co
                                                             brems_params(prm), out);
   NB_CUDA(cudaGetLastError());
   return 0;
+}
+
+int nb_eos(nb_ctx* ctx, int64_t n, const double* rho, const double* u, const nb_params* prm,
+           double* P, double* c_s, double* T, double* beta, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (!prm) return nbk::set_host_error(E, "params missing"), NB_ERR_INPUT;
+  if (prm->eos < 0 || prm->eos > 2) return nbk::set_host_error(E, "unknown equation of state"), NB_ERR_INPUT;
+  NB_TRY(E.ensure_n(std::max<int64_t>(n, 1)));
+  if (n > 0)
+    nbk::count_launch(), k_eos_op<<<nbk::grid_for(n), NB_THREADS, 0, S(stream)>>>(
+        n, rho, u, nbk::eos_of(prm), P, c_s, T, beta, E.d_err);
+  NB_CUDA(cudaGetLastError());
+  return nbk::check_device_error(E, S(stream));
 }
 
 int nb_ledger(nb_ctx* ctx, int64_t n, const double* x, const double* p, const double* u,

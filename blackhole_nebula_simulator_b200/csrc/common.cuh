@@ -21,6 +21,8 @@ enum : int {
   ERR_LEVEL = 5,             // a level beyond K_MAX
   ERR_LIMITER = 6,           // the level limiter did not settle within its sweep bound
   ERR_DT = 7,                // a wanted time step that is not positive
+  ERR_EOS_RANGE = 8,         // u outside the gas + radiation EOS bracket [1, 1e13] K
+  ERR_EOS_CONVERGE = 9,      // the gas + radiation temperature did not converge
 };
 
 __device__ __forceinline__ void set_error(int* err, int code) {

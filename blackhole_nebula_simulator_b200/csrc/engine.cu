@@ -13,6 +13,7 @@
 #include "common.cuh"
 #include "cooling.cuh"
 #include "engine.cuh"
+#include "eos.cuh"
 #include "gravity.cuh"
 #include "sph.cuh"
 #include "steps.cuh"
@@ -167,6 +168,8 @@ int check_device_error(Engine& E, cudaStream_t st) {
     case ERR_LEVEL: msg = "a particle needs a level beyond K_MAX = 40"; ret = NB_ERR_LEVEL; break;
     case ERR_LIMITER: msg = "level limiter did not settle"; ret = -3; break;
     case ERR_DT: msg = "time steps must be positive"; ret = NB_ERR_DT; break;
+    case ERR_EOS_RANGE: msg = "u outside the EOS bracket [1, 1e13] K"; ret = NB_ERR_EOS_RANGE; break;
+    case ERR_EOS_CONVERGE: msg = "gas + radiation EOS: temperature did not converge"; ret = NB_ERR_EOS; break;
   }
   std::snprintf(E.last_error, sizeof(E.last_error), "%s", msg);
   return ret;
@@ -378,15 +381,35 @@ __global__ void k_pack_sorted32(int64_t n, const int32_t* __restrict__ perm,
   out[k] = make_float4(o[0], o[1], o[2], __int_as_float((c[0] << 20) | (c[1] << 10) | c[2]));
 }
 
-// ideal-gas EOS (physics/eos.py:21-28) for every particle; u <= 0 is an error
+// the configured EOS (sim/hydro.py:119-139) for every particle, or for the particles of `mask`
+// when one is given; u <= 0 is an error
 __global__ void k_eos(int64_t n, const double* __restrict__ rho, const double* __restrict__ u,
-                      double gamma, double* __restrict__ P, double* __restrict__ cs, int* err) {
+                      const uint8_t* __restrict__ mask, EosParams ep, double* __restrict__ P,
+                      double* __restrict__ cs, int* err) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (mask && !mask[i]) return;
   double ui = u[i];
-  if (!(ui > 0.0)) set_error(err, ERR_NONPOSITIVE_U);
-  P[i] = (gamma - 1.0) * rho[i] * ui;
-  cs[i] = sqrt(gamma * (gamma - 1.0) * ui);
+  if (!(ui > 0.0)) {
+    set_error(err, ERR_NONPOSITIVE_U);
+    return;
+  }
+  double p, c, t, b;
+  eos_point(ep, rho[i], ui, p, c, t, b, err);
+  P[i] = p;
+  cs[i] = c;
+}
+
+EosParams eos_of(const nb_params* prm) {
+  EosParams ep;
+  ep.kind = prm->eos;
+  ep.gamma = prm->gamma;
+  ep.rho_si = prm->eos_rho_si;
+  ep.u_si = prm->eos_u_si;
+  ep.a1 = prm->eos_a1;
+  ep.kb_mu = prm->eos_a1 / 1.5;
+  ep.a_rad = prm->eos_a_rad;
+  return ep;
 }
 
 // after the force pass: add the disc viscosity, nu, alpha and v_sig of the rows
@@ -933,13 +956,17 @@ int select_mask(Engine& E, int64_t n, const uint8_t* mask, int64_t* out, int64_t
 
 // Fused EOS + force pass for `rows` (caller order) with interacting pairs only (the tightened
 // lists of sim/neighbours.py:284-323, tested on the fly).  Writes a_hydro, dudt, vsig_max,
-// visc_heating (and nu) at the rows.  P and c_s of every particle go to W.d_P / W.d_cs.
+// visc_heating (and nu) at the rows.  P and c_s go to W.d_P / W.d_cs: for every particle with the
+// ideal gas, and with an iterative EOS for the particles of `touched` (every particle when null),
+// a superset of the rows and their interacting neighbours.
 int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, int64_t nrows,
-                  const int64_t* rows, const nb_params* prm, cudaStream_t st) {
+                  const int64_t* rows, const nb_params* prm, const uint8_t* touched,
+                  cudaStream_t st) {
   Workspace& W = E.ws;
   Lists& L = E.lists;
   int64_t n = s->n;
-  count_launch(), k_eos<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->rho, u, prm->gamma, W.d_P, W.d_cs, E.d_err);
+  const uint8_t* eos_mask = prm->eos == 0 ? nullptr : touched;
+  count_launch(), k_eos<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->rho, u, eos_mask, eos_of(prm), W.d_P, W.d_cs, E.d_err);
   if (nrows == 0) return check_device_error(E, st);
   int64_t ns = 0;
   NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));

@@ -115,7 +115,7 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
   }
   if (prm->viscosity)
     count_launch(), k_set_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, prm->alpha_const, s->alpha);
-  return engine_forces(E, s, vel, u, nrows, rows, prm, st);
+  return engine_forces(E, s, vel, u, nrows, rows, prm, W.m_done, st);
 }
 
 // ---------------------------------------------------------------- shared step

@@ -16,7 +16,8 @@ int compute_density(Engine& E, int64_t n, const double* x, const double* mass, d
 int select_mask(Engine& E, int64_t n, const uint8_t* mask, int64_t* out, int64_t* count,
                 cudaStream_t st);
 int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, int64_t nrows,
-                  const int64_t* rows, const nb_params* prm, cudaStream_t st);
+                  const int64_t* rows, const nb_params* prm, const uint8_t* touched,
+                  cudaStream_t st);
 
 int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, const int64_t* rows,
                const double* vel, const double* u, cudaStream_t st);

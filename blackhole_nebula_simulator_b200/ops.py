@@ -253,6 +253,44 @@ def beta_cool(u, u_floor, dt, t_cool):
     return out
 
 
+def _eos_call(hc, rho, u, with_t):
+    from .config import eos_fields
+
+    rho = dev_f64(rho)
+    u = dev_f64(u, rho.shape)
+    prm = _lib.NbParams()
+    prm.gamma = hc.gamma
+    for k, v in eos_fields(hc).items():
+        setattr(prm, k, v)
+    n = len(rho)
+    P, cs = torch.empty_like(rho), torch.empty_like(rho)
+    T = torch.empty_like(rho) if with_t else None
+    beta = torch.empty_like(rho) if with_t else None
+    _call("nb_eos", n, ptr(rho), ptr(u), ctypes.byref(prm), ptr(P), ptr(cs),
+          ptr(T) if with_t else None, ptr(beta) if with_t else None, stream())  # fmt: skip
+    return P, cs, T, beta
+
+
+def eos_state(cfg, rho, u):
+    """sim/hydro.py:121-139 (ideal gas, radiation limit or gas + radiation): (P, c_s) in code
+    units.  Raises FloatingPointError for u <= 0, ValueError for u outside the gas + radiation
+    bracket [1, 1e13] K and RuntimeError if its temperature does not converge, as the reference."""
+    if cfg.isothermal_cs is not None:
+        raise NotImplementedError("isothermal equations of state are not part of the CUDA SPH path")
+    P, cs, _, _ = _eos_call(cfg, rho, u, False)
+    return P, cs
+
+
+def gasrad_state(rho, u, gas_units=None):
+    """gasrad_state_nb (sim/fastphys.py:93-107): (P [code], c_s [c], T [K], beta_gas) of gas +
+    radiation in local thermodynamic equilibrium."""
+    from .config import HydroConfig
+    from .units import GasUnits
+
+    hc = HydroConfig(eos="gasrad", gas_units=gas_units if gas_units is not None else GasUnits())
+    return _eos_call(hc, rho, u, True)
+
+
 def ledger_sums(x, p, u, mass) -> dict:
     """sim/coupled.py:261-270 sums on the device: energy sum m (H + u) (without radiated energy),
     sum m |H|, angular momentum, momentum, mass."""

@@ -15,6 +15,7 @@ M_SUN = 1.98847e30  # kg
 K_B = 1.380649e-23  # J/K
 M_P = 1.67262192369e-27  # kg
 MU = 0.6  # mean molecular weight, fully ionised solar gas
+A_RAD = 7.565733250033929e-16  # radiation constant 4 sigma / c [J m^-3 K^-4]
 X_HYDROGEN = 0.70
 Z_METALS = 0.02
 SGR_A_MASS_MSUN = 4.3e6

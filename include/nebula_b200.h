@@ -31,6 +31,8 @@ extern "C" {
 #define NB_ERR_DT 24              /* [ValueError] time steps must be positive */
 #define NB_ERR_UNSUPPORTED 25     /* [NotImplementedError] option outside the CUDA path */
 #define NB_ERR_INPUT 26           /* [ValueError] bad argument */
+#define NB_ERR_EOS_RANGE 27       /* [ValueError] u outside the gas + radiation EOS bracket [1, 1e13] K */
+#define NB_ERR_EOS 28             /* [RuntimeError] gas + radiation temperature did not converge */
 
 #if defined(__GNUC__)
 #define NB_API __attribute__((visibility("default")))
@@ -71,6 +73,11 @@ typedef struct nb_params {
   double dt_max;          /* block steps: level-0 step */
   int limiter, max_gap;
   nb_mlp_params mlp;      /* cooling 3: the network (weights set by nb_mlp_train / nb_mlp_weights) */
+  int eos;                /* 0 ideal gas (gamma), 1 gas + radiation, 2 radiation limit (P = rho u / 3) */
+  double eos_rho_si;      /* gas + radiation: kg/m^3 per code density (the run's GasUnits) */
+  double eos_u_si;        /* J/kg per code specific energy (c^2) */
+  double eos_a1;          /* 3 k / (2 mu m_p) [J/(kg K)] */
+  double eos_a_rad;       /* radiation constant [J m^-3 K^-4] */
 } nb_params;
 
 /* Device state of a run (the fields of the reference's GasState / BlockState that the step
@@ -162,6 +169,12 @@ NB_API int nb_beta_cool(nb_ctx* ctx, int64_t n, const double* u, const double* u
  * documented in cooling.cuh).  dt NULL: dt_scalar for all. */
 NB_API int nb_brems_cool(nb_ctx* ctx, int64_t n, const double* u, const double* rho, const double* dt,
                   double dt_scalar, const nb_params* prm, double* out, void* stream);
+
+/* eos_state (sim/hydro.py:121-139) with prm->eos: pressure and sound speed (code units) of n
+ * particles; for gas + radiation (gasrad_state_nb, sim/fastphys.py:45-102) also T [K] and
+ * beta_gas (T and beta may be NULL; other equations of state write 0 and 1). */
+NB_API int nb_eos(nb_ctx* ctx, int64_t n, const double* rho, const double* u, const nb_params* prm,
+                  double* P, double* c_s, double* T, double* beta, void* stream);
 
 /* Ledger sums (sim/coupled.py:261-270) into out[9] on the host: sum m (H + u), sum m |H|,
  * angular momentum (3), momentum (3), mass. */

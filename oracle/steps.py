@@ -6,9 +6,9 @@ Restates the reference's step logic on top of the C kernels:
   * blocks:  sim/blocks.py:192-563, 722-787 (_density_touched, _hydro_rows, wanted_dt,
     _choose_levels, _land, _wake, _cut_steps, _cut_to, _open, initialise, advance, run, ledger,
     diagnostics, snapshot) and sim/timesteps.py:21-59 (ticks, level_for_dt, allowed_level).
-Only the options of the CUDA path are restated: GN hole, ideal gas, constant alpha (no switch,
-no reconstruction), optional conductivity and disc viscosity, beta or bremsstrahlung cooling, no
-removal radii and no RESPA.  The heat-budget bookkeeping arrays are not kept.
+Only the options of the CUDA path are restated: GN hole, ideal gas (or, without cooling, the
+radiation limit and gas + radiation), constant alpha (no switch, no reconstruction), optional
+conductivity and disc viscosity, beta or bremsstrahlung cooling, no removal radii and no RESPA.  The heat-budget bookkeeping arrays are not kept.
 """
 
 from __future__ import annotations
@@ -21,6 +21,7 @@ import numpy as np
 
 from . import cooling as ocool
 from . import native
+from .eos import eos_state
 from .sph import C_NORM, KERNEL_IDS, compute_density
 
 K_MAX = 40
@@ -64,10 +65,8 @@ def ledger_sums(mass, x, p, u, e_rad):
 
 
 def _eos(hc, rho, u):
-    """physics/eos.py:21-28 (ideal gas)."""
-    if np.any(u <= 0):
-        raise FloatingPointError(f"non-positive internal energy at {int(np.sum(u <= 0))} particles")
-    return (hc.gamma - 1.0) * rho * u, np.sqrt(hc.gamma * (hc.gamma - 1.0) * u)
+    """sim/hydro.py:119-139: ideal gas, radiation limit or gas + radiation."""
+    return eos_state(hc, rho, u)
 
 
 def _kid(hc):

@@ -243,27 +243,81 @@ def blocks_fixture(blocks, coupled, ics, hydro_cfg):
     _save("blocks.npz", **out)
 
 
+def eos_fixture(hydro_mod, units_mod):
+    """Equations of state of sim/hydro.py:121-139 on seeded (rho, T): ideal, radiation limit and
+    gas + radiation (the Numba T-solve of sim/fastphys.py:45-102), with T and beta_gas."""
+    from nebula.sim.fastphys import gasrad_state_nb
+    from nebula.physics.eos import gasrad_u_si
+
+    rng = np.random.default_rng(SEED + 5)
+    gu = units_mod.GasUnits()
+    rho = 10.0 ** rng.uniform(-12.0, -4.0, 4000)
+    t = 10.0 ** rng.uniform(3.0, 12.0, 4000)
+    u = units_mod.specific_energy_from_si(gasrad_u_si(gu.density_to_si(rho), t))
+    p, cs, tt, beta = gasrad_state_nb(rho, u, gu)
+    out = dict(rho=rho, u=u, gasrad_p=p, gasrad_cs=cs, gasrad_t=tt, gasrad_beta=beta)
+    for eos in ("ideal", "radiation"):
+        hc = hydro_mod.HydroConfig(eos=eos)
+        pe, ce = hydro_mod.eos_state(hc, rho, u)
+        out[f"{eos}_p"], out[f"{eos}_cs"] = pe, ce
+    _save("eos.npz", **out)
+
+
+def gasrad_blocks_fixture(blocks, coupled, ics, hydro_cfg):
+    """Block steps of the 2,048-particle cloud of blocks_fixture with the gas + radiation
+    equation of state (radiation-dominated at 3e8 K), no cooling; 12 system steps."""
+    ic = ics.cloud(2048, radius=20.0, total_mass=1e-3, t_kelvin=3e8, r_peri=60.0, r_apo=400.0,
+                   seed=7)  # fmt: skip
+    rng = np.random.default_rng(SEED + 6)
+    v = ic.v + rng.normal(0.0, 0.002, ic.v.shape)
+    hc = hydro_cfg(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                   conductivity_signal=1, alpha_u=0.05, h_max=200.0, eos="gasrad")  # fmt: skip
+    cc = coupled.CoupledConfig(hydro=hc)
+    bc = blocks.BlockConfig(coupled=cc, dt_max=64.0)
+    st = blocks.initialise(ic.x, v, ic.u, ic.mass, ic.h, bc, t_stop=1e6)
+    fields = ["x", "p", "u", "h", "rho", "omega", "a_hydro", "dudt", "level", "n_beg", "n_end",
+              "vsig_max"]
+    out = dict(x0=ic.x, v0=v, u0=ic.u, mass=ic.mass, h0=ic.h)
+    out.update(_state_arrays("init", st, fields))
+    actives = [len(blocks.advance(st, bc)) for _ in range(12)]
+    out.update(_state_arrays("final", st, fields))
+    out["final_energy"] = blocks.ledger(st, bc)["energy"]
+    out["final_n"] = st.n
+    out["active_counts"] = np.array(actives)
+    _save("gasrad_blocks.npz", **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="root of the reference checkout")
+    ap.add_argument("--only", nargs="*", help="write only these fixtures (names without .npz)")
     args = ap.parse_args()
     sys.path.insert(0, os.path.join(args.reference, "src"))
     sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
     from nebula.physics import cooling, gravity
     from nebula.sim import blocks, coupled, integrator, sph
     from nebula.sim import neighbours as nbmod
+    from nebula import units as units_mod
+    from nebula.sim import hydro as hydro_mod
     from nebula.sim.hydro import HydroConfig
 
     from blackhole_nebula_simulator_b200 import ics
 
-    lists_fixture(nbmod)
-    cloud_lists_fixture(nbmod, ics)
-    density_fixture(sph, nbmod)
-    forces_fixture(sph, nbmod)
-    glf_fixture(integrator, gravity)
-    cooling_fixture(cooling)
-    coupled_fixture(coupled, ics, HydroConfig)
-    blocks_fixture(blocks, coupled, ics, HydroConfig)
+    makers = {
+        "lists": lambda: lists_fixture(nbmod),
+        "cloud_lists": lambda: cloud_lists_fixture(nbmod, ics),
+        "density": lambda: density_fixture(sph, nbmod),
+        "forces": lambda: forces_fixture(sph, nbmod),
+        "glf": lambda: glf_fixture(integrator, gravity),
+        "cooling": lambda: cooling_fixture(cooling),
+        "coupled": lambda: coupled_fixture(coupled, ics, HydroConfig),
+        "blocks": lambda: blocks_fixture(blocks, coupled, ics, HydroConfig),
+        "eos": lambda: eos_fixture(hydro_mod, units_mod),
+        "gasrad_blocks": lambda: gasrad_blocks_fixture(blocks, coupled, ics, HydroConfig),
+    }
+    for name, make in makers.items():
+        if not args.only or name in args.only:
+            make()
 
 
 if __name__ == "__main__":

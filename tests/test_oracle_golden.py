@@ -196,3 +196,61 @@ def test_block_steps_match_reference():
     check("final e_radiated", float(g["final_e_radiated"]), st.e_radiated, rtol=1e-9)
     check("cache builds", int(g["builds"]), st.neighbour_cache.builds)
     check("cache reuses", int(g["reuses"]), st.neighbour_cache.reuses)
+
+
+def test_equations_of_state_match_reference():
+    from blackhole_nebula_simulator_b200.config import HydroConfig
+    from oracle import eos as oeos
+
+    g = golden("eos.npz")
+    gu = HydroConfig().gas_units
+    p, cs, t, beta = oeos.gasrad_state(g["rho"], g["u"], gu.density_kg_m3)
+    check("gasrad T", g["gasrad_t"], t, rtol=1e-13)
+    check("gasrad P", g["gasrad_p"], p, rtol=1e-13)
+    check("gasrad c_s", g["gasrad_cs"], cs, rtol=1e-13)
+    check("gasrad beta", g["gasrad_beta"], beta, rtol=1e-12, atol=1e-300)
+    for eos in ("ideal", "radiation"):
+        pe, ce = oeos.eos_state(HydroConfig(eos=eos), g["rho"], g["u"])
+        check(f"{eos} P", g[f"{eos}_p"], pe, rtol=1e-15)
+        check(f"{eos} c_s", g[f"{eos}_cs"], ce, rtol=1e-15)
+
+
+def test_eos_range_and_sign_errors():
+    from blackhole_nebula_simulator_b200.config import HydroConfig
+    from oracle import eos as oeos
+
+    hc = HydroConfig(eos="gasrad")
+    rho = np.array([1e-8, 1e-8])
+    with pytest.raises(ValueError, match="bracket"):
+        oeos.eos_state(hc, rho, np.array([1e-12, 1e-30]))
+    with pytest.raises(ValueError, match="bracket"):
+        oeos.eos_state(hc, rho, np.array([1e-12, 1e29]))
+    with pytest.raises(FloatingPointError):
+        oeos.eos_state(hc, rho, np.array([1e-12, 0.0]))
+
+
+def test_gasrad_block_steps_match_reference():
+    from blackhole_nebula_simulator_b200.config import BlockConfig, HydroConfig
+
+    g = golden("gasrad_blocks.npz")
+    hc = HydroConfig(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                     conductivity_signal=1, alpha_u=0.05, h_max=200.0, eos="gasrad")  # fmt: skip
+    _, CC = _cfg()
+    bc = BlockConfig(coupled=CC(hydro=hc), dt_max=64.0)
+    st = steps.blocks_initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc, t_stop=1e6)
+    check("init levels", g["init_level"], st.level)
+    check("init n_end", g["init_n_end"], st.n_end)
+    check("init dudt", g["init_dudt"], st.dudt, rtol=1e-9,
+          atol=1e-10 * np.abs(g["init_dudt"]).max())  # fmt: skip
+    check("init acc", g["init_a_hydro"], st.a_hydro, rtol=1e-9, per_vector=True)
+    actives = [len(steps.blocks_advance(st, bc)) for _ in range(len(g["active_counts"]))]
+    check("active counts", g["active_counts"], np.array(actives))
+    check("final tick", int(g["final_n"]), st.n)
+    check("final levels", g["final_level"], st.level)
+    check("final n_end", g["final_n_end"], st.n_end)
+    check("final x", g["final_x"], st.x, rtol=1e-13, per_vector=True)
+    check("final p", g["final_p"], st.p, rtol=1e-11, per_vector=True)
+    check("final u", g["final_u"], st.u, rtol=1e-9)
+    check("final h", g["final_h"], st.h, rtol=1e-9)
+    check("final energy", float(g["final_energy"]), steps.blocks_ledger(st, bc)["energy"],
+          rtol=1e-12)  # fmt: skip
