@@ -75,12 +75,14 @@ def cooling_network():
     return net
 
 
-def workload(name: str, n: int | None, precision: str, seed_shift: int = 0, mlp=None):
+def workload(name: str, n: int | None, precision: str, seed_shift: int = 0, mlp=None,
+             eos: str = "ideal"):
     from blackhole_nebula_simulator_b200 import ics
     from blackhole_nebula_simulator_b200.config import BlockConfig, CoupledConfig, HydroConfig
 
     common = dict(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
-                  conductivity_signal=1, alpha_u=0.05, h_max=200.0, precision=precision)  # fmt: skip
+                  conductivity_signal=1, alpha_u=0.05, h_max=200.0, precision=precision,
+                  eos=eos)  # fmt: skip
     if name == "torus":
         n = n or 4_194_304
         ic = ics.torus(n, seed=4 + seed_shift)
@@ -154,7 +156,7 @@ def profile_read(ctx):
 
     from blackhole_nebula_simulator_b200 import _lib
 
-    names = ["lists", "density", "forces", "flow", "marks", "levels", "cooling"]
+    names = ["lists", "density", "forces", "flow", "marks", "levels", "cooling", "eos"]
     out = (ctypes.c_double * (4 * len(names)))()
     _lib.check(ctx, _lib.lib().nb_profile_read(ctx, out))
     return {names[c]: {"ms": out[4 * c], "launches": int(out[4 * c + 1]), "units": out[4 * c + 2],
@@ -221,7 +223,7 @@ def run_gpu(args, rank, world, precision=None, use_mlp=None, e2e=True):
     precision = precision or args.precision
     use_mlp = (precision == "fp32") if use_mlp is None else use_mlp
     net = cooling_network() if use_mlp else None
-    ic, bc = workload(args.workload, args.n, precision, seed_shift=rank, mlp=net)
+    ic, bc = workload(args.workload, args.n, precision, seed_shift=rank, mlp=net, eos=args.eos)
     st = blocks.initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=bc.dt_max * 2.0**20)
     led_init = blocks.ledger(st, bc)  # every particle is at a step boundary here
     for _ in range(args.warmup):
@@ -330,7 +332,7 @@ def cpu_reference(args, steps, warmup, sample_n=None):
 
     n_full = {"torus": 4_194_304, "streams": 1_048_576, "cloud": 262_144}[args.workload]
     n = sample_n or min(args.n or n_full, 32_768)
-    ic, bc = workload(args.workload, n, "fp64")
+    ic, bc = workload(args.workload, n, "fp64", eos=args.eos)
     st = osteps.blocks_initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=bc.dt_max * 2.0**20)
     for _ in range(warmup):
         osteps.blocks_advance(st, bc)
@@ -355,9 +357,14 @@ def main():
     ap.add_argument("--workload", default="torus", choices=["torus", "streams", "cloud"])
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--eos", default="ideal", choices=["ideal", "gasrad", "radiation"],
+                    help="equation of state (gas + radiation and the radiation limit run without "
+                         "cooling: the cloud workload)")  # fmt: skip
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain comparison form")
     args = ap.parse_args()
+    if args.eos != "ideal" and args.workload != "cloud":
+        ap.error("--eos gasrad/radiation needs a workload without cooling: --workload cloud")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     n_full = args.n or {"torus": 4_194_304, "streams": 1_048_576, "cloud": 262_144}[args.workload]
@@ -365,7 +372,7 @@ def main():
               "particles": n_full,
               "precision": args.precision if args.impl == "ours" else "fp64 (CPU oracle)",
               "l2_flush": "inputs larger than L2",
-              "parallelism": f"replicas x{world}"}  # fmt: skip
+              "parallelism": f"replicas x{world}", "eos": args.eos}  # fmt: skip
     if args.workload == "torus":
         config["disc_alpha_av"] = TORUS_ALPHA_AV
         config["scale_height"] = TORUS_SCALE_HEIGHT

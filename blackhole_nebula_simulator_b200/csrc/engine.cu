@@ -966,7 +966,9 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   Lists& L = E.lists;
   int64_t n = s->n;
   const uint8_t* eos_mask = prm->eos == 0 ? nullptr : touched;
+  E.prof.begin(st);
   count_launch(), k_eos<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->rho, u, eos_mask, eos_of(prm), W.d_P, W.d_cs, E.d_err);
+  E.prof.end(PROF_EOS, st, (double)n, 0.0);
   if (nrows == 0) return check_device_error(E, st);
   int64_t ns = 0;
   NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));

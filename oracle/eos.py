@@ -1,18 +1,18 @@
 """CPU oracle of the equations of state (TEST INFRASTRUCTURE).
 
-NumPy restatement of sim/hydro.py:119-139 (eos_state), physics/eos.py:21-38 (ideal gas,
+NumPy restatement (the T iteration in C, oracle.c) of sim/hydro.py:119-139 (eos_state), physics/eos.py:21-38 (ideal gas,
 radiation limit) and the gas + radiation state of physics/eos.py:60-160 / sim/fastphys.py:45-107:
 T from (rho, u) by Newton's method on log T inside a bisection bracket [1, 1e13] K narrowed every
 iteration (tolerance 1e-12, at most 200 iterations), then P = rho k T/(mu m_p) + a T^4/3,
-beta = P_gas/P, Gamma_1(beta) for gamma = 5/3 and c_s = sqrt(Gamma_1 P / rho).  Pinned to the
-reference's outputs in tests/golden/eos.npz.
+beta = P_gas/P, Gamma_1(beta) for gamma = 5/3 and c_s = sqrt(Gamma_1 P / rho).  Pinned bit for bit
+to the reference's outputs in tests/golden/eos.npz.
 """
 
 from __future__ import annotations
 
-import math
-
 import numpy as np
+
+from . import native
 
 K_B = 1.380649e-23
 M_P = 1.67262192369e-27
@@ -20,53 +20,22 @@ MU = 0.6
 C = 299_792_458.0
 A_RAD = 7.565733250033929e-16
 T_MIN, T_MAX = 1.0, 1.0e13
-TOL = 1e-12
-MAX_ITER = 200
-
-
-def _temperature_one(r, uu, a1):
-    """One element of sim/fastphys.py:45-71 in scalar IEEE arithmetic with the C library's exp,
-    log and pow (as the Numba kernel calls them); None when it does not converge."""
-    lo, hi = math.log(T_MIN), math.log(T_MAX)
-    t0 = min(uu / a1, (uu * r / A_RAD) ** 0.25)
-    lt = math.log(min(max(t0, T_MIN), T_MAX))
-    for _ in range(MAX_ITER):
-        t = math.exp(lt)
-        t2 = t * t
-        t4 = t2 * t2  # Numba evaluates t**4 by squaring
-        f = a1 * t + A_RAD * t4 / r - uu
-        dfdl = a1 * t + 4.0 * A_RAD * t4 / r
-        if f < 0:
-            lo = lt
-        if f > 0:
-            hi = lt
-        new = lt - f / dfdl
-        if new <= lo or new >= hi or not math.isfinite(new):
-            new = 0.5 * (lo + hi)
-        step = abs(new - lt)
-        lt = new
-        if step < TOL:
-            return math.exp(lt)
-    return None
 
 
 def gasrad_temperature(rho_si, u_si):
-    """T [K] of gas + radiation: physics/eos.py:110-144 / sim/fastphys.py:74-89.  Where f(T)
-    rounds to a tiny non-zero value at the root, the reference's bracket test sends the iterate
-    to bisection, so the result depends on the last bit of every operation: hence the scalar
-    libm arithmetic here."""
-    rho = np.asarray(rho_si, float)
-    u = np.broadcast_to(np.asarray(u_si, float), rho.shape)
+    """T [K] of gas + radiation: physics/eos.py:110-144 / sim/fastphys.py:74-89, the iteration in
+    C (``or_gasrad_temperature``) with the C library's exp, log and pow as the Numba kernel calls
+    them.  Where f(T) rounds to a tiny non-zero value at the root, the reference's bracket test
+    sends the iterate into bisection, so the result depends on the last bit of every operation."""
+    rho = np.ravel(np.asarray(rho_si, float))
+    u = np.ravel(np.broadcast_to(np.asarray(u_si, float), np.shape(rho_si)))
     a1 = 1.5 * K_B / (MU * M_P)
     if np.any(u < a1 * T_MIN + A_RAD * T_MIN**4 / rho) or np.any(u > a1 * T_MAX + A_RAD * T_MAX**4 / rho):
         raise ValueError("u outside the EOS bracket [1, 1e13] K")
-    out = np.empty(rho.shape)
-    for k, (r, uu) in enumerate(zip(rho.ravel().tolist(), u.ravel().tolist())):
-        t = _temperature_one(r, uu, a1)
-        if t is None:
-            raise RuntimeError("gas + radiation EOS: temperature did not converge")
-        out.flat[k] = t
-    return out
+    t, ok = native.gasrad_temperature(rho, u, a1, A_RAD)
+    if not np.all(ok):
+        raise RuntimeError("gas + radiation EOS: temperature did not converge")
+    return t.reshape(np.shape(rho_si))
 
 
 def gamma1(beta, gamma: float = 5.0 / 3.0):

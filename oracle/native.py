@@ -60,6 +60,7 @@ def lib():
         L.or_wake_targets.argtypes = [_I, _i64, _I, _I, _I, _i64, _I]
         L.or_mark_neighbours.argtypes = [_i64, _I, _I, _I, _U8]
         L.or_kernel_f.restype = _dbl
+        L.or_gasrad_temperature.argtypes = [_i64, _D, _D, _dbl, _dbl, _D, _U8]
         L.or_kernel_f.argtypes = [_dbl, _int]
         L.or_kernel_df.restype = _dbl
         L.or_kernel_df.argtypes = [_dbl, _int]
@@ -261,3 +262,12 @@ def with_neighbours(nb: Neighbours, rows, n):
     rows = np.ascontiguousarray(rows, np.int64)
     lib().or_mark_neighbours(len(rows), rows, nb.offset, nb.index, mark)
     return np.flatnonzero(mark)
+
+
+def gasrad_temperature(rho_si, u_si, a1, a_rad):
+    """sim/fastphys.py:45-71 element by element: (T [K], converged flags)."""
+    rho, u = _f64(rho_si), _f64(u_si)
+    out = np.empty(len(rho))
+    ok = np.empty(len(rho), np.uint8)
+    lib().or_gasrad_temperature(len(rho), rho, u, a1, a_rad, out, ok)
+    return out, ok.astype(bool)

@@ -739,3 +739,39 @@ void or_mark_neighbours(int64_t nrows, const int64_t* rows, const int64_t* offse
     for (int64_t k = offset[i]; k < offset[i + 1]; ++k) mark[index[k]] = 1;
   }
 }
+
+/* sim/fastphys.py:45-71 (_gasrad_t_kernel): T [K] of gas + radiation from rho [kg/m^3] and
+ * u [J/kg] by Newton on log T inside the bracket [1, 1e13] K narrowed every iteration, tolerance
+ * 1e-12, at most 200 iterations; ok[i] = 0 where it does not converge.  t**4 is evaluated by
+ * squaring, as Numba lowers it. */
+void or_gasrad_temperature(int64_t n, const double* rho, const double* u, double a1, double a_rad,
+                           double* out, uint8_t* ok) {
+  const double lt_min = log(1.0), lt_max = log(1.0e13);
+  const double t_min = exp(lt_min), t_max = exp(lt_max);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < n; ++i) {
+    const double r = rho[i], uu = u[i];
+    double lo = lt_min, hi = lt_max;
+    double t0 = fmin(uu / a1, pow(uu * r / a_rad, 0.25));
+    double lt = log(fmin(fmax(t0, t_min), t_max));
+    ok[i] = 0;
+    for (int it = 0; it < 200; ++it) {
+      double t = exp(lt);
+      double t2 = t * t;
+      double t4 = t2 * t2;
+      double f = a1 * t + a_rad * t4 / r - uu;
+      double dfdl = a1 * t + 4.0 * a_rad * t4 / r;
+      if (f < 0) lo = lt;
+      if (f > 0) hi = lt;
+      double nw = lt - f / dfdl;
+      if (nw <= lo || nw >= hi || !isfinite(nw)) nw = 0.5 * (lo + hi);
+      double step = fabs(nw - lt);
+      lt = nw;
+      if (step < 1e-12) {
+        ok[i] = 1;
+        break;
+      }
+    }
+    out[i] = exp(lt);
+  }
+}

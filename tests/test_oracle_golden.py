@@ -205,10 +205,11 @@ def test_equations_of_state_match_reference():
     g = golden("eos.npz")
     gu = HydroConfig().gas_units
     p, cs, t, beta = oeos.gasrad_state(g["rho"], g["u"], gu.density_kg_m3)
-    check("gasrad T", g["gasrad_t"], t, rtol=1e-13)
-    check("gasrad P", g["gasrad_p"], p, rtol=1e-13)
-    check("gasrad c_s", g["gasrad_cs"], cs, rtol=1e-13)
-    check("gasrad beta", g["gasrad_beta"], beta, rtol=1e-12, atol=1e-300)
+    # bit for bit: the C iteration calls the same C-library exp, log and pow as the reference
+    check("gasrad T", g["gasrad_t"], t)
+    check("gasrad P", g["gasrad_p"], p)
+    check("gasrad c_s", g["gasrad_cs"], cs)
+    check("gasrad beta", g["gasrad_beta"], beta)
     for eos in ("ideal", "radiation"):
         pe, ce = oeos.eos_state(HydroConfig(eos=eos), g["rho"], g["u"])
         check(f"{eos} P", g[f"{eos}_p"], pe, rtol=1e-15)
