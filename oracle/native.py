@@ -49,7 +49,11 @@ def lib():
         L.or_density.argtypes = [_i64, _D, _D, _D, _D, _I, _I, _D, _int, _dbl, _dbl, _dbl, _dbl,
                                  _i64, _I, _D, _D, _D, _I, _I]  # fmt: skip
         L.or_forces.argtypes = [_D, _D, _D, _D, _D, _D, _D, _D, _D, _D, _I, _I, _D, _int, _dbl,
-                                _int, _int, _dbl, _dbl, _int, _i64, _I, _D, _D, _D, _D, _D]  # fmt: skip
+                                _int, _int, _dbl, _dbl, _int, _int, _int, _dbl, _dbl, _int, _D,
+                                _i64, _I, _D, _D, _D, _D, _D]  # fmt: skip
+        L.or_gradients.argtypes = [_D, _D, _D, _D, _D, _I, _I, _D, _int, _dbl, _i64, _I, _D, _D,
+                                   _D]  # fmt: skip
+        L.or_velocity_gradients.argtypes = [_D, _D, _D, _D, _I, _I, _D, _int, _dbl, _i64, _I, _D]
         L.or_disc_forces.argtypes = [_D, _D, _D, _D, _D, _D, _D, _dbl, _I, _I, _D, _int, _dbl,
                                      _i64, _I, _D, _D]  # fmt: skip
         L.or_glf_many.argtypes = [_i64, _D, _D, _D, _D, _D, _I]
@@ -166,9 +170,11 @@ def density(pos, mass, h_start, nb: Neighbours, h_search, kid, cnorm, eta, tol=1
 
 
 def forces(pos, vel, mass, h, rho, omega, pressure, nb: Neighbours, kid, cnorm, u=None,
-           c_s=None, alpha=None, beta=2.0, alpha_u=1.0, cond_signal=0, rows=None):  # fmt: skip
-    """sim/sph.py:655-690 forces_numba (no reconstruction): (acc, dudt, vsig, dudt_visc,
-    dudt_cond) in rows order."""
+           c_s=None, alpha=None, beta=2.0, alpha_u=1.0, cond_signal=0, rows=None, grad_v=None,
+           closeness=True, eta_crit=1.0 / 1.2, eta_fold=0.2, gate=2):  # fmt: skip
+    """sim/sph.py:655-690 forces_numba: (acc, dudt, vsig, dudt_visc, dudt_cond) in rows order;
+    velocity reconstruction (with the ShockCapturing fields closeness, eta_crit, eta_fold,
+    recon_gate) when ``grad_v`` (N, 3, 3) is given."""
     pos = _f64(pos)
     n = len(pos)
     rows = _rows(rows, n)
@@ -177,15 +183,44 @@ def forces(pos, vel, mass, h, rho, omega, pressure, nb: Neighbours, kid, cnorm, 
     use_cond = use_visc and u is not None
     z = np.zeros(n)
     arr = lambda a: z if a is None else _f64(a, (n,))  # noqa: E731
+    use_recon = use_visc and grad_v is not None
+    gv = _f64(grad_v, (n, 3, 3)).reshape(-1) if use_recon else np.zeros(9)
     acc = np.empty((m, 3))
     dudt, vsig, vh, ch = np.empty(m), np.empty(m), np.empty(m), np.empty(m)
     lib().or_forces(
         pos.reshape(-1), _f64(vel).reshape(-1), _f64(mass, (n,)), _f64(h), _f64(rho),
         _f64(omega), _f64(pressure), arr(u), arr(c_s), arr(alpha), nb.offset, nb.index,
         _box3(nb.box), int(kid), float(cnorm), int(use_visc), int(use_cond), float(beta),
-        float(alpha_u), int(cond_signal), m, rows, acc.reshape(-1), dudt, vsig, vh, ch,
+        float(alpha_u), int(cond_signal), int(use_recon), int(bool(closeness)), float(eta_crit),
+        float(eta_fold), int(gate), gv, m, rows, acc.reshape(-1), dudt, vsig, vh, ch,
     )  # fmt: skip
     return acc, dudt, vsig, vh, ch
+
+
+def gradients(pos, vel, acc, mass, h, nb: Neighbours, kid, cnorm, rows=None):
+    """sim/sph.py:883-902 gradients_numba: (div v, |curl v|, d(div v)/dt) in rows order."""
+    pos = _f64(pos)
+    n = len(pos)
+    rows = _rows(rows, n)
+    m = len(rows)
+    div, curl, ddiv = np.empty(m), np.empty(m), np.empty(m)
+    lib().or_gradients(pos.reshape(-1), _f64(vel).reshape(-1), _f64(acc).reshape(-1),
+                       _f64(mass, (n,)), _f64(h, (n,)), nb.offset, nb.index, _box3(nb.box),
+                       int(kid), float(cnorm), m, rows, div, curl, ddiv)  # fmt: skip
+    return div, curl, ddiv
+
+
+def velocity_gradients(pos, vel, mass, h, nb: Neighbours, kid, cnorm, rows=None, out=None):
+    """sim/sph.py:827-846 velocity_gradients_numba: fills out (N, 3, 3; zeros if not given) at
+    rows and returns it."""
+    pos = _f64(pos)
+    n = len(pos)
+    rows = _rows(rows, n)
+    out = np.zeros((n, 3, 3)) if out is None else out
+    lib().or_velocity_gradients(pos.reshape(-1), _f64(vel).reshape(-1), _f64(mass, (n,)),
+                                _f64(h, (n,)), nb.offset, nb.index, _box3(nb.box), int(kid),
+                                float(cnorm), len(rows), rows, out.reshape(-1))  # fmt: skip
+    return out
 
 
 def disc_forces(pos, vel, mass, h, rho, omega, c_s, alpha_av, nb: Neighbours, kid, cnorm,

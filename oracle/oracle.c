@@ -461,20 +461,127 @@ void or_density(int64_t n, const double* pos, const double* mass, const double* 
 }
 
 /* ------------------------------------------------------------------ forces
- * sim/sph.py:519-652 (_dwdr, _forces_kernel) without velocity reconstruction: pressure force,
- * P dV work, signal-velocity viscosity with shock heating, optional conductivity. */
+ * sim/sph.py:519-652 (_dwdr, _forces_kernel): pressure force, P dV work, signal-velocity
+ * viscosity with shock heating (optionally on the reconstructed velocity jump), optional
+ * conductivity. */
 static inline double dwdr(double r, double h, int kid, double cnorm) {
   double h2 = h * h;
   return cnorm / (h2 * h2) * kernel_df(r / h, kid);
+}
+
+/* ------------------------------------------------------------------ gradients
+ * sim/sph.py:693-902: corrected gradients dv^k/dx^j = (G R^-1)_kj with
+ * R_lj = sum_b m_b (x_b - x_a)^l dW_ab(h_a)/dx_a^j, G_kj = sum_b m_b (v_b - v_a)^k dW/dx_a^j;
+ * fewer than 4 list entries, tr R <= 0 or |det R| < 1e-6 (tr R / 3)^3: G / (tr R / 3) instead
+ * (0 without neighbours). R^-1 as the adjugate over the determinant. */
+#define SINGULAR_TOL 1e-6
+
+static double det3(const double m[9]) {
+  return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+         m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+
+/* out = g R^-1 (or the fallback) for each of ng gradient sums g (3x3, row-major) */
+static void corrected(const double rm[9], int64_t cnt, int ng, double* const* g, double* const* out) {
+  double scale = (rm[0] + rm[4] + rm[8]) / 3.0;
+  double det = det3(rm);
+  int singular = cnt < 4 || !(scale > 0.0) || !(fabs(det) >= SINGULAR_TOL * scale * scale * scale);
+  if (singular) {
+    double inv_s = scale > 0.0 ? 1.0 / scale : 0.0;
+    for (int k = 0; k < ng; ++k)
+      for (int e = 0; e < 9; ++e) out[k][e] = g[k][e] * inv_s;
+    return;
+  }
+  double ri[9];
+  ri[0] = (rm[4] * rm[8] - rm[5] * rm[7]) / det;
+  ri[1] = (rm[2] * rm[7] - rm[1] * rm[8]) / det;
+  ri[2] = (rm[1] * rm[5] - rm[2] * rm[4]) / det;
+  ri[3] = (rm[5] * rm[6] - rm[3] * rm[8]) / det;
+  ri[4] = (rm[0] * rm[8] - rm[2] * rm[6]) / det;
+  ri[5] = (rm[2] * rm[3] - rm[0] * rm[5]) / det;
+  ri[6] = (rm[3] * rm[7] - rm[4] * rm[6]) / det;
+  ri[7] = (rm[1] * rm[6] - rm[0] * rm[7]) / det;
+  ri[8] = (rm[0] * rm[4] - rm[1] * rm[3]) / det;
+  for (int k = 0; k < ng; ++k)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        out[k][3 * i + j] = g[k][3 * i + 0] * ri[0 + j] + g[k][3 * i + 1] * ri[3 + j] +
+                            g[k][3 * i + 2] * ri[6 + j];
+}
+
+/* sums of one row: R, G (velocities) and, if acc is given, the acceleration gradient sum */
+static int64_t gradient_sums(int64_t a, const double* pos, const double* vel, const double* acc,
+                             const double* mass, const double* h, const int64_t* offset,
+                             const int64_t* index, const double* box, int kid, double cnorm,
+                             double rm[9], double gv[9], double ga[9]) {
+  for (int e = 0; e < 9; ++e) rm[e] = gv[e] = ga[e] = 0.0;
+  int64_t cnt = 0;
+  for (int64_t k = offset[a]; k < offset[a + 1]; ++k) {
+    int64_t b = index[k];
+    if (b == a) continue;
+    cnt += 1;
+    double dx[3];
+    for (int c = 0; c < 3; ++c) dx[c] = min_image(pos[3 * a + c] - pos[3 * b + c], box[c]);
+    double r = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+    double g = dwdr(r, h[a], kid, cnorm) / r;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        double gj = mass[b] * g * dx[j];
+        rm[3 * i + j] -= dx[i] * gj;
+        gv[3 * i + j] += (vel[3 * b + i] - vel[3 * a + i]) * gj;
+        if (acc) ga[3 * i + j] += (acc[3 * b + i] - acc[3 * a + i]) * gj;
+      }
+  }
+  return cnt;
+}
+
+/* sim/sph.py:850-902 (_gradients_kernel): div v, |curl v| and d(div v)/dt in rows order */
+void or_gradients(const double* pos, const double* vel, const double* acc, const double* mass,
+                  const double* h, const int64_t* offset, const int64_t* index, const double* box,
+                  int kid, double cnorm, int64_t nrows, const int64_t* rows, double* div,
+                  double* curl, double* ddiv) {
+#pragma omp parallel for schedule(dynamic, 32)
+  for (int64_t q = 0; q < nrows; ++q) {
+    int64_t a = rows[q];
+    double rm[9], gv[9], ga[9], dv[9], da[9];
+    int64_t cnt = gradient_sums(a, pos, vel, acc, mass, h, offset, index, box, kid, cnorm, rm, gv, ga);
+    double* g[2] = {gv, ga};
+    double* o[2] = {dv, da};
+    corrected(rm, cnt, 2, g, o);
+    div[q] = dv[0] + dv[4] + dv[8];
+    double c0 = dv[7] - dv[5], c1 = dv[2] - dv[6], c2 = dv[3] - dv[1];
+    curl[q] = sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+    double sdd = 0.0;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) sdd += dv[3 * i + j] * dv[3 * j + i];
+    ddiv[q] = da[0] + da[4] + da[8] - sdd;
+  }
+}
+
+/* sim/sph.py:797-846 (_velocity_gradient_kernel): out[a] = dv/dx (3x3) for a in rows */
+void or_velocity_gradients(const double* pos, const double* vel, const double* mass,
+                           const double* h, const int64_t* offset, const int64_t* index,
+                           const double* box, int kid, double cnorm, int64_t nrows,
+                           const int64_t* rows, double* out) {
+#pragma omp parallel for schedule(dynamic, 32)
+  for (int64_t q = 0; q < nrows; ++q) {
+    int64_t a = rows[q];
+    double rm[9], gv[9], ga[9];
+    int64_t cnt = gradient_sums(a, pos, vel, NULL, mass, h, offset, index, box, kid, cnorm, rm, gv, ga);
+    double* g[1] = {gv};
+    double* o[1] = {out + 9 * a};
+    corrected(rm, cnt, 1, g, o);
+  }
 }
 
 void or_forces(const double* pos, const double* vel, const double* mass, const double* h,
                const double* rho, const double* omega, const double* pressure, const double* u,
                const double* c_s, const double* alpha, const int64_t* offset,
                const int64_t* index, const double* box, int kid, double cnorm, int use_visc,
-               int use_cond, double beta, double alpha_u, int cond_signal, int64_t nrows,
-               const int64_t* rows, double* acc, double* dudt, double* vsig_max, double* vheat,
-               double* cheat) {
+               int use_cond, double beta, double alpha_u, int cond_signal, int use_recon,
+               int closeness, double eta_crit, double eta_fold, int gate, const double* gvel,
+               int64_t nrows, const int64_t* rows, double* acc, double* dudt, double* vsig_max,
+               double* vheat, double* cheat) {
 #pragma omp parallel for schedule(dynamic, 32)
   for (int64_t q = 0; q < nrows; ++q) {
     int64_t a = rows[q];
@@ -495,7 +602,51 @@ void or_forces(const double* pos, const double* vel, const double* mass, const d
       double vdotr = (vel[3 * a + 0] - vel[3 * b + 0]) * rx + (vel[3 * a + 1] - vel[3 * b + 1]) * ry +
                      (vel[3 * a + 2] - vel[3 * b + 2]) * rz;
       double num_a = pressure[a], num_b = pressure[b];
-      if (use_visc) {
+      if (use_visc && use_recon) {
+        /* physics/viscosity.py:116-158: limiter ratio, van Leer limiter, closeness factor and
+         * the jump reconstructed to the pair midpoint (projections G x, x = x_a - x_b) */
+        const double* G = gvel + 9 * a;
+        const double* H = gvel + 9 * b;
+        double ga0 = G[0] * dx0 + G[1] * dx1 + G[2] * dx2;
+        double ga1 = G[3] * dx0 + G[4] * dx1 + G[5] * dx2;
+        double ga2 = G[6] * dx0 + G[7] * dx1 + G[8] * dx2;
+        double gb0 = H[0] * dx0 + H[1] * dx1 + H[2] * dx2;
+        double gb1 = H[3] * dx0 + H[4] * dx1 + H[5] * dx2;
+        double gb2 = H[6] * dx0 + H[7] * dx1 + H[8] * dx2;
+        double pa = dx0 * ga0 + dx1 * ga1 + dx2 * ga2;
+        double pb = dx0 * gb0 + dx1 * gb1 + dx2 * gb2;
+        double phi = 0.0;
+        if (pb != 0.0) {
+          double ratio = pa / pb;
+          if (ratio > 0.0) phi = fmin(1.0, 4.0 * ratio / ((1.0 + ratio) * (1.0 + ratio)));
+        }
+        if (closeness) {
+          double eta_ab = fmin(r / h[a], r / h[b]);
+          if (eta_ab < eta_crit) {
+            double t = (eta_ab - eta_crit) / eta_fold;
+            phi *= exp(-t * t);
+          }
+        }
+        double vdr = ((vel[3 * a + 0] - 0.5 * phi * ga0) - (vel[3 * b + 0] + 0.5 * phi * gb0)) * rx +
+                     ((vel[3 * a + 1] - 0.5 * phi * ga1) - (vel[3 * b + 1] + 0.5 * phi * gb1)) * ry +
+                     ((vel[3 * a + 2] - 0.5 * phi * ga2) - (vel[3 * b + 2] + 0.5 * phi * gb2)) * rz;
+        int on = vdr < 0.0 && vdotr < 0.0;
+        if (gate == 1)
+          on = vdr < 0.0;
+        else if (gate == 2 && vdotr > vdr)
+          vdr = vdotr;
+        double vsig_a = alpha[a] * c_s[a] + beta * fabs(vdr);
+        double vsig_b = alpha[b] * c_s[b] + beta * fabs(vdr);
+        double vsig_cfl = alpha[a] * c_s[a] + beta * fabs(vdotr);
+        if (vsig_cfl > vmax) vmax = vsig_cfl;
+        if (on) {
+          num_a += -0.5 * rho[a] * vsig_a * vdr;
+          num_b += -0.5 * rho[b] * vsig_b * vdr;
+          double dh = mass[b] * vsig_a * 0.5 * vdr * vdotr * fa * inv_or_a;
+          heat -= dh;
+          visc_heat -= dh;
+        }
+      } else if (use_visc) {
         double vsig_a = alpha[a] * c_s[a] + beta * fabs(vdotr);
         double vsig_b = alpha[b] * c_s[b] + beta * fabs(vdotr);
         if (vsig_a > vmax) vmax = vsig_a;

@@ -7,8 +7,9 @@ Restates the reference's step logic on top of the C kernels:
     _choose_levels, _land, _wake, _cut_steps, _cut_to, _open, initialise, advance, run, ledger,
     diagnostics, snapshot) and sim/timesteps.py:21-59 (ticks, level_for_dt, allowed_level).
 Only the options of the CUDA path are restated: GN hole, ideal gas (or, without cooling, the
-radiation limit and gas + radiation), constant alpha (no switch, no reconstruction), optional
-conductivity and disc viscosity, beta or bremsstrahlung cooling, no removal radii and no RESPA.  The heat-budget bookkeeping arrays are not kept.
+radiation limit and gas + radiation), constant alpha or the Cullen-Dehnen switch, optional
+velocity reconstruction, conductivity and disc viscosity, beta or bremsstrahlung cooling, no
+removal radii and no RESPA.  The heat-budget bookkeeping arrays are not kept.
 """
 
 from __future__ import annotations
@@ -107,20 +108,45 @@ class GasState:
     nu: np.ndarray = None
 
 
-def _shared_hydro(st: GasState, cc, v, reuse=True) -> GasState:
+def _switch_update(hc, alpha, h, cs, div, curl, ddiv, dt_alpha):
+    """physics/viscosity.py:83-113 (balsara_xi, alpha_local, decay_time, alpha_update)."""
+    d2, c2 = div**2, curl**2
+    with np.errstate(invalid="ignore", divide="ignore"):
+        xi = np.where(d2 + c2 > 0, d2 / (d2 + c2), 0.0)
+    a_loc = np.minimum(10.0 * h * h * (xi * np.maximum(-ddiv, 0.0)) / (cs * cs), 1.0)
+    tau = h / (0.1 * cs)
+    decayed = (alpha + a_loc * dt_alpha / tau) / (1.0 + dt_alpha / tau)
+    return np.where(a_loc > alpha, a_loc, decayed)
+
+
+def _shock_args(hc):
+    """The reconstruction settings of HydroConfig.shock() (sim/hydro.py:92-98)."""
+    return dict(closeness=hc.recon_closeness, eta_crit=1.0 / hc.eta, eta_fold=0.2,
+                gate=hc.recon_gate)  # fmt: skip
+
+
+def _shared_hydro(st: GasState, cc, v, reuse=True, dt_alpha=0.0, a_prev=None) -> GasState:
     """sim/coupled.py:145-195 for the supported options."""
     hc = cc.hydro
     d = compute_density(st.x, st.mass, st.h, kernel_name=hc.kernel, eta=hc.eta, h_max=hc.h_max,
                         cache=st.neighbour_cache, skin=hc.skin, reuse=reuse)  # fmt: skip
     p_gas, cs = _eos(hc, d.rho, st.u)
     nb = native.tighten(d.neighbours, st.x, d.h)
-    alpha = np.full(len(st.x), hc.alpha_const) if hc.viscosity else st.alpha
     kid, cn = _kid(hc)
+    alpha = st.alpha
+    if hc.viscosity and hc.switch and dt_alpha > 0:
+        a0 = np.zeros_like(st.x) if a_prev is None else a_prev
+        div, curl, ddiv = native.gradients(st.x, v, a0, st.mass, d.h, nb, kid, cn)
+        alpha = _switch_update(hc, alpha, d.h, cs, div, curl, ddiv, dt_alpha)
+    elif hc.viscosity and not hc.switch:
+        alpha = np.full(len(st.x), hc.alpha_const)
+    recon = hc.reconstruction and hc.viscosity
+    grad_v = native.velocity_gradients(st.x, v, st.mass, d.h, nb, kid, cn) if recon else None
     acc, dudt, vsig, vh, _ = native.forces(
         st.x, v, st.mass, d.h, d.rho, d.omega, p_gas, nb, kid, cn,
         u=st.u if hc.conductivity else None, c_s=cs if hc.viscosity else None,
         alpha=alpha if hc.viscosity else None, beta=hc.beta, alpha_u=hc.alpha_u,
-        cond_signal=hc.conductivity_signal,
+        cond_signal=hc.conductivity_signal, grad_v=grad_v, **_shock_args(hc),
     )  # fmt: skip
     nu = None
     if hc.disc_alpha_av > 0:
@@ -173,7 +199,7 @@ def coupled_step(st: GasState, cc, dt: float, reuse=True) -> GasState:
         u_half = u_cool
     p_pred = p_flow + 0.5 * dt * st.a_hydro
     pred = replace(st, t=st.t + dt, x=x1, p=p_flow, u=u_half + 0.5 * dt * st.dudt)
-    new = _shared_hydro(pred, cc, native.gn_v_from_p(x1, p_pred), reuse)
+    new = _shared_hydro(pred, cc, native.gn_v_from_p(x1, p_pred), reuse, dt, st.a_hydro)
     return replace(new, p=p_flow + 0.5 * dt * new.a_hydro, u=u_half + 0.5 * dt * new.dudt,
                    e_radiated=e_rad)  # fmt: skip
 
@@ -274,7 +300,7 @@ def _density_touched(st: BlockState, hc, rows, reuse=True):
     raise RuntimeError("neighbour set of the active particles did not settle")
 
 
-def _hydro_rows(st: BlockState, bc, rows, v, u, reuse=True):
+def _hydro_rows(st: BlockState, bc, rows, v, u, reuse=True, dt_alpha=None, a_prev=None):
     """sim/blocks.py:242-315 for the supported options."""
     hc = bc.coupled.hydro
     if np.any(u <= 0):
@@ -283,14 +309,23 @@ def _hydro_rows(st: BlockState, bc, rows, v, u, reuse=True):
     touched = native.with_neighbours(nb, rows, len(st.x))
     p_gas, cs = np.full(len(st.x), np.nan), np.full(len(st.x), np.nan)
     p_gas[touched], cs[touched] = _eos(hc, st.rho[touched], u[touched])
-    if hc.viscosity:
-        st.alpha[rows] = hc.alpha_const
     kid, cn = _kid(hc)
+    if hc.viscosity and hc.switch and dt_alpha is not None and np.any(dt_alpha > 0):
+        div, curl, ddiv = native.gradients(st.x, v, a_prev, st.mass, st.h, nb, kid, cn, rows=rows)
+        st.alpha[rows] = _switch_update(hc, st.alpha[rows], st.h[rows], cs[rows], div, curl, ddiv,
+                                        dt_alpha)  # fmt: skip
+    elif hc.viscosity and not hc.switch:
+        st.alpha[rows] = hc.alpha_const
+    grad_v = None
+    if hc.reconstruction and hc.viscosity:
+        # the touched particles' gradients from the untightened cached lists (sim/blocks.py:271-278)
+        grad_v = native.velocity_gradients(st.x, v, st.mass, st.h, st.neighbour_cache.neighbours,
+                                           kid, cn, rows=touched)  # fmt: skip
     acc, dudt, vsig, _, _ = native.forces(
         st.x, v, st.mass, st.h, st.rho, st.omega, p_gas, nb, kid, cn,
         u=u if hc.conductivity else None, c_s=cs if hc.viscosity else None,
         alpha=st.alpha if hc.viscosity else None, beta=hc.beta, alpha_u=hc.alpha_u,
-        cond_signal=hc.conductivity_signal, rows=rows,
+        cond_signal=hc.conductivity_signal, rows=rows, grad_v=grad_v, **_shock_args(hc),
     )  # fmt: skip
     if hc.disc_alpha_av > 0:
         a_d, u_d = native.disc_forces(st.x, v, st.mass, st.h, st.rho, st.omega, cs,
@@ -448,8 +483,9 @@ def blocks_advance(st: BlockState, bc, reuse=True) -> np.ndarray:
     st.n = n_next
     st.x = x
     st.u = u_pred
+    a_prev = st.a_hydro.copy()
     v_eval = native.gn_v_from_p(x, p_pred)
-    nb = _hydro_rows(st, bc, rows, v_eval, u_pred, reuse)
+    nb = _hydro_rows(st, bc, rows, v_eval, u_pred, reuse, 2.0 * half_len[rows], a_prev)
     t2 = time.perf_counter()
     p_pred[rows] = p_flow[rows] + half_len[rows, None] * st.a_hydro[rows]
     st.u[rows] = st.u_half[rows] + half_len[rows] * st.dudt[rows]

@@ -287,6 +287,121 @@ def gasrad_blocks_fixture(blocks, coupled, ics, hydro_cfg):
     _save("gasrad_blocks.npz", **out)
 
 
+def _shock_blob(rng):
+    """The forces blob plus three isolated particles (no neighbours within h_max) and a planar
+    patch of six (a singular correction matrix): both fallbacks of the corrected gradients."""
+    pos, _ = _blob(rng)
+    iso = np.array([[6.0, 6.0, 6.0], [-6.0, 6.0, 6.0], [6.0, -6.0, 6.0]])
+    gx, gy = np.meshgrid([0.0, 0.12, 0.24], [0.0, 0.12])
+    plane = np.stack([gx.ravel() - 6.0, gy.ravel() - 6.0, np.full(6, -6.0)], axis=1)
+    pos = np.concatenate([pos, iso, plane])
+    return pos, np.full(len(pos), 1.0 / len(pos))
+
+
+def shock_fixture(sph, nbmod):
+    """Corrected velocity / acceleration gradients (sim/sph.py:797-902) and the force pass with
+    velocity reconstruction (sim/sph.py:568-609) for the three gates, with and without the
+    closeness factor, on the blob with a linear velocity field plus noise."""
+    rng = np.random.default_rng(SEED + 7)
+    pos, mass = _shock_blob(rng)
+    n = len(pos)
+    g0 = rng.normal(0.0, 0.4, (3, 3))
+    vel = pos @ g0.T + rng.normal(0.0, 0.05, pos.shape)
+    acc_prev = rng.normal(0.0, 0.2, pos.shape) + pos @ rng.normal(0.0, 0.3, (3, 3)).T
+    u = rng.uniform(0.5, 1.5, n)
+    d = sph.compute_density(pos, mass, np.full(n, 0.05), h_max=0.5)
+    p = (5.0 / 3.0 - 1.0) * d.rho * u
+    cs = np.sqrt(10.0 / 9.0 * u)
+    alpha = rng.uniform(0.0, 1.0, n)
+    nb = nbmod.tighten(d.neighbours, pos, d.h)
+    rows = np.sort(rng.choice(n, 700, replace=False))
+    out = dict(pos=pos, vel=vel, acc_prev=acc_prev, mass=mass, h=d.h, rho=d.rho, omega=d.omega,
+               pressure=p, u=u, c_s=cs, alpha=alpha, offset=nb.offset,
+               index=nb.index.astype(np.int32), rows=rows)  # fmt: skip
+    g = sph.gradients_numba(pos, vel, acc_prev, mass, d.h, nb)
+    out.update(div_v=g.div_v, curl_v=g.curl_v, ddivv_dt=g.ddivv_dt)
+    gr = sph.gradients_numba(pos, vel, acc_prev, mass, d.h, nb, kernel_name="cubic", rows=rows)
+    out.update(cubic_rows_div_v=gr.div_v, cubic_rows_curl_v=gr.curl_v, cubic_rows_ddivv_dt=gr.ddivv_dt)
+    gv = sph.velocity_gradients_numba(pos, vel, mass, d.h, nb)
+    out["grad_v"] = gv
+    # untightened lists (search radius 1.4 h; rebuilt by the tests with the exact list build)
+    full = nbmod.find_neighbours(pos, 1.4 * d.h)
+    out["full_rows_grad_v"] = sph.velocity_gradients_numba(pos, vel, mass, d.h, full, rows=rows)
+    for gate in (0, 1, 2):
+        for close in (True, False):
+            shock = sph.ShockCapturing(beta=2.0, alpha_u=0.5, conductivity_signal=1,
+                                       reconstruction=True, closeness=close,
+                                       eta_crit=1.0 / 1.2, recon_gate=gate)  # fmt: skip
+            f = sph.forces_numba(pos, vel, mass, d.h, d.rho, d.omega, p, nb, u=u, c_s=cs,
+                                 alpha=alpha, shock=shock, grad_v=gv)  # fmt: skip
+            key = f"recon_g{gate}_c{int(close)}"
+            out.update({f"{key}_acc": f.acc, f"{key}_dudt": f.dudt, f"{key}_vsig": f.vsig_max,
+                        f"{key}_visc": f.dudt_visc, f"{key}_cond": f.dudt_cond})  # fmt: skip
+    shock = sph.ShockCapturing(beta=2.0, alpha_u=0.5, conductivity_signal=0, reconstruction=True,
+                               eta_crit=1.0 / 1.2)  # fmt: skip
+    f = sph.forces_numba(pos, vel, mass, d.h, d.rho, d.omega, p, nb, kernel_name="cubic", u=u,
+                         c_s=cs, alpha=alpha, shock=shock, rows=rows, grad_v=gv)  # fmt: skip
+    out.update(recon_rows_cubic_acc=f.acc, recon_rows_cubic_dudt=f.dudt,
+               recon_rows_cubic_vsig=f.vsig_max)  # fmt: skip
+    _save("shock.npz", **out)
+
+
+def switch_coupled_fixture(coupled, ics, hydro_cfg):
+    """Shared steps of the 4,096-particle cloud with the reference's default shock capturing
+    (Cullen-Dehnen switch from alpha = 0, velocity reconstruction with the min-mod gate) and a
+    velocity noise that drives the switch; three steps of stable_dt."""
+    ic = ics.cloud(4096)
+    rng = np.random.default_rng(SEED + 8)
+    v = ic.v + rng.normal(0.0, 3e-4, ic.v.shape)
+    hc = hydro_cfg(kernel="cubic", eta=1.2, switch=True, reconstruction=True,
+                   conductivity_signal=1, alpha_u=0.05, h_max=200.0)  # fmt: skip
+    cc = coupled.CoupledConfig(hydro=hc)
+    st = coupled.initialise(ic.x, v, ic.u, ic.mass, ic.h, cc)
+    fields = ["x", "p", "u", "h", "rho", "alpha", "a_hydro", "dudt", "vsig_max"]
+    out = dict(x0=ic.x, v0=v, u0=ic.u, mass=ic.mass, h0=ic.h)
+    out.update(_state_arrays("init", st, fields))
+    dts = []
+    for k in range(3):
+        dt = coupled.stable_dt(st, cc)
+        dts.append(dt)
+        st = coupled.step(st, cc, dt)
+        out.update(_state_arrays(f"step{k + 1}", st, fields))
+        out[f"step{k + 1}_energy"] = coupled.ledger(st, cc)["energy"]
+    out["dts"] = np.array(dts)
+    out["builds"] = st.neighbour_cache.builds
+    out["reuses"] = st.neighbour_cache.reuses
+    _save("switch_coupled.npz", **out)
+
+
+def switch_blocks_fixture(blocks, coupled, ics, hydro_cfg):
+    """Block steps of the blocks_fixture cloud (level offsets 0-3, beta = 230) with the switch
+    and velocity reconstruction on; 16 system steps."""
+    ic = ics.cloud(2048, radius=20.0, total_mass=1e-3, t_kelvin=3e8, r_peri=60.0, r_apo=400.0,
+                   seed=7)  # fmt: skip
+    rng = np.random.default_rng(SEED)
+    v = ic.v + rng.normal(0.0, 0.002, ic.v.shape)
+    hc = hydro_cfg(kernel="cubic", eta=1.2, switch=True, reconstruction=True,
+                   conductivity_signal=1, alpha_u=0.05, h_max=200.0)  # fmt: skip
+    cc = coupled.CoupledConfig(hydro=hc, cooling_beta=230.0)
+    bc = blocks.BlockConfig(coupled=cc, dt_max=64.0)
+    offset = rng.integers(0, 4, len(ic.x))
+    st = blocks.initialise(ic.x, v, ic.u, ic.mass, ic.h, bc, t_stop=1e6, level_offset=offset)
+    fields = ["x", "p", "u", "h", "rho", "alpha", "a_hydro", "dudt", "level", "n_beg", "n_end",
+              "vsig_max"]
+    out = dict(x0=ic.x, v0=v, u0=ic.u, mass=ic.mass, h0=ic.h, level_offset=offset)
+    out.update(_state_arrays("init", st, fields))
+    actives = [len(blocks.advance(st, bc)) for _ in range(16)]
+    out.update(_state_arrays("final", st, fields))
+    led = blocks.ledger(st, bc)
+    out["final_energy"] = led["energy"]
+    out["final_e_radiated"] = led["e_radiated"]
+    out["final_n"] = st.n
+    out["active_counts"] = np.array(actives)
+    out["builds"] = st.neighbour_cache.builds
+    out["reuses"] = st.neighbour_cache.reuses
+    _save("switch_blocks.npz", **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="root of the reference checkout")
@@ -314,6 +429,9 @@ def main():
         "blocks": lambda: blocks_fixture(blocks, coupled, ics, HydroConfig),
         "eos": lambda: eos_fixture(hydro_mod, units_mod),
         "gasrad_blocks": lambda: gasrad_blocks_fixture(blocks, coupled, ics, HydroConfig),
+        "shock": lambda: shock_fixture(sph, nbmod),
+        "switch_coupled": lambda: switch_coupled_fixture(coupled, ics, HydroConfig),
+        "switch_blocks": lambda: switch_blocks_fixture(blocks, coupled, ics, HydroConfig),
     }
     for name, make in makers.items():
         if not args.only or name in args.only:

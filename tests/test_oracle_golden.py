@@ -255,3 +255,120 @@ def test_gasrad_block_steps_match_reference():
     check("final h", g["final_h"], st.h, rtol=1e-9)
     check("final energy", float(g["final_energy"]), steps.blocks_ledger(st, bc)["energy"],
           rtol=1e-12)  # fmt: skip
+
+
+def _scaled(name, expected, actual, tol):
+    scale = np.abs(expected).max()
+    check(name, expected / scale, actual / scale, atol=tol)
+
+
+def test_gradients_match_reference():
+    g = golden("shock.npz")
+    nb = _nb(g["offset"], g["index"])
+    args = (g["pos"], g["vel"], g["acc_prev"], g["mass"], g["h"], nb)
+    div, curl, ddiv = native.gradients(*args, 1, C_NORM[1])
+    _scaled("div v", g["div_v"], div, 1e-12)
+    _scaled("curl v", g["curl_v"], curl, 1e-12)
+    _scaled("d div v / dt", g["ddivv_dt"], ddiv, 1e-12)
+    div, curl, ddiv = native.gradients(*args, 0, C_NORM[0], rows=g["rows"])
+    _scaled("cubic rows div v", g["cubic_rows_div_v"], div, 1e-12)
+    _scaled("cubic rows curl v", g["cubic_rows_curl_v"], curl, 1e-12)
+    _scaled("cubic rows d div v / dt", g["cubic_rows_ddivv_dt"], ddiv, 1e-12)
+
+
+def test_velocity_gradients_match_reference():
+    g = golden("shock.npz")
+    nb = _nb(g["offset"], g["index"])
+    gv = native.velocity_gradients(g["pos"], g["vel"], g["mass"], g["h"], nb, 1, C_NORM[1])
+    _scaled("grad v (tight lists)", g["grad_v"], gv, 1e-12)
+    full = native.find_neighbours(g["pos"], 1.4 * g["h"])
+    gv = native.velocity_gradients(g["pos"], g["vel"], g["mass"], g["h"], full, 1, C_NORM[1],
+                                   rows=g["rows"])  # fmt: skip
+    _scaled("grad v (untightened lists, rows)", g["full_rows_grad_v"], gv, 1e-12)
+
+
+@pytest.mark.parametrize("gate", [0, 1, 2])
+@pytest.mark.parametrize("close", [True, False])
+def test_reconstructed_forces_match_reference(gate, close):
+    g = golden("shock.npz")
+    nb = _nb(g["offset"], g["index"])
+    args = (g["pos"], g["vel"], g["mass"], g["h"], g["rho"], g["omega"], g["pressure"], nb)
+    acc, dudt, vsig, vh, ch = native.forces(*args, 1, C_NORM[1], u=g["u"], c_s=g["c_s"],
+                                            alpha=g["alpha"], alpha_u=0.5, cond_signal=1,
+                                            grad_v=g["grad_v"], closeness=close, gate=gate)
+    key = f"recon_g{gate}_c{int(close)}"
+    check("acc", g[f"{key}_acc"], acc, rtol=1e-12, per_vector=True)
+    _scaled("dudt", g[f"{key}_dudt"], dudt, 1e-12)
+    check("vsig", g[f"{key}_vsig"], vsig, rtol=1e-14)
+    _scaled("visc heat", g[f"{key}_visc"], vh, 1e-12)
+    _scaled("cond heat", g[f"{key}_cond"], ch, 1e-12)
+
+
+def test_reconstructed_forces_rows_cubic_match_reference():
+    g = golden("shock.npz")
+    nb = _nb(g["offset"], g["index"])
+    args = (g["pos"], g["vel"], g["mass"], g["h"], g["rho"], g["omega"], g["pressure"], nb)
+    acc, dudt, vsig, _, _ = native.forces(*args, 0, C_NORM[0], u=g["u"], c_s=g["c_s"],
+                                          alpha=g["alpha"], alpha_u=0.5, cond_signal=0,
+                                          rows=g["rows"], grad_v=g["grad_v"])  # fmt: skip
+    check("acc", g["recon_rows_cubic_acc"], acc, rtol=1e-12, per_vector=True)
+    _scaled("dudt", g["recon_rows_cubic_dudt"], dudt, 1e-12)
+    check("vsig", g["recon_rows_cubic_vsig"], vsig, rtol=1e-14)
+
+
+def _switch_hc():
+    from blackhole_nebula_simulator_b200.config import HydroConfig
+
+    return HydroConfig(kernel="cubic", eta=1.2, switch=True, reconstruction=True,
+                       conductivity_signal=1, alpha_u=0.05, h_max=200.0)  # fmt: skip
+
+
+def test_switch_shared_steps_match_reference():
+    from blackhole_nebula_simulator_b200.config import CoupledConfig
+
+    g = golden("switch_coupled.npz")
+    cc = CoupledConfig(hydro=_switch_hc())
+    st = steps.coupled_initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], cc)
+    check("init alpha", g["init_alpha"], st.alpha)
+    check("init acc", g["init_a_hydro"], st.a_hydro, rtol=1e-9, per_vector=True)
+    for k in range(3):
+        dt = steps.coupled_stable_dt(st, cc)
+        check(f"dt {k}", g["dts"][k], dt, rtol=1e-12)
+        st = steps.coupled_step(st, cc, dt)
+        check(f"step {k + 1} alpha", g[f"step{k + 1}_alpha"], st.alpha, rtol=1e-9, atol=1e-12)
+        check(f"step {k + 1} x", g[f"step{k + 1}_x"], st.x, rtol=1e-14, per_vector=True)
+        check(f"step {k + 1} p", g[f"step{k + 1}_p"], st.p, rtol=1e-12, per_vector=True)
+        check(f"step {k + 1} u", g[f"step{k + 1}_u"], st.u, rtol=1e-10)
+        check(f"step {k + 1} h", g[f"step{k + 1}_h"], st.h, rtol=1e-10)
+        check(f"step {k + 1} acc", g[f"step{k + 1}_a_hydro"], st.a_hydro, rtol=1e-8,
+              per_vector=True)  # fmt: skip
+        check(f"step {k + 1} energy", g[f"step{k + 1}_energy"],
+              steps.coupled_ledger(st, cc)["energy"], rtol=1e-13)  # fmt: skip
+    check("cache builds", int(g["builds"]), st.neighbour_cache.builds)
+    check("cache reuses", int(g["reuses"]), st.neighbour_cache.reuses)
+
+
+def test_switch_block_steps_match_reference():
+    from blackhole_nebula_simulator_b200.config import BlockConfig, CoupledConfig
+
+    g = golden("switch_blocks.npz")
+    bc = BlockConfig(coupled=CoupledConfig(hydro=_switch_hc(), cooling_beta=230.0), dt_max=64.0)
+    st = steps.blocks_initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc, t_stop=1e6,
+                                 level_offset=g["level_offset"])  # fmt: skip
+    check("init levels", g["init_level"], st.level)
+    check("init acc", g["init_a_hydro"], st.a_hydro, rtol=1e-9, per_vector=True)
+    actives = [len(steps.blocks_advance(st, bc)) for _ in range(len(g["active_counts"]))]
+    check("active counts", g["active_counts"], np.array(actives))
+    check("final tick", int(g["final_n"]), st.n)
+    check("final levels", g["final_level"], st.level)
+    check("final n_end", g["final_n_end"], st.n_end)
+    check("final alpha", g["final_alpha"], st.alpha, rtol=1e-8, atol=1e-12)
+    check("final x", g["final_x"], st.x, rtol=1e-13, per_vector=True)
+    check("final p", g["final_p"], st.p, rtol=1e-11, per_vector=True)
+    check("final u", g["final_u"], st.u, rtol=1e-9)
+    check("final h", g["final_h"], st.h, rtol=1e-9)
+    check("final energy", float(g["final_energy"]), steps.blocks_ledger(st, bc)["energy"],
+          rtol=1e-12)  # fmt: skip
+    check("final e_radiated", float(g["final_e_radiated"]), st.e_radiated, rtol=1e-9)
+    check("cache builds", int(g["builds"]), st.neighbour_cache.builds)
+    check("cache reuses", int(g["reuses"]), st.neighbour_cache.reuses)
