@@ -48,7 +48,8 @@ class NbParams(_c.Structure):
         ("brems_tfac", _dbl), ("brems_b", _dbl), ("brems_kappa", _dbl), ("brems_t_floor", _dbl),
         ("dt_max", _dbl), ("limiter", _int), ("max_gap", _int), ("mlp", NbMlpParams),
         ("eos", _int), ("eos_rho_si", _dbl), ("eos_u_si", _dbl), ("eos_a1", _dbl),
-        ("eos_a_rad", _dbl),
+        ("eos_a_rad", _dbl), ("visc_switch", _int), ("recon", _int), ("recon_closeness", _int),
+        ("recon_gate", _int), ("recon_eta_crit", _dbl), ("recon_eta_fold", _dbl),
     ]  # fmt: skip
 
 
@@ -82,6 +83,13 @@ _SIGS = {
                           _dbl, _vp, _vp, _vp, _vp, _vp, _vp]),
     "nb_forces": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                          _i64, _vp, _int, _dbl, _dbl, _int, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "nb_forces_recon": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                               _vp, _vp, _i64, _vp, _int, _dbl, _dbl, _int, _int, _dbl, _dbl,
+                               _int, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "nb_gradients": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _int, _vp,
+                            _vp, _vp, _vp]),
+    "nb_velocity_gradients": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _int,
+                                     _vp, _vp]),
     "nb_disc_forces": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _dbl, _vp, _vp,
                               _i64, _vp, _int, _vp, _vp, _vp]),
     "nb_glf_step_many": (_int, [_vp, _i64, _vp, _vp, _vp, _dbl, _vp, _vp, _vp, _vp]),

@@ -142,10 +142,8 @@ def check_supported(cc: CoupledConfig) -> None:
     cooling_on = cc.cooling == "brems" or math.isfinite(cc.cooling_beta)
     if hc.eos != "ideal" and cooling_on:
         bad.append(f"cooling with eos={hc.eos!r} (the floor energy then depends on rho)")
-    if hc.viscosity and hc.switch:
-        bad.append("Cullen-Dehnen switch (switch=True)")
-    if hc.viscosity and hc.reconstruction:
-        bad.append("velocity reconstruction (reconstruction=True)")
+    if hc.recon_gate not in (GATE_BOTH, GATE_PUBLISHED, GATE_MINMOD):
+        raise ValueError(f"unknown reconstruction gate {hc.recon_gate!r}")
     if hc.ns_nu > 0 or hc.ns_alpha > 0:
         bad.append("Navier-Stokes viscosity (ns_nu / ns_alpha)")
     if cc.wrong_coupling:

@@ -48,6 +48,11 @@ def make_params(cc: CoupledConfig, dt_max: float = 4096.0, limiter: bool = True,
         p.cooling_beta = cc.cooling_beta
         p.u_floor = floor_energy(hc.gamma, cc.t_floor)
     p.dt_max, p.limiter, p.max_gap = dt_max, int(limiter), int(max_gap)
+    # shock capturing of HydroConfig.shock() (sim/hydro.py:92-98)
+    p.visc_switch = int(hc.viscosity and hc.switch)
+    p.recon = int(hc.viscosity and hc.reconstruction)
+    p.recon_closeness, p.recon_gate = int(bool(hc.recon_closeness)), int(hc.recon_gate)
+    p.recon_eta_crit, p.recon_eta_fold = 1.0 / hc.eta, 0.2
     for k, v in eos_fields(hc).items():
         setattr(p, k, v)
     return p

@@ -202,12 +202,15 @@ int nb_density(nb_ctx* ctx, int64_t n, const double* pos, const double* mass,
   return nbk::check_device_error(E, S(stream));
 }
 
-int nb_forces(nb_ctx* ctx, int64_t n, const double* pos, const double* vel, const double* mass,
-              const double* h, const double* rho, const double* omega, const double* pressure,
-              const double* u, const double* c_s, const double* alpha, const int64_t* offset,
-              const int64_t* index, int64_t nrows, const int64_t* rows, int kernel_id,
-              double beta, double alpha_u, int cond_signal, double* acc, double* dudt,
-              double* vsig_max, double* vheat, double* cheat, void* stream) {
+static int forces_impl(nb_ctx* ctx, int64_t n, const double* pos, const double* vel,
+                       const double* mass, const double* h, const double* rho,
+                       const double* omega, const double* pressure, const double* u,
+                       const double* c_s, const double* alpha, const double* grad_v,
+                       const int64_t* offset, const int64_t* index, int64_t nrows,
+                       const int64_t* rows, int kernel_id, double beta, double alpha_u,
+                       int cond_signal, int closeness, double eta_crit, double eta_fold,
+                       int gate, double* acc, double* dudt, double* vsig_max, double* vheat,
+                       double* cheat, void* stream) {
   NB_TRY(begin(ctx));
   Engine& E = ctx->E;
   if (kernel_id != 0 && kernel_id != 1) return nbk::set_host_error(E, "bad kernel_id"), NB_ERR_INPUT;
@@ -229,6 +232,15 @@ int nb_forces(nb_ctx* ctx, int64_t n, const double* pos, const double* vel, cons
   fp.alpha_u = alpha_u;
   fp.use_disc = 0;
   fp.tighten = 0;
+  if (grad_v && fp.use_visc) {
+    if (gate < 0 || gate > 2) return nbk::set_host_error(E, "bad reconstruction gate"), NB_ERR_INPUT;
+    fp.use_recon = 1;
+    fp.closeness = closeness;
+    fp.eta_crit = eta_crit;
+    fp.eta_fold = eta_fold;
+    fp.gate = gate;
+    fp.gv64 = grad_v;
+  }
   nbk::ForceOut fo;
   fo.acc = acc;
   fo.dudt = dudt;
@@ -237,6 +249,83 @@ int nb_forces(nb_ctx* ctx, int64_t n, const double* pos, const double* vel, cons
   fo.cheat = cheat;
   nbk::launch_forces64<int64_t>(rows ? nrows : n, rows, W.pk0, W.pk1, W.pk2, W.pk3, offset, index,
                                 fp, nullptr, fo, st);
+  NB_CUDA(cudaGetLastError());
+  return nbk::check_device_error(E, st);
+}
+
+int nb_forces(nb_ctx* ctx, int64_t n, const double* pos, const double* vel, const double* mass,
+              const double* h, const double* rho, const double* omega, const double* pressure,
+              const double* u, const double* c_s, const double* alpha, const int64_t* offset,
+              const int64_t* index, int64_t nrows, const int64_t* rows, int kernel_id,
+              double beta, double alpha_u, int cond_signal, double* acc, double* dudt,
+              double* vsig_max, double* vheat, double* cheat, void* stream) {
+  return forces_impl(ctx, n, pos, vel, mass, h, rho, omega, pressure, u, c_s, alpha, nullptr,
+                     offset, index, nrows, rows, kernel_id, beta, alpha_u, cond_signal, 1, 0.0,
+                     0.2, 2, acc, dudt, vsig_max, vheat, cheat, stream);
+}
+
+int nb_forces_recon(nb_ctx* ctx, int64_t n, const double* pos, const double* vel,
+                    const double* mass, const double* h, const double* rho, const double* omega,
+                    const double* pressure, const double* u, const double* c_s,
+                    const double* alpha, const double* grad_v, const int64_t* offset,
+                    const int64_t* index, int64_t nrows, const int64_t* rows, int kernel_id,
+                    double beta, double alpha_u, int cond_signal, int closeness, double eta_crit,
+                    double eta_fold, int gate, double* acc, double* dudt, double* vsig_max,
+                    double* vheat, double* cheat, void* stream) {
+  if (!grad_v) {
+    NB_TRY(begin(ctx));
+    return nbk::set_host_error(ctx->E, "grad_v missing"), NB_ERR_INPUT;
+  }
+  return forces_impl(ctx, n, pos, vel, mass, h, rho, omega, pressure, u, c_s, alpha, grad_v,
+                     offset, index, nrows, rows, kernel_id, beta, alpha_u, cond_signal,
+                     closeness, eta_crit, eta_fold, gate, acc, dudt, vsig_max, vheat, cheat,
+                     stream);
+}
+
+int nb_gradients(nb_ctx* ctx, int64_t n, const double* pos, const double* vel,
+                 const double* acc, const double* mass, const double* h, const int64_t* offset,
+                 const int64_t* index, int64_t nrows, const int64_t* rows, int kernel_id,
+                 double* div_v, double* curl_v, double* ddivv_dt, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (kernel_id != 0 && kernel_id != 1) return nbk::set_host_error(E, "bad kernel_id"), NB_ERR_INPUT;
+  if (!acc) return nbk::set_host_error(E, "accelerations missing"), NB_ERR_INPUT;
+  NB_TRY(E.ws.ensure(E, std::max<int64_t>(n, 1)));
+  nbk::Workspace& W = E.ws;
+  cudaStream_t st = S(stream);
+  nbk::pack_pos(n, pos, nullptr, W.pk0, st);
+  nbk::pack_vm(n, vel, mass, W.pk1, st);
+  nbk::pack4(n, h, nullptr, nullptr, nullptr, W.pk2, st);
+  nbk::pack_pos(n, acc, nullptr, W.pk3, st);
+  nbk::GradParams gp{kernel_id, cnorm_of(kernel_id), 0};
+  nbk::GradOut go;
+  go.div = div_v;
+  go.curl = curl_v;
+  go.ddiv = ddivv_dt;
+  nbk::launch_gradients<int64_t>(rows ? nrows : n, rows, W.pk0, W.pk1, W.pk2, W.pk3, offset,
+                                 index, gp, nullptr, go, st);
+  NB_CUDA(cudaGetLastError());
+  return nbk::check_device_error(E, st);
+}
+
+int nb_velocity_gradients(nb_ctx* ctx, int64_t n, const double* pos, const double* vel,
+                          const double* mass, const double* h, const int64_t* offset,
+                          const int64_t* index, int64_t nrows, const int64_t* rows,
+                          int kernel_id, double* out, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (kernel_id != 0 && kernel_id != 1) return nbk::set_host_error(E, "bad kernel_id"), NB_ERR_INPUT;
+  NB_TRY(E.ws.ensure(E, std::max<int64_t>(n, 1)));
+  nbk::Workspace& W = E.ws;
+  cudaStream_t st = S(stream);
+  nbk::pack_pos(n, pos, nullptr, W.pk0, st);
+  nbk::pack_vm(n, vel, mass, W.pk1, st);
+  nbk::pack4(n, h, nullptr, nullptr, nullptr, W.pk2, st);
+  nbk::GradParams gp{kernel_id, cnorm_of(kernel_id), 0};
+  nbk::GradOut go;
+  go.gv = out;
+  nbk::launch_gradients<int64_t>(rows ? nrows : n, rows, W.pk0, W.pk1, W.pk2, nullptr, offset,
+                                 index, gp, nullptr, go, st);
   NB_CUDA(cudaGetLastError());
   return nbk::check_device_error(E, st);
 }

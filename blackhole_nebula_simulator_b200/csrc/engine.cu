@@ -615,8 +615,25 @@ int Workspace::ensure(Engine& E, int64_t n) {
   return E.ensure_cub(std::max(std::max(need, a), std::max(b, d)) + 4096);
 }
 
+int Workspace::ensure_grad(Engine& E, int64_t n) {
+  if (n <= gcap && gvel) return 0;
+  if (pk4) cudaFree(pk4);
+  if (gvel) cudaFree(gvel);
+  if (gvel32) cudaFree(gvel32);
+  pk4 = nullptr;
+  gvel = nullptr;
+  gvel32 = nullptr;
+  gcap = 0;
+  const int64_t c = std::max<int64_t>(cap, n);
+  NB_CUDA(cudaMalloc((void**)&pk4, sizeof(double4) * c));
+  NB_CUDA(cudaMalloc((void**)&gvel, sizeof(double) * 9 * c));
+  NB_CUDA(cudaMalloc((void**)&gvel32, sizeof(float) * 9 * c));
+  gcap = c;
+  return 0;
+}
+
 void Workspace::release() {
-  void* ps[] = {d_a, d_b, d_c, d_hg, d_hs, d_heff, d_hlim, d_disp, d_P, d_cs, d_vsig, d_ddudt,
+  void* ps[] = {pk4, gvel, gvel32, d_a, d_b, d_c, d_hg, d_hs, d_heff, d_hlim, d_disp, d_P, d_cs, d_vsig, d_ddudt,
                 d_dm, d_tmp, d_uh, v_flow, v_pred, v_eval, v_dacc, v_tmp, pk0, pk1, pk2, pk3, pk32,
                 pf1, pf2, pf3, m_x, m_sorted, m_smark, f_mass,
                 rows, rows_s, rows2, iters, flags, need, i_tmp, pairs, i_lvl, i_tmp2, m_rows, m_done, m_need,
@@ -961,7 +978,7 @@ int select_mask(Engine& E, int64_t n, const uint8_t* mask, int64_t* out, int64_t
 // a superset of the rows and their interacting neighbours.
 int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, int64_t nrows,
                   const int64_t* rows, const nb_params* prm, const uint8_t* touched,
-                  cudaStream_t st) {
+                  const ShockStep& sk, cudaStream_t st) {
   Workspace& W = E.ws;
   Lists& L = E.lists;
   int64_t n = s->n;
@@ -972,14 +989,54 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   if (nrows == 0) return check_device_error(E, st);
   int64_t ns = 0;
   NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));
+  const bool sw_on = prm->viscosity && prm->visc_switch && sk.switch_on;
+  const bool recon = prm->viscosity && prm->recon;
   if (prm->precision == 1) {
     count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, vel, s->mass, nullptr, nullptr, 1, W.pf1);
     count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->h, s->rho, s->omega, W.d_P, 0, W.pf2);
-    count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, 0, W.pf3);
-  } else {
+  }
+  if (prm->precision != 1 || sw_on || recon) {
+    // FP64 packs (the FP32 form needs them only for the gradient passes)
     count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, vel, s->mass, W.pk1);
     count_launch(), k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->h, s->rho, s->omega, W.d_P, W.pk2);
+  }
+  if (sw_on || recon) {
+    NB_TRY(W.ensure_grad(E, n));
+    count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, s->h, W.pk0);
+  }
+  if (sw_on) {
+    // Cullen-Dehnen switch (sim/blocks.py:261-266, sim/coupled.py:159-162): corrected gradients
+    // of the rows over their interacting pairs with the previous accelerations, then alpha of
+    // the rows advanced over their step
+    count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->a_hydro, nullptr, W.pk4);
+    GradParams gp{prm->kernel_id, prm->cnorm, 1};
+    GradOut go;
+    go.alpha = s->alpha;
+    go.cs = W.d_cs;
+    go.h = s->h;
+    go.dt = sk.dt;
+    go.n_beg = sk.n_beg;
+    go.n_end = sk.n_end;
+    go.tick = sk.tick;
+    launch_gradients<int32_t>(nrows, W.rows_s, W.pk0, W.pk1, W.pk2, W.pk4, L.off, L.idx, gp,
+                              L.perm, go, st);
+  }
+  if (prm->precision == 1)
+    count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, 0, W.pf3);
+  else
     count_launch(), k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, W.pk3);
+  if (recon) {
+    // velocity gradients for the reconstruction: block steps, every touched particle over its
+    // untightened cached list (sim/blocks.py:271-278); shared steps, every particle over its
+    // interacting pairs (sim/coupled.py:164-168)
+    GradParams gp{prm->kernel_id, prm->cnorm, sk.recon_full ? 0 : 1,
+                  sk.recon_full ? touched : nullptr};
+    GradOut go;
+    go.gv = W.gvel;
+    launch_gradients<int32_t>(n, nullptr, W.pk0, W.pk1, W.pk2, nullptr, L.off, L.idx, gp, L.perm,
+                              go, st);
+    if (prm->precision == 1)
+      count_launch(), k_to_float<<<grid_for(9 * n), NB_THREADS, 0, st>>>(9 * n, W.gvel, W.gvel32);
   }
   ForceParams fp{};
   fp.kid = prm->kernel_id;
@@ -993,6 +1050,15 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   fp.use_disc = prm->disc_alpha_av > 0;
   fp.disc_alpha_av = prm->disc_alpha_av;
   fp.tighten = 1;
+  if (recon) {
+    fp.use_recon = 1;
+    fp.closeness = prm->recon_closeness;
+    fp.gate = prm->recon_gate;
+    fp.eta_crit = prm->recon_eta_crit;
+    fp.eta_fold = prm->recon_eta_fold;
+    fp.gv64 = W.gvel;
+    fp.gv32 = W.gvel32;
+  }
   ForceOut fo;
   fo.acc = s->a_hydro;
   fo.dudt = s->dudt;

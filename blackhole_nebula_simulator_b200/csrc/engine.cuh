@@ -77,7 +77,14 @@ struct Workspace {
   double* pend_erad = nullptr;
   double* d_scal = nullptr;
   int64_t* d_scal_i = nullptr;
+  // switch and velocity reconstruction only (allocated on first use): sorted accelerations and
+  // the sorted velocity gradients (9 per particle; float copy for the FP32 force pass)
+  int64_t gcap = 0;
+  double4* pk4 = nullptr;
+  double* gvel = nullptr;
+  float* gvel32 = nullptr;
   int ensure(Engine& E, int64_t n);
+  int ensure_grad(Engine& E, int64_t n);
   void release();
 };
 

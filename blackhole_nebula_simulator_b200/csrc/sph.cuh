@@ -22,6 +22,37 @@ struct ForceParams {
   int use_disc;   // disc viscosity (Lodato-Price AV form on every pair)
   double disc_alpha_av;
   int tighten;    // skip list entries with r >= 2 max(h_a, h_b)
+  // velocity reconstruction in the viscosity (physics/viscosity.py:116-158): the velocity
+  // gradients of every particle the pass reads, 9 per particle (row-major dv^i/dx^j) in the
+  // pass's index space, double for the FP64 form and float for the FP32 form
+  int use_recon = 0;
+  int closeness = 1;
+  int gate = 2;   // 0 both jumps approaching, 1 reconstructed jump only, 2 min-mod
+  double eta_crit = 0.0, eta_fold = 0.2;
+  const double* gv64 = nullptr;
+  const float* gv32 = nullptr;
+};
+
+// Corrected velocity (and acceleration) gradients, sim/sph.py:693-902.
+struct GradParams {
+  int kid;
+  double cnorm;
+  int tighten;    // only list entries with r < 2 max(h_a, h_b) (the tightened lists)
+  const uint8_t* mask = nullptr;  // with rows == null: only particles whose mask (caller order,
+                                  // through out_map) is set
+};
+struct GradOut {
+  double* div = nullptr;    // div v, |curl v|, d(div v)/dt at the output index (needs acc)
+  double* curl = nullptr;
+  double* ddiv = nullptr;
+  double* gv = nullptr;     // 9 per particle at the pass's own index
+  // Cullen-Dehnen update of alpha at the output index (physics/viscosity.py:83-113), from the
+  // row's c_s and h (caller order) over dt, or over (n_end - n_beg) tick when n_beg is set
+  double* alpha = nullptr;
+  const double* cs = nullptr;
+  const double* h = nullptr;
+  double dt = 0.0, tick = 0.0;
+  const int64_t *n_beg = nullptr, *n_end = nullptr;
 };
 
 struct ForceOut {
@@ -56,6 +87,11 @@ void launch_forces32(int64_t nrows, const int64_t* rows, const float4* pos, cons
                      const float4* vm, const float4* hydro, const float4* aux,
                      const int64_t* off, const I* idx, ForceParams prm, const int32_t* out_map,
                      ForceOut out, cudaStream_t st);
+
+template <typename I>
+void launch_gradients(int64_t nrows, const int64_t* rows, const double4* pos, const double4* vm,
+                      const double4* hydro, const double4* acc, const int64_t* off, const I* idx,
+                      GradParams prm, const int32_t* out_map, GradOut out, cudaStream_t st);
 
 void pack_pos(int64_t n, const double* pos, const double* w, double4* out, cudaStream_t st);
 void pack4(int64_t n, const double* a, const double* b, const double* c, const double* d,

@@ -23,9 +23,36 @@ void launch_forces64(int64_t nrows, const int64_t* rows, const double4* pos, con
                      ForceParams prm, const int32_t* out_map, ForceOut out, cudaStream_t st) {
   if (nrows <= 0) return;
   Pos64 geo{pos};
-  count_launch(), k_forces_g<double, Pos64, I, double4><<<grid_for(nrows * 8), NB_THREADS, 0, st>>>(
-      nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
+  if (prm.use_recon && prm.use_visc)
+    count_launch(), k_forces_g<double, Pos64, I, double4, true><<<grid_for(nrows * 8), NB_THREADS, 0, st>>>(
+        nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
+  else
+    count_launch(), k_forces_g<double, Pos64, I, double4, false><<<grid_for(nrows * 8), NB_THREADS, 0, st>>>(
+        nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
 }
+
+template <typename I>
+void launch_gradients(int64_t nrows, const int64_t* rows, const double4* pos, const double4* vm,
+                      const double4* hydro, const double4* acc, const int64_t* off, const I* idx,
+                      GradParams prm, const int32_t* out_map, GradOut out, cudaStream_t st) {
+  if (nrows <= 0) return;
+  Pos64 geo{pos};
+  if (acc)
+    count_launch(), k_gradients<I, true><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+        nrows, rows, geo, vm, hydro, acc, off, idx, prm, out_map, out);
+  else
+    count_launch(), k_gradients<I, false><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+        nrows, rows, geo, vm, hydro, acc, off, idx, prm, out_map, out);
+}
+
+template void launch_gradients<int64_t>(int64_t, const int64_t*, const double4*, const double4*,
+                                        const double4*, const double4*, const int64_t*,
+                                        const int64_t*, GradParams, const int32_t*, GradOut,
+                                        cudaStream_t);
+template void launch_gradients<int32_t>(int64_t, const int64_t*, const double4*, const double4*,
+                                        const double4*, const double4*, const int64_t*,
+                                        const int32_t*, GradParams, const int32_t*, GradOut,
+                                        cudaStream_t);
 
 template void launch_density64<int64_t>(int64_t, const int64_t*, const double4*, const double*,
                                         const double*, const double*, const int64_t*,

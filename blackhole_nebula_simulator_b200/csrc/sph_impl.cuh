@@ -443,14 +443,16 @@ __device__ __forceinline__ R dwdr(R r, R h, int kid, R cnorm) {
 
 constexpr int FORCE_QUEUE = 64;  // interacting entries a row queues before its lanes drain them
 // resident blocks per SM the FP32 force pass is compiled for (registers: 65536 / (256 * 3) = 85;
-// the FP64 form keeps 2, its doubles would spill)
+// the FP64 form keeps 2, its doubles would spill; the reconstruction forms, with two 3x3
+// gradients per pair, 2 and 1)
 constexpr int FORCE_BLOCKS_PER_SM_FP32 = 3;
 
 // Fused pressure + artificial viscosity (+ conductivity) + P dV (+ disc viscosity) pass.  Eight
 // lanes per row (lanes 8g .. 8g+7 of a warp), each taking every eighth list entry; the pair terms
 // are summed per lane and then over the row's lanes.
-template <typename R, typename PosT, typename I, typename V4>
-__global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? FORCE_BLOCKS_PER_SM_FP32 : 2)
+template <typename R, typename PosT, typename I, typename V4, bool RECON>
+__global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? (RECON ? 2 : FORCE_BLOCKS_PER_SM_FP32)
+                                                             : (RECON ? 1 : 2))
     k_forces_g(int64_t nrows, const int64_t* __restrict__ rows, PosT geo_in,
              const V4* __restrict__ vm,    // (vx, vy, vz, mass)
              const V4* __restrict__ hydro, // (h, rho, omega, P)
@@ -491,6 +493,76 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? FORCE_BLOCKS_PER_
   const unsigned len = (unsigned)(e_end - e_beg);
   const unsigned maxlen = __reduce_max_sync(FULL, len);
   int pc = 0;
+  // velocity reconstruction (sim/sph.py:568-609; physics/viscosity.py:116-158): the jump that
+  // drives q is the velocity difference extrapolated to the pair midpoint with each side's
+  // gradient, limited by the van Leer limiter of their projections and by the closeness factor;
+  // the shock heating keeps the actual v_ab . r_hat
+  R Ga[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) {
+    if constexpr (!RECON)
+      Ga[e] = R(0);
+    else if constexpr (sizeof(R) == 4)
+      Ga[e] = prm.gv32[9 * a + e];
+    else
+      Ga[e] = (R)prm.gv64[9 * a + e];
+  }
+  const R eta_crit = (R)prm.eta_crit, eta_fold = (R)prm.eta_fold;
+  auto recon_visc = [&](int64_t b, R dx0, R dx1, R dx2, R r, R rx, R ry, R rz, R h_b, R vdotr,
+                        const V4& vb, const V4& xb, R rho_b, R m_b, R fa, R& num_a, R& num_b) {
+    R Gb[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      if constexpr (sizeof(R) == 4)
+        Gb[e] = prm.gv32[9 * b + e];
+      else
+        Gb[e] = (R)prm.gv64[9 * b + e];
+    }
+    const R ga0 = Ga[0] * dx0 + Ga[1] * dx1 + Ga[2] * dx2;
+    const R ga1 = Ga[3] * dx0 + Ga[4] * dx1 + Ga[5] * dx2;
+    const R ga2 = Ga[6] * dx0 + Ga[7] * dx1 + Ga[8] * dx2;
+    const R gb0 = Gb[0] * dx0 + Gb[1] * dx1 + Gb[2] * dx2;
+    const R gb1 = Gb[3] * dx0 + Gb[4] * dx1 + Gb[5] * dx2;
+    const R gb2 = Gb[6] * dx0 + Gb[7] * dx1 + Gb[8] * dx2;
+    const R pa = dx0 * ga0 + dx1 * ga1 + dx2 * ga2;
+    const R pb = dx0 * gb0 + dx1 * gb1 + dx2 * gb2;
+    R phi = R(0);
+    if (pb != R(0)) {
+      const R ratio = pa / pb;
+      if (ratio > R(0)) {
+        const R t = R(4) * ratio / ((R(1) + ratio) * (R(1) + ratio));
+        phi = t < R(1) ? t : R(1);
+      }
+    }
+    if (prm.closeness) {
+      const R e_a = r / h_a, e_b = r / h_b;
+      const R eta_ab = e_b < e_a ? e_b : e_a;
+      if (eta_ab < eta_crit) {
+        const R t = (eta_ab - eta_crit) / eta_fold;
+        phi *= exp(-t * t);
+      }
+    }
+    const R hp = R(0.5) * phi;
+    R vdr = (((R)va.x - hp * ga0) - ((R)vb.x + hp * gb0)) * rx +
+            (((R)va.y - hp * ga1) - ((R)vb.y + hp * gb1)) * ry +
+            (((R)va.z - hp * ga2) - ((R)vb.z + hp * gb2)) * rz;
+    bool on = vdr < R(0) && vdotr < R(0);
+    if (prm.gate == 1)
+      on = vdr < R(0);
+    else if (prm.gate == 2 && vdotr > vdr)
+      vdr = vdotr;
+    const R vsig_a = al_a * cs_a + beta * fabs(vdr);
+    const R vsig_b = (R)xb.z * (R)xb.y + beta * fabs(vdr);
+    const R vsig_cfl = al_a * cs_a + beta * fabs(vdotr);
+    if (vsig_cfl > vmax) vmax = vsig_cfl;
+    if (on) {
+      num_a += R(-0.5) * rho_a * vsig_a * vdr;
+      num_b += R(-0.5) * rho_b * vsig_b * vdr;
+      R dh = m_b * vsig_a * R(0.5) * vdr * vdotr * fa * inv_or_a;
+      heat.add(-dh);
+      vheat.add(-dh);
+    }
+  };
   auto pair = [&](int64_t b) {
     R ddx, ddy, ddz;
     geo.diff(a, b, ddx, ddy, ddz);  // x_b - x_a
@@ -514,15 +586,20 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? FORCE_BLOCKS_PER_
     if (prm.use_sph) {
       if (prm.use_visc) {
         const V4 xb = aux[b];
-        R vsig_a = al_a * cs_a + beta * fabs(vdotr);
-        R vsig_b = (R)xb.z * (R)xb.y + beta * fabs(vdotr);
-        if (vsig_a > vmax) vmax = vsig_a;
-        if (vdotr < R(0)) {
-          num_a += R(-0.5) * rho_a * vsig_a * vdotr;
-          num_b += R(-0.5) * rho_b * vsig_b * vdotr;
-          R dh = m_b * vsig_a * R(0.5) * vdotr * vdotr * fa * inv_or_a;
-          heat.add(-dh);
-          vheat.add(-dh);
+        if constexpr (RECON) {
+          recon_visc(b, -ddx, -ddy, -ddz, r, rx, ry, rz, h_b, vdotr, vb, xb, rho_b, m_b, fa,
+                     num_a, num_b);
+        } else {
+          R vsig_a = al_a * cs_a + beta * fabs(vdotr);
+          R vsig_b = (R)xb.z * (R)xb.y + beta * fabs(vdotr);
+          if (vsig_a > vmax) vmax = vsig_a;
+          if (vdotr < R(0)) {
+            num_a += R(-0.5) * rho_a * vsig_a * vdotr;
+            num_b += R(-0.5) * rho_b * vsig_b * vdotr;
+            R dh = m_b * vsig_a * R(0.5) * vdotr * vdotr * fa * inv_or_a;
+            heat.add(-dh);
+            vheat.add(-dh);
+          }
         }
         if (prm.use_cond) {
           R vu;
@@ -586,15 +663,20 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? FORCE_BLOCKS_PER_
     if (prm.use_sph) {
       if (prm.use_visc) {
         const V4 xb = aux[b];
-        R vsig_a = al_a * cs_a + beta * fabs(vdotr);
-        R vsig_b = (R)xb.z * (R)xb.y + beta * fabs(vdotr);
-        if (vsig_a > vmax) vmax = vsig_a;
-        if (vdotr < R(0)) {
-          num_a += R(-0.5) * rho_a * vsig_a * vdotr;
-          num_b += R(-0.5) * rho_b * vsig_b * vdotr;
-          R dh = m_b * vsig_a * R(0.5) * vdotr * vdotr * fa * inv_or_a;
-          heat.add(-dh);
-          vheat.add(-dh);
+        if constexpr (RECON) {
+          recon_visc(b, -ddx, -ddy, -ddz, r, rx, ry, rz, h_b, vdotr, vb, xb, rho_b, m_b, fa,
+                     num_a, num_b);
+        } else {
+          R vsig_a = al_a * cs_a + beta * fabs(vdotr);
+          R vsig_b = (R)xb.z * (R)xb.y + beta * fabs(vdotr);
+          if (vsig_a > vmax) vmax = vsig_a;
+          if (vdotr < R(0)) {
+            num_a += R(-0.5) * rho_a * vsig_a * vdotr;
+            num_b += R(-0.5) * rho_b * vsig_b * vdotr;
+            R dh = m_b * vsig_a * R(0.5) * vdotr * vdotr * fa * inv_or_a;
+            heat.add(-dh);
+            vheat.add(-dh);
+          }
         }
         if (prm.use_cond) {
           R vu;
@@ -704,6 +786,156 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? FORCE_BLOCKS_PER_
     if (out.ddudt) out.ddudt[o] = s_dheat;
   }
   if (out.pairs) out.pairs[o] = npairs;
+}
+
+// ---------------------------------------------------------------- corrected gradients
+// Reference sim/sph.py:693-902 (_near_singular, _velocity_gradient_kernel, _gradients_kernel):
+//     R_lj = sum_b m_b (x_b - x_a)^l dW_ab(h_a)/dx_a^j,  G_kj = sum_b m_b (v_b - v_a)^k dW/dx_a^j,
+//     dv/dx = G R^-1 (the same with accelerations for d(div v)/dt),
+// with dW_ab(h_a)/dx_a = (x_a - x_b) F(r, h_a) / r.  Fewer than 4 list entries (self excluded),
+// tr R <= 0 or |det R| < 1e-6 (tr R / 3)^3: G / (tr R / 3) instead (0 when tr R <= 0).  R^-1 is
+// the adjugate over the determinant.  Thread per row, FP64 only (the FP32 form converts).
+constexpr double SINGULAR_TOL = 1e-6;
+
+__device__ __forceinline__ double det3(const double* m) {
+  return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+         m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+
+// g <- g R^-1 (or the fallback) for the gradient sums g (3x3 row-major)
+template <int NG>
+__device__ __forceinline__ void corrected_gradients(const double* rm, int64_t cnt, double (*g)[9]) {
+  const double scale = (rm[0] + rm[4] + rm[8]) / 3.0;
+  const double det = det3(rm);
+  const bool singular =
+      cnt < 4 || !(scale > 0.0) || !(fabs(det) >= SINGULAR_TOL * scale * scale * scale);
+  if (singular) {
+    const double inv_s = scale > 0.0 ? 1.0 / scale : 0.0;
+#pragma unroll
+    for (int k = 0; k < NG; ++k)
+#pragma unroll
+      for (int e = 0; e < 9; ++e) g[k][e] = g[k][e] * inv_s;
+    return;
+  }
+  double ri[9];
+  ri[0] = (rm[4] * rm[8] - rm[5] * rm[7]) / det;
+  ri[1] = (rm[2] * rm[7] - rm[1] * rm[8]) / det;
+  ri[2] = (rm[1] * rm[5] - rm[2] * rm[4]) / det;
+  ri[3] = (rm[5] * rm[6] - rm[3] * rm[8]) / det;
+  ri[4] = (rm[0] * rm[8] - rm[2] * rm[6]) / det;
+  ri[5] = (rm[2] * rm[3] - rm[0] * rm[5]) / det;
+  ri[6] = (rm[3] * rm[7] - rm[4] * rm[6]) / det;
+  ri[7] = (rm[1] * rm[6] - rm[0] * rm[7]) / det;
+  ri[8] = (rm[0] * rm[4] - rm[1] * rm[3]) / det;
+#pragma unroll
+  for (int k = 0; k < NG; ++k) {
+    double o[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        o[3 * i + j] = g[k][3 * i + 0] * ri[j] + g[k][3 * i + 1] * ri[3 + j] +
+                       g[k][3 * i + 2] * ri[6 + j];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) g[k][e] = o[e];
+  }
+}
+
+template <typename I, bool ACC>
+__global__ void __launch_bounds__(NB_THREADS)
+    k_gradients(int64_t nrows, const int64_t* __restrict__ rows, Pos64 geo,
+                const double4* __restrict__ vm,     // (vx, vy, vz, mass)
+                const double4* __restrict__ hydro,  // (h, ...)
+                const double4* __restrict__ acc,    // (ax, ay, az, -), with ACC
+                const int64_t* __restrict__ off, const I* __restrict__ idx, GradParams prm,
+                const int32_t* __restrict__ out_map, GradOut out) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  const int64_t a = rows ? rows[q] : q;
+  const int64_t o = out_map ? (int64_t)out_map[a] : q;
+  if (!rows && prm.mask && !prm.mask[o]) return;
+  const double4 va = vm[a];
+  const double h_a = hydro[a].x;
+  double4 aa = make_double4(0.0, 0.0, 0.0, 0.0);
+  if (ACC) aa = acc[a];
+  double rm[9], g[ACC ? 2 : 1][9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) {
+    rm[e] = 0.0;
+    g[0][e] = 0.0;
+    if (ACC) g[ACC ? 1 : 0][e] = 0.0;
+  }
+  int64_t cnt = 0;
+  const int64_t e1 = off[a + 1];
+  for (int64_t k = off[a]; k < e1; ++k) {
+    const int64_t b = (int64_t)ld_stream(idx + k);
+    if (b == a) continue;
+    double ddx, ddy, ddz;
+    geo.diff(a, b, ddx, ddy, ddz);  // x_b - x_a
+    if (prm.tighten) {
+      const double h_b = hydro[b].x;
+      const double rr = 2.0 * (h_a > h_b ? h_a : h_b);
+      if (!(sqdist(ddx, ddy, ddz) < rr * rr)) continue;
+    }
+    cnt += 1;
+    const double dx[3] = {-ddx, -ddy, -ddz};  // x_a - x_b
+    const double r = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+    const double f = dwdr<double>(r, h_a, prm.kid, prm.cnorm) / r;
+    const double4 vb = vm[b];
+    const double dv[3] = {vb.x - va.x, vb.y - va.y, vb.z - va.z};
+    double da[3] = {0.0, 0.0, 0.0};
+    if (ACC) {
+      const double4 ab = acc[b];
+      da[0] = ab.x - aa.x;
+      da[1] = ab.y - aa.y;
+      da[2] = ab.z - aa.z;
+    }
+    const double mf = vb.w * f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const double gj = mf * dx[j];
+        rm[3 * i + j] -= dx[i] * gj;
+        g[0][3 * i + j] += dv[i] * gj;
+        if (ACC) g[ACC ? 1 : 0][3 * i + j] += da[i] * gj;
+      }
+  }
+  corrected_gradients<ACC ? 2 : 1>(rm, cnt, g);
+  const double* dv = g[0];
+  if (out.gv) {
+#pragma unroll
+    for (int e = 0; e < 9; ++e) out.gv[9 * a + e] = dv[e];
+  }
+  if (!ACC) return;
+  const double* dacc = g[ACC ? 1 : 0];
+  const double div = dv[0] + dv[4] + dv[8];
+  const double c0 = dv[7] - dv[5], c1 = dv[2] - dv[6], c2 = dv[3] - dv[1];
+  const double curl = sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+  double sdd = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) sdd += dv[3 * i + j] * dv[3 * j + i];
+  const double ddiv = dacc[0] + dacc[4] + dacc[8] - sdd;
+  if (out.div) out.div[o] = div;
+  if (out.curl) out.curl[o] = curl;
+  if (out.ddiv) out.ddiv[o] = ddiv;
+  if (out.alpha) {
+    // physics/viscosity.py:83-113: xi (Balsara), alpha_loc, decay time, the jump or the decay
+    const double d2 = div * div, cc2 = curl * curl;
+    const double xi = d2 + cc2 > 0.0 ? d2 / (d2 + cc2) : 0.0;
+    const double mdd = -ddiv < 0.0 ? 0.0 : -ddiv;  // max(-d(div v)/dt, 0); NaN stays NaN
+    const double h = out.h[o], cs = out.cs[o];
+    const double al = 10.0 * h * h * (xi * mdd) / (cs * cs);
+    const double a_loc = al > 1.0 ? 1.0 : al;  // min(alpha_loc, alpha_max = 1)
+    const double dt =
+        out.n_beg ? 2.0 * (0.5 * (double)(out.n_end[o] - out.n_beg[o]) * out.tick) : out.dt;
+    const double tau = h / (0.1 * cs);
+    const double alpha = out.alpha[o];
+    const double decayed = (alpha + a_loc * dt / tau) / (1.0 + dt / tau);
+    out.alpha[o] = a_loc > alpha ? a_loc : decayed;
+  }
 }
 
 }  // namespace nbk

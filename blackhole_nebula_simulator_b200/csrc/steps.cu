@@ -57,7 +57,7 @@ static BremsParams brems_of(const nb_params* prm) {
 // every neighbour in the cached lists, widened until every interacting neighbour is fresh; then
 // the fused EOS + force pass for the rows.
 int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, const int64_t* rows,
-               const double* vel, const double* u, cudaStream_t st) {
+               const double* vel, const double* u, cudaStream_t st, const ShockStep& sk) {
   Workspace& W = E.ws;
   int64_t n = s->n;
   NB_TRY(W.ensure(E, n));
@@ -113,9 +113,9 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
       return NB_ERR_TOUCHED;
     }
   }
-  if (prm->viscosity)
+  if (prm->viscosity && !prm->visc_switch)
     count_launch(), k_set_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, prm->alpha_const, s->alpha);
-  return engine_forces(E, s, vel, u, nrows, rows, prm, W.m_done, st);
+  return engine_forces(E, s, vel, u, nrows, rows, prm, W.m_done, sk, st);
 }
 
 // ---------------------------------------------------------------- shared step
@@ -235,7 +235,10 @@ int coupled_step(Engine& E, nb_state* s, const nb_params* prm, double dt, cudaSt
   launch_v_from_p(n, s->x, W.v_tmp, W.v_eval, st);
   count_launch(), k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
   W.rows_ver += 1;
-  NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st));
+  ShockStep sk;
+  sk.switch_on = 1;
+  sk.dt = dt;
+  NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st, sk));
   // closing kick with the new forces
   count_launch(), k_pred_shared<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.v_flow, s->a_hydro, u_half, s->dudt,
                                                     half, s->p, s->u);
@@ -680,7 +683,9 @@ int block_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t 
   count_launch(), k_iota<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.rows);
   W.rows_ver += 1;
   launch_v_from_p(n, s->x, s->p, W.v_eval, st);
-  NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st));
+  ShockStep sk;
+  sk.recon_full = 1;
+  NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st, sk));
   count_launch(), k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, 0, s->level);
   NB_TRY(choose_levels_and_open(E, s, prm, n, W.rows, st));
   return pending_flush(E, st);
@@ -734,7 +739,13 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   }
   s->tick_n = n_next;
   launch_v_from_p(n, s->x, W.v_pred, W.v_eval, st);
-  NB_TRY(hydro_rows(E, s, prm, nrows, W.rows, W.v_eval, s->u, st));
+  ShockStep sk;
+  sk.switch_on = 1;
+  sk.n_beg = s->n_beg;
+  sk.n_end = s->n_end;
+  sk.tick = s->tick;
+  sk.recon_full = 1;
+  NB_TRY(hydro_rows(E, s, prm, nrows, W.rows, W.v_eval, s->u, st, sk));
   count_launch(), k_block_close<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, W.rows, s->tick, s->n_beg, s->n_end,
                                                        W.v_flow, s->a_hydro, s->u_half, s->dudt,
                                                        W.v_pred, s->u);

@@ -10,6 +10,19 @@ namespace nbk {
 
 constexpr int K_MAX = 40;
 
+// How a hydro pass advances the viscosity switch and where the reconstruction's gradients come
+// from: switch_on for a step (not the initialisation) with its length dt, or per row
+// (n_end - n_beg) tick in block steps; recon_full: gradients of the touched particles over
+// their untightened lists (block steps) instead of every particle over its interacting pairs.
+struct ShockStep {
+  int switch_on = 0;
+  double dt = 0.0;
+  const int64_t* n_beg = nullptr;
+  const int64_t* n_end = nullptr;
+  double tick = 0.0;
+  int recon_full = 0;
+};
+
 int compute_density(Engine& E, int64_t n, const double* x, const double* mass, double* h,
                     double* rho, double* omega, int64_t nrows, const int64_t* rows,
                     const nb_params* prm, int64_t* builds, int64_t* reuses, cudaStream_t st);
@@ -17,10 +30,11 @@ int select_mask(Engine& E, int64_t n, const uint8_t* mask, int64_t* out, int64_t
                 cudaStream_t st);
 int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, int64_t nrows,
                   const int64_t* rows, const nb_params* prm, const uint8_t* touched,
-                  cudaStream_t st);
+                  const ShockStep& sk, cudaStream_t st);
 
 int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, const int64_t* rows,
-               const double* vel, const double* u, cudaStream_t st);
+               const double* vel, const double* u, cudaStream_t st,
+               const ShockStep& sk = ShockStep{});
 int coupled_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st);
 int coupled_step(Engine& E, nb_state* s, const nb_params* prm, double dt, cudaStream_t st);
 int coupled_stable_dt(Engine& E, nb_state* s, const nb_params* prm, double* dt, cudaStream_t st);

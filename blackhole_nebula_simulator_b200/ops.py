@@ -119,10 +119,11 @@ class ForceResult:
 def forces_numba(pos, vel, mass, h, rho, omega, pressure, nb: Neighbours,
                  kernel_name=DEFAULT_KERNEL, u=None, c_s=None, alpha=None,
                  shock: ShockCapturing = ShockCapturing(), rows=None, grad_v=None) -> ForceResult:  # fmt: skip
-    """sim/sph.py:655-690 without velocity reconstruction (shock.reconstruction must be off)."""
+    """sim/sph.py:655-690: with ``shock.reconstruction`` the viscosity uses the reconstructed
+    velocity jump (sim/sph.py:568-609) and needs ``grad_v`` (N, 3, 3) of all particles
+    (``velocity_gradients_numba``); ValueError without it, as the reference."""
     use_visc = alpha is not None and c_s is not None
-    if use_visc and shock.reconstruction:
-        raise NotImplementedError("velocity reconstruction is not part of the CUDA SPH path")
+    use_recon = use_visc and shock.reconstruction
     pos = dev_f64(pos)
     n = len(pos)
     rows_t = None if rows is None else dev_i64(rows)
@@ -135,14 +136,68 @@ def forces_numba(pos, vel, mass, h, rho, omega, pressure, nb: Neighbours,
     args = [dev_f64(vel), dev_f64(mass, (n,)), dev_f64(h), dev_f64(rho), dev_f64(omega),
             dev_f64(pressure), opt(u if use_visc else None), opt(c_s if use_visc else None),
             opt(alpha if use_visc else None)]  # fmt: skip
-    _call("nb_forces", n, ptr(pos), *[ptr(a) for a in args], ptr(off), ptr(idx), m, ptr(rows_t),
-          KERNEL_IDS[kernel_name], float(shock.beta), float(shock.alpha_u),
-          int(shock.conductivity_signal), ptr(acc), ptr(dudt), ptr(vsig), ptr(vh), ptr(ch),
-          stream())  # fmt: skip
+    if use_recon:
+        if grad_v is None or tuple(grad_v.shape) != (n, 3, 3):
+            raise ValueError("velocity reconstruction needs grad_v of shape (N, 3, 3)")
+        gv = dev_f64(grad_v, (n, 3, 3))
+        _call("nb_forces_recon", n, ptr(pos), *[ptr(a) for a in args], ptr(gv), ptr(off),
+              ptr(idx), m, ptr(rows_t), KERNEL_IDS[kernel_name], float(shock.beta),
+              float(shock.alpha_u), int(shock.conductivity_signal), int(bool(shock.closeness)),
+              float(shock.eta_crit), float(shock.eta_fold), int(shock.recon_gate), ptr(acc),
+              ptr(dudt), ptr(vsig), ptr(vh), ptr(ch), stream())  # fmt: skip
+    else:
+        _call("nb_forces", n, ptr(pos), *[ptr(a) for a in args], ptr(off), ptr(idx), m,
+              ptr(rows_t), KERNEL_IDS[kernel_name], float(shock.beta), float(shock.alpha_u),
+              int(shock.conductivity_signal), ptr(acc), ptr(dudt), ptr(vsig), ptr(vh), ptr(ch),
+              stream())  # fmt: skip
     if not use_visc:
         vh.zero_()
         ch.zero_()
     return ForceResult(acc, dudt, vsig, vh, ch)
+
+
+@dataclass
+class Gradients:
+    """sim/sph.py:708-712."""
+
+    div_v: torch.Tensor
+    curl_v: torch.Tensor  # magnitude |curl v|
+    ddivv_dt: torch.Tensor
+
+
+def gradients_numba(pos, vel, acc, mass, h, nb: Neighbours, kernel_name=DEFAULT_KERNEL,
+                    rows=None) -> Gradients:  # fmt: skip
+    """sim/sph.py:883-902: corrected div v, |curl v| and d(div v)/dt (Cullen & Dehnen 2010
+    App. B3) of ``rows`` (in that order; default all) from velocities and accelerations."""
+    pos = dev_f64(pos)
+    n = len(pos)
+    rows_t = None if rows is None else dev_i64(rows)
+    m = n if rows_t is None else len(rows_t)
+    div, curl, ddiv = (torch.empty(m, dtype=torch.float64, device=pos.device) for _ in range(3))
+    off, idx = dev_i64(nb.offset), dev_i64(nb.index)
+    ins = [dev_f64(vel), dev_f64(acc), dev_f64(mass, (n,)), dev_f64(h)]
+    _call("nb_gradients", n, ptr(pos), *[ptr(a) for a in ins], ptr(off), ptr(idx), m,
+          ptr(rows_t), KERNEL_IDS[kernel_name], ptr(div), ptr(curl), ptr(ddiv), stream())
+    return Gradients(div, curl, ddiv)
+
+
+def velocity_gradients_numba(pos, vel, mass, h, nb: Neighbours, kernel_name=DEFAULT_KERNEL,
+                             rows=None, out=None) -> torch.Tensor:  # fmt: skip
+    """sim/sph.py:827-846: fills ``out`` (N, 3, 3; zeros if not given) with the corrected
+    gradients dv^i/dx^j of ``rows`` (default all) and returns it."""
+    pos = dev_f64(pos)
+    n = len(pos)
+    rows_t = None if rows is None else dev_i64(rows)
+    m = n if rows_t is None else len(rows_t)
+    if out is None:
+        out = torch.zeros((n, 3, 3), dtype=torch.float64, device=pos.device)
+    elif out.dtype != torch.float64 or not out.is_cuda or not out.is_contiguous():
+        raise ValueError("out must be a contiguous float64 CUDA tensor of shape (N, 3, 3)")
+    off, idx = dev_i64(nb.offset), dev_i64(nb.index)
+    ins = [dev_f64(vel), dev_f64(mass, (n,)), dev_f64(h)]
+    _call("nb_velocity_gradients", n, ptr(pos), *[ptr(a) for a in ins], ptr(off), ptr(idx), m,
+          ptr(rows_t), KERNEL_IDS[kernel_name], ptr(out), stream())
+    return out
 
 
 def disc_forces_numba(pos, vel, mass, h, rho, omega, c_s, alpha_av, nb: Neighbours,

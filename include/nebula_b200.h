@@ -78,6 +78,12 @@ typedef struct nb_params {
   double eos_u_si;        /* J/kg per code specific energy (c^2) */
   double eos_a1;          /* 3 k / (2 mu m_p) [J/(kg K)] */
   double eos_a_rad;       /* radiation constant [J m^-3 K^-4] */
+  int visc_switch;        /* Cullen-Dehnen switch: alpha of the rows advanced at each step */
+  int recon;              /* velocity reconstruction in the viscosity */
+  int recon_closeness;    /* its closeness factor (Frontiere et al. 2017 Eq. 51) */
+  int recon_gate;         /* 0 both jumps approaching, 1 reconstructed jump only, 2 min-mod */
+  double recon_eta_crit;  /* 1 / hfact */
+  double recon_eta_fold;
 } nb_params;
 
 /* Device state of a run (the fields of the reference's GasState / BlockState that the step
@@ -135,6 +141,33 @@ NB_API int nb_forces(nb_ctx* ctx, int64_t n, const double* pos, const double* ve
               const int64_t* index, int64_t nrows, const int64_t* rows, int kernel_id,
               double beta, double alpha_u, int cond_signal, double* acc, double* dudt,
               double* vsig_max, double* vheat, double* cheat, void* stream);
+
+/* forces_numba with velocity reconstruction (sim/sph.py:655-690 with shock.reconstruction,
+ * the branch at sim/sph.py:568-609): nb_forces plus grad_v (n, 3, 3) of every particle, the
+ * closeness factor switch, eta_crit, eta_fold and the gate (ShockCapturing.recon_gate). */
+NB_API int nb_forces_recon(nb_ctx* ctx, int64_t n, const double* pos, const double* vel,
+                    const double* mass, const double* h, const double* rho, const double* omega,
+                    const double* pressure, const double* u, const double* c_s,
+                    const double* alpha, const double* grad_v, const int64_t* offset,
+                    const int64_t* index, int64_t nrows, const int64_t* rows, int kernel_id,
+                    double beta, double alpha_u, int cond_signal, int closeness, double eta_crit,
+                    double eta_fold, int gate, double* acc, double* dudt, double* vsig_max,
+                    double* vheat, double* cheat, void* stream);
+
+/* gradients_numba (sim/sph.py:883-902): corrected div v, |curl v| and d(div v)/dt of `rows`
+ * (all when NULL; results in rows order) from velocities and accelerations over the given
+ * lists. */
+NB_API int nb_gradients(nb_ctx* ctx, int64_t n, const double* pos, const double* vel,
+                 const double* acc, const double* mass, const double* h, const int64_t* offset,
+                 const int64_t* index, int64_t nrows, const int64_t* rows, int kernel_id,
+                 double* div_v, double* curl_v, double* ddivv_dt, void* stream);
+
+/* velocity_gradients_numba (sim/sph.py:827-846): out (n, 3, 3) = dv^i/dx^j at the particles of
+ * `rows` (all when NULL); the other entries of out are left as they are. */
+NB_API int nb_velocity_gradients(nb_ctx* ctx, int64_t n, const double* pos, const double* vel,
+                          const double* mass, const double* h, const int64_t* offset,
+                          const int64_t* index, int64_t nrows, const int64_t* rows,
+                          int kernel_id, double* out, void* stream);
 
 /* disc_forces_numba (sim/sph.py:1120-1137). */
 NB_API int nb_disc_forces(nb_ctx* ctx, int64_t n, const double* pos, const double* vel,
