@@ -76,11 +76,13 @@ def cooling_network():
 
 
 def workload(name: str, n: int | None, precision: str, seed_shift: int = 0, mlp=None,
-             eos: str = "ideal"):
+             eos: str = "ideal", shock: bool = False):
     from blackhole_nebula_simulator_b200 import ics
     from blackhole_nebula_simulator_b200.config import BlockConfig, CoupledConfig, HydroConfig
 
-    common = dict(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+    # shock: the reference's default shock capturing (Cullen-Dehnen switch from alpha = 0 and
+    # velocity reconstruction), else constant alpha
+    common = dict(kernel="cubic", eta=1.2, switch=shock, reconstruction=shock,
                   conductivity_signal=1, alpha_u=0.05, h_max=200.0, precision=precision,
                   eos=eos)  # fmt: skip
     if name == "torus":
@@ -156,7 +158,7 @@ def profile_read(ctx):
 
     from blackhole_nebula_simulator_b200 import _lib
 
-    names = ["lists", "density", "forces", "flow", "marks", "levels", "cooling", "eos"]
+    names = ["lists", "density", "forces", "flow", "marks", "levels", "cooling", "eos", "gradients"]
     out = (ctypes.c_double * (4 * len(names)))()
     _lib.check(ctx, _lib.lib().nb_profile_read(ctx, out))
     return {names[c]: {"ms": out[4 * c], "launches": int(out[4 * c + 1]), "units": out[4 * c + 2],
@@ -223,7 +225,8 @@ def run_gpu(args, rank, world, precision=None, use_mlp=None, e2e=True):
     precision = precision or args.precision
     use_mlp = (precision == "fp32") if use_mlp is None else use_mlp
     net = cooling_network() if use_mlp else None
-    ic, bc = workload(args.workload, args.n, precision, seed_shift=rank, mlp=net, eos=args.eos)
+    ic, bc = workload(args.workload, args.n, precision, seed_shift=rank, mlp=net, eos=args.eos,
+                      shock=args.shock)
     st = blocks.initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=bc.dt_max * 2.0**20)
     led_init = blocks.ledger(st, bc)  # every particle is at a step boundary here
     for _ in range(args.warmup):
@@ -332,7 +335,7 @@ def cpu_reference(args, steps, warmup, sample_n=None):
 
     n_full = {"torus": 4_194_304, "streams": 1_048_576, "cloud": 262_144}[args.workload]
     n = sample_n or min(args.n or n_full, 32_768)
-    ic, bc = workload(args.workload, n, "fp64", eos=args.eos)
+    ic, bc = workload(args.workload, n, "fp64", eos=args.eos, shock=args.shock)
     st = osteps.blocks_initialise(ic.x, ic.v, ic.u, ic.mass, ic.h, bc, t_stop=bc.dt_max * 2.0**20)
     for _ in range(warmup):
         osteps.blocks_advance(st, bc)
@@ -357,6 +360,9 @@ def main():
     ap.add_argument("--workload", default="torus", choices=["torus", "streams", "cloud"])
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--shock", action="store_true",
+                    help="the reference's default shock capturing: Cullen-Dehnen switch and "
+                         "velocity reconstruction (else constant alpha)")  # fmt: skip
     ap.add_argument("--eos", default="ideal", choices=["ideal", "gasrad", "radiation"],
                     help="equation of state (gas + radiation and the radiation limit run without "
                          "cooling: the cloud workload)")  # fmt: skip
@@ -372,7 +378,8 @@ def main():
               "particles": n_full,
               "precision": args.precision if args.impl == "ours" else "fp64 (CPU oracle)",
               "l2_flush": "inputs larger than L2",
-              "parallelism": f"replicas x{world}", "eos": args.eos}  # fmt: skip
+              "parallelism": f"replicas x{world}", "eos": args.eos,
+              "shock_capturing": "switch + reconstruction" if args.shock else "constant alpha"}  # fmt: skip
     if args.workload == "torus":
         config["disc_alpha_av"] = TORUS_ALPHA_AV
         config["scale_height"] = TORUS_SCALE_HEIGHT

@@ -1004,13 +1004,17 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
     NB_TRY(W.ensure_grad(E, n));
     count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, s->h, W.pk0);
   }
-  if (sw_on) {
+  if (sw_on || recon) {
     // Cullen-Dehnen switch (sim/blocks.py:261-266, sim/coupled.py:159-162): corrected gradients
     // of the rows over their interacting pairs with the previous accelerations, then alpha of
-    // the rows advanced over their step
-    count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->a_hydro, nullptr, W.pk4);
-    GradParams gp{prm->kernel_id, prm->cnorm, 1};
+    // the rows advanced over their step; velocity gradients for the reconstruction: block
+    // steps, every touched particle over its untightened cached list (sim/blocks.py:271-278),
+    // shared steps, every particle over its interacting pairs (sim/coupled.py:164-168).  One
+    // pass for both; W.m_sorted holds the rows' sorted mask (rows_sorted above).
+    if (sw_on)
+      count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->a_hydro, nullptr, W.pk4);
     GradOut go;
+    go.gv = W.gvel;
     go.alpha = s->alpha;
     go.cs = W.d_cs;
     go.h = s->h;
@@ -1018,26 +1022,19 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
     go.n_beg = sk.n_beg;
     go.n_end = sk.n_end;
     go.tick = sk.tick;
-    launch_gradients<int32_t>(nrows, W.rows_s, W.pk0, W.pk1, W.pk2, W.pk4, L.off, L.idx, gp,
-                              L.perm, go, st);
+    E.prof.begin(st);
+    launch_shock_gradients(n, W.pk0, W.pk1, W.pk2, W.pk4, L.off, L.idx, prm->kernel_id,
+                           prm->cnorm, recon ? 1 : 0, sk.recon_full,
+                           sk.recon_full ? touched : nullptr, sw_on ? W.m_sorted : nullptr,
+                           L.perm, go, st);
+    E.prof.end(PROF_GRAD, st, (double)n, 0.0);
+    if (recon && prm->precision == 1)
+      count_launch(), k_to_float<<<grid_for(9 * n), NB_THREADS, 0, st>>>(9 * n, W.gvel, W.gvel32);
   }
   if (prm->precision == 1)
     count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, 0, W.pf3);
   else
     count_launch(), k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, W.pk3);
-  if (recon) {
-    // velocity gradients for the reconstruction: block steps, every touched particle over its
-    // untightened cached list (sim/blocks.py:271-278); shared steps, every particle over its
-    // interacting pairs (sim/coupled.py:164-168)
-    GradParams gp{prm->kernel_id, prm->cnorm, sk.recon_full ? 0 : 1,
-                  sk.recon_full ? touched : nullptr};
-    GradOut go;
-    go.gv = W.gvel;
-    launch_gradients<int32_t>(n, nullptr, W.pk0, W.pk1, W.pk2, nullptr, L.off, L.idx, gp, L.perm,
-                              go, st);
-    if (prm->precision == 1)
-      count_launch(), k_to_float<<<grid_for(9 * n), NB_THREADS, 0, st>>>(9 * n, W.gvel, W.gvel32);
-  }
   ForceParams fp{};
   fp.kid = prm->kernel_id;
   fp.cnorm = prm->cnorm;

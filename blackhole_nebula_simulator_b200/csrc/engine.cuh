@@ -94,7 +94,7 @@ struct Workspace {
 // the steps it times.
 enum ProfCat {
   PROF_LISTS = 0, PROF_DENSITY = 1, PROF_FORCES = 2, PROF_FLOW = 3, PROF_MARKS = 4,
-  PROF_LEVELS = 5, PROF_COOL = 6, PROF_EOS = 7, PROF_NCAT = 8
+  PROF_LEVELS = 5, PROF_COOL = 6, PROF_EOS = 7, PROF_GRAD = 8, PROF_NCAT = 9
 };
 struct Prof {
   static constexpr int POOL = 1024;

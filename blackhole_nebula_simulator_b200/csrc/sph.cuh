@@ -93,6 +93,16 @@ void launch_gradients(int64_t nrows, const int64_t* rows, const double4* pos, co
                       const double4* hydro, const double4* acc, const int64_t* off, const I* idx,
                       GradParams prm, const int32_t* out_map, GradOut out, cudaStream_t st);
 
+// The switch and the reconstruction's gradients of one step in one pass over the sorted lists:
+// gv (sorted) for the particles of live_mask (caller order; null = all) when recon, over their
+// untightened lists when recon_full; the switch's alpha update for the rows of row_sorted
+// (sorted mask; null = no switch) with acc (sorted previous accelerations).
+void launch_shock_gradients(int64_t n, const double4* pos, const double4* vm,
+                            const double4* hydro, const double4* acc, const int64_t* off,
+                            const int32_t* idx, int kid, double cnorm, int recon, int recon_full,
+                            const uint8_t* live_mask, const uint8_t* row_sorted,
+                            const int32_t* perm, GradOut out, cudaStream_t st);
+
 void pack_pos(int64_t n, const double* pos, const double* w, double4* out, cudaStream_t st);
 void pack4(int64_t n, const double* a, const double* b, const double* c, const double* d,
            double4* out, cudaStream_t st);

@@ -38,11 +38,28 @@ void launch_gradients(int64_t nrows, const int64_t* rows, const double4* pos, co
   if (nrows <= 0) return;
   Pos64 geo{pos};
   if (acc)
-    count_launch(), k_gradients<I, true><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+    count_launch(), k_gradients<I, true><<<grid_for(nrows * 8), NB_THREADS, 0, st>>>(
         nrows, rows, geo, vm, hydro, acc, off, idx, prm, out_map, out);
   else
-    count_launch(), k_gradients<I, false><<<grid_for(nrows), NB_THREADS, 0, st>>>(
+    count_launch(), k_gradients<I, false><<<grid_for(nrows * 8), NB_THREADS, 0, st>>>(
         nrows, rows, geo, vm, hydro, acc, off, idx, prm, out_map, out);
+}
+
+void launch_shock_gradients(int64_t n, const double4* pos, const double4* vm,
+                            const double4* hydro, const double4* acc, const int64_t* off,
+                            const int32_t* idx, int kid, double cnorm, int recon, int recon_full,
+                            const uint8_t* live_mask, const uint8_t* row_sorted,
+                            const int32_t* perm, GradOut out, cudaStream_t st) {
+  if (n <= 0) return;
+  Pos64 geo{pos};
+  if (row_sorted)
+    count_launch(), k_shock_grad<int32_t, true><<<grid_for(n * 8), NB_THREADS, 0, st>>>(
+        n, geo, vm, hydro, acc, off, idx, kid, cnorm, recon, recon_full, live_mask, row_sorted,
+        perm, out);
+  else
+    count_launch(), k_shock_grad<int32_t, false><<<grid_for(n * 8), NB_THREADS, 0, st>>>(
+        n, geo, vm, hydro, acc, off, idx, kid, cnorm, recon, recon_full, live_mask, row_sorted,
+        perm, out);
 }
 
 template void launch_gradients<int64_t>(int64_t, const int64_t*, const double4*, const double4*,

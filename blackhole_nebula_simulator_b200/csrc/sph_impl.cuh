@@ -794,7 +794,7 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? (RECON ? 2 : FORC
 //     dv/dx = G R^-1 (the same with accelerations for d(div v)/dt),
 // with dW_ab(h_a)/dx_a = (x_a - x_b) F(r, h_a) / r.  Fewer than 4 list entries (self excluded),
 // tr R <= 0 or |det R| < 1e-6 (tr R / 3)^3: G / (tr R / 3) instead (0 when tr R <= 0).  R^-1 is
-// the adjugate over the determinant.  Thread per row, FP64 only (the FP32 form converts).
+// the adjugate over the determinant.  Eight lanes per row, FP64 only (the FP32 form converts).
 constexpr double SINGULAR_TOL = 1e-6;
 
 __device__ __forceinline__ double det3(const double* m) {
@@ -841,6 +841,25 @@ __device__ __forceinline__ void corrected_gradients(const double* rm, int64_t cn
   }
 }
 
+// physics/viscosity.py:83-113: xi (Balsara), alpha_loc, decay time, then the jump to alpha_loc
+// or the backward-Euler decay toward it, for the particle at output index o
+__device__ __forceinline__ void switch_update(const GradOut& out, int64_t o, double div,
+                                              double curl, double ddiv) {
+  // physics/viscosity.py:83-113: xi (Balsara), alpha_loc, decay time, the jump or the decay
+  const double d2 = div * div, cc2 = curl * curl;
+  const double xi = d2 + cc2 > 0.0 ? d2 / (d2 + cc2) : 0.0;
+  const double mdd = -ddiv < 0.0 ? 0.0 : -ddiv;  // max(-d(div v)/dt, 0); NaN stays NaN
+  const double h = out.h[o], cs = out.cs[o];
+  const double al = 10.0 * h * h * (xi * mdd) / (cs * cs);
+  const double a_loc = al > 1.0 ? 1.0 : al;  // min(alpha_loc, alpha_max = 1)
+  const double dt =
+      out.n_beg ? 2.0 * (0.5 * (double)(out.n_end[o] - out.n_beg[o]) * out.tick) : out.dt;
+  const double tau = h / (0.1 * cs);
+  const double alpha = out.alpha[o];
+  const double decayed = (alpha + a_loc * dt / tau) / (1.0 + dt / tau);
+  out.alpha[o] = a_loc > alpha ? a_loc : decayed;
+}
+
 template <typename I, bool ACC>
 __global__ void __launch_bounds__(NB_THREADS)
     k_gradients(int64_t nrows, const int64_t* __restrict__ rows, Pos64 geo,
@@ -849,11 +868,18 @@ __global__ void __launch_bounds__(NB_THREADS)
                 const double4* __restrict__ acc,    // (ax, ay, az, -), with ACC
                 const int64_t* __restrict__ off, const I* __restrict__ idx, GradParams prm,
                 const int32_t* __restrict__ out_map, GradOut out) {
-  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= nrows) return;
-  const int64_t a = rows ? rows[q] : q;
-  const int64_t o = out_map ? (int64_t)out_map[a] : q;
-  if (!rows && prm.mask && !prm.mask[o]) return;
+  const unsigned FULL = 0xffffffffu;
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t q = t >> 3;
+  const int gl = (int)(t & 7);
+  bool live = q < nrows;
+  int64_t a = 0, o = 0;
+  if (live) {
+    a = rows ? rows[q] : q;
+    o = out_map ? (int64_t)out_map[a] : q;
+    if (!rows && prm.mask && !prm.mask[o]) live = false;
+  }
+  if (!__any_sync(FULL, live)) return;  // warp-uniform
   const double4 va = vm[a];
   const double h_a = hydro[a].x;
   double4 aa = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -865,9 +891,11 @@ __global__ void __launch_bounds__(NB_THREADS)
     g[0][e] = 0.0;
     if (ACC) g[ACC ? 1 : 0][e] = 0.0;
   }
-  int64_t cnt = 0;
-  const int64_t e1 = off[a + 1];
-  for (int64_t k = off[a]; k < e1; ++k) {
+  int cnt = 0;
+  // eight lanes per row, each taking every eighth list entry; the sums are then added over
+  // the row's lanes
+  const int64_t e0 = live ? off[a] : 0, e1 = live ? off[a + 1] : 0;
+  for (int64_t k = e0 + gl; k < e1; k += 8) {
     const int64_t b = (int64_t)ld_stream(idx + k);
     if (b == a) continue;
     double ddx, ddy, ddz;
@@ -901,6 +929,17 @@ __global__ void __launch_bounds__(NB_THREADS)
         if (ACC) g[ACC ? 1 : 0][3 * i + j] += da[i] * gj;
       }
   }
+#pragma unroll
+  for (int of = 4; of > 0; of >>= 1) {
+    cnt += __shfl_xor_sync(FULL, cnt, of);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      rm[e] += __shfl_xor_sync(FULL, rm[e], of);
+      g[0][e] += __shfl_xor_sync(FULL, g[0][e], of);
+      if (ACC) g[ACC ? 1 : 0][e] += __shfl_xor_sync(FULL, g[ACC ? 1 : 0][e], of);
+    }
+  }
+  if (!live || gl != 0) return;
   corrected_gradients<ACC ? 2 : 1>(rm, cnt, g);
   const double* dv = g[0];
   if (out.gv) {
@@ -921,20 +960,126 @@ __global__ void __launch_bounds__(NB_THREADS)
   if (out.div) out.div[o] = div;
   if (out.curl) out.curl[o] = curl;
   if (out.ddiv) out.ddiv[o] = ddiv;
-  if (out.alpha) {
-    // physics/viscosity.py:83-113: xi (Balsara), alpha_loc, decay time, the jump or the decay
-    const double d2 = div * div, cc2 = curl * curl;
-    const double xi = d2 + cc2 > 0.0 ? d2 / (d2 + cc2) : 0.0;
-    const double mdd = -ddiv < 0.0 ? 0.0 : -ddiv;  // max(-d(div v)/dt, 0); NaN stays NaN
-    const double h = out.h[o], cs = out.cs[o];
-    const double al = 10.0 * h * h * (xi * mdd) / (cs * cs);
-    const double a_loc = al > 1.0 ? 1.0 : al;  // min(alpha_loc, alpha_max = 1)
-    const double dt =
-        out.n_beg ? 2.0 * (0.5 * (double)(out.n_end[o] - out.n_beg[o]) * out.tick) : out.dt;
-    const double tau = h / (0.1 * cs);
-    const double alpha = out.alpha[o];
-    const double decayed = (alpha + a_loc * dt / tau) / (1.0 + dt / tau);
-    out.alpha[o] = a_loc > alpha ? a_loc : decayed;
+  if (out.alpha) switch_update(out, o, div, curl, ddiv);
+}
+
+// The switch and the reconstruction's gradients of a step in one walk of the cached lists
+// (sorted order).  A list entry adds to R, G (and the acceleration sum) only where
+// F(r, h_a) != 0, i.e. r / h_a < 2, and such an entry always passes the tightening test
+// (r < 2 h_a <= 2 max(h_a, h_b)); the other entries add exact zeros.  So the sums over a row's
+// tightened list (the switch, and the reconstruction of shared steps) and over its untightened
+// list (the reconstruction of block steps) are the same sums over the same nonzero terms in
+// the same order, and only the entry counts of the singular-matrix test differ: both are kept.
+//   live: particles whose gradient the reconstruction needs (mask, caller order; null = all),
+//         or none without it; rows: the switch's rows (sorted mask; null = no switch)
+template <typename I, bool SW>
+__global__ void __launch_bounds__(NB_THREADS)
+    k_shock_grad(int64_t n, Pos64 geo, const double4* __restrict__ vm,
+                 const double4* __restrict__ hydro, const double4* __restrict__ acc,
+                 const int64_t* __restrict__ off, const I* __restrict__ idx, int kid,
+                 double cnorm, int recon, int recon_full, const uint8_t* __restrict__ live_mask,
+                 const uint8_t* __restrict__ row_sorted, const int32_t* __restrict__ perm,
+                 GradOut out) {
+  const unsigned FULL = 0xffffffffu;
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t a = t >> 3;
+  const int gl = (int)(t & 7);
+  bool need_g = false, is_row = false;
+  int64_t o = 0;
+  if (a < n) {
+    o = perm[a];
+    need_g = recon && (!live_mask || live_mask[o]);
+    is_row = SW && row_sorted[a];
+  }
+  const bool live = need_g || is_row;
+  if (!__any_sync(FULL, live)) return;  // warp-uniform
+  const double4 va = vm[live ? a : 0];
+  const double h_a = hydro[live ? a : 0].x;
+  double4 aa = make_double4(0.0, 0.0, 0.0, 0.0);
+  if (SW && is_row) aa = acc[a];
+  double rm[9], gv[9], ga[SW ? 9 : 1];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) {
+    rm[e] = 0.0;
+    gv[e] = 0.0;
+    if (SW) ga[SW ? e : 0] = 0.0;
+  }
+  int cnt_f = 0, cnt_t = 0;
+  const int64_t e0 = live ? off[a] : 0, e1 = live ? off[a + 1] : 0;
+  for (int64_t k = e0 + gl; k < e1; k += 8) {
+    const int64_t b = (int64_t)ld_stream(idx + k);
+    if (b == a) continue;
+    cnt_f += 1;
+    double ddx, ddy, ddz;
+    geo.diff(a, b, ddx, ddy, ddz);  // x_b - x_a
+    const double d2 = sqdist(ddx, ddy, ddz);
+    const double h_b = hydro[b].x;
+    const double rr = 2.0 * (h_a > h_b ? h_a : h_b);
+    if (d2 < rr * rr) cnt_t += 1;
+    const double dx[3] = {-ddx, -ddy, -ddz};  // x_a - x_b
+    const double r = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+    if (!(r / h_a < 2.0)) continue;  // F(r, h_a) = 0: every term below is an exact zero
+    const double f = dwdr<double>(r, h_a, kid, cnorm) / r;
+    const double4 vb = vm[b];
+    const double dv[3] = {vb.x - va.x, vb.y - va.y, vb.z - va.z};
+    double da[3] = {0.0, 0.0, 0.0};
+    if (SW && is_row) {
+      const double4 ab = acc[b];
+      da[0] = ab.x - aa.x;
+      da[1] = ab.y - aa.y;
+      da[2] = ab.z - aa.z;
+    }
+    const double mf = vb.w * f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const double gj = mf * dx[j];
+        rm[3 * i + j] -= dx[i] * gj;
+        gv[3 * i + j] += dv[i] * gj;
+        if (SW) ga[SW ? 3 * i + j : 0] += da[i] * gj;
+      }
+  }
+#pragma unroll
+  for (int of = 4; of > 0; of >>= 1) {
+    cnt_f += __shfl_xor_sync(FULL, cnt_f, of);
+    cnt_t += __shfl_xor_sync(FULL, cnt_t, of);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      rm[e] += __shfl_xor_sync(FULL, rm[e], of);
+      gv[e] += __shfl_xor_sync(FULL, gv[e], of);
+      if (SW) ga[SW ? e : 0] += __shfl_xor_sync(FULL, ga[SW ? e : 0], of);
+    }
+  }
+  if (!live || gl != 0) return;
+  if (need_g) {
+    double g1[1][9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) g1[0][e] = gv[e];
+    corrected_gradients<1>(rm, recon_full ? cnt_f : cnt_t, g1);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) out.gv[9 * a + e] = g1[0][e];
+  }
+  if (SW && is_row) {
+    double g2[2][9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      g2[0][e] = gv[e];
+      g2[1][e] = ga[SW ? e : 0];
+    }
+    corrected_gradients<2>(rm, cnt_t, g2);
+    const double* dvm = g2[0];
+    const double* dam = g2[1];
+    const double div = dvm[0] + dvm[4] + dvm[8];
+    const double c0 = dvm[7] - dvm[5], c1 = dvm[2] - dvm[6], c2 = dvm[3] - dvm[1];
+    const double curl = sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+    double sdd = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) sdd += dvm[3 * i + j] * dvm[3 * j + i];
+    const double ddiv = dam[0] + dam[4] + dam[8] - sdd;
+    switch_update(out, o, div, curl, ddiv);
   }
 }
 

@@ -274,9 +274,10 @@ NB_API int nb_density_noalloc(int64_t n, const double* pos, const double* mass,
 NB_API const char* nb_noalloc_last_error(void);
 
 /* Live kernel timing with CUDA events on the launching stream: nb_profile(ctx, 1) resets and
- * starts, nb_profile_read fills out[32] = for each of {list build, density, forces, gravity
- * flow, touched-set marks, level choice (limiter, wake-up, opening), cooling, equation of state}:
- * (milliseconds, launches, rows or particles processed, pair evaluations). */
+ * starts, nb_profile_read fills out[36] = for each of {list build, density, forces, gravity
+ * flow, touched-set marks, level choice (limiter, wake-up, opening), cooling, equation of state,
+ * gradients (switch and reconstruction)}: (milliseconds, launches, rows or particles processed,
+ * pair evaluations). */
 NB_API int nb_profile(nb_ctx* ctx, int on);
 NB_API int nb_profile_read(nb_ctx* ctx, double* out);
 
