@@ -90,6 +90,13 @@ _SIGS = {
                             _vp, _vp, _vp]),
     "nb_velocity_gradients": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _int,
                                      _vp, _vp]),
+    "nb_deposit_log": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _int,
+                              _int, _int, _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "nb_deposit_box": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _int,
+                              _int, _vp, _vp, _vp, _vp]),
+    "nb_grid_finish": (_int, [_vp, _i64, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "nb_refine_sums": (_int, [_vp, _vp, _vp, _int, _int, _int, _vp, _int, _int, _int, _int, _int,
+                              _int, _vp, _vp]),
     "nb_disc_forces": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _dbl, _vp, _vp,
                               _i64, _vp, _int, _vp, _vp, _vp]),
     "nb_glf_step_many": (_int, [_vp, _i64, _vp, _vp, _vp, _dbl, _vp, _vp, _vp, _vp]),

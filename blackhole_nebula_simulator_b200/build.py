@@ -31,6 +31,7 @@ SOURCES = {
     "capi.cu": False,
     "noalloc.cu": False,
     "mlp.cu": True,
+    "deposit.cu": False,
 }
 
 

@@ -6,6 +6,7 @@
 #include "../../include/nebula_b200.h"
 #include "common.cuh"
 #include "cooling.cuh"
+#include "deposit.cuh"
 #include "engine.cuh"
 #include "eos.cuh"
 #include "gravity.cuh"
@@ -444,6 +445,88 @@ int nb_eos(nb_ctx* ctx, int64_t n, const double* rho, const double* u, const nb_
         n, rho, u, nbk::eos_of(prm), P, c_s, T, beta, E.d_err);
   NB_CUDA(cudaGetLastError());
   return nbk::check_device_error(E, S(stream));
+}
+
+// ---------------------------------------------------------------- grid deposition
+static int deposit_finish_host(nbk::Engine& E, double* outside, int64_t* n_trilinear,
+                               cudaStream_t st) {
+  NB_CUDA(cudaGetLastError());
+  NB_CUDA(cudaMemcpyAsync(outside, E.ws.d_scal, sizeof(double), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaMemcpyAsync(n_trilinear, E.ws.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  return 0;
+}
+
+int nb_deposit_log(nb_ctx* ctx, int64_t n, const double* x, const double* h, const double* m,
+                   const double* t, const double* v, double r_min, double dlnr, double dth,
+                   double dph, int nr, int nth, int nph, int kernel_id, const double* sth,
+                   const double* cth, const double* dcth, const double* cph, const double* sph,
+                   double* acc, double* outside, int64_t* n_trilinear, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (kernel_id != 0 && kernel_id != 1) return nbk::set_host_error(E, "bad kernel_id"), NB_ERR_INPUT;
+  if (nr < 1 || nth < 2 || nph < 1 || !(r_min > 0.0) || !(dlnr > 0.0))
+    return nbk::set_host_error(E, "bad log-spherical grid"), NB_ERR_INPUT;
+  if (!outside || !n_trilinear) return nbk::set_host_error(E, "outputs missing"), NB_ERR_INPUT;
+  cudaStream_t st = S(stream);
+  NB_TRY(E.ws.ensure(E, std::max<int64_t>(E.ws.cap, 1024)));
+  const int64_t ncell = (int64_t)nr * nth * nph;
+  NB_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * nbk::DEP_FIELDS * ncell, st));
+  NB_CUDA(cudaMemsetAsync(E.ws.d_scal, 0, sizeof(double), st));
+  NB_CUDA(cudaMemsetAsync(E.ws.d_i64, 0, sizeof(int64_t), st));
+  nbk::LogGeom g{r_min, dlnr, dth, dph, nr, nth, nph, sth, cth, dcth, cph, sph};
+  nbk::launch_deposit_log(n, x, h, m, t, v, g, kernel_id, acc, E.ws.d_scal,
+                          (unsigned long long*)E.ws.d_i64, st);
+  return deposit_finish_host(E, outside, n_trilinear, st);
+}
+
+int nb_deposit_box(nb_ctx* ctx, int64_t n, const double* x, const double* h, const double* m,
+                   const double* t, const double* v, double x0, double y0, double z0, double dx,
+                   int nb, int kernel_id, double* acc, double* outside, int64_t* n_trilinear,
+                   void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (kernel_id != 0 && kernel_id != 1) return nbk::set_host_error(E, "bad kernel_id"), NB_ERR_INPUT;
+  if (nb < 1 || !(dx > 0.0)) return nbk::set_host_error(E, "bad box"), NB_ERR_INPUT;
+  if (!outside || !n_trilinear) return nbk::set_host_error(E, "outputs missing"), NB_ERR_INPUT;
+  cudaStream_t st = S(stream);
+  NB_TRY(E.ws.ensure(E, std::max<int64_t>(E.ws.cap, 1024)));
+  const int64_t ncell = (int64_t)nb * nb * nb;
+  NB_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * nbk::DEP_FIELDS * ncell, st));
+  NB_CUDA(cudaMemsetAsync(E.ws.d_scal, 0, sizeof(double), st));
+  NB_CUDA(cudaMemsetAsync(E.ws.d_i64, 0, sizeof(int64_t), st));
+  nbk::launch_deposit_box(n, x, h, m, t, v, x0, y0, z0, dx, nb, kernel_id, acc, E.ws.d_scal,
+                          (unsigned long long*)E.ws.d_i64, st);
+  return deposit_finish_host(E, outside, n_trilinear, st);
+}
+
+int nb_grid_finish(nb_ctx* ctx, int64_t ncell, const double* acc, const double* vol,
+                   int64_t cells_per_volume, double* mass, float* rho, float* t_mass,
+                   float* t_em, float* vel, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (cells_per_volume < 1) return nbk::set_host_error(E, "bad volume layout"), NB_ERR_INPUT;
+  nbk::launch_grid_finish(ncell, acc, vol, cells_per_volume, mass, rho, t_mass, t_em, vel,
+                          S(stream));
+  NB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int nb_refine_sums(nb_ctx* ctx, const double* acc_c, const double* vol_c, int nrc, int nthc,
+                   int nphc, const double* vol_f, int nr, int nth, int nph, int cr, int ct,
+                   int cp, double* out, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (cr < 1 || ct < 1 || cp < 1 || nrc < 1 || nthc < 1 || nphc < 1 || nrc * cr != nr ||
+      nthc * ct != nth || nphc * cp != nph)
+    return nbk::set_host_error(E, "coarse grid does not divide the fine grid"), NB_ERR_INPUT;
+  cudaStream_t st = S(stream);
+  NB_TRY(E.ws.ensure(E, std::max<int64_t>(E.ws.cap, 1024)));
+  NB_CUDA(cudaMemsetAsync(E.ws.d_scal, 0, 2 * sizeof(double), st));
+  nbk::launch_refine_sums(acc_c, vol_c, nrc, nthc, nphc, vol_f, nr, nth, nph, cr, ct, cp, out,
+                          E.ws.d_scal, st);
+  NB_CUDA(cudaGetLastError());
+  return 0;
 }
 
 int nb_ledger(nb_ctx* ctx, int64_t n, const double* x, const double* p, const double* u,

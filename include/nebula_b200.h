@@ -273,6 +273,40 @@ NB_API int nb_density_noalloc(int64_t n, const double* pos, const double* mass,
                               int64_t* iters, int64_t* flags, void* stream);
 NB_API const char* nb_noalloc_last_error(void);
 
+/* ---------------------------------------------------------------- grid deposition
+ * Particle -> render grid deposition (render/gasgrid.py:316-597): fields (m, m T, m T^4, m v)
+ * of each particle to the cells whose centres lie inside its support, weights f(q) V_c
+ * normalised to 1, or trilinear weights when fewer than 8 centres are inside; acc (cells x 6,
+ * cell index (i * nth + j) * nph + k, zeroed by the call) receives the sums, *outside the mass
+ * beyond the grid and *n_trilinear the fallback count (the call synchronises its stream).
+ * nb_deposit_log: the log-spherical grid (render/gasgrid.py:52-83) with its theta / phi
+ * cell-centre tables sin th_j, cos th_j, cos th_j1 - cos th_j2, cos ph_k, sin ph_k
+ * (render/gasgrid.py:688-692); kernel_id 0 cubic, 1 Wendland C4. */
+NB_API int nb_deposit_log(nb_ctx* ctx, int64_t n, const double* x, const double* h,
+                   const double* m, const double* t, const double* v, double r_min, double dlnr,
+                   double dth, double dph, int nr, int nth, int nph, int kernel_id,
+                   const double* sth, const double* cth, const double* dcth, const double* cph,
+                   const double* sph, double* acc, double* outside, int64_t* n_trilinear,
+                   void* stream);
+/* nb_deposit_box: a Cartesian box of nb^3 cells of edge dx from the corner (x0, y0, z0)
+ * (render/gasgrid.py:534-597, 811-825). */
+NB_API int nb_deposit_box(nb_ctx* ctx, int64_t n, const double* x, const double* h,
+                   const double* m, const double* t, const double* v, double x0, double y0,
+                   double z0, double dx, int nb, int kernel_id, double* acc, double* outside,
+                   int64_t* n_trilinear, void* stream);
+/* _finish (render/gasgrid.py:293-313): mass (float64), rho, mass-weighted T, emission-weighted
+ * T and mass-weighted v (float32) per cell from acc; vol[cell / cells_per_volume] is a cell's
+ * volume (nph for the log grid's (nr, nth) volumes, ncell for a box's single volume). */
+NB_API int nb_grid_finish(nb_ctx* ctx, int64_t ncell, const double* acc, const double* vol,
+                   int64_t cells_per_volume, double* mass, float* rho, float* t_mass,
+                   float* t_em, float* vel, void* stream);
+/* refine_sums (render/gasgrid.py:757-788): coarse log-grid sums (nrc, nthc, nphc, 6) with
+ * their (nrc, nthc) volumes -> fine sums (nr, nth, nph, 6) written to out, rescaled to the
+ * coarse mass; the coarsening (cr, ct, cp) must divide the fine grid. */
+NB_API int nb_refine_sums(nb_ctx* ctx, const double* acc_c, const double* vol_c, int nrc,
+                   int nthc, int nphc, const double* vol_f, int nr, int nth, int nph, int cr,
+                   int ct, int cp, double* out, void* stream);
+
 /* Live kernel timing with CUDA events on the launching stream: nb_profile(ctx, 1) resets and
  * starts, nb_profile_read fills out[36] = for each of {list build, density, forces, gravity
  * flow, touched-set marks, level choice (limiter, wake-up, opening), cooling, equation of state,

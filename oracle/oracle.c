@@ -926,3 +926,288 @@ void or_gasrad_temperature(int64_t n, const double* rho, const double* u, double
     out[i] = exp(lt);
   }
 }
+
+/* ------------------------------------------------------------------ grid deposition
+ * render/gasgrid.py:316-532 (_nb_log_kernel_pass, _nb_log_deposit_chunk) and 534-597
+ * (_nb_box_deposit_chunk): each particle's fields vals (6 per particle: m, m T, m T^4, m v)
+ * go to the cells whose centres lie inside its support (q < 2), weighted by f(q) V_c and
+ * normalised; fewer than 8 such centres: trilinear weights in index space.  Particles are dealt
+ * to nchunk chunks in turn (p -> chunk p mod nchunk) into separate grids, summed in order, as
+ * the reference does (render/gasgrid.py:660-676). */
+#define DEP_FIELDS 6
+#define DEP_MIN_CELLS 8
+#define DEP_INNER_VIRTUAL 64
+
+static double dep_kernel_f(double q, int kid) {
+  if (q >= 2.0) return 0.0;
+  if (kid == 0) {
+    if (q < 1.0) return 1.0 - 1.5 * q * q + 0.75 * q * q * q;
+    double t = 2.0 - q;
+    return 0.25 * t * t * t;
+  }
+  double x = 1.0 - 0.5 * q;
+  double x2 = x * x;
+  return x2 * x2 * x2 * (35.0 / 12.0 * q * q + 3.0 * q + 1.0);
+}
+
+typedef struct {
+  double r_min, dlnr, dth, dph;
+  int nr, nth, nph;
+  const double *sth, *cth, *dcth, *cph, *sph;
+} dep_log_grid;
+
+/* one pass over the centres inside the support; mode 0 counts and sums f V, mode 1 adds */
+static void dep_log_pass(const dep_log_grid* g, double xp, double yp, double zp, double rr,
+                         double th, double ph, double hp, int i_lo, int i_hi, int kid, int mode,
+                         double inv, const double* vals, double m, double* acc, double* wsum,
+                         int64_t* n_in, double* outside) {
+  double big = 2.0 * hp;
+  double ct0 = cos(th), st0 = sin(th);
+  for (int i = i_lo; i <= i_hi; ++i) {
+    double rc = g->r_min * exp((i + 0.5) * g->dlnr);
+    double cos_a = (rc * rc + rr * rr - big * big) / (2.0 * rc * rr);
+    if (cos_a > 1.0) continue;
+    int j0, j1;
+    if (cos_a <= -1.0) {
+      j0 = 0;
+      j1 = g->nth - 1;
+    } else {
+      double a = acos(cos_a);
+      j0 = (int)floor((th - a) / g->dth) - 1;
+      if (j0 < 0) j0 = 0;
+      j1 = (int)floor((th + a) / g->dth) + 1;
+      if (j1 > g->nth - 1) j1 = g->nth - 1;
+    }
+    double r1 = g->r_min * exp(i * g->dlnr);
+    double r2 = r1 * exp(g->dlnr);
+    double vr = (r2 * r2 * r2 - r1 * r1 * r1) / 3.0;
+    int ing = 0 <= i && i < g->nr;
+    for (int j = j0; j <= j1; ++j) {
+      double ss = st0 * g->sth[j];
+      int full = 1;
+      int k0 = 0, k1 = g->nph - 1;
+      if (ss > 1e-300 && cos_a > -1.0) {
+        double cd = (cos_a - ct0 * g->cth[j]) / ss;
+        if (cd > 1.0 + 1e-12) continue;
+        if (cd > -1.0) {
+          double dp = acos(fmin(cd, 1.0));
+          k0 = (int)ceil((ph - dp) / g->dph - 0.5) - 1;
+          k1 = (int)floor((ph + dp) / g->dph - 0.5) + 1;
+          if (k1 - k0 + 1 < g->nph) full = 0;
+        }
+      }
+      if (full) {
+        k0 = 0;
+        k1 = g->nph - 1;
+      }
+      double rst = rc * g->sth[j];
+      double dzc = rc * g->cth[j] - zp;
+      double vrt = vr * g->dcth[j] * g->dph;
+      for (int kk = k0; kk <= k1; ++kk) {
+        int k = ((kk % g->nph) + g->nph) % g->nph;
+        double dxc = rst * g->cph[k] - xp;
+        double dyc = rst * g->sph[k] - yp;
+        double q = sqrt(dxc * dxc + dyc * dyc + dzc * dzc) / hp;
+        if (q < 2.0) {
+          if (mode == 0) {
+            *n_in += 1;
+            *wsum += dep_kernel_f(q, kid) * vrt;
+          } else {
+            double w = dep_kernel_f(q, kid) * vrt * inv;
+            if (ing) {
+              double* c = acc + (((int64_t)i * g->nth + j) * g->nph + k) * DEP_FIELDS;
+              for (int f = 0; f < DEP_FIELDS; ++f) c[f] += w * vals[f];
+            } else {
+              *outside += w * m;
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+static double py_mod(double a, double b) {  /* Python's a % b for b > 0 */
+  double r = fmod(a, b);
+  if (r != 0.0 && r < 0.0) r += b;
+  return r;
+}
+
+static int py_imod(int a, int b) { return ((a % b) + b) % b; }
+
+void or_deposit_log(int64_t n, const double* x, const double* h, const double* m,
+                    const double* vals, double r_min, double dlnr, double dth, double dph, int nr,
+                    int nth, int nph, int kid, const double* sth, const double* cth,
+                    const double* dcth, const double* cph, const double* sph, int nchunk,
+                    double* acc, double* outside_out, int64_t* n_tri_out) {
+  dep_log_grid g = {r_min, dlnr, dth, dph, nr, nth, nph, sth, cth, dcth, cph, sph};
+  const int64_t ncell = (int64_t)nr * nth * nph * DEP_FIELDS;
+  double* part = (double*)calloc((size_t)ncell * nchunk, sizeof(double));
+  double outside = 0.0;
+  int64_t n_tri = 0;
+  double lnr0 = log(r_min);
+  double two_pi = 2.0 * 3.141592653589793;
+  for (int c = 0; c < nchunk; ++c) {
+    double* a = part + ncell * c;
+    double out_c = 0.0;
+    for (int64_t p = c; p < n; p += nchunk) {
+      double xp = x[3 * p], yp = x[3 * p + 1], zp = x[3 * p + 2];
+      double rr = sqrt(xp * xp + yp * yp + zp * zp);
+      double hp = h[p];
+      double big = 2.0 * hp;
+      int i_hi = (int)floor((log(rr + big) - lnr0) / dlnr);
+      int i_lo;
+      if (big >= rr) {
+        i_lo = -DEP_INNER_VIRTUAL;
+      } else {
+        i_lo = (int)floor((log(rr - big) - lnr0) / dlnr);
+        if (i_lo < -DEP_INNER_VIRTUAL) i_lo = -DEP_INNER_VIRTUAL;
+      }
+      double th = acos(fmin(1.0, fmax(-1.0, zp / rr)));
+      double ph = py_mod(atan2(yp, xp), two_pi);
+      double wsum = 0.0, dummy = 0.0;
+      int64_t n_in = 0;
+      dep_log_pass(&g, xp, yp, zp, rr, th, ph, hp, i_lo, i_hi, kid, 0, 0.0, vals + 6 * p, m[p],
+                   a, &wsum, &n_in, &dummy);
+      if (n_in >= DEP_MIN_CELLS) {
+        double o = 0.0;
+        int64_t dn = 0;
+        dep_log_pass(&g, xp, yp, zp, rr, th, ph, hp, i_lo, i_hi, kid, 1, 1.0 / wsum,
+                     vals + 6 * p, m[p], a, &dummy, &dn, &o);
+        out_c += o;
+        continue;
+      }
+      n_tri += 1;
+      double fr = log(rr / r_min) / dlnr - 0.5;
+      double fth = th / dth - 0.5;
+      double fph = ph / dph - 0.5;
+      int i0 = (int)floor(fr), j0 = (int)floor(fth), k0 = (int)floor(fph);
+      double ti = fr - i0, tj = fth - j0, tk = fph - k0;
+      if (j0 < 0) {
+        j0 = 0;
+        tj = 0.0;
+      }
+      if (j0 > nth - 2) {
+        j0 = nth - 2;
+        tj = 1.0;
+      }
+      for (int di = 0; di < 2; ++di) {
+        double wi = di == 1 ? ti : 1.0 - ti;
+        for (int dj = 0; dj < 2; ++dj) {
+          double wj = dj == 1 ? tj : 1.0 - tj;
+          for (int dk = 0; dk < 2; ++dk) {
+            double wk = dk == 1 ? tk : 1.0 - tk;
+            double w = wi * wj * wk;
+            int i = i0 + di;
+            if (0 <= i && i < nr) {
+              int k = py_imod(k0 + dk, nph);
+              double* cc = a + (((int64_t)i * nth + j0 + dj) * nph + k) * DEP_FIELDS;
+              for (int f = 0; f < DEP_FIELDS; ++f) cc[f] += w * vals[6 * p + f];
+            } else {
+              out_c += w * m[p];
+            }
+          }
+        }
+      }
+    }
+    outside += out_c;
+  }
+  for (int64_t e = 0; e < ncell; ++e) {
+    double s = part[e];
+    for (int c = 1; c < nchunk; ++c) s += part[ncell * c + e];
+    acc[e] = s;
+  }
+  free(part);
+  *outside_out = outside;
+  *n_tri_out = n_tri;
+}
+
+void or_deposit_box(int64_t n, const double* x, const double* h, const double* m,
+                    const double* vals, double x0, double y0, double z0, double dx, int nb,
+                    int kid, int nchunk, double* acc, double* outside_out, int64_t* n_tri_out) {
+  const int64_t ncell = (int64_t)nb * nb * nb * DEP_FIELDS;
+  double* part = (double*)calloc((size_t)ncell * nchunk, sizeof(double));
+  double outside = 0.0;
+  int64_t n_tri = 0;
+  for (int c = 0; c < nchunk; ++c) {
+    double* A = part + ncell * c;
+    double out_c = 0.0;
+    for (int64_t p = c; p < n; p += nchunk) {
+      double xp = x[3 * p], yp = x[3 * p + 1], zp = x[3 * p + 2];
+      double hp = h[p];
+      double big = 2.0 * hp;
+      int a0 = (int)floor((xp - big - x0) / dx), a1 = (int)floor((xp + big - x0) / dx);
+      int b0 = (int)floor((yp - big - y0) / dx), b1 = (int)floor((yp + big - y0) / dx);
+      int c0 = (int)floor((zp - big - z0) / dx), c1 = (int)floor((zp + big - z0) / dx);
+      double wsum = 0.0;
+      int64_t n_in = 0;
+      for (int a = a0; a <= a1; ++a) {
+        double dxc = x0 + (a + 0.5) * dx - xp;
+        for (int b = b0; b <= b1; ++b) {
+          double dyc = y0 + (b + 0.5) * dx - yp;
+          for (int cz = c0; cz <= c1; ++cz) {
+            double dzc = z0 + (cz + 0.5) * dx - zp;
+            double q = sqrt(dxc * dxc + dyc * dyc + dzc * dzc) / hp;
+            if (q < 2.0) {
+              n_in += 1;
+              wsum += dep_kernel_f(q, kid);
+            }
+          }
+        }
+      }
+      if (n_in >= DEP_MIN_CELLS) {
+        double inv = 1.0 / wsum;
+        for (int a = a0; a <= a1; ++a) {
+          double dxc = x0 + (a + 0.5) * dx - xp;
+          for (int b = b0; b <= b1; ++b) {
+            double dyc = y0 + (b + 0.5) * dx - yp;
+            for (int cz = c0; cz <= c1; ++cz) {
+              double dzc = z0 + (cz + 0.5) * dx - zp;
+              double q = sqrt(dxc * dxc + dyc * dyc + dzc * dzc) / hp;
+              if (q < 2.0) {
+                double w = dep_kernel_f(q, kid) * inv;
+                if (0 <= a && a < nb && 0 <= b && b < nb && 0 <= cz && cz < nb) {
+                  double* cc = A + (((int64_t)a * nb + b) * nb + cz) * DEP_FIELDS;
+                  for (int f = 0; f < DEP_FIELDS; ++f) cc[f] += w * vals[6 * p + f];
+                } else {
+                  out_c += w * m[p];
+                }
+              }
+            }
+          }
+        }
+        continue;
+      }
+      n_tri += 1;
+      double fa = (xp - x0) / dx - 0.5, fb = (yp - y0) / dx - 0.5, fc = (zp - z0) / dx - 0.5;
+      int ia = (int)floor(fa), ib = (int)floor(fb), ic = (int)floor(fc);
+      double ta = fa - ia, tb = fb - ib, tc = fc - ic;
+      for (int da = 0; da < 2; ++da) {
+        double wa = da == 1 ? ta : 1.0 - ta;
+        for (int db = 0; db < 2; ++db) {
+          double wb = db == 1 ? tb : 1.0 - tb;
+          for (int dc = 0; dc < 2; ++dc) {
+            double wc = dc == 1 ? tc : 1.0 - tc;
+            double w = wa * wb * wc;
+            int a = ia + da, b = ib + db, cz = ic + dc;
+            if (0 <= a && a < nb && 0 <= b && b < nb && 0 <= cz && cz < nb) {
+              double* cc = A + (((int64_t)a * nb + b) * nb + cz) * DEP_FIELDS;
+              for (int f = 0; f < DEP_FIELDS; ++f) cc[f] += w * vals[6 * p + f];
+            } else {
+              out_c += w * m[p];
+            }
+          }
+        }
+      }
+    }
+    outside += out_c;
+  }
+  for (int64_t e = 0; e < ncell; ++e) {
+    double s = part[e];
+    for (int c = 1; c < nchunk; ++c) s += part[ncell * c + e];
+    acc[e] = s;
+  }
+  free(part);
+  *outside_out = outside;
+  *n_tri_out = n_tri;
+}

@@ -402,6 +402,62 @@ def switch_blocks_fixture(blocks, coupled, ics, hydro_cfg):
     _save("switch_blocks.npz", **out)
 
 
+def _grid_fields(prefix, gg):
+    return {f"{prefix}_mass": gg.mass, f"{prefix}_rho": gg.rho, f"{prefix}_t_mass": gg.t_mass,
+            f"{prefix}_t_em": gg.t_em, f"{prefix}_vel": gg.vel,
+            f"{prefix}_outside": np.float64(gg.outside),
+            f"{prefix}_n_tri": np.int64(gg.n_trilinear)}  # fmt: skip
+
+
+def deposit_fixture(gasgrid):
+    """Particle -> grid deposition (render/gasgrid.py): the log-spherical grid and a Cartesian
+    box, both kernels, on seeded particles with h from 0.1 to 10 local cells, including
+    particles beyond the outer radius, on the phi seam and near both poles; the split
+    deposition with half the particles wide."""
+    rng = np.random.default_rng(SEED + 9)
+    g = gasgrid.LogSphericalGrid(r_min=2.0, r_max=200.0, nr=24, nth=12, nph=24)
+    n = 400
+    lnr = rng.uniform(np.log(2.5), np.log(240.0), n)
+    r = np.exp(lnr)
+    cth = rng.uniform(-1.0, 1.0, n)
+    cth[:25] = 1.0 - rng.uniform(0.0, 0.004, 25)  # near the north pole
+    cth[25:50] = -1.0 + rng.uniform(0.0, 0.004, 25)  # near the south pole
+    ph = rng.uniform(0.0, 2.0 * np.pi, n)
+    ph[50:90] = rng.uniform(-0.04, 0.04, 40) % (2.0 * np.pi)  # on the seam
+    sth = np.sqrt(1.0 - cth * cth)
+    x = np.c_[r * sth * np.cos(ph), r * sth * np.sin(ph), r * cth]
+    h = r * g.dlnr * np.exp(rng.uniform(np.log(0.1), np.log(10.0), n))
+    m = rng.uniform(0.3, 3.0, n)
+    t = np.exp(rng.uniform(np.log(3e3), np.log(3e7), n))
+    v = rng.normal(0.0, 0.05, (n, 3))
+    out = dict(x=x, h=h, m=m, t=t, v=v, log_grid=np.array([g.r_min, g.r_max, g.nr, g.nth, g.nph]))
+    for kern in ("wendland_c4", "cubic"):
+        out.update(_grid_fields(f"log_{kern}", gasgrid.deposit_log(x, h, m, t, v, g, kern)))
+    b = gasgrid.CartesianBox(centre=(20.0, -10.0, 5.0), size=80.0, n=20)
+    xb = np.asarray(b.centre) + rng.uniform(-0.6, 0.6, (n, 3)) * b.size
+    hb = b.dx * np.exp(rng.uniform(np.log(0.1), np.log(10.0), n))
+    out.update(xb=xb, hb=hb, box=np.array([*b.centre, b.size, b.n]))
+    for kern in ("wendland_c4", "cubic"):
+        out.update(_grid_fields(f"box_{kern}", gasgrid.deposit_box(xb, hb, m, t, v, b, kern)))
+    # split: a coarser-divisible grid, half the particles wide
+    gs = gasgrid.LogSphericalGrid(r_min=2.0, r_max=2000.0, nr=32, nth=16, nph=32)
+    ns = 1200
+    rs = np.exp(rng.uniform(np.log(30.0), np.log(600.0), ns))
+    d = rng.normal(size=(ns, 3))
+    xs = rs[:, None] * d / np.linalg.norm(d, axis=1, keepdims=True)
+    hs = np.where(np.arange(ns) < ns // 2, 0.2, 3.0) * rs
+    ms = np.full(ns, 1e-4)
+    ts = rng.uniform(1e4, 1e5, ns)
+    vs = rng.normal(0.0, 0.01, (ns, 3))
+    out.update(xs=xs, hs=hs, ms=ms, ts=ts, vs=vs,
+               split_grid=np.array([gs.r_min, gs.r_max, gs.nr, gs.nth, gs.nph]),
+               split_wide=gasgrid.wide_particles(xs, hs, gs))  # fmt: skip
+    sp = gasgrid.deposit_log_split(xs, hs, ms, ts, vs, gs)
+    out.update(_grid_fields("split", sp))
+    out["split_n_wide"] = np.int64(sp.extra["n_wide"])
+    _save("deposit.npz", **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="root of the reference checkout")
@@ -415,6 +471,7 @@ def main():
     from nebula import units as units_mod
     from nebula.sim import hydro as hydro_mod
     from nebula.sim.hydro import HydroConfig
+    from nebula.render import gasgrid
 
     from blackhole_nebula_simulator_b200 import ics
 
@@ -432,6 +489,7 @@ def main():
         "shock": lambda: shock_fixture(sph, nbmod),
         "switch_coupled": lambda: switch_coupled_fixture(coupled, ics, HydroConfig),
         "switch_blocks": lambda: switch_blocks_fixture(blocks, coupled, ics, HydroConfig),
+        "deposit": lambda: deposit_fixture(gasgrid),
     }
     for name, make in makers.items():
         if not args.only or name in args.only:

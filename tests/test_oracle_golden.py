@@ -372,3 +372,73 @@ def test_switch_block_steps_match_reference():
     check("final e_radiated", float(g["final_e_radiated"]), st.e_radiated, rtol=1e-9)
     check("cache builds", int(g["builds"]), st.neighbour_cache.builds)
     check("cache reuses", int(g["reuses"]), st.neighbour_cache.reuses)
+
+
+def _dep_grids(g):
+    from blackhole_nebula_simulator_b200.gasgrid import CartesianBox, LogSphericalGrid
+
+    lg = LogSphericalGrid(r_min=float(g["log_grid"][0]), r_max=float(g["log_grid"][1]),
+                          nr=int(g["log_grid"][2]), nth=int(g["log_grid"][3]),
+                          nph=int(g["log_grid"][4]))  # fmt: skip
+    bx = CartesianBox(centre=tuple(float(c) for c in g["box"][:3]), size=float(g["box"][3]),
+                      n=int(g["box"][4]))  # fmt: skip
+    sg = LogSphericalGrid(r_min=float(g["split_grid"][0]), r_max=float(g["split_grid"][1]),
+                          nr=int(g["split_grid"][2]), nth=int(g["split_grid"][3]),
+                          nph=int(g["split_grid"][4]))  # fmt: skip
+    return lg, bx, sg
+
+
+def _check_grid(name, g, prefix, res, exact=False):
+    tol = {} if exact else {"rtol": 1e-12}
+    scale = np.abs(g[f"{prefix}_mass"]).max()
+    if exact:
+        check(f"{name} mass", g[f"{prefix}_mass"], res["mass"])
+    else:
+        check(f"{name} mass", g[f"{prefix}_mass"] / scale, res["mass"] / scale, atol=1e-12)
+    check(f"{name} outside", float(g[f"{prefix}_outside"]), res["outside"], **tol)
+    check(f"{name} trilinear count", int(g[f"{prefix}_n_tri"]), res["n_trilinear"])
+    for f in ("rho", "t_mass", "t_em", "vel"):
+        a = g[f"{prefix}_{f}"].astype(np.float64)
+        check(f"{name} {f}", a, res[f].astype(np.float64), atol=1e-6 * float(np.abs(a).max()))
+
+
+@pytest.mark.parametrize("kernel", ["wendland_c4", "cubic"])
+def test_log_deposition_matches_reference(kernel):
+    from oracle import deposit as odep
+
+    g = golden("deposit.npz")
+    lg, _, _ = _dep_grids(g)
+    res = odep.deposit_log(g["x"], g["h"], g["m"], g["t"], g["v"], lg, kernel)
+    _check_grid(f"log {kernel}", g, f"log_{kernel}", res, exact=True)
+
+
+@pytest.mark.parametrize("kernel", ["wendland_c4", "cubic"])
+def test_box_deposition_matches_reference(kernel):
+    from oracle import deposit as odep
+
+    g = golden("deposit.npz")
+    _, bx, _ = _dep_grids(g)
+    res = odep.deposit_box(g["xb"], g["hb"], g["m"], g["t"], g["v"], bx, kernel)
+    _check_grid(f"box {kernel}", g, f"box_{kernel}", res, exact=True)
+
+
+def test_split_deposition_matches_reference():
+    from blackhole_nebula_simulator_b200.gasgrid import coarse_log_grid
+    from oracle import deposit as odep
+
+    g = golden("deposit.npz")
+    _, _, sg = _dep_grids(g)
+    check("wide particles", g["split_wide"], odep.wide_particles(g["xs"], g["hs"], sg))
+    res = odep.deposit_log_split(g["xs"], g["hs"], g["ms"], g["ts"], g["vs"], sg,
+                                 coarse_log_grid(sg))  # fmt: skip
+    check("wide count", int(g["split_n_wide"]), res["n_wide"])
+    _check_grid("split", g, "split", res)
+
+
+def test_log_grid_volumes_fill_the_shell():
+    """Cell volumes add up to the shell volume 4/3 pi (r_max^3 - r_min^3)."""
+    from blackhole_nebula_simulator_b200.gasgrid import LogSphericalGrid
+
+    g = LogSphericalGrid(r_min=2.0, r_max=200.0, nr=24, nth=12, nph=24)
+    check("sum of cell volumes", 4.0 / 3.0 * np.pi * (g.r_max**3 - g.r_min**3),
+          g.volumes().sum() * g.nph, rtol=1e-12)  # fmt: skip
