@@ -351,13 +351,140 @@ def cpu_reference(args, steps, warmup, sample_n=None):
             f"{cores} OpenMP threads"}  # fmt: skip
 
 
+# deposition frame: the 4M torus snapshot onto the reference's default log-spherical render grid
+# (192 x 96 x 192, wide particles through the coarse grid; its cells are wider than the torus
+# particles' kernels, so they take the trilinear weights) and a detail box of 160^3 cells of
+# 0.4 across the torus' ring at x = 100 (kernel weights over ~4^3 cells per particle)
+DEPOSIT_BOX = dict(centre=(100.0, 0.0, 0.0), size=64.0, n=160)
+
+
+def deposit_inputs(n, seed=4):
+    from blackhole_nebula_simulator_b200 import ics, units
+
+    ic = ics.torus(n, seed=seed)
+    t = ic.u / units.gas_u_from_temperature(1.0)  # the ideal-gas temperature of u (linear in T)
+    return ic.x, ic.h, ic.mass, t, ic.v
+
+
+def deposit_frame(gg, x, h, m, t, v, grid, box, host=False):
+    a = gg.deposit_log_split(x, h, m, t, v, grid)
+    b = gg.deposit_box(x, h, m, t, v, box)
+    if host:  # the renderer's float32 fields and the ledgers back on the host
+        return [f.cpu() for f in (a.rho, a.t_mass, a.t_em, a.vel, b.rho, b.t_mass, b.t_em, b.vel)]
+    return a, b
+
+
+def cpu_deposit(n_sample):
+    """The reference's deposition on the host cores: the oracle (C, one thread, the reference's
+    two fixed chunks one after the other) on the first n_sample particles of the frame."""
+    from blackhole_nebula_simulator_b200 import gasgrid as gg
+    from oracle import deposit as odep
+
+    x, h, m, t, v = deposit_inputs(n_sample)
+    grid, box = gg.LogSphericalGrid(), gg.CartesianBox(**DEPOSIT_BOX)
+    t0 = time.perf_counter()
+    odep.deposit_log_split(x, h, m, t, v, grid, gg.coarse_log_grid(grid))
+    odep.deposit_box(x, h, m, t, v, box)
+    dt = time.perf_counter() - t0
+    return {"value": n_sample / dt, "unit": "particles/s", "cores": 1, "kind": "port",
+            "sample": f"torus snapshot, {n_sample} particles, one frame (log-spherical 192x96x192 "
+                      "split + 160^3 box), oracle in C on one thread"}  # fmt: skip
+
+
+def run_deposit(args, rank, world):
+    """One step = one render frame's deposition of the whole snapshot (inputs resident)."""
+    import torch
+
+    from blackhole_nebula_simulator_b200 import _lib
+    from blackhole_nebula_simulator_b200 import gasgrid as gg
+    from blackhole_nebula_simulator_b200.device import ctx
+
+    n = args.n or 4_194_304
+    config = {"workload": f"deposit: torus snapshot, {n} particles -> log-spherical grid "
+                          "192x96x192 (wide particles on the coarse grid) + 160^3 box",
+              "particles": n, "l2_flush": "inputs and grids larger than L2",
+              "parallelism": f"replicas x{world}"}  # fmt: skip
+    metric = "particles deposited/s"
+    if args.impl == "reference":
+        if rank == 0:
+            cb = cpu_deposit(min(n, 16_384))
+            print(json.dumps({"metric": metric, "value": cb["value"], "unit": "particles/s",
+                              "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                              "higher_is_better": True, "impl": "reference", "dtype": "f64",
+                              "data": "synthetic", "config": config, "cpu_baseline": cb,
+                              "e2e": {"value": cb["value"], "unit": "particles/s",
+                                      "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))  # fmt: skip
+        return
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    xs, hs, ms, ts, vs = deposit_inputs(n, seed=4 + rank)
+    x, h, m, t, v = (torch.as_tensor(a, dtype=torch.float64, device=dev) for a in (xs, hs, ms, ts, vs))
+    grid, box = gg.LogSphericalGrid(), gg.CartesianBox(**DEPOSIT_BOX)
+    for _ in range(args.warmup):
+        deposit_frame(gg, x, h, m, t, v, grid, box)
+    stream = torch.cuda.current_stream()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches0 = _lib.lib().nb_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev.index) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            a, b = deposit_frame(gg, x, h, m, t, v, grid, box)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = _lib.lib().nb_launch_count() - launches0
+    ms_t = e0.elapsed_time(e1)
+    total = float(n * args.steps)
+    if world > 1:
+        ms_t, total = combine_ranks(ms_t, n * args.steps, dev)
+    ledger = (float(a.mass.sum()) + a.outside) / float(ms.sum())
+    # the same frames through the public API from host arrays, fields back on the host
+    pinned = [torch.as_tensor(q).pin_memory() for q in (xs, hs, ms, ts, vs)]
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        deposit_frame(gg, *[q.to(dev, non_blocking=True) for q in pinned], grid, box, host=True)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+    ncell = grid.nr * grid.nth * grid.nph + box.n**3
+    in_bytes = n * 9 * 8  # x, h, m, t, v
+    out_bytes = ncell * 6 * 4  # rho, T, T_em (float32) and v (3 x float32)
+    # roofline: algorithmic bytes of one frame (particle inputs read twice, one per grid; the
+    # 6 FP64 sums of every cell written and read back; the float32 fields and masses written)
+    alg = 2 * in_bytes + ncell * (6 * 8 * 2 + 8 + 6 * 4)
+    pk = peaks()
+    achieved = alg / (ms_t / args.steps * 1e-3) / 1e9
+    if rank == 0:
+        cb = None if args.no_cpu_baseline else cpu_deposit(min(n, 16_384))
+        print(json.dumps({
+            "metric": metric, "value": total / (ms_t * 1e-3), "unit": "particles/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_t / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded torus snapshot)",
+            "config": config,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": pk["hbm_gbs"],
+                         "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 5), "traffic": None,
+                         "peak_source": pk["source"], "bytes_per_launch": alg,
+                         "note": "scattered FP64 atomic adds, not a streaming kernel"},
+            "clocks": clk.summary(),
+            "e2e": {"value": n * args.steps / (ms_e2e * 1e-3), "unit": "particles/s",
+                    "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": out_bytes},
+            "gpu_launches": launches, "mass_ledger": ledger, "n_wide": a.extra["n_wide"],
+            "n_trilinear": [a.n_trilinear, b.n_trilinear], "cpu_baseline": cb,
+        }))  # fmt: skip
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="torus", choices=["torus", "streams", "cloud"])
+    ap.add_argument("--workload", default="torus", choices=["torus", "streams", "cloud", "deposit"])
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--shock", action="store_true",
@@ -373,6 +500,15 @@ def main():
         ap.error("--eos gasrad/radiation needs a workload without cooling: --workload cloud")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.workload == "deposit":
+        if world > 1 and args.impl == "ours":
+            import torch
+
+            torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        run_deposit(args, rank, world)
+        if world > 1 and args.impl == "ours":
+            torch.distributed.destroy_process_group()
+        return
     n_full = args.n or {"torus": 4_194_304, "streams": 1_048_576, "cloud": 262_144}[args.workload]
     config = {"workload": f"{args.workload}, {n_full} particles, block time steps",
               "particles": n_full,

@@ -191,21 +191,48 @@ __global__ void k_deposit_box(int64_t n, const double* __restrict__ x,
   const int a0 = (int)floor((xp - big - x0) / dx), a1 = (int)floor((xp + big - x0) / dx);
   const int b0 = (int)floor((yp - big - y0) / dx), b1 = (int)floor((yp + big - y0) / dx);
   const int c0 = (int)floor((zp - big - z0) / dx), c1 = (int)floor((zp + big - z0) / dx);
+  // The candidate block holds every centre with q < 2.  Two shortcuts leave the result as the
+  // full walk gives it: a row (a, b) only visits the chord of the support plus one cell each
+  // side (the other centres fail q < 2), and a distance is compared as d^2 against (2h)^2
+  // with a relative margin of 1e-12, taking sqrt(d^2) / h only inside the margin.
+  const double big2 = big * big;
+  const double in2 = big2 * (1.0 - 1e-12), out2 = big2 * (1.0 + 1e-12);
+  auto inside = [&](double dd) {
+    if (dd < in2) return true;
+    if (dd >= out2) return false;
+    return sqrt(dd) / hp < 2.0;
+  };
+  auto chord = [&](double dxy2, int& lo, int& hi) {
+    const double s = sqrt(fmax(out2 - dxy2, 0.0));
+    lo = max(c0, (int)floor((zp - s - z0) / dx) - 1);
+    hi = min(c1, (int)floor((zp + s - z0) / dx) + 1);
+  };
+  // a block wholly beyond the box puts all the particle's mass outside: only the count of
+  // centres inside the support (kernel weights or trilinear fallback) is needed
+  const bool beyond = a1 < 0 || a0 >= nb || b1 < 0 || b0 >= nb || c1 < 0 || c0 >= nb;
   double wsum = 0.0, out = 0.0;
   int n_in = 0;
   for (int a = a0; a <= a1; ++a) {
     const double dxc = x0 + (a + 0.5) * dx - xp;
     for (int b = b0; b <= b1; ++b) {
       const double dyc = y0 + (b + 0.5) * dx - yp;
-      for (int c = c0; c <= c1; ++c) {
+      const double dxy2 = dxc * dxc + dyc * dyc;
+      if (dxy2 >= out2) continue;
+      int cl, ch;
+      chord(dxy2, cl, ch);
+      for (int c = cl; c <= ch; ++c) {
         const double dzc = z0 + (c + 0.5) * dx - zp;
-        const double q = sqrt(dxc * dxc + dyc * dyc + dzc * dzc) / hp;
-        if (q < 2.0) {
+        const double dd = dxc * dxc + dyc * dyc + dzc * dzc;
+        if (inside(dd)) {
           n_in += 1;
-          wsum += kernel_f<double>(q, kid);
+          if (!beyond) wsum += kernel_f<double>(sqrt(dd) / hp, kid);
         }
       }
     }
+  }
+  if (n_in >= DEP_MIN_CELLS && beyond) {
+    atomicAdd(outside_sum, vals[0]);
+    return;
   }
   if (n_in >= DEP_MIN_CELLS) {
     const double inv = 1.0 / wsum;
@@ -213,11 +240,15 @@ __global__ void k_deposit_box(int64_t n, const double* __restrict__ x,
       const double dxc = x0 + (a + 0.5) * dx - xp;
       for (int b = b0; b <= b1; ++b) {
         const double dyc = y0 + (b + 0.5) * dx - yp;
-        for (int c = c0; c <= c1; ++c) {
+        const double dxy2 = dxc * dxc + dyc * dyc;
+        if (dxy2 >= out2) continue;
+        int cl, ch;
+        chord(dxy2, cl, ch);
+        for (int c = cl; c <= ch; ++c) {
           const double dzc = z0 + (c + 0.5) * dx - zp;
-          const double q = sqrt(dxc * dxc + dyc * dyc + dzc * dzc) / hp;
-          if (q < 2.0) {
-            const double w = kernel_f<double>(q, kid) * inv;
+          const double dd = dxc * dxc + dyc * dyc + dzc * dzc;
+          if (inside(dd)) {
+            const double w = kernel_f<double>(sqrt(dd) / hp, kid) * inv;
             if (0 <= a && a < nb && 0 <= b && b < nb && 0 <= c && c < nb)
               add_cell(acc, ((int64_t)a * nb + b) * nb + c, w, vals);
             else
