@@ -18,6 +18,7 @@ import numpy as np
 import torch
 
 from . import _lib, ops
+from .accretion import RemovedLedger, record_removal
 from .config import BlockConfig
 from .coupled import make_params
 from .device import ctx, dev_f64, dev_i64, ptr, stream, to_numpy
@@ -60,6 +61,14 @@ class BlockState:
     builds: int = 0
     reuses: int = 0
     timers: dict = field(default_factory=lambda: {"step": 0.0})
+    # removal bookkeeping (sim/blocks.py:134-139): original ids, starting radius and |L|,
+    # inward flag at the last active time, pericentre passed
+    ids: torch.Tensor = None
+    r0: torch.Tensor = None
+    L0: torch.Tensor = None
+    vr_neg: torch.Tensor = None
+    passed_peri: torch.Tensor = None
+    removed: RemovedLedger = field(default_factory=RemovedLedger)
     _params: object = field(default=None, repr=False)
     _rows: torch.Tensor = field(default=None, repr=False)
 
@@ -103,8 +112,10 @@ def _params(st: BlockState, cfg: BlockConfig):
     if st._params is None:
         if cfg.respa:
             raise NotImplementedError("RESPA gravity sub-steps are not part of the CUDA SPH path")
-        if cfg.r_acc is not None or cfg.r_escape is not None:
-            raise NotImplementedError("removal radii are not part of the CUDA SPH path")
+        if (cfg.r_acc is not None or cfg.r_escape is not None) and cfg.removal_sync:
+            raise NotImplementedError("removal with removal_sync=True (forces of the survivors "
+                                      "recomputed at the removal) is not part of the CUDA SPH "
+                                      "path; removal_sync=False is")  # fmt: skip
         if not cfg.hydro:
             raise NotImplementedError("gravity-only block steps are not part of the CUDA SPH path")
         st._params = make_params(cfg.coupled, cfg.dt_max, cfg.limiter, cfg.max_gap)
@@ -136,6 +147,11 @@ def initialise(x, v, u, mass, h_guess, cfg: BlockConfig, t_stop: float, t0: floa
         n_stop=int(round((t_stop - t0) / tick)), luminosity=z(), visc_heating=z(), nu=z(), c_s=z(),
     )  # fmt: skip
     st._rows = torch.empty(n, dtype=torch.int64, device=d)
+    st.ids = torch.arange(n, dtype=torch.int64, device=d)
+    st.r0 = torch.linalg.norm(st.x, dim=1)
+    st.L0 = torch.linalg.norm(torch.linalg.cross(st.x, st.p, dim=1), dim=1)
+    st.vr_neg = torch.sum(st.x * ops.gn_v_from_p(st.x, st.p), dim=1) < 0
+    st.passed_peri = torch.zeros(n, dtype=torch.bool, device=d)
     prm = _params(st, cfg)
     c = ctx()
     s = _state_struct(st)
@@ -155,8 +171,57 @@ def advance(st: BlockState, cfg: BlockConfig) -> torch.Tensor:
     _pull(st, s)
     na = int(s.last_active)
     st.active_counts.append(na)
+    rows = st._rows[:na].clone()
+    if cfg.r_acc is not None or cfg.r_escape is not None:
+        rows = _swallow(st, cfg, rows)
     st.timers["step"] += time.perf_counter() - t0
-    return st._rows[:na].clone()
+    return rows
+
+
+def _gn_hamiltonian(x, p):
+    """physics/gravity.py:92-102 for the few removed particles."""
+    r = torch.linalg.norm(x, dim=1)
+    a, c = (r - 2.0) / r, -2.0 * (r - 2.0) / r**4
+    px = torch.sum(p * x, dim=1)
+    return 0.5 * a * torch.sum(p * p, dim=1) + 0.5 * c * px**2 - 1.0 / r
+
+
+def _swallow(st: BlockState, cfg: BlockConfig, rows):
+    """sim/blocks.py:673-719 (_swallow, _swallow_keep, _prune; removal_sync=False): the active
+    rows' pericentre flags; those inside r_acc or beyond r_escape (their state true at their own
+    step end) go into the removed ledger and out of every per-particle array.  The engine
+    rebuilds its lists for the new particle count.  Returns the remaining rows, renumbered."""
+    rows = torch.sort(rows).values  # ascending, as the reference's rows (and so its log order)
+    x, p = st.x[rows], st.p[rows]
+    r = torch.linalg.norm(x, dim=1)
+    vr = torch.sum(x * ops.gn_v_from_p(x, p), dim=1)
+    turned = st.vr_neg[rows] & (vr > 0) & (r < 0.5 * st.r0[rows])
+    st.passed_peri[rows] |= turned
+    st.vr_neg[rows] = vr < 0
+    none = torch.zeros(len(rows), dtype=torch.bool, device=r.device)
+    acc = r < cfg.r_acc if cfg.r_acc is not None else none
+    esc = r > cfg.r_escape if cfg.r_escape is not None else none
+    gone_mask = acc | esc
+    if not bool(torch.any(gone_mask)):
+        return rows
+    for mask, reason in ((acc, "accreted"), (esc, "escaped")):
+        g = rows[mask]
+        if len(g) == 0:
+            continue
+        xs, ps = st.x[g], st.p[g]
+        h = lambda a: a.detach().cpu().numpy()  # noqa: E731
+        record_removal(st.removed, st.t, h(st.ids[g]), h(st.mass[g]), h(_gn_hamiltonian(xs, ps)),
+                       h(st.u[g]), h(torch.linalg.cross(xs, ps, dim=1)), h(ps),
+                       h(torch.linalg.norm(xs, dim=1)), h(st.passed_peri[g]), h(st.L0[g]),
+                       reason)  # fmt: skip
+    n = len(st.x)
+    keep = torch.ones(n, dtype=torch.bool, device=r.device)
+    keep[rows[gone_mask]] = False
+    for name, value in list(vars(st).items()):
+        if isinstance(value, torch.Tensor) and value.shape[:1] == (n,):
+            setattr(st, name, value[keep].contiguous())
+    new_index = torch.cumsum(keep.to(torch.int64), 0) - 1
+    return new_index[rows[keep[rows]]]
 
 
 def run(st: BlockState, cfg: BlockConfig, t_end: float, callback=None) -> BlockState:
@@ -177,11 +242,13 @@ def run(st: BlockState, cfg: BlockConfig, t_end: float, callback=None) -> BlockS
 
 
 def ledger(st: BlockState, cfg: BlockConfig) -> dict:
-    """sim/blocks.py:742-758 (no removed particles in the CUDA path)."""
+    """sim/blocks.py:742-758, the removed particles' totals included."""
     s = ops.ledger_sums(st.x, st.p, st.u, st.mass)
-    return {"energy": s["energy"] + st.e_radiated, "e_radiated": st.e_radiated,
-            "abs_h": s["abs_h"], "angmom": s["angmom"], "momentum": s["momentum"],
-            "mass": s["mass"], "removed_mass": 0.0, "removed_count": 0}  # fmt: skip
+    rm = st.removed
+    return {"energy": s["energy"] + rm.energy + st.e_radiated, "e_radiated": st.e_radiated,
+            "abs_h": s["abs_h"], "angmom": np.asarray(s["angmom"]) + rm.angmom,
+            "momentum": np.asarray(s["momentum"]) + rm.momentum, "mass": s["mass"] + rm.mass,
+            "removed_mass": rm.mass, "removed_count": rm.count}  # fmt: skip
 
 
 def diagnostics(st: BlockState) -> dict:

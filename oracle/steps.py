@@ -273,6 +273,12 @@ class BlockState:
     luminosity: np.ndarray = None
     nu: np.ndarray = None
     timers: dict = field(default_factory=lambda: {"flow": 0.0, "hydro": 0.0, "levels": 0.0})
+    ids: np.ndarray = None  # original particle numbers
+    r0: np.ndarray = None  # starting radius
+    L0: np.ndarray = None  # starting |angular momentum|
+    vr_neg: np.ndarray = None  # radial velocity < 0 at the last active time
+    passed_peri: np.ndarray = None  # has turned outward near the hole
+    removed: "RemovedLedger" = None
 
     @property
     def t(self):
@@ -450,6 +456,12 @@ def blocks_initialise(x, v, u, mass, h_guess, bc, t_stop, t0=0.0, level_offset=N
     )  # fmt: skip
     st.luminosity = np.zeros(n)
     st.nu = np.zeros(n)
+    st.ids = np.arange(n)
+    st.r0 = np.linalg.norm(x, axis=1)
+    st.L0 = np.linalg.norm(np.cross(x, p), axis=1)
+    st.vr_neg = np.sum(x * native.gn_v_from_p(x, p), axis=1) < 0
+    st.passed_peri = np.zeros(n, bool)
+    st.removed = RemovedLedger()
     rows = np.arange(n)
     nb = _hydro_rows(st, bc, rows, native.gn_v_from_p(x, p), st.u, reuse)
     st.level[:] = 0
@@ -497,7 +509,72 @@ def blocks_advance(st: BlockState, bc, reuse=True) -> np.ndarray:
     st.timers["levels"] += time.perf_counter() - t2
     st.active_counts.append(len(rows))
     st.particle_steps += len(rows)
+    if getattr(bc, "r_acc", None) is not None or getattr(bc, "r_escape", None) is not None:
+        if bc.removal_sync:
+            raise NotImplementedError("removal with removal_sync=True is not restated")
+        rows = _swallow(st, bc, rows)
     return rows
+
+
+@dataclass
+class RemovedLedger:
+    """sim/accretion.py:19-44: totals and a log of the removed particles."""
+
+    mass: float = 0.0
+    energy: float = 0.0
+    angmom: np.ndarray = field(default_factory=lambda: np.zeros(3))
+    momentum: np.ndarray = field(default_factory=lambda: np.zeros(3))
+    log: list = field(default_factory=list)
+
+    @property
+    def count(self) -> int:
+        return len(self.log)
+
+
+def _record_removal(led, t, ids, mass, ham, u, am, p, r, passed, L0, reason):
+    """sim/accretion.py:47-62."""
+    for k in range(len(ids)):
+        led.momentum = led.momentum + mass[k] * np.asarray(p[k], float)
+        led.mass += float(mass[k])
+        led.energy += float(mass[k] * (ham[k] + u[k]))
+        led.angmom = led.angmom + mass[k] * np.asarray(am[k], float)
+        led.log.append({"t": float(t), "id": int(ids[k]), "reason": reason, "r": float(r[k]),
+                        "m": float(mass[k]), "H": float(ham[k]), "u": float(u[k]),
+                        "L": float(np.linalg.norm(am[k])), "L0": float(L0[k]),
+                        "first_pass": not bool(passed[k])})  # fmt: skip
+
+
+def _swallow(st: BlockState, bc, rows):
+    """sim/blocks.py:673-719 (_swallow, _swallow_keep, _prune) for the GN hole: pericentre
+    flags of the active rows, removal of those inside r_acc or beyond r_escape (their state is
+    true at their own step end) into the ledger; returns the remaining rows, renumbered."""
+    x, p = st.x[rows], st.p[rows]
+    r = np.linalg.norm(x, axis=1)
+    vr = np.sum(x * native.gn_v_from_p(x, p), axis=1)
+    turned = st.vr_neg[rows] & (vr > 0) & (r < 0.5 * st.r0[rows])
+    st.passed_peri[rows] |= turned
+    st.vr_neg[rows] = vr < 0
+    acc = r < bc.r_acc if bc.r_acc is not None else np.zeros(len(rows), bool)
+    esc = r > bc.r_escape if bc.r_escape is not None else np.zeros(len(rows), bool)
+    if not (np.any(acc) or np.any(esc)):
+        return rows
+    for mask, reason in ((acc, "accreted"), (esc, "escaped")):
+        g = rows[mask]
+        if len(g) == 0:
+            continue
+        xs, ps = st.x[g], st.p[g]
+        _record_removal(st.removed, st.t, st.ids[g], st.mass[g], gn_hamiltonian(xs, ps), st.u[g],
+                        np.cross(xs, ps), ps, np.linalg.norm(xs, axis=1), st.passed_peri[g],
+                        st.L0[g], reason)  # fmt: skip
+    keep = np.ones(len(st.x), bool)
+    keep[rows[acc | esc]] = False
+    n = len(keep)
+    for name, value in vars(st).items():
+        if isinstance(value, np.ndarray) and value.shape[:1] == (n,):
+            setattr(st, name, value[keep])
+    st.neighbour_cache = None
+    new_index = np.cumsum(keep) - 1
+    return new_index[rows[keep[rows]]]
 
 
 def blocks_run(st: BlockState, bc, t_end, callback=None, reuse=True) -> BlockState:
@@ -520,7 +597,15 @@ def blocks_run(st: BlockState, bc, t_end, callback=None, reuse=True) -> BlockSta
 
 
 def blocks_ledger(st: BlockState, bc) -> dict:
-    return ledger_sums(st.mass, st.x, st.p, st.u, st.e_radiated)
+    """sim/blocks.py:742-758, the removed particles' totals included."""
+    led = ledger_sums(st.mass, st.x, st.p, st.u, st.e_radiated)
+    rm = st.removed
+    if rm is not None:
+        led["energy"] += rm.energy
+        led["angmom"] = led["angmom"] + rm.angmom
+        led["momentum"] = led["momentum"] + rm.momentum
+        led["mass"] += rm.mass
+    return led
 
 
 def blocks_snapshot(st: BlockState, bc, t):

@@ -458,6 +458,35 @@ def deposit_fixture(gasgrid):
     _save("deposit.npz", **out)
 
 
+def removal_blocks_fixture(blocks, coupled, ics, hydro_cfg):
+    """Block steps with removal at the end of each particle's own step (removal_sync=False,
+    sim/blocks.py:673-719, sim/accretion.py): a 1,024-particle cloud centred at r = 5.2, falling
+    in at 0.3 c, accretion radius 4.4 and escape radius 6.0; 120 system steps."""
+    ic = ics.cloud(1024, radius=1.0, total_mass=1e-6, t_kelvin=1e6, r_peri=6.0, r_apo=10.0,
+                   seed=11)  # fmt: skip
+    c = ic.x.mean(axis=0)
+    chat = c / np.linalg.norm(c)
+    x = ic.x - c + 5.2 * chat
+    v = 0.5 * ic.v - 0.3 * chat
+    hc = hydro_cfg(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                   conductivity_signal=1, alpha_u=0.05, h_max=200.0)  # fmt: skip
+    cc = coupled.CoupledConfig(hydro=hc)
+    bc = blocks.BlockConfig(coupled=cc, dt_max=4.0, r_acc=4.4, r_escape=6.0, removal_sync=False)
+    st = blocks.initialise(x, v, ic.u, ic.mass, ic.h, bc, t_stop=1e6)
+    out = dict(x0=x, v0=v, u0=ic.u, mass=ic.mass, h0=ic.h)
+    actives = [len(blocks.advance(st, bc)) for _ in range(120)]
+    fields = ["x", "p", "u", "h", "level", "n_end", "ids", "vr_neg", "passed_peri"]
+    out.update(_state_arrays("final", st, fields))
+    rm = st.removed
+    out.update(active_counts=np.array(actives), final_n=st.n, removed_mass=rm.mass,
+               removed_energy=rm.energy, removed_angmom=rm.angmom, removed_momentum=rm.momentum,
+               final_energy=blocks.ledger(st, bc)["energy"])  # fmt: skip
+    for k in ("t", "id", "r", "m", "H", "u", "L", "L0", "first_pass"):
+        out[f"log_{k}"] = np.array([e[k] for e in rm.log])
+    out["log_escaped"] = np.array([e["reason"] == "escaped" for e in rm.log])
+    _save("removal_blocks.npz", **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="root of the reference checkout")
@@ -490,6 +519,7 @@ def main():
         "switch_coupled": lambda: switch_coupled_fixture(coupled, ics, HydroConfig),
         "switch_blocks": lambda: switch_blocks_fixture(blocks, coupled, ics, HydroConfig),
         "deposit": lambda: deposit_fixture(gasgrid),
+        "removal_blocks": lambda: removal_blocks_fixture(blocks, coupled, ics, HydroConfig),
     }
     for name, make in makers.items():
         if not args.only or name in args.only:

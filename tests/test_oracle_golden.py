@@ -442,3 +442,40 @@ def test_log_grid_volumes_fill_the_shell():
     g = LogSphericalGrid(r_min=2.0, r_max=200.0, nr=24, nth=12, nph=24)
     check("sum of cell volumes", 4.0 / 3.0 * np.pi * (g.r_max**3 - g.r_min**3),
           g.volumes().sum() * g.nph, rtol=1e-12)  # fmt: skip
+
+
+def _removal_bc():
+    from blackhole_nebula_simulator_b200.config import BlockConfig, CoupledConfig, HydroConfig
+
+    hc = HydroConfig(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                     conductivity_signal=1, alpha_u=0.05, h_max=200.0)  # fmt: skip
+    return BlockConfig(coupled=CoupledConfig(hydro=hc), dt_max=4.0, r_acc=4.4, r_escape=6.0,
+                       removal_sync=False)  # fmt: skip
+
+
+def test_removal_block_steps_match_reference():
+    g = golden("removal_blocks.npz")
+    bc = _removal_bc()
+    st = steps.blocks_initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc, t_stop=1e6)
+    actives = [len(steps.blocks_advance(st, bc)) for _ in range(len(g["active_counts"]))]
+    check("active counts", g["active_counts"], np.array(actives))
+    check("final tick", int(g["final_n"]), st.n)
+    check("remaining ids", g["final_ids"], st.ids)
+    check("final levels", g["final_level"], st.level)
+    check("final n_end", g["final_n_end"], st.n_end)
+    check("pericentre flags", g["final_passed_peri"], st.passed_peri)
+    check("inward flags", g["final_vr_neg"], st.vr_neg)
+    check("final x", g["final_x"], st.x, rtol=1e-13, per_vector=True)
+    check("final p", g["final_p"], st.p, rtol=1e-11, per_vector=True)
+    check("final u", g["final_u"], st.u, rtol=1e-9)
+    check("final h", g["final_h"], st.h, rtol=1e-9)
+    log = st.removed.log
+    check("removed ids in order", g["log_id"], np.array([e["id"] for e in log]))
+    check("removal reasons", g["log_escaped"], np.array([e["reason"] == "escaped" for e in log]))
+    check("removal times", g["log_t"], np.array([e["t"] for e in log]), rtol=1e-15)
+    check("first pass flags", g["log_first_pass"], np.array([e["first_pass"] for e in log]))
+    check("removed mass", float(g["removed_mass"]), st.removed.mass, rtol=1e-13)
+    check("removed energy", float(g["removed_energy"]), st.removed.energy, rtol=1e-10)
+    check("removed angmom", g["removed_angmom"], st.removed.angmom, rtol=1e-10, per_vector=True)
+    check("final energy", float(g["final_energy"]), steps.blocks_ledger(st, bc)["energy"],
+          rtol=1e-12)  # fmt: skip
