@@ -66,6 +66,7 @@ def test_block_state_checkpoint_resumes(tmp_path):
     for f in ("level", "n_beg", "n_end"):
         check(f, st.__getattribute__(f).cpu().numpy(), rs.__getattribute__(f).cpu().numpy())
     check("x", st.x.cpu().numpy(), rs.x.cpu().numpy(), rtol=1e-13, per_vector=True)
-    check("p", st.p.cpu().numpy(), rs.p.cpu().numpy(), rtol=1e-11, per_vector=True)
+    # the resumed run rebuilds its lists: sums in another curve order, hence rounding
+    check("p", st.p.cpu().numpy(), rs.p.cpu().numpy(), rtol=1e-10, per_vector=True)
     check("u", st.u.cpu().numpy(), rs.u.cpu().numpy(), rtol=1e-9)
     check("energy", blocks.ledger(st, bc)["energy"], blocks.ledger(rs, bc)["energy"], rtol=1e-12)
