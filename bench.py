@@ -407,7 +407,7 @@ def run_deposit(args, rank, world):
     metric = "particles deposited/s"
     if args.impl == "reference":
         if rank == 0:
-            cb = cpu_deposit(min(n, 16_384))
+            cb = cpu_deposit(min(n, 4_096))
             print(json.dumps({"metric": metric, "value": cb["value"], "unit": "particles/s",
                               "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                               "higher_is_better": True, "impl": "reference", "dtype": "f64",
@@ -459,7 +459,7 @@ def run_deposit(args, rank, world):
     pk = peaks()
     achieved = alg / (ms_t / args.steps * 1e-3) / 1e9
     if rank == 0:
-        cb = None if args.no_cpu_baseline else cpu_deposit(min(n, 16_384))
+        cb = None if args.no_cpu_baseline else cpu_deposit(min(n, 4_096))
         print(json.dumps({
             "metric": metric, "value": total / (ms_t * 1e-3), "unit": "particles/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
