@@ -114,6 +114,11 @@ _SIGS = {
     "nb_block_initialise": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams), _vp]),
     "nb_block_advance": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams), _vp, _vp]),
     "nb_block_land": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams), _vp]),
+    "nb_block_advance_split": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams), _vp, _vp, _vp,
+                                      _vp]),
+    "nb_block_finish": (_int, [_vp, _c.POINTER(NbState), _c.POINTER(NbParams), _i64, _vp, _int,
+                               _vp, _vp, _vp]),
+    "nb_block_wake_doomed": (_int, [_vp, _c.POINTER(NbState), _i64, _vp, _vp, _vp]),
     "nb_mlp_data": (_int, [_vp, _i64, _c.c_uint64, _c.POINTER(NbMlpParams), _vp, _vp, _vp, _vp]),
     "nb_mlp_grad": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _c.POINTER(_dbl), _vp]),
     "nb_mlp_train": (_int, [_vp, _c.POINTER(NbMlpParams), _i64, _i64, _int, _dbl, _c.c_uint64,

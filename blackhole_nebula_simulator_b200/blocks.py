@@ -68,6 +68,7 @@ class BlockState:
     L0: torch.Tensor = None
     vr_neg: torch.Tensor = None
     passed_peri: torch.Tensor = None
+    doomed: torch.Tensor = None  # next step ends beyond a removal radius (removal_sync)
     removed: RemovedLedger = field(default_factory=RemovedLedger)
     _params: object = field(default=None, repr=False)
     _rows: torch.Tensor = field(default=None, repr=False)
@@ -112,10 +113,6 @@ def _params(st: BlockState, cfg: BlockConfig):
     if st._params is None:
         if cfg.respa:
             raise NotImplementedError("RESPA gravity sub-steps are not part of the CUDA SPH path")
-        if (cfg.r_acc is not None or cfg.r_escape is not None) and cfg.removal_sync:
-            raise NotImplementedError("removal with removal_sync=True (forces of the survivors "
-                                      "recomputed at the removal) is not part of the CUDA SPH "
-                                      "path; removal_sync=False is")  # fmt: skip
         if not cfg.hydro:
             raise NotImplementedError("gravity-only block steps are not part of the CUDA SPH path")
         st._params = make_params(cfg.coupled, cfg.dt_max, cfg.limiter, cfg.max_gap)
@@ -152,17 +149,26 @@ def initialise(x, v, u, mass, h_guess, cfg: BlockConfig, t_stop: float, t0: floa
     st.L0 = torch.linalg.norm(torch.linalg.cross(st.x, st.p, dim=1), dim=1)
     st.vr_neg = torch.sum(st.x * ops.gn_v_from_p(st.x, st.p), dim=1) < 0
     st.passed_peri = torch.zeros(n, dtype=torch.bool, device=d)
+    st.doomed = torch.zeros(n, dtype=torch.bool, device=d)
     prm = _params(st, cfg)
     c = ctx()
     s = _state_struct(st)
     _lib.check(c, _lib.lib().nb_block_initialise(c, ctypes.byref(s), ctypes.byref(prm), stream()))
     _pull(st, s)
+    if _removal(cfg) and cfg.removal_sync:  # sim/blocks.py:497-498
+        _wake_for_removal(st, cfg, torch.arange(n, dtype=torch.int64, device=d))
     return st
+
+
+def _removal(cfg: BlockConfig) -> bool:
+    return cfg.r_acc is not None or cfg.r_escape is not None
 
 
 def advance(st: BlockState, cfg: BlockConfig) -> torch.Tensor:
     """sim/blocks.py:502-563: one system step to the earliest step end; returns the active rows."""
     prm = _params(st, cfg)
+    if _removal(cfg) and cfg.removal_sync:
+        return _advance_sync(st, cfg, prm)
     t0 = time.perf_counter()
     c = ctx()
     s = _state_struct(st)
@@ -172,10 +178,69 @@ def advance(st: BlockState, cfg: BlockConfig) -> torch.Tensor:
     na = int(s.last_active)
     st.active_counts.append(na)
     rows = st._rows[:na].clone()
-    if cfg.r_acc is not None or cfg.r_escape is not None:
-        rows = _swallow(st, cfg, rows)
+    if _removal(cfg):
+        rows = _swallow_keep(st, cfg, rows)[0]
     st.timers["step"] += time.perf_counter() - t0
     return rows
+
+
+def _advance_sync(st: BlockState, cfg: BlockConfig, prm) -> torch.Tensor:
+    """sim/blocks.py:502-563 with removal_sync (module docstring of sim/blocks.py, Removal): the
+    active particles inside r_acc or beyond r_escape are removed after the closing kicks, the
+    forces of the remaining active particles are recomputed without them at the same predicted
+    velocities and energies, then levels and openings, then the doomed particles' neighbours
+    are cut to end their steps with theirs (sim/blocks.py:566-627)."""
+    t0 = time.perf_counter()
+    c = ctx()
+    n = len(st.x)
+    v_eval = torch.empty((n, 3), dtype=torch.float64, device=st.x.device)
+    u_eval = torch.empty(n, dtype=torch.float64, device=st.x.device)
+    s = _state_struct(st)
+    _lib.check(c, _lib.lib().nb_block_advance_split(c, ctypes.byref(s), ctypes.byref(prm),
+                                                    ptr(st._rows), ptr(v_eval), ptr(u_eval),
+                                                    stream()))  # fmt: skip
+    _pull(st, s)
+    na = int(s.last_active)
+    st.active_counts.append(na)
+    rows, keep = _swallow_keep(st, cfg, st._rows[:na].clone())
+    redo = 0
+    if keep is not None:
+        v_eval, u_eval = v_eval[keep].contiguous(), u_eval[keep].contiguous()
+        redo = int(len(rows) > 0)
+    s = _state_struct(st)
+    _lib.check(c, _lib.lib().nb_block_finish(c, ctypes.byref(s), ctypes.byref(prm), len(rows),
+                                             ptr(rows), redo, ptr(v_eval), ptr(u_eval),
+                                             stream()))  # fmt: skip
+    _pull(st, s)
+    _wake_for_removal(st, cfg, rows)
+    st.timers["step"] += time.perf_counter() - t0
+    return rows
+
+
+def _wake_for_removal(st: BlockState, cfg: BlockConfig, rows) -> None:
+    """sim/blocks.py:593-627: flag the active particles whose gravity flow over the step just
+    opened ends inside r_acc or beyond r_escape; the running steps of every neighbour of a
+    flagged particle (and of active particles next to one still in its step) are cut to end
+    with its step (on the device, over the cached lists)."""
+    if len(rows) == 0:
+        return
+    length = (st.n_end[rows] - st.n_beg[rows]).to(torch.float64) * st.tick
+    x_end, _, _ = ops.glf_step_many(st.x_beg[rows], st.p_half[rows], length)
+    r = torch.linalg.norm(x_end, dim=1)
+    doomed = torch.zeros(len(rows), dtype=torch.bool, device=r.device)
+    if cfg.r_acc is not None:
+        doomed |= r < cfg.r_acc
+    if cfg.r_escape is not None:
+        doomed |= r > cfg.r_escape
+    st.doomed[rows] = doomed
+    if not bool(torch.any(st.doomed)):
+        return
+    c = ctx()
+    s = _state_struct(st)
+    flags = st.doomed.to(torch.uint8).contiguous()
+    _lib.check(c, _lib.lib().nb_block_wake_doomed(c, ctypes.byref(s), len(rows), ptr(rows),
+                                                  ptr(flags), stream()))  # fmt: skip
+    _pull(st, s)
 
 
 def _gn_hamiltonian(x, p):
@@ -186,11 +251,12 @@ def _gn_hamiltonian(x, p):
     return 0.5 * a * torch.sum(p * p, dim=1) + 0.5 * c * px**2 - 1.0 / r
 
 
-def _swallow(st: BlockState, cfg: BlockConfig, rows):
-    """sim/blocks.py:673-719 (_swallow, _swallow_keep, _prune; removal_sync=False): the active
-    rows' pericentre flags; those inside r_acc or beyond r_escape (their state true at their own
-    step end) go into the removed ledger and out of every per-particle array.  The engine
-    rebuilds its lists for the new particle count.  Returns the remaining rows, renumbered."""
+def _swallow_keep(st: BlockState, cfg: BlockConfig, rows):
+    """sim/blocks.py:673-719 (_swallow, _swallow_keep, _prune): the active rows' pericentre
+    flags; those inside r_acc or beyond r_escape (their state true at their own step end) go into
+    the removed ledger and out of every per-particle array.  The engine rebuilds its lists for
+    the new particle count.  Returns the remaining rows, renumbered, and the mask of the kept
+    particles (None when none was removed)."""
     rows = torch.sort(rows).values  # ascending, as the reference's rows (and so its log order)
     x, p = st.x[rows], st.p[rows]
     r = torch.linalg.norm(x, dim=1)
@@ -203,7 +269,7 @@ def _swallow(st: BlockState, cfg: BlockConfig, rows):
     esc = r > cfg.r_escape if cfg.r_escape is not None else none
     gone_mask = acc | esc
     if not bool(torch.any(gone_mask)):
-        return rows
+        return rows, None
     for mask, reason in ((acc, "accreted"), (esc, "escaped")):
         g = rows[mask]
         if len(g) == 0:
@@ -221,7 +287,7 @@ def _swallow(st: BlockState, cfg: BlockConfig, rows):
         if isinstance(value, torch.Tensor) and value.shape[:1] == (n,):
             setattr(st, name, value[keep].contiguous())
     new_index = torch.cumsum(keep.to(torch.int64), 0) - 1
-    return new_index[rows[keep[rows]]]
+    return new_index[rows[keep[rows]]].contiguous(), keep
 
 
 def run(st: BlockState, cfg: BlockConfig, t_end: float, callback=None) -> BlockState:

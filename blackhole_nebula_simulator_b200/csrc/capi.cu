@@ -574,6 +574,31 @@ int nb_block_advance(nb_ctx* ctx, nb_state* st, const nb_params* prm, int64_t* r
   return nbk::block_advance(ctx->E, st, prm, rows_out, S(stream));
 }
 
+int nb_block_advance_split(nb_ctx* ctx, nb_state* st, const nb_params* prm, int64_t* rows_out,
+                           double* v_eval_out, double* u_eval_out, void* stream) {
+  NB_TRY(begin(ctx));
+  NB_TRY(check_params(ctx->E, prm));
+  if (!v_eval_out || !u_eval_out)
+    return nbk::set_host_error(ctx->E, "evaluation buffers missing"), NB_ERR_INPUT;
+  return nbk::block_advance(ctx->E, st, prm, rows_out, S(stream), v_eval_out, u_eval_out);
+}
+
+int nb_block_finish(nb_ctx* ctx, nb_state* st, const nb_params* prm, int64_t nrows,
+                    const int64_t* rows, int redo, const double* v_eval, const double* u_eval,
+                    void* stream) {
+  NB_TRY(begin(ctx));
+  NB_TRY(check_params(ctx->E, prm));
+  if (redo && (!v_eval || !u_eval))
+    return nbk::set_host_error(ctx->E, "evaluation buffers missing"), NB_ERR_INPUT;
+  return nbk::block_finish(ctx->E, st, prm, nrows, rows, redo, v_eval, u_eval, S(stream));
+}
+
+int nb_block_wake_doomed(nb_ctx* ctx, nb_state* st, int64_t nrows, const int64_t* rows,
+                         const uint8_t* doomed, void* stream) {
+  NB_TRY(begin(ctx));
+  return nbk::block_wake_doomed(ctx->E, st, nrows, rows, doomed, S(stream));
+}
+
 int nb_block_land(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* stream) {
   NB_TRY(begin(ctx));
   NB_TRY(check_params(ctx->E, prm));

@@ -694,7 +694,7 @@ int block_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t 
 // sim/blocks.py:502-563 (advance): one system step to the earliest step end.  rows_out (optional,
 // device, n) receives the active rows; their number is s->last_active.
 int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_out,
-                  cudaStream_t st) {
+                  cudaStream_t st, double* v_eval_out, double* u_eval_out) {
   Workspace& W = E.ws;
   int64_t n = s->n;
   NB_TRY(W.ensure(E, n));
@@ -746,19 +746,138 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   sk.tick = s->tick;
   sk.recon_full = 1;
   NB_TRY(hydro_rows(E, s, prm, nrows, W.rows, W.v_eval, s->u, st, sk));
+  // the evaluation's velocities and (predicted) energies, for a removal that recomputes forces
+  const bool split = v_eval_out != nullptr;
+  if (split) {
+    NB_CUDA(cudaMemcpyAsync(v_eval_out, W.v_eval, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, st));
+    NB_CUDA(cudaMemcpyAsync(u_eval_out, s->u, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  }
   count_launch(), k_block_close<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, W.rows, s->tick, s->n_beg, s->n_end,
                                                        W.v_flow, s->a_hydro, s->u_half, s->dudt,
                                                        W.v_pred, s->u);
   NB_CUDA(cudaMemcpyAsync(s->p, W.v_pred, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, st));
-  E.prof.begin(st);
-  NB_TRY(choose_levels_and_open(E, s, prm, nrows, W.rows, st));
-  E.prof.end(PROF_LEVELS, st, (double)nrows, 0.0);
+  if (!split) {
+    E.prof.begin(st);
+    NB_TRY(choose_levels_and_open(E, s, prm, nrows, W.rows, st));
+    E.prof.end(PROF_LEVELS, st, (double)nrows, 0.0);
+  }
   NB_TRY(pending_flush(E, st));
   if (rows_out && nrows > 0)
     NB_CUDA(cudaMemcpyAsync(rows_out, W.rows, sizeof(int64_t) * nrows, cudaMemcpyDeviceToDevice, st));
   s->last_active = nrows;
   s->particle_steps += nrows;
   return 0;
+}
+
+// The second half of a split system step (removal with removal_sync, sim/blocks.py:541-549):
+// rows (caller order, already renumbered by the caller's removal) get their forces again at the
+// evaluation's velocities and energies (the switch not advanced), or not when redo == 0; then
+// their levels are chosen and their next steps opened.
+int block_finish(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, const int64_t* rows,
+                 int redo, const double* v_eval, const double* u_eval, cudaStream_t st) {
+  Workspace& W = E.ws;
+  const int64_t n = s->n;
+  NB_TRY(W.ensure(E, n));
+  if (nrows > 0)
+    NB_CUDA(cudaMemcpyAsync(W.rows, rows, sizeof(int64_t) * nrows, cudaMemcpyDeviceToDevice, st));
+  W.rows_ver += 1;
+  if (redo && nrows > 0) {
+    ShockStep sk;
+    sk.recon_full = 1;
+    NB_TRY(hydro_rows(E, s, prm, nrows, W.rows, v_eval, u_eval, st, sk));
+  }
+  E.prof.begin(st);
+  NB_TRY(choose_levels_and_open(E, s, prm, nrows, W.rows, st));
+  E.prof.end(PROF_LEVELS, st, (double)nrows, 0.0);
+  return pending_flush(E, st);
+}
+
+// sim/blocks.py:593-627 (_wake_for_removal, its list walk and _cut_to): for every pair (a, b) of
+// a row's cached list, a doomed particle's neighbour must end its step by the doomed one's end
+// (its level label raised to the doomed one's), in both directions; running steps that end later
+// are cut, the opening kick corrected to the new length (Durier Eq. C5).
+__global__ void k_doomed_walk(int64_t nrows, const int64_t* __restrict__ rows_s,
+                              const int64_t* __restrict__ off, const int32_t* __restrict__ idx,
+                              const int32_t* __restrict__ perm, const uint8_t* __restrict__ doomed,
+                              const int64_t* __restrict__ n_end, const int64_t* __restrict__ level,
+                              unsigned long long* end, long long* label) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  const int64_t as = rows_s[q];
+  const int64_t a = perm[as];
+  const bool da = doomed[a];
+  for (int64_t k = off[as]; k < off[as + 1]; ++k) {
+    const int64_t bs = idx[k];
+    if (bs == as) continue;
+    const int64_t b = perm[bs];
+    if (da) {
+      atomicMin(end + b, (unsigned long long)n_end[a]);
+      atomicMax(label + b, (long long)level[a]);
+    }
+    if (doomed[b]) {
+      atomicMin(end + a, (unsigned long long)n_end[b]);
+      atomicMax(label + a, (long long)level[b]);
+    }
+  }
+}
+
+__global__ void k_cut_doomed(int64_t n, int64_t tick_n, double tick,
+                             const unsigned long long* __restrict__ end,
+                             const long long* __restrict__ label, int64_t* __restrict__ n_end,
+                             int64_t* __restrict__ level, double* __restrict__ p_half,
+                             double* __restrict__ u_half, const double* __restrict__ a,
+                             const double* __restrict__ dudt, unsigned long long* woken) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t e = (int64_t)end[i];
+  if (!(e < n_end[i] && n_end[i] > tick_n)) return;
+  level[i] = (int64_t)label[i];
+  const double d_len = (double)(e - n_end[i]) * tick;
+  for (int c = 0; c < 3; ++c) p_half[3 * i + c] += 0.5 * d_len * a[3 * i + c];
+  u_half[i] += 0.5 * d_len * dudt[i];
+  n_end[i] = e;
+  atomicAdd(woken, 1ull);
+}
+
+__global__ void k_fill_u64(int64_t n, unsigned long long v, unsigned long long* out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = v;
+}
+
+__global__ void k_copy_level(int64_t n, const int64_t* __restrict__ level, long long* out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (long long)level[i];
+}
+
+int block_wake_doomed(Engine& E, nb_state* s, int64_t nrows, const int64_t* rows,
+                      const uint8_t* doomed, cudaStream_t st) {
+  Workspace& W = E.ws;
+  const int64_t n = s->n;
+  NB_TRY(W.ensure(E, n));
+  if (nrows == 0) return 0;
+  if (E.lists.n != n) {
+    std::snprintf(E.last_error, sizeof(E.last_error), "no cached lists for the current particles");
+    return NB_ERR_INPUT;
+  }
+  Lists& L = E.lists;
+  NB_CUDA(cudaMemcpyAsync(W.rows, rows, sizeof(int64_t) * nrows, cudaMemcpyDeviceToDevice, st));
+  W.rows_ver += 1;
+  int64_t ns = 0;
+  NB_TRY(sorted_rows_and_pack(E, nrows, W.rows, s->x, s->h, &ns, st));
+  unsigned long long* end = reinterpret_cast<unsigned long long*>(W.i_tmp);
+  long long* label = reinterpret_cast<long long*>(W.i_tmp2);
+  count_launch(), k_fill_u64<<<grid_for(n), NB_THREADS, 0, st>>>(n, 0x7fffffffffffffffull, end);
+  count_launch(), k_copy_level<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->level, label);
+  count_launch(), k_doomed_walk<<<grid_for(ns), NB_THREADS, 0, st>>>(
+      ns, W.rows_s, L.off, L.idx, L.perm, doomed, s->n_end, s->level, end, label);
+  NB_CUDA(cudaMemsetAsync(W.d_i64, 0, sizeof(int64_t), st));
+  count_launch(), k_cut_doomed<<<grid_for(n), NB_THREADS, 0, st>>>(
+      n, s->tick_n, s->tick, end, label, s->n_end, s->level, s->p_half, s->u_half, s->a_hydro,
+      s->dudt, reinterpret_cast<unsigned long long*>(W.d_i64));
+  NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  s->woken += W.h_i64[0];
+  return check_device_error(E, st);
 }
 
 // run()'s prologue (sim/blocks.py:727-734): re-open the steps opened at this tick that would end

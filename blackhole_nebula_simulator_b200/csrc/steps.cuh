@@ -39,8 +39,14 @@ int coupled_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_
 int coupled_step(Engine& E, nb_state* s, const nb_params* prm, double dt, cudaStream_t st);
 int coupled_stable_dt(Engine& E, nb_state* s, const nb_params* prm, double* dt, cudaStream_t st);
 int block_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st);
+// with v_eval_out (n x 3) and u_eval_out (n): stops after the closing kicks (the first half of a
+// split step) and leaves the evaluation's velocities and energies there
 int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_out,
-                  cudaStream_t st);
+                  cudaStream_t st, double* v_eval_out = nullptr, double* u_eval_out = nullptr);
+int block_finish(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, const int64_t* rows,
+                 int redo, const double* v_eval, const double* u_eval, cudaStream_t st);
+int block_wake_doomed(Engine& E, nb_state* s, int64_t nrows, const int64_t* rows,
+                      const uint8_t* doomed, cudaStream_t st);
 int block_land(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st);
 
 // launchers of engine.cu kernels used by steps.cu

@@ -252,6 +252,23 @@ NB_API int nb_coupled_stable_dt(nb_ctx* ctx, nb_state* st, const nb_params* prm,
 NB_API int nb_block_initialise(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* stream);
 NB_API int nb_block_advance(nb_ctx* ctx, nb_state* st, const nb_params* prm, int64_t* rows_out,
                      void* stream);
+/* A system step split for removal with removal_sync (sim/blocks.py:502-563, 566-627):
+ * nb_block_advance_split does the step up to and including the closing kicks and leaves the
+ * evaluation's velocities (n x 3) and predicted energies (n) in v_eval_out / u_eval_out; the
+ * caller removes particles (renumbering rows and state); nb_block_finish recomputes the forces
+ * of rows at v_eval / u_eval when redo != 0 (the switch not advanced), then chooses their levels
+ * and opens their next steps.  nb_block_wake_doomed (sim/blocks.py:593-627): with doomed (n,
+ * caller order) the particles whose next step ends beyond a removal radius, cuts the running
+ * steps of their list neighbours among and around rows to end with theirs (st->woken counts
+ * them). */
+NB_API int nb_block_advance_split(nb_ctx* ctx, nb_state* st, const nb_params* prm,
+                           int64_t* rows_out, double* v_eval_out, double* u_eval_out,
+                           void* stream);
+NB_API int nb_block_finish(nb_ctx* ctx, nb_state* st, const nb_params* prm, int64_t nrows,
+                    const int64_t* rows, int redo, const double* v_eval, const double* u_eval,
+                    void* stream);
+NB_API int nb_block_wake_doomed(nb_ctx* ctx, nb_state* st, int64_t nrows, const int64_t* rows,
+                         const uint8_t* doomed, void* stream);
 /* Re-open the steps just opened so they land on n_stop (sim/blocks.py:722-734, run's prologue). */
 NB_API int nb_block_land(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* stream);
 

@@ -278,6 +278,7 @@ class BlockState:
     L0: np.ndarray = None  # starting |angular momentum|
     vr_neg: np.ndarray = None  # radial velocity < 0 at the last active time
     passed_peri: np.ndarray = None  # has turned outward near the hole
+    doomed: np.ndarray = None  # next step ends beyond a removal radius (removal_sync)
     removed: "RemovedLedger" = None
 
     @property
@@ -461,12 +462,16 @@ def blocks_initialise(x, v, u, mass, h_guess, bc, t_stop, t0=0.0, level_offset=N
     st.L0 = np.linalg.norm(np.cross(x, p), axis=1)
     st.vr_neg = np.sum(x * native.gn_v_from_p(x, p), axis=1) < 0
     st.passed_peri = np.zeros(n, bool)
+    st.doomed = np.zeros(n, bool)
     st.removed = RemovedLedger()
     rows = np.arange(n)
     nb = _hydro_rows(st, bc, rows, native.gn_v_from_p(x, p), st.u, reuse)
     st.level[:] = 0
     _choose_levels(st, bc, rows, nb)
     _open(st, rows)
+    if (getattr(bc, "r_acc", None) is not None or getattr(bc, "r_escape", None) is not None) \
+            and bc.removal_sync:  # fmt: skip
+        _wake_for_removal(st, bc, rows, nb)
     return st
 
 
@@ -499,21 +504,78 @@ def blocks_advance(st: BlockState, bc, reuse=True) -> np.ndarray:
     v_eval = native.gn_v_from_p(x, p_pred)
     nb = _hydro_rows(st, bc, rows, v_eval, u_pred, reuse, 2.0 * half_len[rows], a_prev)
     t2 = time.perf_counter()
+    removal = getattr(bc, "r_acc", None) is not None or getattr(bc, "r_escape", None) is not None
+    sync = removal and bc.removal_sync
+    u_eval = u_pred.copy() if sync else None
     p_pred[rows] = p_flow[rows] + half_len[rows, None] * st.a_hydro[rows]
     st.u[rows] = st.u_half[rows] + half_len[rows] * st.dudt[rows]
     st.p = p_pred
+    n_active = len(rows)
+    if sync:
+        rows, nb = _remove(st, bc, rows, nb, v_eval, u_eval, reuse)
     _choose_levels(st, bc, rows, nb)
     _open(st, rows)
+    if sync:
+        _wake_for_removal(st, bc, rows, nb)
     st.timers["flow"] += t1 - t0
     st.timers["hydro"] += t2 - t1
     st.timers["levels"] += time.perf_counter() - t2
-    st.active_counts.append(len(rows))
-    st.particle_steps += len(rows)
-    if getattr(bc, "r_acc", None) is not None or getattr(bc, "r_escape", None) is not None:
-        if bc.removal_sync:
-            raise NotImplementedError("removal with removal_sync=True is not restated")
-        rows = _swallow(st, bc, rows)
+    st.active_counts.append(n_active)
+    st.particle_steps += n_active
+    if removal and not sync:
+        rows = _swallow_keep(st, bc, rows)[0]
     return rows
+
+
+def _remove(st: BlockState, bc, rows, nb, v_eval, u_eval, reuse=True):
+    """sim/blocks.py:566-590: removal after the closing kicks, then the remaining active rows'
+    forces again without the removed particles (same predicted velocities and energies, switch
+    not advanced); returns the remaining rows and their pair lists, renumbered."""
+    n_old = len(st.x)
+    new_rows, keep = _swallow_keep(st, bc, rows)
+    if keep is None:
+        return new_rows, nb
+    owner = np.repeat(np.arange(n_old), np.diff(nb.offset))
+    new_index = np.cumsum(keep) - 1
+    mask = keep[owner] & keep[nb.index]
+    counts = np.bincount(new_index[owner[mask]], minlength=len(st.x))
+    offset = np.zeros(len(st.x) + 1, np.int64)
+    np.cumsum(counts, out=offset[1:])
+    nb = native.Neighbours(offset, new_index[nb.index[mask]], nb.box)
+    if len(new_rows):
+        _hydro_rows(st, bc, new_rows, v_eval[keep], u_eval[keep], reuse,
+                    np.zeros(len(new_rows)), None)  # fmt: skip
+    return new_rows, nb
+
+
+def _wake_for_removal(st: BlockState, bc, rows, nb):
+    """sim/blocks.py:593-627."""
+    if len(rows) == 0:
+        return
+    length = (st.n_end[rows] - st.n_beg[rows]) * st.tick
+    x_end, _, _ = native.glf_step_many(st.x_beg[rows], st.p_half[rows], length)
+    r = np.linalg.norm(x_end, axis=1)
+    doomed = np.zeros(len(rows), bool)
+    if bc.r_acc is not None:
+        doomed |= r < bc.r_acc
+    if bc.r_escape is not None:
+        doomed |= r > bc.r_escape
+    st.doomed[rows] = doomed
+    lists = nb if st.neighbour_cache is None else st.neighbour_cache.neighbours
+    src = np.zeros(len(st.x), bool)
+    src[rows] = True
+    owner = np.repeat(np.arange(len(st.x)), np.diff(lists.offset))
+    keep = src[owner]
+    owner, other = owner[keep], lists.index[keep]
+    end = np.full(len(st.x), np.iinfo(np.int64).max)
+    label = st.level.copy()
+    for a, b in ((owner, other), (other, owner)):
+        m = st.doomed[a] & (a != b)
+        np.minimum.at(end, b[m], st.n_end[a[m]])
+        np.maximum.at(label, b[m], st.level[a[m]])
+    j = np.flatnonzero((end < st.n_end) & (st.n_end > st.n))
+    if len(j):
+        _cut_to(st, j, end[j], label[j])
 
 
 @dataclass
@@ -544,10 +606,11 @@ def _record_removal(led, t, ids, mass, ham, u, am, p, r, passed, L0, reason):
                         "first_pass": not bool(passed[k])})  # fmt: skip
 
 
-def _swallow(st: BlockState, bc, rows):
+def _swallow_keep(st: BlockState, bc, rows):
     """sim/blocks.py:673-719 (_swallow, _swallow_keep, _prune) for the GN hole: pericentre
     flags of the active rows, removal of those inside r_acc or beyond r_escape (their state is
-    true at their own step end) into the ledger; returns the remaining rows, renumbered."""
+    true at their own step end) into the ledger; returns the remaining rows, renumbered, and the
+    mask of the kept particles (None when none was removed)."""
     x, p = st.x[rows], st.p[rows]
     r = np.linalg.norm(x, axis=1)
     vr = np.sum(x * native.gn_v_from_p(x, p), axis=1)
@@ -557,7 +620,7 @@ def _swallow(st: BlockState, bc, rows):
     acc = r < bc.r_acc if bc.r_acc is not None else np.zeros(len(rows), bool)
     esc = r > bc.r_escape if bc.r_escape is not None else np.zeros(len(rows), bool)
     if not (np.any(acc) or np.any(esc)):
-        return rows
+        return rows, None
     for mask, reason in ((acc, "accreted"), (esc, "escaped")):
         g = rows[mask]
         if len(g) == 0:
@@ -574,7 +637,7 @@ def _swallow(st: BlockState, bc, rows):
             setattr(st, name, value[keep])
     st.neighbour_cache = None
     new_index = np.cumsum(keep) - 1
-    return new_index[rows[keep[rows]]]
+    return new_index[rows[keep[rows]]], keep
 
 
 def blocks_run(st: BlockState, bc, t_end, callback=None, reuse=True) -> BlockState:

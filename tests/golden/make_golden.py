@@ -458,10 +458,12 @@ def deposit_fixture(gasgrid):
     _save("deposit.npz", **out)
 
 
-def removal_blocks_fixture(blocks, coupled, ics, hydro_cfg):
-    """Block steps with removal at the end of each particle's own step (removal_sync=False,
-    sim/blocks.py:673-719, sim/accretion.py): a 1,024-particle cloud centred at r = 5.2, falling
-    in at 0.3 c, accretion radius 4.4 and escape radius 6.0; 120 system steps."""
+def removal_blocks_fixture(blocks, coupled, ics, hydro_cfg, sync=False):
+    """Block steps with removal at the end of each particle's own step (sim/blocks.py:566-719,
+    sim/accretion.py), without (removal_blocks.npz) and with removal_sync (removal_sync_blocks.npz:
+    survivors' forces recomputed, doomed particles' neighbours cut): a 1,024-particle cloud
+    centred at r = 5.2, falling in at 0.3 c, accretion radius 4.4 and escape radius 6.0; 120
+    system steps."""
     ic = ics.cloud(1024, radius=1.0, total_mass=1e-6, t_kelvin=1e6, r_peri=6.0, r_apo=10.0,
                    seed=11)  # fmt: skip
     c = ic.x.mean(axis=0)
@@ -471,11 +473,11 @@ def removal_blocks_fixture(blocks, coupled, ics, hydro_cfg):
     hc = hydro_cfg(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
                    conductivity_signal=1, alpha_u=0.05, h_max=200.0)  # fmt: skip
     cc = coupled.CoupledConfig(hydro=hc)
-    bc = blocks.BlockConfig(coupled=cc, dt_max=4.0, r_acc=4.4, r_escape=6.0, removal_sync=False)
+    bc = blocks.BlockConfig(coupled=cc, dt_max=4.0, r_acc=4.4, r_escape=6.0, removal_sync=sync)
     st = blocks.initialise(x, v, ic.u, ic.mass, ic.h, bc, t_stop=1e6)
     out = dict(x0=x, v0=v, u0=ic.u, mass=ic.mass, h0=ic.h)
     actives = [len(blocks.advance(st, bc)) for _ in range(120)]
-    fields = ["x", "p", "u", "h", "level", "n_end", "ids", "vr_neg", "passed_peri"]
+    fields = ["x", "p", "u", "h", "level", "n_end", "ids", "vr_neg", "passed_peri", "doomed"]
     out.update(_state_arrays("final", st, fields))
     rm = st.removed
     out.update(active_counts=np.array(actives), final_n=st.n, removed_mass=rm.mass,
@@ -484,7 +486,32 @@ def removal_blocks_fixture(blocks, coupled, ics, hydro_cfg):
     for k in ("t", "id", "r", "m", "H", "u", "L", "L0", "first_pass"):
         out[f"log_{k}"] = np.array([e[k] for e in rm.log])
     out["log_escaped"] = np.array([e["reason"] == "escaped" for e in rm.log])
-    _save("removal_blocks.npz", **out)
+    out["woken"] = st.woken
+    _save("removal_sync_blocks.npz" if sync else "removal_blocks.npz", **out)
+
+
+def removal_wake_fixture(blocks, coupled, ics, hydro_cfg):
+    """removal_sync's wake-up of the doomed particles' neighbours (sim/blocks.py:593-627): the
+    multi-level cloud of blocks_fixture (level offsets 0-3, beta = 230) with an accretion radius
+    of 382 that its inner edge crosses within the 16 system steps."""
+    ic = ics.cloud(2048, radius=20.0, total_mass=1e-3, t_kelvin=3e8, r_peri=60.0, r_apo=400.0,
+                   seed=7)  # fmt: skip
+    rng = np.random.default_rng(SEED)
+    v = ic.v + rng.normal(0.0, 0.002, ic.v.shape)
+    hc = hydro_cfg(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                   conductivity_signal=1, alpha_u=0.05, h_max=200.0)  # fmt: skip
+    cc = coupled.CoupledConfig(hydro=hc, cooling_beta=230.0)
+    offset = rng.integers(0, 4, len(ic.x))
+    bc = blocks.BlockConfig(coupled=cc, dt_max=64.0, r_acc=382.0, removal_sync=True)
+    st = blocks.initialise(ic.x, v, ic.u, ic.mass, ic.h, bc, t_stop=1e6, level_offset=offset)
+    out = dict(x0=ic.x, v0=v, u0=ic.u, mass=ic.mass, h0=ic.h, level_offset=offset)
+    actives = [len(blocks.advance(st, bc)) for _ in range(16)]
+    fields = ["x", "p", "u", "h", "level", "n_beg", "n_end", "ids", "doomed"]
+    out.update(_state_arrays("final", st, fields))
+    out.update(active_counts=np.array(actives), final_n=st.n, woken=st.woken,
+               removed_mass=st.removed.mass, final_energy=blocks.ledger(st, bc)["energy"],
+               log_id=np.array([e["id"] for e in st.removed.log]))  # fmt: skip
+    _save("removal_wake_blocks.npz", **out)
 
 
 def main():
@@ -520,6 +547,9 @@ def main():
         "switch_blocks": lambda: switch_blocks_fixture(blocks, coupled, ics, HydroConfig),
         "deposit": lambda: deposit_fixture(gasgrid),
         "removal_blocks": lambda: removal_blocks_fixture(blocks, coupled, ics, HydroConfig),
+        "removal_sync_blocks": lambda: removal_blocks_fixture(blocks, coupled, ics, HydroConfig,
+                                                              sync=True),
+        "removal_wake": lambda: removal_wake_fixture(blocks, coupled, ics, HydroConfig),
     }
     for name, make in makers.items():
         if not args.only or name in args.only:

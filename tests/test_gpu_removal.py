@@ -1,6 +1,8 @@
-"""Removal of particles at the end of their own steps (removal_sync=False: sim/blocks.py:673-719,
-sim/accretion.py) on the GPU against the reference's block steps (tests/golden/removal_blocks.npz):
-a cloud falling past the accretion radius 4.4 and spilling over the escape radius 6.0.
+"""Removal of particles at the end of their own steps (sim/blocks.py:566-719, sim/accretion.py)
+on the GPU against the reference's block steps, without removal_sync (tests/golden/
+removal_blocks.npz) and with it (removal_sync_blocks.npz: the survivors' forces recomputed after
+a removal, the doomed particles' neighbours cut): a cloud falling past the accretion radius 4.4
+and spilling over the escape radius 6.0.
 
 Active counts, remaining ids, levels, tick counters, pericentre flags and the removal log (ids,
 reasons, times, first-pass flags) exactly; the state at the block-step tolerances; the removed
@@ -31,9 +33,10 @@ def _np(t):
     return t.detach().cpu().numpy()
 
 
-def test_removal_block_steps_match_reference(blocks):
-    g = golden("removal_blocks.npz")
-    bc = _removal_bc()
+@pytest.mark.parametrize("sync", [False, True])
+def test_removal_block_steps_match_reference(blocks, sync):
+    g = golden("removal_sync_blocks.npz" if sync else "removal_blocks.npz")
+    bc = _removal_bc(sync)
     st = blocks.initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc, t_stop=1e6)
     actives = [len(blocks.advance(st, bc)) for _ in range(len(g["active_counts"]))]
     check("active counts", g["active_counts"], np.array(actives))
@@ -43,6 +46,8 @@ def test_removal_block_steps_match_reference(blocks):
     check("final n_end", g["final_n_end"], _np(st.n_end))
     check("pericentre flags", g["final_passed_peri"], _np(st.passed_peri))
     check("inward flags", g["final_vr_neg"], _np(st.vr_neg))
+    check("doomed flags", g["final_doomed"], _np(st.doomed))
+    check("woken", int(g["woken"]), st.woken)
     check("final x", g["final_x"], _np(st.x), rtol=1e-13, per_vector=True)
     check("final p", g["final_p"], _np(st.p), rtol=1e-11, per_vector=True)
     check("final u", g["final_u"], _np(st.u), rtol=1e-9)
@@ -60,10 +65,23 @@ def test_removal_block_steps_match_reference(blocks):
     check("removed count", len(g["log_id"]), led["removed_count"])
 
 
-def test_removal_with_sync_is_refused(blocks):
-    import dataclasses
+def test_removal_wake_matches_reference(blocks):
+    """The doomed particles' neighbours cut to end their steps with theirs (multi-level cloud,
+    accretion radius 382 crossed by its inner edge)."""
+    from tests.test_oracle_golden import _wake_bc
 
-    g = golden("removal_blocks.npz")
-    bc = dataclasses.replace(_removal_bc(), removal_sync=True)
-    with pytest.raises(NotImplementedError, match="removal_sync"):
-        blocks.initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc, t_stop=1e6)
+    g = golden("removal_wake_blocks.npz")
+    bc = _wake_bc()
+    st = blocks.initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc, t_stop=1e6,
+                           level_offset=g["level_offset"])  # fmt: skip
+    actives = [len(blocks.advance(st, bc)) for _ in range(len(g["active_counts"]))]
+    check("active counts", g["active_counts"], np.array(actives))
+    check("woken", int(g["woken"]), st.woken)
+    check("removed ids", g["log_id"], np.array([e["id"] for e in st.removed.log]))
+    check("remaining ids", g["final_ids"], _np(st.ids))
+    for f in ("level", "n_beg", "n_end", "doomed"):
+        check(f"final {f}", g[f"final_{f}"], _np(getattr(st, f)))
+    check("final x", g["final_x"], _np(st.x), rtol=1e-13, per_vector=True)
+    check("final p", g["final_p"], _np(st.p), rtol=1e-11, per_vector=True)
+    check("final u", g["final_u"], _np(st.u), rtol=1e-9)
+    check("final energy", float(g["final_energy"]), blocks.ledger(st, bc)["energy"], rtol=1e-12)

@@ -444,18 +444,19 @@ def test_log_grid_volumes_fill_the_shell():
           g.volumes().sum() * g.nph, rtol=1e-12)  # fmt: skip
 
 
-def _removal_bc():
+def _removal_bc(sync=False):
     from blackhole_nebula_simulator_b200.config import BlockConfig, CoupledConfig, HydroConfig
 
     hc = HydroConfig(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
                      conductivity_signal=1, alpha_u=0.05, h_max=200.0)  # fmt: skip
     return BlockConfig(coupled=CoupledConfig(hydro=hc), dt_max=4.0, r_acc=4.4, r_escape=6.0,
-                       removal_sync=False)  # fmt: skip
+                       removal_sync=sync)  # fmt: skip
 
 
-def test_removal_block_steps_match_reference():
-    g = golden("removal_blocks.npz")
-    bc = _removal_bc()
+@pytest.mark.parametrize("sync", [False, True])
+def test_removal_block_steps_match_reference(sync):
+    g = golden("removal_sync_blocks.npz" if sync else "removal_blocks.npz")
+    bc = _removal_bc(sync)
     st = steps.blocks_initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc, t_stop=1e6)
     actives = [len(steps.blocks_advance(st, bc)) for _ in range(len(g["active_counts"]))]
     check("active counts", g["active_counts"], np.array(actives))
@@ -465,6 +466,8 @@ def test_removal_block_steps_match_reference():
     check("final n_end", g["final_n_end"], st.n_end)
     check("pericentre flags", g["final_passed_peri"], st.passed_peri)
     check("inward flags", g["final_vr_neg"], st.vr_neg)
+    check("doomed flags", g["final_doomed"], st.doomed)
+    check("woken", int(g["woken"]), st.woken)
     check("final x", g["final_x"], st.x, rtol=1e-13, per_vector=True)
     check("final p", g["final_p"], st.p, rtol=1e-11, per_vector=True)
     check("final u", g["final_u"], st.u, rtol=1e-9)
@@ -477,5 +480,32 @@ def test_removal_block_steps_match_reference():
     check("removed mass", float(g["removed_mass"]), st.removed.mass, rtol=1e-13)
     check("removed energy", float(g["removed_energy"]), st.removed.energy, rtol=1e-10)
     check("removed angmom", g["removed_angmom"], st.removed.angmom, rtol=1e-10, per_vector=True)
+    check("final energy", float(g["final_energy"]), steps.blocks_ledger(st, bc)["energy"],
+          rtol=1e-12)  # fmt: skip
+
+
+def _wake_bc():
+    from blackhole_nebula_simulator_b200.config import BlockConfig, CoupledConfig
+
+    hc, CC = _cfg()
+    return BlockConfig(coupled=CC(hydro=hc, cooling_beta=230.0), dt_max=64.0, r_acc=382.0,
+                       removal_sync=True)  # fmt: skip
+
+
+def test_removal_wake_matches_reference():
+    g = golden("removal_wake_blocks.npz")
+    bc = _wake_bc()
+    st = steps.blocks_initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc, t_stop=1e6,
+                                 level_offset=g["level_offset"])  # fmt: skip
+    actives = [len(steps.blocks_advance(st, bc)) for _ in range(len(g["active_counts"]))]
+    check("active counts", g["active_counts"], np.array(actives))
+    check("woken", int(g["woken"]), st.woken)
+    check("removed ids", g["log_id"], np.array([e["id"] for e in st.removed.log]))
+    check("remaining ids", g["final_ids"], st.ids)
+    for f in ("level", "n_beg", "n_end", "doomed"):
+        check(f"final {f}", g[f"final_{f}"], getattr(st, f))
+    check("final x", g["final_x"], st.x, rtol=1e-13, per_vector=True)
+    check("final p", g["final_p"], st.p, rtol=1e-11, per_vector=True)
+    check("final u", g["final_u"], st.u, rtol=1e-9)
     check("final energy", float(g["final_energy"]), steps.blocks_ledger(st, bc)["energy"],
           rtol=1e-12)  # fmt: skip
