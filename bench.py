@@ -380,21 +380,23 @@ def deposit_frame(gg, x, h, m, t, v, grid, box, host=False):
     return a, b
 
 
-def cpu_deposit(n_sample):
+def cpu_deposit(n_sample, n_full=4_194_304):
     """The reference's deposition on the host cores: the oracle (C, one thread, the reference's
-    two fixed chunks one after the other) on the first n_sample particles of the frame."""
+    two fixed chunks one after the other) on the first n_sample particles of the frame's
+    snapshot (the same smoothing lengths as the whole snapshot's)."""
     from blackhole_nebula_simulator_b200 import gasgrid as gg
     from oracle import deposit as odep
 
-    x, h, m, t, v = deposit_inputs(n_sample)
+    x, h, m, t, v = (a[:n_sample] for a in deposit_inputs(n_full))
     grid, box = gg.LogSphericalGrid(), gg.CartesianBox(**DEPOSIT_BOX)
     t0 = time.perf_counter()
     odep.deposit_log_split(x, h, m, t, v, grid, gg.coarse_log_grid(grid))
     odep.deposit_box(x, h, m, t, v, box)
     dt = time.perf_counter() - t0
     return {"value": n_sample / dt, "unit": "particles/s", "cores": 1, "kind": "port",
-            "sample": f"torus snapshot, {n_sample} particles, one frame (log-spherical 192x96x192 "
-                      "split + 160^3 box), oracle in C on one thread"}  # fmt: skip
+            "sample": f"the first {n_sample} particles of the {n_full}-particle torus snapshot, one "
+                      "frame (log-spherical 192x96x192 split + 160^3 box), oracle in C on one "
+                      "thread"}  # fmt: skip
 
 
 def run_deposit(args, rank, world):
@@ -413,7 +415,7 @@ def run_deposit(args, rank, world):
     metric = "particles deposited/s"
     if args.impl == "reference":
         if rank == 0:
-            cb = cpu_deposit(min(n, 4_096))
+            cb = cpu_deposit(min(n, 131_072), n)
             print(json.dumps({"metric": metric, "value": cb["value"], "unit": "particles/s",
                               "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                               "higher_is_better": True, "impl": "reference", "dtype": "f64",
@@ -465,7 +467,7 @@ def run_deposit(args, rank, world):
     pk = peaks()
     achieved = alg / (ms_t / args.steps * 1e-3) / 1e9
     if rank == 0:
-        cb = None if args.no_cpu_baseline else cpu_deposit(min(n, 4_096))
+        cb = None if args.no_cpu_baseline else cpu_deposit(min(n, 131_072), n)
         print(json.dumps({
             "metric": metric, "value": total / (ms_t * 1e-3), "unit": "particles/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,

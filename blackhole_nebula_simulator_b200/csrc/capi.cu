@@ -448,6 +448,35 @@ int nb_eos(nb_ctx* ctx, int64_t n, const double* rho, const double* u, const nb_
 }
 
 // ---------------------------------------------------------------- grid deposition
+// Large inputs are deposited in the spatial order of their centres' cells (sorted keys, gathered
+// copies of the particle data): neighbouring threads then add to neighbouring cells.
+constexpr int64_t DEPOSIT_SORT_MIN = 1 << 16;
+
+static int deposit_order(Engine& E, int64_t n, int kind, const nbk::LogGeom& g, double x0,
+                         double y0, double z0, double dx, int nb, const double*& x,
+                         const double*& h, const double*& m, const double*& t, const double*& v,
+                         cudaStream_t st) {
+  if (n < DEPOSIT_SORT_MIN) return 0;
+  NB_TRY(E.ensure_deposit(n));
+  nbk::launch_deposit_keys(n, x, kind, g, x0, y0, z0, dx, nb, E.dep_k0, E.dep_i0, st);
+  const unsigned long long max_key =
+      kind == 0 ? (unsigned long long)(g.nr + 2) * g.nth * g.nph
+                : (unsigned long long)(nb + 2) * (nb + 2) * (nb + 2);
+  int bits = 1;
+  while (bits < 64 && (1ull << bits) <= max_key) ++bits;
+  cub::DoubleBuffer<unsigned long long> kb(E.dep_k0, E.dep_k1);
+  cub::DoubleBuffer<int32_t> vb(E.dep_i0, E.dep_i1);
+  size_t tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceRadixSort::SortPairs(E.cub_tmp, tmp, kb, vb, (int)n, 0, bits, st));
+  nbk::launch_deposit_gather(n, vb.Current(), x, h, m, t, v, E.dep_buf, st);
+  x = E.dep_buf;
+  h = E.dep_buf + 3 * n;
+  m = h + n;
+  t = m + n;
+  v = t + n;
+  return 0;
+}
+
 static int deposit_finish_host(nbk::Engine& E, double* outside, int64_t* n_trilinear,
                                cudaStream_t st) {
   NB_CUDA(cudaGetLastError());
@@ -475,6 +504,7 @@ int nb_deposit_log(nb_ctx* ctx, int64_t n, const double* x, const double* h, con
   NB_CUDA(cudaMemsetAsync(E.ws.d_scal, 0, sizeof(double), st));
   NB_CUDA(cudaMemsetAsync(E.ws.d_i64, 0, sizeof(int64_t), st));
   nbk::LogGeom g{r_min, dlnr, dth, dph, nr, nth, nph, sth, cth, dcth, cph, sph};
+  NB_TRY(deposit_order(E, n, 0, g, 0.0, 0.0, 0.0, 0.0, 0, x, h, m, t, v, st));
   nbk::launch_deposit_log(n, x, h, m, t, v, g, kernel_id, acc, E.ws.d_scal,
                           (unsigned long long*)E.ws.d_i64, st);
   return deposit_finish_host(E, outside, n_trilinear, st);
@@ -495,6 +525,8 @@ int nb_deposit_box(nb_ctx* ctx, int64_t n, const double* x, const double* h, con
   NB_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * nbk::DEP_FIELDS * ncell, st));
   NB_CUDA(cudaMemsetAsync(E.ws.d_scal, 0, sizeof(double), st));
   NB_CUDA(cudaMemsetAsync(E.ws.d_i64, 0, sizeof(int64_t), st));
+  const nbk::LogGeom none{};
+  NB_TRY(deposit_order(E, n, 1, none, x0, y0, z0, dx, nb, x, h, m, t, v, st));
   nbk::launch_deposit_box(n, x, h, m, t, v, x0, y0, z0, dx, nb, kernel_id, acc, E.ws.d_scal,
                           (unsigned long long*)E.ws.d_i64, st);
   return deposit_finish_host(E, outside, n_trilinear, st);

@@ -366,6 +366,78 @@ __global__ void k_refine_scale(int64_t nval, const double* __restrict__ sums, do
   if (fine > 0.0) out[e] *= coarse / fine;
 }
 
+// ---------------------------------------------------------------- spatial order
+// The particles are dealt to the deposition threads in the order of the cell holding their
+// centre, so neighbouring threads add to neighbouring cells while those lines sit in L2 (in the
+// caller's order each atomic add of a large grid travels to DRAM).  Keys: the grid's own linear
+// cell index, with the out-of-grid cells clamped to one layer beyond each face.
+__global__ void k_dep_keys_box(int64_t n, const double* __restrict__ x, double x0, double y0,
+                               double z0, double dx, int nb, unsigned long long* keys,
+                               int32_t* idx) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int e = nb + 2;
+  const int a = min(max((int)floor((x[3 * p] - x0) / dx), -1), nb) + 1;
+  const int b = min(max((int)floor((x[3 * p + 1] - y0) / dx), -1), nb) + 1;
+  const int c = min(max((int)floor((x[3 * p + 2] - z0) / dx), -1), nb) + 1;
+  keys[p] = ((unsigned long long)a * e + b) * e + c;
+  idx[p] = (int32_t)p;
+}
+
+__global__ void k_dep_keys_log(int64_t n, const double* __restrict__ x, double r_min, double dlnr,
+                               double dth, double dph, int nr, int nth, int nph,
+                               unsigned long long* keys, int32_t* idx) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double xp = x[3 * p], yp = x[3 * p + 1], zp = x[3 * p + 2];
+  const double rr = sqrt(xp * xp + yp * yp + zp * zp);
+  const int i = min(max((int)floor(log(rr / r_min) / dlnr), -1), nr) + 1;
+  const int j = min(max((int)floor(acos(fmin(1.0, fmax(-1.0, zp / rr))) / dth), 0), nth - 1);
+  const int k = min(max((int)floor(py_mod(atan2(yp, xp), 2.0 * 3.141592653589793) / dph), 0), nph - 1);
+  keys[p] = ((unsigned long long)i * nth + j) * nph + k;
+  idx[p] = (int32_t)p;
+}
+
+__global__ void k_dep_gather(int64_t n, const int32_t* __restrict__ idx,
+                             const double* __restrict__ x, const double* __restrict__ h,
+                             const double* __restrict__ m, const double* __restrict__ t,
+                             const double* __restrict__ v, double* __restrict__ out) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int64_t p = idx[q];
+  double* xs = out;
+  double* hs = out + 3 * n;
+  double* ms = hs + n;
+  double* ts = ms + n;
+  double* vs = ts + n;
+  for (int c = 0; c < 3; ++c) {
+    xs[3 * q + c] = x[3 * p + c];
+    vs[3 * q + c] = v[3 * p + c];
+  }
+  hs[q] = h[p];
+  ms[q] = m[p];
+  ts[q] = t[p];
+}
+
+void launch_deposit_keys(int64_t n, const double* x, int grid_kind, const LogGeom& g, double x0,
+                         double y0, double z0, double dx, int nb, unsigned long long* keys,
+                         int32_t* idx, cudaStream_t st) {
+  if (n <= 0) return;
+  if (grid_kind == 0)
+    count_launch(), k_dep_keys_log<<<grid_for(n), NB_THREADS, 0, st>>>(
+        n, x, g.r_min, g.dlnr, g.dth, g.dph, g.nr, g.nth, g.nph, keys, idx);
+  else
+    count_launch(), k_dep_keys_box<<<grid_for(n), NB_THREADS, 0, st>>>(n, x, x0, y0, z0, dx, nb,
+                                                                        keys, idx);
+}
+
+void launch_deposit_gather(int64_t n, const int32_t* idx, const double* x, const double* h,
+                           const double* m, const double* t, const double* v, double* out,
+                           cudaStream_t st) {
+  if (n > 0)
+    count_launch(), k_dep_gather<<<grid_for(n), NB_THREADS, 0, st>>>(n, idx, x, h, m, t, v, out);
+}
+
 // ---------------------------------------------------------------- launchers
 void launch_deposit_log(int64_t n, const double* x, const double* h, const double* m,
                         const double* t, const double* v, const LogGeom& g, int kid,

@@ -29,4 +29,13 @@ void launch_refine_sums(const double* acc_c, const double* vol_c, int nrc, int n
                         const double* vol_f, int nr, int nth, int nph, int cr, int ct, int cp,
                         double* out, double* sums2, cudaStream_t st);
 
+// spatial order of the particles (grid_kind 0: log grid g, 1: box): keys and identity indices
+void launch_deposit_keys(int64_t n, const double* x, int grid_kind, const LogGeom& g, double x0,
+                         double y0, double z0, double dx, int nb, unsigned long long* keys,
+                         int32_t* idx, cudaStream_t st);
+// out (9 n doubles): x (3n), h, m, t, v (3n) gathered in idx order
+void launch_deposit_gather(int64_t n, const int32_t* idx, const double* x, const double* h,
+                           const double* m, const double* t, const double* v, double* out,
+                           cudaStream_t st);
+
 }  // namespace nbk

@@ -131,6 +131,30 @@ int Engine::ensure_ell(int64_t m) {
   return grow(E, ell, cap_ell, m);
 }
 
+int Engine::ensure_deposit(int64_t n) {
+  Engine& E = *this;
+  if (n > dep_cap || !dep_buf) {
+    void* ps[] = {dep_k0, dep_k1, dep_i0, dep_i1, dep_buf};
+    for (void* p : ps)
+      if (p) cudaFree(p);
+    dep_k0 = dep_k1 = nullptr;
+    dep_i0 = dep_i1 = nullptr;
+    dep_buf = nullptr;
+    const int64_t c = std::max<int64_t>(n + n / 4, 1024);
+    NB_CUDA(cudaMalloc((void**)&dep_k0, sizeof(unsigned long long) * c));
+    NB_CUDA(cudaMalloc((void**)&dep_k1, sizeof(unsigned long long) * c));
+    NB_CUDA(cudaMalloc((void**)&dep_i0, sizeof(int32_t) * c));
+    NB_CUDA(cudaMalloc((void**)&dep_i1, sizeof(int32_t) * c));
+    NB_CUDA(cudaMalloc((void**)&dep_buf, sizeof(double) * 9 * c));
+    dep_cap = c;
+  }
+  size_t b = 0;
+  cub::DeviceRadixSort::SortPairs((void*)nullptr, b, (unsigned long long*)nullptr,
+                                  (unsigned long long*)nullptr, (int32_t*)nullptr,
+                                  (int32_t*)nullptr, (int)dep_cap);
+  return ensure_cub(b);
+}
+
 int Engine::ensure_sort_keys(int64_t m) {
   Engine& E = *this;
   NB_TRY(grow(E, sort_keys, cap_sort, m));
@@ -138,7 +162,7 @@ int Engine::ensure_sort_keys(int64_t m) {
 }
 
 void Engine::release() {
-  void* ps[] = {d_err, bbox, bbox_part, keys_a, keys_b, vals_a, counts, node_lo, node_hi, sub_lo, sub_hi,
+  void* ps[] = {dep_k0, dep_k1, dep_i0, dep_i1, dep_buf, d_err, bbox, bbox_part, keys_a, keys_b, vals_a, counts, node_lo, node_hi, sub_lo, sub_hi,
                 cub_tmp, sort_keys, red, lists.perm, lists.inv_perm, lists.spos, lists.off,
                 lists.idx, ell, d_rowmax, tidx};
   for (void* p : ps)

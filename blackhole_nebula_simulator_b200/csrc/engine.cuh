@@ -164,6 +164,13 @@ struct Engine {
   void* cub_tmp = nullptr;
   size_t cub_bytes = 0;
   int64_t* sort_keys = nullptr;
+  // particle -> grid deposition: spatial sort keys / indices (double buffers) and the gathered
+  // particle data (9 doubles per particle)
+  unsigned long long *dep_k0 = nullptr, *dep_k1 = nullptr;
+  int32_t *dep_i0 = nullptr, *dep_i1 = nullptr;
+  double* dep_buf = nullptr;
+  int64_t dep_cap = 0;
+  int ensure_deposit(int64_t n);
   // one-pass list build: rows written to fixed-width slots (row_cap entries each), then packed
   int32_t* ell = nullptr;
   int64_t cap_ell = 0, row_cap = 256;

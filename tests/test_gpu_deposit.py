@@ -99,3 +99,34 @@ def test_empty_and_bad_inputs(gg):
         gg.deposit_box(g["xb"], g["hb"], g["m"], g["t"], g["v"], bx, "quintic")
     with pytest.raises(ValueError, match="divisible"):
         gg.coarse_log_grid(gg.LogSphericalGrid(nr=63, nth=32, nph=64), (2, 4, 4))
+
+
+def test_large_inputs_in_spatial_order_match_the_oracle(gg):
+    """70,000 particles: above the size from which the device deals particles to threads in the
+    spatial order of their cells; against the CPU oracle (the reference's order)."""
+    from oracle import deposit as odep
+
+    rng = np.random.default_rng(21)
+    n = 70_000
+    lg = gg.LogSphericalGrid(r_min=2.0, r_max=200.0, nr=24, nth=12, nph=24)
+    r = np.exp(rng.uniform(np.log(3.0), np.log(220.0), n))
+    d = rng.normal(size=(n, 3))
+    x = r[:, None] * d / np.linalg.norm(d, axis=1, keepdims=True)
+    h = r * lg.dlnr * np.exp(rng.uniform(np.log(0.2), np.log(3.0), n))
+    m = rng.uniform(0.5, 2.0, n)
+    t = np.exp(rng.uniform(np.log(1e4), np.log(1e7), n))
+    v = rng.normal(0.0, 0.05, (n, 3))
+    ref = odep.deposit_log(x, h, m, t, v, lg)
+    res = gg.deposit_log(x, h, m, t, v, lg)
+    scale = np.abs(ref["mass"]).max()
+    check("log mass", ref["mass"] / scale, _np(res.mass) / scale, atol=1e-12)
+    check("log outside", ref["outside"], res.outside, rtol=1e-12)
+    check("log trilinear count", ref["n_trilinear"], res.n_trilinear)
+    bx = gg.CartesianBox(centre=(0.0, 0.0, 0.0), size=300.0, n=32)
+    hb = bx.dx * np.exp(rng.uniform(np.log(0.2), np.log(2.0), n))
+    ref = odep.deposit_box(x, hb, m, t, v, bx)
+    res = gg.deposit_box(x, hb, m, t, v, bx)
+    scale = np.abs(ref["mass"]).max()
+    check("box mass", ref["mass"] / scale, _np(res.mass) / scale, atol=1e-12)
+    check("box outside", ref["outside"], res.outside, rtol=1e-12)
+    check("box trilinear count", ref["n_trilinear"], res.n_trilinear)
