@@ -49,6 +49,12 @@ __device__ void log_pass(const LogGeom& g, double xp, double yp, double zp, doub
                          double& outside) {
   const double big = 2.0 * hp;
   const double ct0 = cos(th), st0 = sin(th);
+  // q < 2 decided on d^2 against (2h)^2 with a relative margin of 1e-12 (sqrt(d^2) / h only
+  // inside the margin); the weights take q = sqrt(d^2) (1 / h), within an ulp of the
+  // reference's quotient
+  const double big2 = big * big;
+  const double in2 = big2 * (1.0 - 1e-12), out2 = big2 * (1.0 + 1e-12);
+  const double ih = 1.0 / hp;
   for (int i = i_lo; i <= i_hi; ++i) {
     const double rc = g.r_min * exp((i + 0.5) * g.dlnr);
     const double cos_a = (rc * rc + rr * rr - big * big) / (2.0 * rc * rr);
@@ -91,8 +97,12 @@ __device__ void log_pass(const LogGeom& g, double xp, double yp, double zp, doub
         const int k = py_imod(kk, g.nph);
         const double dxc = rst * g.cph[k] - xp;
         const double dyc = rst * g.sph[k] - yp;
-        const double q = sqrt(dxc * dxc + dyc * dyc + dzc * dzc) / hp;
-        if (q < 2.0) {
+        const double dd = dxc * dxc + dyc * dyc + dzc * dzc;
+        if (dd >= out2) continue;
+        const double r = sqrt(dd);
+        if (dd >= in2 && !(r / hp < 2.0)) continue;
+        const double q = r * ih;
+        {
           if (MODE == 0) {
             n_in += 1;
             wsum += kernel_f<double>(q, kid) * vrt;
@@ -202,6 +212,7 @@ __global__ void k_deposit_box(int64_t n, const double* __restrict__ x,
     if (dd >= out2) return false;
     return sqrt(dd) / hp < 2.0;
   };
+  const double ih = 1.0 / hp;  // weights take q = sqrt(d^2) (1 / h), within an ulp of d / h
   auto chord = [&](double dxy2, int& lo, int& hi) {
     const double s = sqrt(fmax(out2 - dxy2, 0.0));
     lo = max(c0, (int)floor((zp - s - z0) / dx) - 1);
@@ -225,7 +236,7 @@ __global__ void k_deposit_box(int64_t n, const double* __restrict__ x,
         const double dd = dxc * dxc + dyc * dyc + dzc * dzc;
         if (inside(dd)) {
           n_in += 1;
-          if (!beyond) wsum += kernel_f<double>(sqrt(dd) / hp, kid);
+          if (!beyond) wsum += kernel_f<double>(sqrt(dd) * ih, kid);
         }
       }
     }
@@ -248,7 +259,7 @@ __global__ void k_deposit_box(int64_t n, const double* __restrict__ x,
           const double dzc = z0 + (c + 0.5) * dx - zp;
           const double dd = dxc * dxc + dyc * dyc + dzc * dzc;
           if (inside(dd)) {
-            const double w = kernel_f<double>(sqrt(dd) / hp, kid) * inv;
+            const double w = kernel_f<double>(sqrt(dd) * ih, kid) * inv;
             if (0 <= a && a < nb && 0 <= b && b < nb && 0 <= c && c < nb)
               add_cell(acc, ((int64_t)a * nb + b) * nb + c, w, vals);
             else
