@@ -1071,6 +1071,17 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   fp.use_disc = prm->disc_alpha_av > 0;
   fp.disc_alpha_av = prm->disc_alpha_av;
   fp.tighten = 1;
+  const bool want_tight = sk.want_tight && prm->limiter && rows == W.rows;
+  W.tight_ver = -1;
+  if (want_tight) {
+    NB_TRY(E.ensure_tight(L.total));
+    fp.tidx = E.tidx;
+    fp.tcnt = W.i32a;
+    if (prm->precision == 1) {
+      count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, s->h, W.pk0);
+      fp.pos64 = W.pk0;
+    }
+  }
   if (recon) {
     fp.use_recon = 1;
     fp.closeness = prm->recon_closeness;
@@ -1098,6 +1109,11 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
     E.prof.begin(st);
     launch_forces64<int32_t>(nrows, W.rows_s, W.pk0, W.pk1, W.pk2, W.pk3, L.off, L.idx, fp,
                              L.perm, fo, st);
+  }
+  if (want_tight) {
+    W.tight_ver = W.rows_ver;
+    W.tight_gen = L.gen;
+    W.tight_n = nrows;
   }
   if (E.prof.on) {
     E.prof.end(PROF_FORCES, st, (double)nrows, 0.0);

@@ -70,6 +70,9 @@ struct Workspace {
   // W.rows (the active rows of the current step) changes version whenever it is rewritten; the
   // sorted copy in rows_s is kept while the rows and the lists stay the same
   int64_t rows_ver = 0, rs_ver = -1, rs_gen = -1, rs_n = -1, rs_count = 0;
+  // the rows' interacting entries in E.tidx / i32a, written by the force pass of these rows
+  // (rows version, lists generation, row count), for the level choice that follows
+  int64_t tight_ver = -1, tight_gen = -1, tight_n = -1;
   // checks whose results are read at the next host synchronisation instead of a round trip of
   // their own: the device error word, the flow's worst iteration code (d_scal_i[0]) and a
   // radiated-energy sum (d_scal[0]) to add to *pend_erad

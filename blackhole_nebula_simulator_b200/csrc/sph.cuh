@@ -31,6 +31,12 @@ struct ForceParams {
   double eta_crit = 0.0, eta_fold = 0.2;
   const double* gv64 = nullptr;
   const float* gv32 = nullptr;
+  // the rows' interacting entries for the level limiter (self included, list order) into tidx
+  // (the lists' layout) and their counts into tcnt (row order); the FP32 form decides entries
+  // within 1e-5 of the boundary from the sorted FP64 (x, y, z, h) in pos64
+  int32_t* tidx = nullptr;
+  int32_t* tcnt = nullptr;
+  const double4* pos64 = nullptr;
 };
 
 // Corrected velocity (and acceleration) gradients, sim/sph.py:693-902.

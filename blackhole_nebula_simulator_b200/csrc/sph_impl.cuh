@@ -718,8 +718,12 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? (RECON ? 2 : FORC
     __syncwarp();
     pc = 0;
   };
+  // with prm.tidx the row's interacting entries (self included), in list order, are also
+  // written out for the level limiter: exactly the reference's FP64 test, which the FP32 form
+  // takes from prm.pos64 where its float test falls within 1e-5 of the boundary
+  int m_tot = 0;
   for (unsigned base = 0; base < maxlen; base += 8) {
-    bool take = false;
+    bool take = false, tight = false;
     int64_t b = 0;
     if (base + gl < len) {
       b = (int64_t)ld_stream(idx + e_beg + base + gl);
@@ -730,16 +734,34 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? (RECON ? 2 : FORC
           geo.diff(a, b, ddx, ddy, ddz);
           const R h_b = (R)hydro[b].x;
           R rr = R(2) * (h_a > h_b ? h_a : h_b);
-          take = sqdist(ddx, ddy, ddz) < rr * rr;
+          const R d2 = sqdist(ddx, ddy, ddz), r2 = rr * rr;
+          take = d2 < r2;
+          if constexpr (sizeof(R) == 4) {
+            if (prm.pos64 && d2 > r2 * R(1.0 - 1e-5) && d2 < r2 * R(1.0 + 1e-5)) {
+              const double4 pa = prm.pos64[a], pb = prm.pos64[b];
+              const double e2 = d2_exact(pb.x - pa.x, pb.y - pa.y, pb.z - pa.z);
+              const double er = 2.0 * fmax(pa.w, pb.w);
+              take = e2 < er * er;
+            }
+          }
         }
+        tight = take;
+      } else {
+        tight = true;  // self: listed for the limiter, not a pair
       }
     }
     unsigned seg = (__ballot_sync(FULL, take) >> (8 * g)) & 0xffu;
     if (take) pq[pc + __popc(seg & ((1u << gl) - 1u))] = (int32_t)b;
     pc += __popc(seg);
+    if (prm.tidx) {
+      const unsigned tseg = (__ballot_sync(FULL, tight) >> (8 * g)) & 0xffu;
+      if (tight) prm.tidx[e_beg + m_tot + __popc(tseg & ((1u << gl) - 1u))] = (int32_t)b;
+      m_tot += __popc(tseg);
+    }
     if (__any_sync(FULL, pc > FORCE_QUEUE - 8)) drain();
   }
   drain();
+  if (prm.tcnt && live && gl == 0) prm.tcnt[q] = m_tot;
   // sums over the row's eight lanes (uniform flags: every lane takes part in every reduction)
   double s_ax = 0, s_ay = 0, s_az = 0, s_work = 0, s_heat = 0, s_vheat = 0, s_cheat = 0;
   double s_dax = 0, s_day = 0, s_daz = 0, s_dheat = 0;

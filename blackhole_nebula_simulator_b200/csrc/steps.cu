@@ -626,10 +626,15 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
     // curve-ordered rows, sorted (x, h) and a sorted copy of the levels
     NB_TRY(sorted_rows_and_pack(E, nrows, rows, s->x, s->h, &ns, st));
     count_launch(), k_gather_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, W.i_lvl);
-    // the rows' interacting entries, once for every sweep and the wake-up walk
-    NB_TRY(E.ensure_tight(L.total));
-    count_launch(), k_tight_rows<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,
-                                                                       E.tidx, W.i32a);
+    // the rows' interacting entries, once for every sweep and the wake-up walk (already written
+    // by the force pass of these rows on these lists, when it ran just before)
+    const bool have_tight = rows == W.rows && W.tight_ver == W.rows_ver &&
+                            W.tight_gen == L.gen && W.tight_n == nrows;
+    if (!have_tight) {
+      NB_TRY(E.ensure_tight(L.total));
+      count_launch(), k_tight_rows<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,
+                                                                         E.tidx, W.i32a);
+    }
     bool settled = false;
     for (int sweep = 0; sweep < 4096; ++sweep) {
       NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
@@ -685,6 +690,7 @@ int block_initialise(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t 
   launch_v_from_p(n, s->x, s->p, W.v_eval, st);
   ShockStep sk;
   sk.recon_full = 1;
+  sk.want_tight = 1;
   NB_TRY(hydro_rows(E, s, prm, n, W.rows, W.v_eval, s->u, st, sk));
   count_launch(), k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, 0, s->level);
   NB_TRY(choose_levels_and_open(E, s, prm, n, W.rows, st));
@@ -745,6 +751,7 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   sk.n_end = s->n_end;
   sk.tick = s->tick;
   sk.recon_full = 1;
+  sk.want_tight = 1;
   NB_TRY(hydro_rows(E, s, prm, nrows, W.rows, W.v_eval, s->u, st, sk));
   // the evaluation's velocities and (predicted) energies, for a removal that recomputes forces
   const bool split = v_eval_out != nullptr;
@@ -784,6 +791,7 @@ int block_finish(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, co
   if (redo && nrows > 0) {
     ShockStep sk;
     sk.recon_full = 1;
+  sk.want_tight = 1;
     NB_TRY(hydro_rows(E, s, prm, nrows, W.rows, v_eval, u_eval, st, sk));
   }
   E.prof.begin(st);

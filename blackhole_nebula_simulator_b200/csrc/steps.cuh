@@ -21,6 +21,7 @@ struct ShockStep {
   const int64_t* n_end = nullptr;
   double tick = 0.0;
   int recon_full = 0;
+  int want_tight = 0;  // block steps: the force pass also writes the rows' interacting entries
 };
 
 int compute_density(Engine& E, int64_t n, const double* x, const double* mass, double* h,
