@@ -41,7 +41,7 @@ FLOP_PER_FORCE_PAIR = 75.0  # pressure + viscosity + P dV (+20 with disc viscosi
 # DRAM bytes (read + write) per row of one launch, from ncu captures of the FP32 kernels on the
 # 1,048,576-particle torus (profiles/k_forces_g_torus1m.md, profiles/k_density_torus1m.md),
 # scaled to a launch by its rows
-DRAM_BYTES_PER_ROW = {"forces": 1209.0, "density": 1003.0}
+DRAM_BYTES_PER_ROW = {"forces": 1768.0, "density": 1003.0}
 
 
 def peaks():
