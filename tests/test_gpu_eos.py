@@ -115,3 +115,30 @@ def test_gasrad_block_steps_match_reference(nb):
     check("final dudt", g["final_dudt"], _np(st.dudt), rtol=1e-8,
           atol=1e-9 * np.abs(g["final_dudt"]).max())  # fmt: skip
     check("final energy", float(g["final_energy"]), blocks.ledger(st, bc)["energy"], rtol=1e-12)
+
+
+def test_gasrad_fp32_within_stated_tolerance(nb):
+    """The FP32 form with gas + radiation against the FP64 form on the gasrad_blocks cloud
+    (12 block steps; levels and active counts must agree, the rest at the FP32 tolerances of
+    tests/test_gpu_fp32_errors.py)."""
+    from blackhole_nebula_simulator_b200.config import BlockConfig, CoupledConfig, HydroConfig
+    from tests.test_gpu_fp32_errors import TOL
+
+    _, blocks = nb
+    g = golden("gasrad_blocks.npz")
+    out = []
+    for prec in ("fp64", "fp32"):
+        hc = HydroConfig(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                         conductivity_signal=1, alpha_u=0.05, h_max=200.0, eos="gasrad",
+                         precision=prec)  # fmt: skip
+        bc = BlockConfig(coupled=CoupledConfig(hydro=hc), dt_max=64.0)
+        st = blocks.initialise(g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc, t_stop=1e6)
+        act = [len(blocks.advance(st, bc)) for _ in range(12)]
+        out.append((st, act))
+    (a, act_a), (b, act_b) = out
+    check("active counts", np.array(act_a), np.array(act_b))
+    check("levels", _np(a.level), _np(b.level))
+    for f in ("h", "rho", "u"):
+        check(f, _np(getattr(a, f)), _np(getattr(b, f)), rtol=TOL[f])
+    check("x", _np(a.x), _np(b.x), rtol=TOL["x"], per_vector=True)
+    check("p", _np(a.p), _np(b.p), rtol=TOL["p"], per_vector=True)
