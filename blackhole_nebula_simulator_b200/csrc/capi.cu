@@ -30,6 +30,7 @@ int begin(nb_ctx* ctx) {
   // checks left pending by a call that failed part-way belong to that call
   E.ws.pend_err = E.ws.pend_glf = false;
   E.ws.pend_erad = nullptr;
+  E.ws.pend_woken = nullptr;
   NB_CUDA(cudaSetDevice(E.device));
   return 0;
 }

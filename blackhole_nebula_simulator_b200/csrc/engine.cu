@@ -749,6 +749,8 @@ int pending_enqueue(Engine& E, cudaStream_t st) {
     NB_CUDA(cudaMemcpyAsync(W.h_i64 + 8, W.d_scal_i, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   if (W.pend_erad)
     NB_CUDA(cudaMemcpyAsync(W.h_dbl + 72, W.d_scal, sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (W.pend_woken)
+    NB_CUDA(cudaMemcpyAsync(W.h_i64 + 10, W.d_scal_i + 2, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   return 0;
 }
 
@@ -757,6 +759,10 @@ int pending_finish(Engine& E, cudaStream_t st) {
   if (W.pend_erad) {
     *W.pend_erad += W.h_dbl[72];
     W.pend_erad = nullptr;
+  }
+  if (W.pend_woken) {
+    *W.pend_woken += W.h_i64[10];
+    W.pend_woken = nullptr;
   }
   if (W.pend_glf) {
     W.pend_glf = false;
@@ -780,7 +786,7 @@ int pending_finish(Engine& E, cudaStream_t st) {
 // the pending checks on their own (at the end of a step entry point)
 int pending_flush(Engine& E, cudaStream_t st) {
   Workspace& W = E.ws;
-  if (!W.pend_err && !W.pend_glf && !W.pend_erad) return 0;
+  if (!W.pend_err && !W.pend_glf && !W.pend_erad && !W.pend_woken) return 0;
   NB_TRY(pending_enqueue(E, st));
   NB_CUDA(cudaStreamSynchronize(st));
   return pending_finish(E, st);

@@ -78,6 +78,7 @@ struct Workspace {
   // radiated-energy sum (d_scal[0]) to add to *pend_erad
   bool pend_err = false, pend_glf = false;
   double* pend_erad = nullptr;
+  int64_t* pend_woken = nullptr;  // the level choice's wake-up count (d_scal_i[2]) to add here
   double* d_scal = nullptr;
   int64_t* d_scal_i = nullptr;
   // switch and velocity reconstruction only (allocated on first use): sorted accelerations and

@@ -635,12 +635,18 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
       count_launch(), k_tight_rows<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,
                                                                          E.tidx, W.i32a);
     }
+    // small active sets: sweeps in batches of 4 between host reads (a sweep costs microseconds,
+    // a round trip more), each with its own change flag; a sweep that changes nothing leaves a
+    // fixed point, which later sweeps keep, so the batch's last flag says whether the levels
+    // have settled.  Large sets: one sweep per read (a sweep costs more than the round trip).
+    const int batch = ns < 65536 ? 4 : 1;
     bool settled = false;
-    for (int sweep = 0; sweep < 4096; ++sweep) {
-      NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
-      count_launch(), k_limit_sweep_t<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, E.tidx, W.i32a,
-                                                                           prm->max_gap, W.i_lvl, W.d_int);
-      NB_CUDA(cudaMemcpyAsync(W.h_int, W.d_int, sizeof(int), cudaMemcpyDeviceToHost, st));
+    for (int sweep = 0; sweep < 4096; sweep += batch) {
+      NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int) * batch, st));
+      for (int b = 0; b < batch; ++b)
+        count_launch(), k_limit_sweep_t<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(
+            ns, W.rows_s, L.off, E.tidx, W.i32a, prm->max_gap, W.i_lvl, W.d_int + b);
+      NB_CUDA(cudaMemcpyAsync(W.h_int, W.d_int + batch - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
       NB_TRY(pending_enqueue(E, st));
       NB_CUDA(cudaStreamSynchronize(st));
       NB_TRY(pending_finish(E, st));
@@ -661,15 +667,13 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
     count_launch(), k_wake_need_t<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, E.tidx, W.i32a,
                                                                      W.i_lvl, prm->max_gap, W.i_tmp2);
     count_launch(), k_scatter_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, W.i_tmp2, W.need);
-    NB_CUDA(cudaMemsetAsync(W.d_i64, 0, sizeof(int64_t), st));
+    // the wake-up count is read with the step's last checks (no round trip of its own)
+    if (W.pend_woken) NB_TRY(pending_flush(E, st));
+    NB_CUDA(cudaMemsetAsync(W.d_scal_i + 2, 0, sizeof(int64_t), st));
     count_launch(), k_cut_steps<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->tick_n, s->tick, W.need, s->a_hydro,
                                                     s->dudt, s->level, s->n_end, s->p_half,
-                                                    s->u_half, (unsigned long long*)W.d_i64, E.d_err);
-    NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    NB_TRY(pending_enqueue(E, st));
-    NB_CUDA(cudaStreamSynchronize(st));
-    NB_TRY(pending_finish(E, st));
-    s->woken += W.h_i64[0];
+                                                    s->u_half, (unsigned long long*)(W.d_scal_i + 2), E.d_err);
+    W.pend_woken = &s->woken;
   }
   count_launch(), k_open<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, s->tick_n, s->tick, s->level, s->x,
                                                  s->p, s->u, s->a_hydro, s->dudt, s->n_beg,
