@@ -107,6 +107,30 @@ def density_numba(pos, mass, h_start, nb: Neighbours, h_search, kernel_name=DEFA
     return DensityResult(h_out, rho, om, it, fl, nb)
 
 
+FLAG_SEARCH_TOO_SMALL = 2  # sim/sph.py density flags: the search radius was too small
+
+
+def compute_density(pos, mass, h_guess, kernel_name=DEFAULT_KERNEL, eta=DEFAULT_ETA, tol=1e-4,
+                    h_max=math.inf, skin=1.4) -> DensityResult:  # fmt: skip
+    """sim/sph.py:329-387 without a list cache (each call builds its lists): lists with search
+    radius 2 min(h_guess, h_max) x skin; particles whose h outgrows the search are redone with
+    rebuilt lists and their search doubled, up to 12 rounds (RuntimeError beyond)."""
+    pos = dev_f64(pos)
+    n = len(pos)
+    h_guess = dev_f64(h_guess, (n,)).clone()
+    h_search = torch.clamp(h_guess, max=h_max) * skin
+    for _ in range(12):
+        nb = find_neighbours(pos, h_search)
+        res = density_numba(pos, mass, h_guess, nb, h_search, kernel_name, eta, tol, h_max)
+        grow = res.flags == FLAG_SEARCH_TOO_SMALL
+        if not bool(torch.any(grow)):
+            return res
+        h_search = h_search.clone()
+        h_search[grow] = h_search[grow] * 2.0
+        h_guess = res.h.clone()
+    raise RuntimeError("smoothing lengths kept outgrowing the neighbour search")
+
+
 @dataclass
 class ForceResult:
     acc: torch.Tensor

@@ -514,6 +514,24 @@ def removal_wake_fixture(blocks, coupled, ics, hydro_cfg):
     _save("removal_wake_blocks.npz", **out)
 
 
+def phantom_fixture(reference, units_mod, coupled):
+    """The reference's external golden vectors (tests/data/phantom_force_sample.npz: one
+    Phantom derivative evaluation with the reference's formulas patched in, 8,931 particles,
+    Wendland C4, gas + radiation, reconstruction on and off) with the particle mass converted to
+    the reference's code units and the reference's default hydro settings, as its test
+    tests/sim/test_phantom_patch.py:34-72 uses them."""
+    d = dict(np.load(os.path.join(reference, "tests", "data", "phantom_force_sample.npz")))
+    hc = coupled.CoupledConfig().hydro
+    m = d["mass_phantom"] * units_mod.BlackHoleUnits().mass_kg / hc.gas_units.mass_kg_per_code
+    out = {k: d[k] for k in ("x", "v", "u", "h_phantom", "alpha", "pressure", "acc_on", "dudt_on",
+                             "acc_off", "dudt_off", "center", "r_in")}  # fmt: skip
+    out.update(mass=np.full(len(d["x"]), m), mratio=np.float64(d["mass_phantom"] / m),
+               kernel=np.array(hc.kernel), eta=hc.eta, h_max=hc.h_max, alpha_u=hc.alpha_u,
+               beta=hc.beta, conductivity_signal=hc.conductivity_signal,
+               recon_closeness=hc.recon_closeness, recon_gate=hc.recon_gate)  # fmt: skip
+    _save("phantom_forces.npz", **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="root of the reference checkout")
@@ -550,6 +568,7 @@ def main():
         "removal_sync_blocks": lambda: removal_blocks_fixture(blocks, coupled, ics, HydroConfig,
                                                               sync=True),
         "removal_wake": lambda: removal_wake_fixture(blocks, coupled, ics, HydroConfig),
+        "phantom": lambda: phantom_fixture(args.reference, units_mod, coupled),
     }
     for name, make in makers.items():
         if not args.only or name in args.only:

@@ -10,7 +10,7 @@ import pytest
 
 from oracle import cooling as ocool
 from oracle import native, steps
-from oracle.sph import C_NORM, compute_density
+from oracle.sph import C_NORM, KERNEL_IDS, compute_density
 from tests.conftest import check, golden
 
 
@@ -509,3 +509,58 @@ def test_removal_wake_matches_reference():
     check("final u", g["final_u"], st.u, rtol=1e-9)
     check("final energy", float(g["final_energy"]), steps.blocks_ledger(st, bc)["energy"],
           rtol=1e-12)  # fmt: skip
+
+
+def _phantom_rel(ours, theirs):
+    """tests/sim/test_phantom_patch.py:75-81: per-particle relative difference."""
+    if ours.ndim == 2:
+        mag, diff = np.linalg.norm(ours, axis=1), np.linalg.norm(ours - theirs, axis=1)
+    else:
+        mag, diff = np.abs(ours), np.abs(ours - theirs)
+    return diff / np.maximum(mag, 1e-6 * np.median(mag))
+
+
+def phantom_hydro(g, recon):
+    from blackhole_nebula_simulator_b200.config import HydroConfig
+
+    return HydroConfig(kernel=str(g["kernel"]), eta=float(g["eta"]), h_max=float(g["h_max"]),
+                       alpha_u=float(g["alpha_u"]), beta=float(g["beta"]),
+                       conductivity_signal=int(g["conductivity_signal"]),
+                       recon_closeness=bool(g["recon_closeness"]), recon_gate=int(g["recon_gate"]),
+                       eos="gasrad", reconstruction=recon)  # fmt: skip
+
+
+@pytest.mark.parametrize("recon", [True, False], ids=["recon_on", "recon_off"])
+def test_oracle_matches_phantom_golden_vectors(recon):
+    """The reference's cross-code check (tests/sim/test_phantom_patch.py:86-98): density, EOS,
+    velocity gradients and forces of the default hydro settings with gas + radiation against
+    Phantom's derivatives on 8,931 particles; median relative difference 1e-5, 99th percentile
+    1e-3 over the 2,203 particles within 600 of the centre (Phantom's pressure used, as there)."""
+    from oracle import eos as oeos
+    from oracle.sph import compute_density as ocompute
+
+    g = golden("phantom_forces.npz")
+    hc = phantom_hydro(g, recon)
+    inner = np.linalg.norm(g["x"] - g["center"], axis=1) < g["r_in"]
+    check("particles compared", 2203, int(inner.sum()))
+    kid = KERNEL_IDS[hc.kernel]
+    dens = ocompute(g["x"], g["mass"], g["h_phantom"], kernel_name=hc.kernel, eta=hc.eta,
+                    h_max=hc.h_max, reuse=False)  # fmt: skip
+    nb = native.tighten(dens.neighbours, g["x"], dens.h)
+    p_ours, cs_ours = oeos.eos_state(hc, dens.rho, g["u"])
+    p = g["pressure"] / g["mratio"]
+    cs = cs_ours * np.sqrt(p / p_ours)
+    gv = native.velocity_gradients(g["x"], g["v"], g["mass"], dens.h, nb, kid, C_NORM[kid])
+    acc, dudt, _, _, _ = native.forces(g["x"], g["v"], g["mass"], dens.h, dens.rho, dens.omega, p,
+                                       nb, kid, C_NORM[kid], u=g["u"], c_s=cs, alpha=g["alpha"],
+                                       beta=hc.beta, alpha_u=hc.alpha_u,
+                                       cond_signal=hc.conductivity_signal,
+                                       grad_v=gv if recon else None, closeness=hc.recon_closeness,
+                                       eta_crit=1.0 / hc.eta, gate=hc.recon_gate)  # fmt: skip
+    tag = "on" if recon else "off"
+    ra = _phantom_rel(acc, g[f"acc_{tag}"])[inner]
+    ru = _phantom_rel(dudt, g[f"dudt_{tag}"])[inner]
+    check("|a| median", 0.0, float(np.median(ra)), atol=1e-5)
+    check("|a| 99th percentile", 0.0, float(np.percentile(ra, 99)), atol=1e-3)
+    check("du/dt median", 0.0, float(np.median(ru)), atol=1e-5)
+    check("du/dt 99th percentile", 0.0, float(np.percentile(ru, 99)), atol=1e-3)
