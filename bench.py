@@ -298,10 +298,14 @@ def snapshot_state(st):
 # the block-state fields a system step reads (sim/blocks.py:502-563): the step's starts, half
 # kicks and tick counters, levels, the accelerations and du/dt of the predictor, masses, smoothing
 # lengths (the density's start), alpha (the neighbours' viscosity), rho (the predicted cooling of
-# every particle).  x, p, u are overwritten for every particle by the flow, the predictor and the
-# cooling; omega, c_s, vsig_max, nu and the heating terms are recomputed where they are read.
+# every particle), the heat budget (added to at every kick) and the parts of du/dt (read by the
+# kicks of the particles whose steps the wake-up cuts).  x, p, u are overwritten for every
+# particle by the flow, the predictor and the cooling; omega, c_s, vsig_max and nu are recomputed
+# where they are read.
 STEP_READS = ("x_beg", "p_half", "u_half", "n_beg", "n_end", "level", "level_offset", "a_hydro",
-              "dudt", "mass", "h", "alpha", "rho")  # fmt: skip
+              "dudt", "mass", "h", "alpha", "rho", "visc_heating", "cond_heating",
+              "disk_heating", "heat_visc", "heat_cond", "heat_disk", "heat_pdv",
+              "heat_cool")  # fmt: skip
 
 
 def run_e2e(args, st, bc, snap):

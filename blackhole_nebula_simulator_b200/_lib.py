@@ -62,6 +62,8 @@ class NbState(_c.Structure):
         ("tick_n", _i64), ("n_stop", _i64), ("t0", _dbl), ("tick", _dbl), ("e_radiated", _dbl),
         ("particle_steps", _i64), ("woken", _i64), ("last_active", _i64), ("pairs", _i64),
         ("builds", _i64), ("reuses", _i64),
+        *[(f, _vp) for f in ("cond_heating", "disk_heating", "heat_visc", "heat_cond", "heat_disk",
+                             "heat_pdv", "heat_cool")],
     ]  # fmt: skip
 
 
@@ -72,6 +74,8 @@ _SIGS = {
     "nb_destroy": (None, [_vp]),
     "nb_last_error": (_c.c_char_p, [_vp]),
     "nb_version": (_int, []),
+    "nb_state_size": (_i64, []),
+    "nb_params_size": (_i64, []),
     "nb_launch_count": (_i64, []),
     "nb_reset_cache": (_int, [_vp]),
     "nb_profile": (_int, [_vp, _int]),
@@ -147,6 +151,10 @@ def lib():
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
+        for mirror, size_of in ((NbState, L.nb_state_size), (NbParams, L.nb_params_size)):
+            if _c.sizeof(mirror) != size_of():
+                raise ImportError(f"{LIB_PATH}: {mirror.__name__} is {_c.sizeof(mirror)} bytes, "
+                                  f"the library's struct {size_of()} (stale build?)")  # fmt: skip
         _lib = L
     return _lib
 

@@ -70,6 +70,15 @@ class BlockState:
     passed_peri: torch.Tensor = None
     doomed: torch.Tensor = None  # next step ends beyond a removal radius (removal_sync)
     removed: RemovedLedger = field(default_factory=RemovedLedger)
+    # parts of du/dt at each particle's last force evaluation and the heat budget since the
+    # start, what each part of du/dt and the cooling added to u (sim/blocks.py:142-154)
+    cond_heating: torch.Tensor = None
+    disk_heating: torch.Tensor = None
+    heat_visc: torch.Tensor = None
+    heat_cond: torch.Tensor = None
+    heat_disk: torch.Tensor = None
+    heat_pdv: torch.Tensor = None
+    heat_cool: torch.Tensor = None
     _params: object = field(default=None, repr=False)
     _rows: torch.Tensor = field(default=None, repr=False)
 
@@ -86,7 +95,10 @@ class BlockState:
 
 _FIELDS = ("x", "p", "u", "mass", "h", "alpha", "a_hydro", "dudt", "rho", "omega", "c_s",
            "vsig_max", "nu", "visc_heating", "level", "n_beg", "n_end", "level_offset", "x_beg",
-           "p_half", "u_half", "luminosity")  # fmt: skip
+           "p_half", "u_half", "luminosity", "cond_heating", "disk_heating", "heat_visc",
+           "heat_cond", "heat_disk", "heat_pdv", "heat_cool")  # fmt: skip
+HEAT_FIELDS = ("cond_heating", "disk_heating", "heat_visc", "heat_cond", "heat_disk", "heat_pdv",
+               "heat_cool")
 
 
 def _state_struct(st: BlockState) -> _lib.NbState:
@@ -143,6 +155,8 @@ def initialise(x, v, u, mass, h_guess, cfg: BlockConfig, t_stop: float, t0: floa
         vsig_max=z(), level_offset=zi() if level_offset is None else dev_i64(level_offset),
         n_stop=int(round((t_stop - t0) / tick)), luminosity=z(), visc_heating=z(), nu=z(), c_s=z(),
     )  # fmt: skip
+    for name in HEAT_FIELDS:
+        setattr(st, name, z())
     st._rows = torch.empty(n, dtype=torch.int64, device=d)
     st.ids = torch.arange(n, dtype=torch.int64, device=d)
     st.r0 = torch.linalg.norm(st.x, dim=1)

@@ -119,6 +119,8 @@ int check_params(Engine& E, const nb_params* prm) {
 extern "C" {
 
 int nb_version(void) { return 1; }
+int64_t nb_state_size(void) { return (int64_t)sizeof(nb_state); }
+int64_t nb_params_size(void) { return (int64_t)sizeof(nb_params); }
 
 int64_t nb_launch_count(void) { return (int64_t)__atomic_load_n(&nbk::g_launch_count, __ATOMIC_RELAXED); }
 

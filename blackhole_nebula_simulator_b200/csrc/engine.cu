@@ -443,13 +443,14 @@ __global__ void k_combine_rows(int64_t nrows, const int64_t* __restrict__ rows, 
                                const double* __restrict__ cs, const double* __restrict__ h,
                                const double* __restrict__ vsig_f, double* __restrict__ acc,
                                double* __restrict__ dudt, double* __restrict__ vsig,
-                               double* __restrict__ nu) {
+                               double* __restrict__ nu, double* __restrict__ disk_heating) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= nrows) return;
   int64_t i = rows[q];
   if (disc_alpha_av > 0) {
     for (int c = 0; c < 3; ++c) acc[3 * i + c] += dacc[3 * i + c];
     dudt[i] += ddudt[i];
+    if (disk_heating) disk_heating[i] = ddudt[i];
     if (nu) nu[i] = disc_alpha_av * cs[i] * h[i] / 10.0;
   }
   vsig[i] = use_visc ? vsig_f[i] : cs[i];
@@ -1102,6 +1103,7 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   fo.dudt = s->dudt;
   fo.vsig = W.d_vsig;
   fo.vheat = s->visc_heating;
+  fo.cheat = s->cond_heating;
   fo.dacc = W.v_dacc;
   fo.ddudt = W.d_ddudt;
   fo.pairs = W.pairs;
@@ -1128,7 +1130,7 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   }
   count_launch(), k_combine_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(
       nrows, rows, prm->viscosity, prm->disc_alpha_av, W.v_dacc, W.d_ddudt, W.d_cs, s->h,
-      W.d_vsig, s->a_hydro, s->dudt, s->vsig_max, s->nu);
+      W.d_vsig, s->a_hydro, s->dudt, s->vsig_max, s->nu, s->disk_heating);
   NB_CUDA(cudaGetLastError());
   return check_device_error(E, st);
 }

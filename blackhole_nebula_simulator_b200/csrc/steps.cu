@@ -42,6 +42,42 @@ __global__ void k_iota(int64_t n, int64_t* __restrict__ out) {
   if (i < n) out[i] = i;
 }
 
+// Heat budget of the block steps (sim/blocks.py:434-440): a kick u += dt du/dt of particle i split
+// into its viscous, conductive, disc-viscous and P dV parts.  hv null: no budget kept.
+struct HeatBook {
+  const double* vh = nullptr;  // parts of du/dt at the last force evaluation
+  const double* ch = nullptr;
+  const double* dh = nullptr;
+  double* hv = nullptr;  // accumulated parts
+  double* hc = nullptr;
+  double* hd = nullptr;
+  double* hp = nullptr;
+};
+
+static HeatBook heat_of(const nb_state* s) {
+  HeatBook b;
+  if (!s->heat_visc) return b;
+  b.vh = s->visc_heating;
+  b.ch = s->cond_heating;
+  b.dh = s->disk_heating;
+  b.hv = s->heat_visc;
+  b.hc = s->heat_cond;
+  b.hd = s->heat_disk;
+  b.hp = s->heat_pdv;
+  return b;
+}
+
+__device__ __forceinline__ void book_heat(const HeatBook& b, int64_t i, double dt, double dudt) {
+  if (!b.hv) return;
+  const double v = b.vh ? b.vh[i] : 0.0;
+  const double c = b.ch ? b.ch[i] : 0.0;
+  const double d = b.dh ? b.dh[i] : 0.0;
+  b.hv[i] += dt * v;
+  b.hc[i] += dt * c;
+  b.hd[i] += dt * d;
+  b.hp[i] += dt * (dudt - v - c - d);
+}
+
 static BremsParams brems_of(const nb_params* prm) {
   BremsParams b;
   b.tfac = prm->brems_tfac;
@@ -327,7 +363,8 @@ __global__ void k_block_cool(int64_t n, int law, int64_t n_next, double tick,
                              const double* __restrict__ dudt, double beta, double u_floor,
                              BremsParams bp, const double* __restrict__ uc_in,
                              double* __restrict__ u_half, double* __restrict__ u,
-                             double* __restrict__ lum, double* __restrict__ dm) {
+                             double* __restrict__ lum, double* __restrict__ dm,
+                             double* __restrict__ heat_cool) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   double s = (double)(n_next - n_beg[i]) * tick;
@@ -351,6 +388,7 @@ __global__ void k_block_cool(int64_t n, int law, int64_t n_next, double tick,
     dm[i] = d;
     if (act) {
       lum[i] = d / (2.0 * half_len);
+      if (heat_cool) heat_cool[i] += uh - uc;
       u_half[i] = uc;
     }
   }
@@ -382,13 +420,14 @@ __global__ void k_block_close(int64_t nrows, const int64_t* __restrict__ rows, d
                               const int64_t* __restrict__ n_beg, const int64_t* __restrict__ n_end,
                               const double* __restrict__ p_flow, const double* __restrict__ a,
                               const double* __restrict__ u_half, const double* __restrict__ dudt,
-                              double* __restrict__ p_pred, double* __restrict__ u) {
+                              double* __restrict__ p_pred, double* __restrict__ u, HeatBook hb) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= nrows) return;
   int64_t i = rows[q];
   double half_len = 0.5 * (double)(n_end[i] - n_beg[i]) * tick;
   for (int c = 0; c < 3; ++c) p_pred[3 * i + c] = p_flow[3 * i + c] + half_len * a[3 * i + c];
   u[i] = u_half[i] + half_len * dudt[i];
+  book_heat(hb, i, half_len, dudt[i]);
 }
 
 // wanted level of the rows: orbit, Courant, force and viscous criteria (sim/blocks.py:318-334),
@@ -565,7 +604,8 @@ __global__ void k_cut_steps(int64_t n, int64_t tick_n, double tick, const int64_
                             const double* __restrict__ a, const double* __restrict__ dudt,
                             int64_t* __restrict__ level, int64_t* __restrict__ n_end,
                             double* __restrict__ p_half, double* __restrict__ u_half,
-                            unsigned long long* __restrict__ woken, const int* __restrict__ err) {
+                            unsigned long long* __restrict__ woken, const int* __restrict__ err,
+                            HeatBook hb) {
   int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (j >= n || *err) return;  // a failed landing leaves the state as it was
   int64_t nd = need[j];
@@ -577,6 +617,7 @@ __global__ void k_cut_steps(int64_t n, int64_t tick_n, double tick, const int64_
     double d_len = (double)(end_new - n_end[j]) * tick;
     for (int c = 0; c < 3; ++c) p_half[3 * j + c] += 0.5 * d_len * a[3 * j + c];
     u_half[j] += 0.5 * d_len * dudt[j];
+    book_heat(hb, j, 0.5 * d_len, dudt[j]);
     n_end[j] = end_new;
     atomicAdd(woken, 1ull);
   }
@@ -589,7 +630,7 @@ __global__ void k_open(int64_t nrows, const int64_t* __restrict__ rows, int64_t 
                        const double* __restrict__ a, const double* __restrict__ dudt,
                        int64_t* __restrict__ n_beg, int64_t* __restrict__ n_end,
                        double* __restrict__ x_beg, double* __restrict__ p_half,
-                       double* __restrict__ u_half, const int* __restrict__ err) {
+                       double* __restrict__ u_half, const int* __restrict__ err, HeatBook hb) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= nrows || *err) return;  // a failed landing leaves the state as it was
   int64_t i = rows[q];
@@ -602,6 +643,7 @@ __global__ void k_open(int64_t nrows, const int64_t* __restrict__ rows, int64_t 
     p_half[3 * i + c] = p[3 * i + c] + 0.5 * length * a[3 * i + c];
   }
   u_half[i] = u[i] + 0.5 * length * dudt[i];
+  book_heat(hb, i, 0.5 * length, dudt[i]);
 }
 
 __global__ void k_fill_i64(int64_t n, int64_t v, int64_t* __restrict__ a) {
@@ -672,12 +714,14 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
     NB_CUDA(cudaMemsetAsync(W.d_scal_i + 2, 0, sizeof(int64_t), st));
     count_launch(), k_cut_steps<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->tick_n, s->tick, W.need, s->a_hydro,
                                                     s->dudt, s->level, s->n_end, s->p_half,
-                                                    s->u_half, (unsigned long long*)(W.d_scal_i + 2), E.d_err);
+                                                    s->u_half, (unsigned long long*)(W.d_scal_i + 2), E.d_err,
+                                                    heat_of(s));
     W.pend_woken = &s->woken;
   }
   count_launch(), k_open<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, s->tick_n, s->tick, s->level, s->x,
                                                  s->p, s->u, s->a_hydro, s->dudt, s->n_beg,
-                                                 s->n_end, s->x_beg, s->p_half, s->u_half, E.d_err);
+                                                 s->n_end, s->x_beg, s->p_half, s->u_half, E.d_err,
+                                                 heat_of(s));
   NB_CUDA(cudaGetLastError());
   return 0;
 }
@@ -739,7 +783,7 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   count_launch(), k_block_cool<<<grid_for(n), NB_THREADS, 0, st>>>(
       n, prm->cooling, n_next, s->tick, s->n_beg, s->n_end, s->x_beg, s->x, s->rho, s->mass,
       s->dudt, prm->cooling_beta, prm->u_floor, brems_of(prm), W.d_c, s->u_half, s->u,
-      s->luminosity, W.d_dm);
+      s->luminosity, W.d_dm, s->heat_visc ? s->heat_cool : nullptr);
   E.prof.end(PROF_COOL, st, (double)nrows, 0.0);
   if (prm->cooling != 0) {
     // radiated energy of the closing steps, added to the ledger at the next read
@@ -765,7 +809,7 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   }
   count_launch(), k_block_close<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, W.rows, s->tick, s->n_beg, s->n_end,
                                                        W.v_flow, s->a_hydro, s->u_half, s->dudt,
-                                                       W.v_pred, s->u);
+                                                       W.v_pred, s->u, heat_of(s));
   NB_CUDA(cudaMemcpyAsync(s->p, W.v_pred, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, st));
   if (!split) {
     E.prof.begin(st);
@@ -838,7 +882,8 @@ __global__ void k_cut_doomed(int64_t n, int64_t tick_n, double tick,
                              const long long* __restrict__ label, int64_t* __restrict__ n_end,
                              int64_t* __restrict__ level, double* __restrict__ p_half,
                              double* __restrict__ u_half, const double* __restrict__ a,
-                             const double* __restrict__ dudt, unsigned long long* woken) {
+                             const double* __restrict__ dudt, unsigned long long* woken,
+                             HeatBook hb) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int64_t e = (int64_t)end[i];
@@ -847,6 +892,7 @@ __global__ void k_cut_doomed(int64_t n, int64_t tick_n, double tick,
   const double d_len = (double)(e - n_end[i]) * tick;
   for (int c = 0; c < 3; ++c) p_half[3 * i + c] += 0.5 * d_len * a[3 * i + c];
   u_half[i] += 0.5 * d_len * dudt[i];
+  book_heat(hb, i, 0.5 * d_len, dudt[i]);
   n_end[i] = e;
   atomicAdd(woken, 1ull);
 }
@@ -885,7 +931,7 @@ int block_wake_doomed(Engine& E, nb_state* s, int64_t nrows, const int64_t* rows
   NB_CUDA(cudaMemsetAsync(W.d_i64, 0, sizeof(int64_t), st));
   count_launch(), k_cut_doomed<<<grid_for(n), NB_THREADS, 0, st>>>(
       n, s->tick_n, s->tick, end, label, s->n_end, s->level, s->p_half, s->u_half, s->a_hydro,
-      s->dudt, reinterpret_cast<unsigned long long*>(W.d_i64));
+      s->dudt, reinterpret_cast<unsigned long long*>(W.d_i64), heat_of(s));
   NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   NB_CUDA(cudaStreamSynchronize(st));
   s->woken += W.h_i64[0];
@@ -906,7 +952,8 @@ __global__ void k_open_only(int64_t nrows, const int64_t* __restrict__ rows, int
                             const double* __restrict__ u, const double* __restrict__ a,
                             const double* __restrict__ dudt, int64_t* __restrict__ n_beg,
                             int64_t* __restrict__ n_end, double* __restrict__ x_beg,
-                            double* __restrict__ p_half, double* __restrict__ u_half) {
+                            double* __restrict__ p_half, double* __restrict__ u_half,
+                            HeatBook hb) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= nrows) return;
   int64_t i = rows[q];
@@ -919,6 +966,8 @@ __global__ void k_open_only(int64_t nrows, const int64_t* __restrict__ rows, int
     p_half[3 * i + c] = p[3 * i + c] + 0.5 * length * a[3 * i + c];
   }
   u_half[i] = u[i] + 0.5 * length * dudt[i];
+  // run() re-opens through _open, which books the opening kick again (sim/blocks.py:733, 451)
+  book_heat(hb, i, 0.5 * length, dudt[i]);
 }
 
 int block_land(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st) {
@@ -934,7 +983,8 @@ int block_land(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st) {
   NB_TRY(check_device_error(E, st));
   count_launch(), k_open_only<<<grid_for(nf), NB_THREADS, 0, st>>>(nf, W.rows2, s->tick_n, s->tick, s->level, s->x,
                                                    s->p, s->u, s->a_hydro, s->dudt, s->n_beg,
-                                                   s->n_end, s->x_beg, s->p_half, s->u_half);
+                                                   s->n_end, s->x_beg, s->p_half, s->u_half,
+                                                   heat_of(s));
   NB_CUDA(cudaGetLastError());
   return 0;
 }

@@ -105,7 +105,7 @@ def blocks_payload(st) -> dict:
 def restore_blocks(payload: dict, device=None):
     """A BlockState on the device from ``blocks_payload`` output; the engine rebuilds its lists
     at the next step (as the reference does after loading a checkpoint without its cache)."""
-    from .blocks import BlockState
+    from .blocks import HEAT_FIELDS, BlockState
     from .device import require_cuda
 
     dev = device or require_cuda()
@@ -116,5 +116,11 @@ def restore_blocks(payload: dict, device=None):
         v = payload[f.name]
         kw[f.name] = torch.as_tensor(v, device=dev).clone() if isinstance(v, np.ndarray) else v
     st = BlockState(**kw)
-    st._rows = torch.empty(len(st.x), dtype=torch.int64, device=dev)
+    n = len(st.x)
+    # outputs and budgets absent from an older checkpoint start at zero from the resume
+    # (sim/blocks.py:172-188)
+    for name in ("luminosity", "visc_heating", "nu", "c_s") + HEAT_FIELDS:
+        if getattr(st, name) is None:
+            setattr(st, name, torch.zeros(n, dtype=torch.float64, device=dev))
+    st._rows = torch.empty(n, dtype=torch.int64, device=dev)
     return st

@@ -99,6 +99,12 @@ typedef struct nb_state {
   double e_radiated;
   int64_t particle_steps, woken, last_active, pairs;
   int64_t builds, reuses;
+  /* block steps: the parts of du/dt at each particle's last force evaluation (viscous heating is
+   * visc_heating above) and the heat budget since the start, what each part of du/dt and the
+   * cooling added to u (sim/blocks.py:142-154, 434-440).  heat_visc NULL: no budget kept;
+   * cond_heating / disk_heating may be NULL without conductivity / disc viscosity. */
+  double *cond_heating, *disk_heating;
+  double *heat_visc, *heat_cond, *heat_disk, *heat_pdv, *heat_cool;
 } nb_state;
 
 /* ---------------------------------------------------------------- context */
@@ -106,6 +112,9 @@ NB_API nb_ctx* nb_create(int device);
 NB_API void nb_destroy(nb_ctx* ctx);
 NB_API const char* nb_last_error(nb_ctx* ctx);
 NB_API int nb_version(void);
+/* sizeof(nb_state) and sizeof(nb_params) of this build (bindings check their mirrors). */
+NB_API int64_t nb_state_size(void);
+NB_API int64_t nb_params_size(void);
 /* Number of this library's own kernels launched so far by this process (all contexts). */
 NB_API int64_t nb_launch_count(void);
 

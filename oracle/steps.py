@@ -9,7 +9,8 @@ Restates the reference's step logic on top of the C kernels:
 Only the options of the CUDA path are restated: GN hole, ideal gas (or, without cooling, the
 radiation limit and gas + radiation), constant alpha or the Cullen-Dehnen switch, optional
 velocity reconstruction, conductivity and disc viscosity, beta or bremsstrahlung cooling, no
-removal radii and no RESPA.  The heat-budget bookkeeping arrays are not kept.
+accretion and escape radii (with or without removal_sync), the per-particle heat budget, no
+RESPA.
 """
 
 from __future__ import annotations
@@ -280,6 +281,16 @@ class BlockState:
     passed_peri: np.ndarray = None  # has turned outward near the hole
     doomed: np.ndarray = None  # next step ends beyond a removal radius (removal_sync)
     removed: "RemovedLedger" = None
+    # parts of du/dt at each particle's last force evaluation, and the heat budget since the
+    # start: what each part of du/dt and the cooling added to u (sim/blocks.py:142-154)
+    visc_heating: np.ndarray = None
+    cond_heating: np.ndarray = None
+    disk_heating: np.ndarray = None
+    heat_visc: np.ndarray = None
+    heat_cond: np.ndarray = None
+    heat_disk: np.ndarray = None
+    heat_pdv: np.ndarray = None
+    heat_cool: np.ndarray = None
 
     @property
     def t(self):
@@ -328,7 +339,7 @@ def _hydro_rows(st: BlockState, bc, rows, v, u, reuse=True, dt_alpha=None, a_pre
         # the touched particles' gradients from the untightened cached lists (sim/blocks.py:271-278)
         grad_v = native.velocity_gradients(st.x, v, st.mass, st.h, st.neighbour_cache.neighbours,
                                            kid, cn, rows=touched)  # fmt: skip
-    acc, dudt, vsig, _, _ = native.forces(
+    acc, dudt, vsig, vh, ch = native.forces(
         st.x, v, st.mass, st.h, st.rho, st.omega, p_gas, nb, kid, cn,
         u=u if hc.conductivity else None, c_s=cs if hc.viscosity else None,
         alpha=st.alpha if hc.viscosity else None, beta=hc.beta, alpha_u=hc.alpha_u,
@@ -338,11 +349,23 @@ def _hydro_rows(st: BlockState, bc, rows, v, u, reuse=True, dt_alpha=None, a_pre
         a_d, u_d = native.disc_forces(st.x, v, st.mass, st.h, st.rho, st.omega, cs,
                                       hc.disc_alpha_av, nb, kid, cn, rows=rows)  # fmt: skip
         acc, dudt = acc + a_d, dudt + u_d
+        st.disk_heating[rows] = u_d
         st.nu[rows] = hc.disc_alpha_av * cs[rows] * st.h[rows] / 10.0
     st.a_hydro[rows] = acc
     st.dudt[rows] = dudt
     st.vsig_max[rows] = vsig if hc.viscosity else cs[rows]
+    st.visc_heating[rows] = vh
+    st.cond_heating[rows] = ch
     return nb
+
+
+def _add_heat(st: BlockState, rows, dt):
+    """sim/blocks.py:434-440: the kick u += dt du/dt of ``rows`` split into its parts."""
+    visc, cond, disk = st.visc_heating[rows], st.cond_heating[rows], st.disk_heating[rows]
+    st.heat_visc[rows] += dt * visc
+    st.heat_cond[rows] += dt * cond
+    st.heat_disk[rows] += dt * disk
+    st.heat_pdv[rows] += dt * (st.dudt[rows] - visc - cond - disk)
 
 
 def wanted_dt(st: BlockState, bc, rows):
@@ -384,11 +407,12 @@ def _land(st: BlockState, k):
 
 
 def _cut_to(st: BlockState, j, end_new, level):
-    """sim/blocks.py:420-431 (without the heat budget and RESPA bookkeeping)."""
+    """sim/blocks.py:420-431 (without the RESPA bookkeeping)."""
     st.level[j] = level
     d_len = (end_new - st.n_end[j]) * st.tick
     st.p_half[j] += 0.5 * d_len[:, None] * st.a_hydro[j]
     st.u_half[j] += 0.5 * d_len * st.dudt[j]
+    _add_heat(st, j, 0.5 * d_len)
     st.n_end[j] = end_new
     st.woken += len(j)
 
@@ -432,6 +456,7 @@ def _open(st: BlockState, rows):
     st.x_beg[rows] = st.x[rows]
     st.p_half[rows] = st.p[rows] + 0.5 * length[:, None] * st.a_hydro[rows]
     st.u_half[rows] = st.u[rows] + 0.5 * length * st.dudt[rows]
+    _add_heat(st, rows, 0.5 * length)
 
 
 def blocks_initialise(x, v, u, mass, h_guess, bc, t_stop, t0=0.0, level_offset=None,
@@ -457,6 +482,9 @@ def blocks_initialise(x, v, u, mass, h_guess, bc, t_stop, t0=0.0, level_offset=N
     )  # fmt: skip
     st.luminosity = np.zeros(n)
     st.nu = np.zeros(n)
+    for name in ("visc_heating", "cond_heating", "disk_heating", "heat_visc", "heat_cond",
+                 "heat_disk", "heat_pdv", "heat_cool"):  # fmt: skip
+        setattr(st, name, np.zeros(n))
     st.ids = np.arange(n)
     st.r0 = np.linalg.norm(x, axis=1)
     st.L0 = np.linalg.norm(np.cross(x, p), axis=1)
@@ -476,7 +504,7 @@ def blocks_initialise(x, v, u, mass, h_guess, bc, t_stop, t0=0.0, level_offset=N
 
 
 def blocks_advance(st: BlockState, bc, reuse=True) -> np.ndarray:
-    """sim/blocks.py:502-563 (no RESPA, no removal radii)."""
+    """sim/blocks.py:502-563 (no RESPA)."""
     cc = bc.coupled
     t0 = time.perf_counter()
     n_next = int(np.min(st.n_end))
@@ -494,6 +522,7 @@ def blocks_advance(st: BlockState, bc, reuse=True) -> np.ndarray:
         st.e_radiated += float(np.sum(dm))
         st.luminosity[rows] = dm / (2.0 * half_len[rows])
         u_pred = u_half_c + (s - half_len) * st.dudt
+        st.heat_cool[rows] += st.u_half[rows] - u_half_c[rows]
         st.u_half[rows] = u_half_c[rows]
     else:
         u_pred = st.u_half + (s - half_len) * st.dudt
@@ -509,6 +538,7 @@ def blocks_advance(st: BlockState, bc, reuse=True) -> np.ndarray:
     u_eval = u_pred.copy() if sync else None
     p_pred[rows] = p_flow[rows] + half_len[rows, None] * st.a_hydro[rows]
     st.u[rows] = st.u_half[rows] + half_len[rows] * st.dudt[rows]
+    _add_heat(st, rows, half_len[rows])
     st.p = p_pred
     n_active = len(rows)
     if sync:

@@ -514,6 +514,48 @@ def removal_wake_fixture(blocks, coupled, ics, hydro_cfg):
     _save("removal_wake_blocks.npz", **out)
 
 
+HEAT_FIELDS = ["u", "u_half", "visc_heating", "cond_heating", "disk_heating", "heat_visc",
+               "heat_cond", "heat_disk", "heat_pdv", "heat_cool"]  # fmt: skip
+
+
+def heat_fixture(blocks, coupled, ics, hydro_cfg):
+    """The per-particle heat budget (sim/blocks.py:142-154, 434-440, 531, 546) on the multi-level
+    cloud of blocks_fixture with disc viscosity (alpha_AV = 1) on top of viscosity, conductivity
+    and beta-cooling: (sync) initialise with t_stop = 192 and run to 192, a full sync point;
+    (reopen) initialise without a near stop and run to 0.75, so that run() re-opens every
+    step to land on it (its _open books the opening kick a second time); (removal) the
+    removal_sync run of removal_wake_fixture, 16 system steps (survivors' forces redone, the
+    doomed particles' neighbours cut, removed particles' budgets dropped)."""
+    ic = ics.cloud(2048, radius=20.0, total_mass=1e-3, t_kelvin=3e8, r_peri=60.0, r_apo=400.0,
+                   seed=7)  # fmt: skip
+    rng = np.random.default_rng(SEED)
+    v = ic.v + rng.normal(0.0, 0.002, ic.v.shape)
+    offset = rng.integers(0, 4, len(ic.x))
+    hc = hydro_cfg(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                   conductivity_signal=1, alpha_u=0.05, h_max=200.0, disc_alpha_av=1.0)  # fmt: skip
+    cc = coupled.CoupledConfig(hydro=hc, cooling_beta=230.0)
+    bc = blocks.BlockConfig(coupled=cc, dt_max=64.0)
+    out = dict(x0=ic.x, v0=v, u0=ic.u, mass=ic.mass, h0=ic.h, level_offset=offset)
+    st = blocks.initialise(ic.x, v, ic.u, ic.mass, ic.h, bc, t_stop=192.0, level_offset=offset)
+    blocks.run(st, bc, 192.0)
+    out.update(_state_arrays("sync", st, HEAT_FIELDS))
+    out.update(sync_e_radiated=st.e_radiated, sync_n=st.n)
+    st = blocks.initialise(ic.x, v, ic.u, ic.mass, ic.h, bc, t_stop=1e6, level_offset=offset)
+    blocks.run(st, bc, 0.75)
+    out.update(_state_arrays("reopen", st, HEAT_FIELDS + ["level", "n_end"]))
+    out.update(reopen_n=st.n)
+    hc = hydro_cfg(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                   conductivity_signal=1, alpha_u=0.05, h_max=200.0)  # fmt: skip
+    cc = coupled.CoupledConfig(hydro=hc, cooling_beta=230.0)
+    bc = blocks.BlockConfig(coupled=cc, dt_max=64.0, r_acc=382.0, removal_sync=True)
+    st = blocks.initialise(ic.x, v, ic.u, ic.mass, ic.h, bc, t_stop=1e6, level_offset=offset)
+    for _ in range(16):
+        blocks.advance(st, bc)
+    out.update(_state_arrays("removal", st, HEAT_FIELDS + ["ids"]))
+    out.update(removal_e_radiated=st.e_radiated, removal_n=st.n)
+    _save("heat_blocks.npz", **out)
+
+
 def phantom_fixture(reference, units_mod, coupled):
     """The reference's external golden vectors (tests/data/phantom_force_sample.npz: one
     Phantom derivative evaluation with the reference's formulas patched in, 8,931 particles,
@@ -569,6 +611,7 @@ def main():
                                                               sync=True),
         "removal_wake": lambda: removal_wake_fixture(blocks, coupled, ics, HydroConfig),
         "phantom": lambda: phantom_fixture(args.reference, units_mod, coupled),
+        "heat_blocks": lambda: heat_fixture(blocks, coupled, ics, HydroConfig),
     }
     for name, make in makers.items():
         if not args.only or name in args.only:

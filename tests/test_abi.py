@@ -36,6 +36,19 @@ def test_library_exports_every_declared_symbol():
     assert set(_declared()) == set(_lib.EXPORTED)
 
 
+def test_struct_mirrors_match_the_library():
+    """nb_state and nb_params as the ctypes binding lays them out are the library's own."""
+    import ctypes
+
+    from blackhole_nebula_simulator_b200 import _lib
+
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libnebula_b200.so not built")
+    L = _lib.lib()
+    assert ctypes.sizeof(_lib.NbState) == L.nb_state_size()
+    assert ctypes.sizeof(_lib.NbParams) == L.nb_params_size()
+
+
 def test_product_never_imports_the_oracle():
     pkg = os.path.join(ROOT, "blackhole_nebula_simulator_b200")
     for dirpath, _, files in os.walk(pkg):

@@ -564,3 +564,69 @@ def test_oracle_matches_phantom_golden_vectors(recon):
     check("|a| 99th percentile", 0.0, float(np.percentile(ra, 99)), atol=1e-3)
     check("du/dt median", 0.0, float(np.median(ru)), atol=1e-5)
     check("du/dt 99th percentile", 0.0, float(np.percentile(ru, 99)), atol=1e-3)
+
+
+HEAT_PARTS = ("heat_visc", "heat_cond", "heat_disk", "heat_pdv", "heat_cool")
+
+
+def heat_runs(g, initialise, run, advance, **hydro):
+    """The three runs of tests/golden/heat_blocks.npz through a block-step API (the oracle's or
+    the device facade's): yields (prefix, state) after each."""
+    from blackhole_nebula_simulator_b200.config import BlockConfig, CoupledConfig, HydroConfig
+
+    hc = HydroConfig(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                     conductivity_signal=1, alpha_u=0.05, h_max=200.0, disc_alpha_av=1.0,
+                     **hydro)  # fmt: skip
+    bc = BlockConfig(coupled=CoupledConfig(hydro=hc, cooling_beta=230.0), dt_max=64.0)
+    args = (g["x0"], g["v0"], g["u0"], g["mass"], g["h0"], bc)
+    st = initialise(*args, t_stop=192.0, level_offset=g["level_offset"])
+    yield "sync", run(st, bc, 192.0)
+    st = initialise(*args, t_stop=1e6, level_offset=g["level_offset"])
+    yield "reopen", run(st, bc, 0.75)
+    bc = _wake_bc()
+    st = initialise(*args[:5], bc, t_stop=1e6, level_offset=g["level_offset"])
+    for _ in range(16):
+        advance(st, bc)
+    yield "removal", st
+
+
+def check_heat(g, pre, arrays, e_radiated, tol):
+    """Every heat-budget array against the reference's, each to ``tol`` of its largest value;
+    the budget identity u_half - u_0 = visc + cond + disk + pdv - cool (the reference's own
+    test, tests/sim/test_heat_budget.py:19-46) where the reference has it (sync, removal: to
+    1e-12 of max u_0) and its failure by the twice-booked opening kick where run() re-opens
+    (reopen), equal to the reference's; the cooling budget against the radiated energy."""
+    scale = {}
+    for f in ("u_half",) + HEAT_PARTS + ("visc_heating", "cond_heating", "disk_heating"):
+        ref = g[f"{pre}_{f}"]
+        scale[f] = float(np.abs(ref).max())
+        check(f"{pre} {f}", ref, arrays[f], atol=tol * max(scale[f], 1e-300))
+    u0 = g["u0"] if pre != "removal" else g["u0"][g["removal_ids"]]
+    parts = (arrays["heat_visc"] + arrays["heat_cond"] + arrays["heat_disk"] + arrays["heat_pdv"]
+             - arrays["heat_cool"])  # fmt: skip
+    gap = arrays["u_half"] - u0 - parts
+    ref_parts = sum(g[f"{pre}_{f}"] for f in HEAT_PARTS[:4]) - g[f"{pre}_heat_cool"]
+    ref_gap = g[f"{pre}_u_half"] - u0 - ref_parts
+    umax = float(np.abs(u0).max())
+    if pre == "reopen":
+        check("reopen: the budget is off by the second opening kick", ref_gap, gap,
+              atol=tol * float(np.abs(ref_gap).max()))  # fmt: skip
+    else:
+        check(f"{pre}: u_half - u0 = visc + cond + disk + pdv - cool", 0.0,
+              float(np.abs(gap).max()) / umax, atol=1e-12)  # fmt: skip
+    if pre == "sync":
+        check("cooling budget equals the radiated energy", float(g["sync_e_radiated"]),
+              e_radiated, rtol=1e-9)  # fmt: skip
+        check("sum m heat_cool = e_radiated", e_radiated,
+              float(np.sum(g["mass"] * arrays["heat_cool"])), rtol=1e-12)  # fmt: skip
+
+
+def test_heat_budget_matches_reference():
+    g = golden("heat_blocks.npz")
+    for pre, st in heat_runs(g, steps.blocks_initialise, steps.blocks_run, steps.blocks_advance):
+        check(f"{pre} tick", int(g[f"{pre}_n"]), st.n)
+        if pre == "removal":
+            check("removal ids", g["removal_ids"], st.ids)
+        arrays = {k: getattr(st, k) for k in ("u_half", "visc_heating", "cond_heating",
+                                              "disk_heating") + HEAT_PARTS}  # fmt: skip
+        check_heat(g, pre, arrays, st.e_radiated, 1e-9)
