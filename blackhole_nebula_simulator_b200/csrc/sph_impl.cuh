@@ -272,6 +272,9 @@ struct DensityEntry<double> {
   static constexpr int BLOCKS = 4;
 };
 constexpr int DENSITY_THREADS = 128;  // 16 rows per block
+#ifndef DENSITY_UNROLL
+#define DENSITY_UNROLL 4
+#endif
 
 // Eight lanes per row, four rows per warp.  The lanes of a row split its list (entry e to lane
 // e mod 8, coalesced index loads) and store the distance and mass of every entry inside the search
@@ -315,29 +318,49 @@ __global__ void __launch_bounds__(DENSITY_THREADS, DensityEntry<R>::BLOCKS)
   const unsigned len = (unsigned)(e1 - e0);
   const unsigned maxlen = __reduce_max_sync(FULL, len);
   int cnt = 0;
-  for (unsigned b = 0; b < maxlen; b += 8) {
-    bool inr = false;
-    R r = R(0), m = R(0);
-    if (b + gl < len) {
-      int64_t j = (int64_t)ld_stream(idx + e0 + b + gl);
-      R dx, dy, dz;
-      geo.diff(i, j, dx, dy, dz);
-      R d2 = sqdist(dx, dy, dz);
-      if (d2 < r2max) {
-        inr = true;
-        r = sqrt(d2);
-        m = prm.massf ? (R)prm.massf[j] : (R)mass[j];
+  // DENSITY_UNROLL rounds of 8 entries per pass: their index, position and mass loads are issued
+  // together (the walk is bound by the latency of those dependent gathers), then the rounds are
+  // appended to the cache one after the other, so the cache holds the entries in list order
+  constexpr int U = DENSITY_UNROLL;
+  for (unsigned b = 0; b < maxlen; b += 8 * U) {
+    int64_t jj[U];
+    bool inr[U];
+    R rr[U], mm[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const unsigned e = b + 8 * u + gl;
+      jj[u] = e < len ? (int64_t)ld_stream(idx + e0 + e) : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      inr[u] = false;
+      rr[u] = R(0);
+      mm[u] = R(0);
+      if (jj[u] >= 0) {
+        R dx, dy, dz;
+        geo.diff(i, jj[u], dx, dy, dz);
+        R d2 = sqdist(dx, dy, dz);
+        if (d2 < r2max) {
+          inr[u] = true;
+          rr[u] = sqrt(d2);
+        }
       }
     }
-    unsigned seg = (__ballot_sync(FULL, inr) >> (8 * g)) & 0xffu;
-    int pos = cnt + __popc(seg & ((1u << gl) - 1u));
-    if (inr && pos < CAP) {
-      E2 v;
-      v.x = r;
-      v.y = m;
-      cache[pos] = v;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (inr[u]) mm[u] = prm.massf ? (R)prm.massf[jj[u]] : (R)mass[jj[u]];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      unsigned seg = (__ballot_sync(FULL, inr[u]) >> (8 * g)) & 0xffu;
+      int pos = cnt + __popc(seg & ((1u << gl) - 1u));
+      if (inr[u] && pos < CAP) {
+        E2 v;
+        v.x = rr[u];
+        v.y = mm[u];
+        cache[pos] = v;
+      }
+      cnt += __popc(seg);
     }
-    cnt += __popc(seg);
   }
   __syncwarp();
   const bool cached = cnt <= CAP;
@@ -442,10 +465,15 @@ __device__ __forceinline__ R dwdr(R r, R h, int kid, R cnorm) {
 }
 
 constexpr int FORCE_QUEUE = 64;  // interacting entries a row queues before its lanes drain them
+#ifndef FORCE_UNROLL
+#define FORCE_UNROLL 4
+#endif
 // resident blocks per SM the FP32 force pass is compiled for (registers: 65536 / (256 * 3) = 85;
 // the FP64 form keeps 2, its doubles would spill; the reconstruction forms, with two 3x3
 // gradients per pair, 2 and 1)
-constexpr int FORCE_BLOCKS_PER_SM_FP32 = 3;
+#ifndef FORCE_BLOCKS_PER_SM_FP32
+#define FORCE_BLOCKS_PER_SM_FP32 3
+#endif
 
 // Fused pressure + artificial viscosity (+ conductivity) + P dV (+ disc viscosity) pass.  Eight
 // lanes per row (lanes 8g .. 8g+7 of a warp), each taking every eighth list entry; the pair terms
@@ -486,7 +514,7 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? (RECON ? 2 : FORC
   // the row's list in rounds of eight entries: lanes test their entry, the interacting ones are
   // queued in shared memory in list order, and full queues are drained with all eight lanes
   // busy on pair terms
-  __shared__ int32_t queue_s[NB_THREADS / 8][FORCE_QUEUE + 8];
+  __shared__ int32_t queue_s[NB_THREADS / 8][FORCE_QUEUE + 8 * FORCE_UNROLL];
   int32_t* pq = queue_s[threadIdx.x >> 3];
   const int g = (threadIdx.x & 31) >> 3;
   const int64_t e_beg = live ? off[a] : 0, e_end = live ? off[a + 1] : 0;
@@ -722,41 +750,59 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? (RECON ? 2 : FORC
   // written out for the level limiter: exactly the reference's FP64 test, which the FP32 form
   // takes from prm.pos64 where its float test falls within 1e-5 of the boundary
   int m_tot = 0;
-  for (unsigned base = 0; base < maxlen; base += 8) {
-    bool take = false, tight = false;
-    int64_t b = 0;
-    if (base + gl < len) {
-      b = (int64_t)ld_stream(idx + e_beg + base + gl);
-      if (b != a) {
-        take = true;
-        if (prm.tighten) {
-          R ddx, ddy, ddz;
-          geo.diff(a, b, ddx, ddy, ddz);
-          const R h_b = (R)hydro[b].x;
-          R rr = R(2) * (h_a > h_b ? h_a : h_b);
-          const R d2 = sqdist(ddx, ddy, ddz), r2 = rr * rr;
-          take = d2 < r2;
-          if constexpr (sizeof(R) == 4) {
-            if (prm.pos64 && d2 > r2 * R(1.0 - 1e-5) && d2 < r2 * R(1.0 + 1e-5)) {
-              const double4 pa = prm.pos64[a], pb = prm.pos64[b];
-              const double e2 = d2_exact(pb.x - pa.x, pb.y - pa.y, pb.z - pa.z);
-              const double er = 2.0 * fmax(pa.w, pb.w);
-              take = e2 < er * er;
+  // FORCE_UNROLL rounds of eight entries at a time: their index and position loads are issued
+  // together, then the rounds are queued one after the other in list order
+  constexpr int FU = FORCE_UNROLL;
+  for (unsigned base = 0; base < maxlen; base += 8 * FU) {
+    int64_t bb[FU];
+    bool take[FU], tight[FU];
+#pragma unroll
+    for (int u = 0; u < FU; ++u) {
+      const unsigned e = base + 8 * u + gl;
+      bb[u] = e < len ? (int64_t)ld_stream(idx + e_beg + e) : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < FU; ++u) {
+      const int64_t b = bb[u];
+      take[u] = false;
+      tight[u] = false;
+      if (b >= 0) {
+        if (b != a) {
+          bool tk = true;
+          if (prm.tighten) {
+            R ddx, ddy, ddz;
+            geo.diff(a, b, ddx, ddy, ddz);
+            const R h_b = (R)hydro[b].x;
+            R rr = R(2) * (h_a > h_b ? h_a : h_b);
+            const R d2 = sqdist(ddx, ddy, ddz), r2 = rr * rr;
+            tk = d2 < r2;
+            if constexpr (sizeof(R) == 4) {
+              if (prm.pos64 && d2 > r2 * R(1.0 - 1e-5) && d2 < r2 * R(1.0 + 1e-5)) {
+                const double4 pa = prm.pos64[a], pb = prm.pos64[b];
+                const double e2 = d2_exact(pb.x - pa.x, pb.y - pa.y, pb.z - pa.z);
+                const double er = 2.0 * fmax(pa.w, pb.w);
+                tk = e2 < er * er;
+              }
             }
           }
+          take[u] = tk;
+          tight[u] = tk;
+        } else {
+          tight[u] = true;  // self: listed for the limiter, not a pair
         }
-        tight = take;
-      } else {
-        tight = true;  // self: listed for the limiter, not a pair
       }
     }
-    unsigned seg = (__ballot_sync(FULL, take) >> (8 * g)) & 0xffu;
-    if (take) pq[pc + __popc(seg & ((1u << gl) - 1u))] = (int32_t)b;
-    pc += __popc(seg);
-    if (prm.tidx) {
-      const unsigned tseg = (__ballot_sync(FULL, tight) >> (8 * g)) & 0xffu;
-      if (tight) prm.tidx[e_beg + m_tot + __popc(tseg & ((1u << gl) - 1u))] = (int32_t)b;
-      m_tot += __popc(tseg);
+#pragma unroll
+    for (int u = 0; u < FU; ++u) {
+      unsigned seg = (__ballot_sync(FULL, take[u]) >> (8 * g)) & 0xffu;
+      if (take[u]) pq[pc + __popc(seg & ((1u << gl) - 1u))] = (int32_t)bb[u];
+      pc += __popc(seg);
+      if (prm.tidx) {
+        const unsigned tseg = (__ballot_sync(FULL, tight[u]) >> (8 * g)) & 0xffu;
+        if (tight[u])
+          prm.tidx[e_beg + m_tot + __popc(tseg & ((1u << gl) - 1u))] = (int32_t)bb[u];
+        m_tot += __popc(tseg);
+      }
     }
     if (__any_sync(FULL, pc > FORCE_QUEUE - 8)) drain();
   }
