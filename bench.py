@@ -40,8 +40,10 @@ FLOP_PER_DENSITY_EVAL = 25.0  # distance + kernel + two sums per pair evaluation
 FLOP_PER_FORCE_PAIR = 75.0  # pressure + viscosity + P dV (+20 with disc viscosity)
 # DRAM bytes (read + write) per row of one launch, from ncu captures of the FP32 kernels on the
 # 1,048,576-particle torus (profiles/k_forces_g_torus1m.md, profiles/k_density_torus1m.md),
-# scaled to a launch by its rows
-DRAM_BYTES_PER_ROW = {"forces": 1768.0, "density": 1003.0}
+# scaled to a launch by its rows; for a list build, the traversal's bytes per particle from the
+# capture of a whole-set build (profiles/k_lists_sub_torus1m.md: 404.0 MB read + 1,289.2 MB
+# written over 1,048,576 rows; the same FP64 kernel in both forms)
+DRAM_BYTES_PER_ROW = {"forces": 1768.0, "density": 1003.0, "lists": 1615.0}
 
 
 def peaks():
@@ -190,7 +192,8 @@ def roofline(prof, precision, disc, pk):
     gbs = bytes_ / (ms * 1e-3) / 1e9
     pipe_peak = FP32_NOMINAL_TFLOPS if precision == "fp32" else FP64_NOMINAL_TFLOPS
     traffic = (DRAM_BYTES_PER_ROW[dom] * units
-               if precision == "fp32" and dom in DRAM_BYTES_PER_ROW else None)  # fmt: skip
+               if (precision == "fp32" or dom == "lists") and dom in DRAM_BYTES_PER_ROW
+               else None)  # fmt: skip
     rf = {"bound": "hbm", "kernel": dom, "achieved": round(gbs, 2), "peak": pk["hbm_gbs"],
           "unit": "GB/s", "frac": round(gbs / pk["hbm_gbs"], 4), "traffic": traffic,
           "peak_source": pk["source"], "ms_per_launch": round(ms, 4),
