@@ -525,7 +525,8 @@ def heat_fixture(blocks, coupled, ics, hydro_cfg):
     (reopen) initialise without a near stop and run to 0.75, so that run() re-opens every
     step to land on it (its _open books the opening kick a second time); (removal) the
     removal_sync run of removal_wake_fixture, 16 system steps (survivors' forces redone, the
-    doomed particles' neighbours cut, removed particles' budgets dropped)."""
+    doomed particles' neighbours cut, removed particles' budgets dropped); (wake) 5 % of the
+    particles forced 5 levels finer, run to 64, so that the limiter wakes neighbours up."""
     ic = ics.cloud(2048, radius=20.0, total_mass=1e-3, t_kelvin=3e8, r_peri=60.0, r_apo=400.0,
                    seed=7)  # fmt: skip
     rng = np.random.default_rng(SEED)
@@ -553,6 +554,19 @@ def heat_fixture(blocks, coupled, ics, hydro_cfg):
         blocks.advance(st, bc)
     out.update(_state_arrays("removal", st, HEAT_FIELDS + ["ids"]))
     out.update(removal_e_radiated=st.e_radiated, removal_n=st.n)
+    # (wake) as (sync) with 5 % of the particles forced 5 levels finer, so that the limiter wakes
+    # their neighbours up (steps cut short, the opening half-kick corrected and booked)
+    hc = hydro_cfg(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
+                   conductivity_signal=1, alpha_u=0.05, h_max=200.0, disc_alpha_av=1.0)  # fmt: skip
+    bc = blocks.BlockConfig(coupled=coupled.CoupledConfig(hydro=hc, cooling_beta=230.0),
+                            dt_max=64.0)  # fmt: skip
+    wake_offset = np.where(rng.random(len(ic.x)) < 0.05, 5, 0)
+    st = blocks.initialise(ic.x, v, ic.u, ic.mass, ic.h, bc, t_stop=64.0,
+                           level_offset=wake_offset)  # fmt: skip
+    blocks.run(st, bc, 64.0)
+    out.update(_state_arrays("wake", st, HEAT_FIELDS))
+    out.update(wake_offset=wake_offset, wake_n=st.n, wake_woken=st.woken,
+               wake_e_radiated=st.e_radiated)  # fmt: skip
     _save("heat_blocks.npz", **out)
 
 

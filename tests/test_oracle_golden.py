@@ -569,9 +569,10 @@ def test_oracle_matches_phantom_golden_vectors(recon):
 HEAT_PARTS = ("heat_visc", "heat_cond", "heat_disk", "heat_pdv", "heat_cool")
 
 
-def heat_runs(g, initialise, run, advance, **hydro):
-    """The three runs of tests/golden/heat_blocks.npz through a block-step API (the oracle's or
-    the device facade's): yields (prefix, state) after each."""
+def heat_runs(g, initialise, run, advance, wake=False, **hydro):
+    """The runs of tests/golden/heat_blocks.npz through a block-step API (the oracle's or the
+    device facade's): yields (prefix, state) after each; with ``wake`` also the run whose
+    limiter wakes particles up."""
     from blackhole_nebula_simulator_b200.config import BlockConfig, CoupledConfig, HydroConfig
 
     hc = HydroConfig(kernel="cubic", eta=1.2, switch=False, reconstruction=False,
@@ -588,6 +589,10 @@ def heat_runs(g, initialise, run, advance, **hydro):
     for _ in range(16):
         advance(st, bc)
     yield "removal", st
+    if wake:
+        bc = BlockConfig(coupled=CoupledConfig(hydro=hc, cooling_beta=230.0), dt_max=64.0)
+        st = initialise(*args[:5], bc, t_stop=64.0, level_offset=g["wake_offset"])
+        yield "wake", run(st, bc, 64.0)
 
 
 def check_heat(g, pre, arrays, e_radiated, tol):
@@ -623,8 +628,11 @@ def check_heat(g, pre, arrays, e_radiated, tol):
 
 def test_heat_budget_matches_reference():
     g = golden("heat_blocks.npz")
-    for pre, st in heat_runs(g, steps.blocks_initialise, steps.blocks_run, steps.blocks_advance):
+    for pre, st in heat_runs(g, steps.blocks_initialise, steps.blocks_run, steps.blocks_advance,
+                             wake=True):  # fmt: skip
         check(f"{pre} tick", int(g[f"{pre}_n"]), st.n)
+        if pre == "wake":
+            check("wake-ups", int(g["wake_woken"]), st.woken)
         if pre == "removal":
             check("removal ids", g["removal_ids"], st.ids)
         arrays = {k: getattr(st, k) for k in ("u_half", "visc_heating", "cond_heating",
