@@ -10,73 +10,103 @@ for plots and rendering are float32 npz files, converted on the device before th
 
 from __future__ import annotations
 
+import dataclasses
 import json
+import math
+import os
 import pickle
 import platform
 import time
-from dataclasses import asdict, fields, is_dataclass
+from dataclasses import fields
 from pathlib import Path
 
 import numpy as np
 import torch
 
+MANIFEST = "manifest.json"
+CHECKPOINT = "checkpoint.pkl"
+CHECKPOINT_TMP = "checkpoint.tmp"  # the partial file a crash may leave; never read
 
-def _jsonable(obj):
-    """sim/runio.py:45-55."""
-    if is_dataclass(obj):
-        return {k: _jsonable(v) for k, v in asdict(obj).items()}
+
+def _plain(obj):
+    """A JSON-ready copy of ``obj``: dataclasses become dicts, tuples lists, NumPy scalars and
+    arrays Python values, and non-finite floats their text ("inf", "nan"), which strict JSON
+    cannot hold."""
+    if dataclasses.is_dataclass(obj) and not isinstance(obj, type):
+        obj = {f.name: getattr(obj, f.name) for f in fields(obj)}
+    if isinstance(obj, np.ndarray):
+        obj = obj.tolist()
+    elif isinstance(obj, np.generic):
+        obj = obj.item()
     if isinstance(obj, dict):
-        return {k: _jsonable(v) for k, v in obj.items()}
+        return {key: _plain(val) for key, val in obj.items()}
     if isinstance(obj, (list, tuple)):
-        return [_jsonable(v) for v in obj]
-    if isinstance(obj, np.generic):
-        return obj.item()
-    if isinstance(obj, float) and not np.isfinite(obj):
-        return str(obj)
+        return [_plain(val) for val in obj]
+    if isinstance(obj, float) and not math.isfinite(obj):
+        return repr(obj)
     return obj
 
 
-def _versions() -> dict:
-    return {"python": platform.python_version(), "numpy": np.__version__,
-            "torch": torch.__version__, "cuda": torch.version.cuda}  # fmt: skip
+def _replace_atomically(path: Path, data: bytes, tmp_name: str | None = None) -> None:
+    """Write ``data`` beside ``path`` and rename it over ``path``: a reader sees the old file or
+    the new one, never a half-written one."""
+    tmp = path.with_name(tmp_name or f".{path.name}.tmp")
+    with open(tmp, "wb") as f:
+        f.write(data)
+        f.flush()
+        os.fsync(f.fileno())
+    os.replace(tmp, path)
+
+
+def _manifest_write(folder: Path, manifest: dict) -> None:
+    _replace_atomically(Path(folder) / MANIFEST, json.dumps(manifest, indent=2).encode())
+
+
+def _environment() -> dict:
+    """Library versions and the machine the run started on."""
+    versions = {"python": platform.python_version(), "numpy": np.__version__,
+                "torch": torch.__version__, "cuda": torch.version.cuda}  # fmt: skip
+    machine = {key: getattr(platform, key)() for key in ("platform", "processor", "machine")}
+    return {"versions": versions, "machine": machine}
 
 
 def new_run(runs: Path, name: str, config: dict) -> Path:
-    """sim/runio.py:58-72: create <runs>/<name>/ (refuses an existing one) and its manifest."""
+    """Create the run folder <runs>/<name>/ with its snapshots/ folder and manifest (keys as in
+    sim/runio.py:58-72: name, config, versions, machine, seed, start, end, resumed).  An existing
+    folder is never reused: FileExistsError."""
     folder = Path(runs) / name
     folder.mkdir(parents=True, exist_ok=False)
     (folder / "snapshots").mkdir()
-    manifest = {
-        "name": name, "config": _jsonable(config), "versions": _versions(),
-        "machine": {"platform": platform.platform(), "processor": platform.processor(),
-                    "machine": platform.machine()},
-        "seed": None, "start": time.strftime("%Y-%m-%d %H:%M:%S %Z"), "end": None, "resumed": [],
-    }  # fmt: skip
-    (folder / "manifest.json").write_text(json.dumps(manifest, indent=2))
+    env = _environment()
+    _manifest_write(folder, {
+        "name": name, "config": _plain(config), "versions": env["versions"],
+        "machine": env["machine"], "seed": None, "start": time.strftime("%Y-%m-%d %H:%M:%S %Z"),
+        "end": None, "resumed": [],
+    })  # fmt: skip
     return folder
 
 
-def update_manifest(folder: Path, **fields_) -> None:
-    """sim/runio.py:75-83."""
-    path = Path(folder) / "manifest.json"
-    manifest = json.loads(path.read_text())
-    for k, v in fields_.items():
-        if k == "resumed":
-            manifest["resumed"].append({"time": v})
-        else:
-            manifest[k] = _jsonable(v)
-    path.write_text(json.dumps(manifest, indent=2))
+def update_manifest(folder: Path, **changes) -> None:
+    """Set manifest keys; ``resumed=t`` appends a resume record {"time": t} instead."""
+    manifest = json.loads((Path(folder) / MANIFEST).read_text())
+    resumed = changes.pop("resumed", None)
+    if resumed is not None:
+        manifest.setdefault("resumed", []).append({"time": _plain(resumed)})
+    manifest.update({key: _plain(val) for key, val in changes.items()})
+    _manifest_write(folder, manifest)
 
 
 def save_checkpoint(folder: Path, payload) -> None:
-    """sim/runio.py:86-90: pickle ``payload`` atomically."""
-    tmp = Path(folder) / "checkpoint.tmp"
-    tmp.write_bytes(pickle.dumps(payload, protocol=pickle.HIGHEST_PROTOCOL))
-    tmp.replace(Path(folder) / "checkpoint.pkl")
+    """The whole float64 state as a pickle in <folder>/checkpoint.pkl, replaced atomically
+    through checkpoint.tmp (the reference's file names, sim/runio.py:86-90)."""
+    data = pickle.dumps(payload, protocol=pickle.HIGHEST_PROTOCOL)
+    _replace_atomically(Path(folder) / CHECKPOINT, data, CHECKPOINT_TMP)
 
 
 def load_checkpoint(folder: Path):
-    return pickle.loads((Path(folder) / "checkpoint.pkl").read_bytes())
+    """The payload of the last completed ``save_checkpoint``."""
+    with open(Path(folder) / CHECKPOINT, "rb") as f:
+        return pickle.load(f)
 
 
 def save_snapshot(folder: Path, index: int, t: float, **arrays) -> None:
