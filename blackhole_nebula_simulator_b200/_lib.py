@@ -82,6 +82,10 @@ _SIGS = {
     "nb_profile_read": (_int, [_vp, _c.POINTER(_dbl)]),
     "nb_find_neighbours": (_int, [_vp, _i64, _vp, _vp, _vp, _c.POINTER(_i64), _vp]),
     "nb_neighbours_export": (_int, [_vp, _vp, _vp, _vp]),
+    "nb_cell_geometry": (_int, [_vp, _i64, _vp, _vp, _c.POINTER(_dbl), _c.POINTER(_dbl),
+                                _c.POINTER(_i64), _vp]),
+    "nb_build_cells": (_int, [_vp, _i64, _vp, _c.POINTER(_dbl), _c.POINTER(_dbl),
+                              _c.POINTER(_i64), _vp, _vp, _vp]),
     "nb_tighten": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
     "nb_density": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _int, _dbl, _dbl,
                           _dbl, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -175,6 +175,25 @@ int nb_neighbours_export(nb_ctx* ctx, int64_t* offset, int64_t* index, void* str
   return nbk::export_lists(ctx->E, offset, index, S(stream));
 }
 
+int nb_cell_geometry(nb_ctx* ctx, int64_t n, const double* pos, const double* h, double* lo,
+                     double* inv_cell, int64_t* ncell, void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (n <= 0 || n > 2000000000) return nbk::set_host_error(E, "n out of range"), NB_ERR_INPUT;
+  int r = nbk::cell_geometry(E, n, pos, h, lo, inv_cell, ncell, S(stream));
+  return r == -1 ? NB_ERR_INPUT : r;
+}
+
+int nb_build_cells(nb_ctx* ctx, int64_t n, const double* pos, const double* lo,
+                   const double* inv_cell, const int64_t* ncell, int64_t* start, int64_t* order,
+                   void* stream) {
+  NB_TRY(begin(ctx));
+  Engine& E = ctx->E;
+  if (n < 0 || n > 2000000000) return nbk::set_host_error(E, "n out of range"), NB_ERR_INPUT;
+  int r = nbk::build_cells(E, n, pos, lo, inv_cell, ncell, start, order, S(stream));
+  return r == -1 ? NB_ERR_INPUT : r;
+}
+
 int nb_tighten(nb_ctx* ctx, int64_t n, const double* pos, const double* h, const int64_t* offset,
                const int64_t* index, int64_t nrows, const int64_t* rows, int64_t* counts,
                const int64_t* out_off, int64_t* out_idx, void* stream) {

@@ -208,6 +208,10 @@ int mlp_cool(Engine& E, int64_t n, const double* u, const double* rho, const dou
              cudaStream_t st);
 int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaStream_t st);
 int export_lists_offsets(Engine& E, int64_t* off_out, cudaStream_t st);
+int build_cells(Engine& E, int64_t n, const double* pos, const double* lo, const double* inv_cell,
+                const int64_t* ncell, int64_t* start, int64_t* order, cudaStream_t st);
+int cell_geometry(Engine& E, int64_t n, const double* pos, const double* h, double* lo,
+                  double* inv_cell, int64_t* ncell, cudaStream_t st);
 int export_lists(Engine& E, int64_t* off_out, int64_t* idx_out, cudaStream_t st);
 
 inline int set_host_error(Engine& E, const char* msg) {

@@ -609,6 +609,117 @@ int export_lists(Engine& E, int64_t* off_out, int64_t* idx_out, cudaStream_t st)
   return check_device_error(E, st);
 }
 
+// ---------------------------------------------------------------- the reference's cell grid
+// sim/neighbours.py:95-126 (_cell_of, _build_grid): per axis k = floor((x - lo) * inv_cell),
+// clamped to [0, ncell - 1], cell = (cx * ny + cy) * nz + cz, and a stable counting sort of the
+// particles by cell (start: ncell + 1 offsets, order: particles by cell, ascending index within a
+// cell).  The subtraction and product round as the reference's (no fused multiply-add), so the
+// assignment is the same bit for bit.  The lists above do not need these cells (their tree
+// prunes with exact tests); this is the reference's cell assignment on its own, for callers and
+// for the parity tests.
+__global__ void k_cell_index(int64_t n, const double* __restrict__ pos, double lo0, double lo1,
+                             double lo2, double ic0, double ic1, double ic2, int64_t n0,
+                             int64_t n1, int64_t n2, uint32_t* __restrict__ cell,
+                             int32_t* __restrict__ iota,
+                             unsigned long long* __restrict__ per_cell) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double lo[3] = {lo0, lo1, lo2}, ic[3] = {ic0, ic1, ic2};
+  const int64_t nc[3] = {n0, n1, n2};
+  int64_t k[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    double t = __dmul_rn(__dsub_rn(pos[3 * i + c], lo[c]), ic[c]);
+    int64_t v = (int64_t)floor(t);
+    k[c] = v < 0 ? 0 : (v >= nc[c] ? nc[c] - 1 : v);
+  }
+  const int64_t id = (k[0] * n1 + k[1]) * n2 + k[2];
+  cell[i] = (uint32_t)id;
+  iota[i] = (int32_t)i;
+  atomicAdd(per_cell + id, 1ull);
+}
+
+__global__ void k_widen_order(int64_t n, const int32_t* __restrict__ src, int64_t* __restrict__ dst) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < n) dst[k] = src[k];
+}
+
+int build_cells(Engine& E, int64_t n, const double* pos, const double* lo, const double* inv_cell,
+                const int64_t* ncell, int64_t* start, int64_t* order, cudaStream_t st) {
+  const int64_t total = ncell[0] * ncell[1] * ncell[2];
+  if (ncell[0] < 1 || ncell[1] < 1 || ncell[2] < 1 || total > (int64_t)INT32_MAX)
+    return set_host_error(E, "cell counts must be positive and hold at most 2^31 cells");
+  NB_TRY(E.ensure_n(std::max<int64_t>(n, 1)));
+  NB_TRY(E.ensure_sort_keys(total));
+  unsigned long long* per_cell = reinterpret_cast<unsigned long long*>(E.sort_keys);
+  NB_CUDA(cudaMemsetAsync(per_cell, 0, sizeof(int64_t) * total, st));
+  NB_CUDA(cudaMemsetAsync(start, 0, sizeof(int64_t), st));
+  if (n > 0) {
+    uint32_t* cell = reinterpret_cast<uint32_t*>(E.keys_a);
+    uint32_t* cell_sorted = reinterpret_cast<uint32_t*>(E.keys_b);
+    int32_t* by_cell = reinterpret_cast<int32_t*>(E.keys_b) + E.cap_n;  // second half of keys_b
+    count_launch(), k_cell_index<<<grid_for(n), NB_THREADS, 0, st>>>(
+        n, pos, lo[0], lo[1], lo[2], inv_cell[0], inv_cell[1], inv_cell[2], ncell[0], ncell[1],
+        ncell[2], cell, E.vals_a, per_cell);
+    int end_bit = 1;
+    while (end_bit < 32 && (int64_t(1) << end_bit) < total) ++end_bit;
+    size_t tmp = 0;
+    NB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, cell, cell_sorted, E.vals_a, by_cell,
+                                            (int)n, 0, end_bit, st));
+    NB_TRY(E.ensure_cub(tmp));
+    tmp = E.cub_bytes;
+    // radix sort is stable: within a cell the particles keep ascending index, as the reference's
+    // counting sort leaves them
+    NB_CUDA(cub::DeviceRadixSort::SortPairs(E.cub_tmp, tmp, cell, cell_sorted, E.vals_a, by_cell,
+                                            (int)n, 0, end_bit, st));
+    count_launch(), k_widen_order<<<grid_for(n), NB_THREADS, 0, st>>>(n, by_cell, order);
+  }
+  size_t tmp = 0;
+  const int64_t* counts = reinterpret_cast<const int64_t*>(per_cell);
+  NB_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp, counts, start + 1, (int)total, st));
+  NB_TRY(E.ensure_cub(tmp));
+  tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, counts, start + 1, (int)total, st));
+  return check_device_error(E, st);
+}
+
+// sim/neighbours.py:250-265 (find_neighbours_numba, no periodic box): lo = the smallest
+// coordinates, cell = max(R_KERN * median(h) / 2, max(span) / 160, 1e-300), ncell = floor(span /
+// cell) + 1 per axis, inv_cell = 1 / cell (host outputs; the call synchronises its stream).
+int cell_geometry(Engine& E, int64_t n, const double* pos, const double* h, double* lo,
+                  double* inv_cell, int64_t* ncell, cudaStream_t st) {
+  if (n <= 0) return set_host_error(E, "the cell grid needs at least one particle");
+  NB_TRY(E.ensure_n(n));
+  int nbb = (int)std::min<int64_t>(grid_for(n), 1184);
+  count_launch(), k_bbox_partial<<<nbb, NB_THREADS, 0, st>>>(n, pos, E.bbox_part);
+  count_launch(), k_bbox_final<<<1, NB_THREADS, 0, st>>>(nbb, E.bbox_part, E.bbox);
+  double* h_sorted = reinterpret_cast<double*>(E.keys_b);
+  size_t tmp = 0;
+  NB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, h, h_sorted, (int)n, 0, 64, st));
+  NB_TRY(E.ensure_cub(tmp));
+  tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceRadixSort::SortKeys(E.cub_tmp, tmp, h, h_sorted, (int)n, 0, 64, st));
+  double box[6], mid[2];
+  NB_CUDA(cudaMemcpyAsync(box, E.bbox, sizeof(box), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaMemcpyAsync(mid, h_sorted + (n - 1) / 2, sizeof(double) * (n % 2 ? 1 : 2),
+                          cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  // numpy's median: the middle value, or the mean of the two middle values for even n
+  const double median = n % 2 ? mid[0] : (mid[0] + mid[1]) / 2.0;
+  double span[3], smax = 0.0;
+  for (int c = 0; c < 3; ++c) {
+    lo[c] = box[c];
+    span[c] = box[3 + c] - box[c];
+    smax = std::max(smax, span[c]);
+  }
+  const double cell = std::max(std::max(0.5 * 2.0 * median, smax / 160.0), 1e-300);
+  for (int c = 0; c < 3; ++c) {
+    ncell[c] = std::max<int64_t>((int64_t)std::floor(span[c] / cell) + 1, 1);
+    inv_cell[c] = 1.0 / cell;
+  }
+  return check_device_error(E, st);
+}
+
 size_t cub_bytes_needed(int64_t n, int64_t m) {
   size_t a = 0, b = 0, c = 0, d = 0;
   cub::DeviceRadixSort::SortPairs((void*)nullptr, a, (uint64_t*)nullptr, (uint64_t*)nullptr,

@@ -70,6 +70,12 @@ int nb_density_noalloc(int64_t n, const double* pos, const double* mass, const d
                   (long long)n, (int)NB_NOALLOC_MAX_N);
     return NB_ERR_INPUT;
   }
+  if (rows && (nrows < 0 || nrows > n)) {
+    std::snprintf(g_msg, sizeof(g_msg),
+                  "nb_density_noalloc: nrows = %lld rows of n = %lld particles (must be 0..n)",
+                  (long long)nrows, (long long)n);
+    return NB_ERR_INPUT;
+  }
   if (kernel_id != 0 && kernel_id != 1) {
     std::snprintf(g_msg, sizeof(g_msg), "nb_density_noalloc: kernel_id must be 0 or 1");
     return NB_ERR_INPUT;

@@ -59,6 +59,32 @@ def find_neighbours(pos, h, box=None) -> Neighbours:
     return Neighbours(off, idx[: total.value], None)
 
 
+def cell_geometry(pos, h):
+    """sim/neighbours.py:250-265 (find_neighbours_numba's grid, no periodic box): (lo, inv_cell,
+    ncell) as host arrays, float64 (3), float64 (3), int64 (3)."""
+    import numpy as np
+
+    pos, h = dev_f64(pos), dev_f64(h)
+    lo, ic, nc = (ctypes.c_double * 3)(), (ctypes.c_double * 3)(), (ctypes.c_int64 * 3)()
+    _call("nb_cell_geometry", len(pos), ptr(pos), ptr(h), lo, ic, nc, stream())
+    return np.array(lo[:]), np.array(ic[:]), np.array(nc[:], dtype=np.int64)
+
+
+def build_grid(pos, lo, inv_cell, ncell):
+    """sim/neighbours.py:106-126 (_build_grid): (start, order) of the stable counting sort of the
+    particles by cell (cx * ny + cy) * nz + cz, as int64 CUDA tensors."""
+    pos = dev_f64(pos)
+    n = len(pos)
+    lo3 = (ctypes.c_double * 3)(*[float(v) for v in lo])
+    ic3 = (ctypes.c_double * 3)(*[float(v) for v in inv_cell])
+    nc3 = (ctypes.c_int64 * 3)(*[int(v) for v in ncell])
+    total = int(nc3[0]) * int(nc3[1]) * int(nc3[2])
+    start = torch.empty(total + 1, dtype=torch.int64, device=pos.device)
+    order = torch.empty(max(n, 1), dtype=torch.int64, device=pos.device)
+    _call("nb_build_cells", n, ptr(pos), lo3, ic3, nc3, ptr(start), ptr(order), stream())
+    return start, order[:n]
+
+
 def tighten(nb: Neighbours, pos, h, rows=None) -> Neighbours:
     """sim/neighbours.py:306-323: keep r < 2 max(h_i, h_j), lists for ``rows`` only."""
     pos = dev_f64(pos)

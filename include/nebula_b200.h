@@ -129,6 +129,20 @@ NB_API int nb_find_neighbours(nb_ctx* ctx, int64_t n, const double* pos, const d
                        int64_t* total, void* stream);
 NB_API int nb_neighbours_export(nb_ctx* ctx, int64_t* offset, int64_t* index, void* stream);
 
+/* The reference's cell grid.  nb_cell_geometry: find_neighbours_numba's grid geometry without
+ * a periodic box (sim/neighbours.py:250-265): lo (3) = the smallest coordinates, cell = max(
+ * median(h), max(span) / 160, 1e-300), ncell (3) = floor(span / cell) + 1, inv_cell (3) = 1 /
+ * cell, written to host memory (the call synchronises its stream).  nb_build_cells: _build_grid
+ * (sim/neighbours.py:106-126): cell (cx * ny + cy) * nz + cz of each particle with
+ * k = floor((x - lo) * inv_cell) clamped to [0, ncell - 1], rounded as the reference's, and the
+ * stable counting sort: start (ncx * ncy * ncz + 1) and order (n, ascending index within a
+ * cell); lo, inv_cell and ncell are host arrays. */
+NB_API int nb_cell_geometry(nb_ctx* ctx, int64_t n, const double* pos, const double* h,
+                            double* lo, double* inv_cell, int64_t* ncell, void* stream);
+NB_API int nb_build_cells(nb_ctx* ctx, int64_t n, const double* pos, const double* lo,
+                          const double* inv_cell, const int64_t* ncell, int64_t* start,
+                          int64_t* order, void* stream);
+
 /* tighten (sim/neighbours.py:284-323), two calls: out_off == NULL writes counts (n) of the kept
  * entries per row; then with out_off (n+1, the caller's prefix sum) writes out_idx. */
 NB_API int nb_tighten(nb_ctx* ctx, int64_t n, const double* pos, const double* h, const int64_t* offset,
@@ -289,7 +303,11 @@ NB_API int nb_block_land(nb_ctx* ctx, nb_state* st, const nb_params* prm, void* 
  * that loads the library until exit; larger n returns NB_ERR_INPUT.  The first call on a device
  * looks up that array's device address (cudaGetSymbolAddress), so make it before any stream
  * capture.  All calls share the array: calls that overlap on the GPU race and must be
- * serialised by the caller.  Messages of failed calls: nb_noalloc_last_error (per host thread). */
+ * serialised by the caller.  offset (n + 1) and index must describe lists over [0, n), and with
+ * rows given, 0 <= nrows <= n and every rows[k] in [0, n): the call does not read them back to
+ * check, and an index at or beyond n would read entries of the shared array left by an earlier
+ * call (stale positions) instead of failing.  nrows beyond n or negative returns NB_ERR_INPUT.
+ * Messages of failed calls: nb_noalloc_last_error (per host thread). */
 #define NB_NOALLOC_MAX_N 262144
 NB_API int nb_density_noalloc(int64_t n, const double* pos, const double* mass,
                               const double* h_start, const double* h_search,

@@ -1,8 +1,9 @@
 """Per-particle heat budget of the block steps (sim/blocks.py:142-154, 434-440, 531, 546) on the
 GPU against the reference's (tests/golden/heat_blocks.npz): the multi-level cloud with viscosity,
 conductivity, disc viscosity and beta-cooling run to a sync point, run() re-opening every step to
-land on a near stop (the opening kick booked twice, as the reference does), and removal_sync
-dropping removed particles' budgets.
+land on a near stop (the opening kick booked twice, as the reference does), removal_sync
+dropping removed particles' budgets, and a run whose level limiter wakes neighbours up (5 % of
+the particles forced 5 levels finer), so the corrected half kick of a wake-up is booked.
 
 Tolerances: every array to 1e-9 of its largest value (the block-step tolerance of u); the budget
 identity u_half - u_0 = visc + cond + disk + pdv - cool to 1e-12 of max u_0 where it holds, and
@@ -32,13 +33,18 @@ def blocks():
 
 def test_heat_budget_matches_reference(blocks):
     g = golden("heat_blocks.npz")
-    for pre, st in heat_runs(g, blocks.initialise, blocks.run, blocks.advance):
+    seen = []
+    for pre, st in heat_runs(g, blocks.initialise, blocks.run, blocks.advance, wake=True):
+        seen.append(pre)
         check(f"{pre} tick", int(g[f"{pre}_n"]), st.n)
+        if pre == "wake":
+            check("wake-ups", int(g["wake_woken"]), st.woken)
         if pre == "removal":
             check("removal ids", g["removal_ids"], st.ids.cpu().numpy())
         arrays = {k: getattr(st, k).cpu().numpy() for k in (
             "u_half", "visc_heating", "cond_heating", "disk_heating") + HEAT_PARTS}  # fmt: skip
         check_heat(g, pre, arrays, st.e_radiated, 1e-9)
+    check("runs checked", ["sync", "reopen", "removal", "wake"], seen)
 
 
 def test_heat_budget_fp32_adds_up(blocks):

@@ -56,6 +56,42 @@ def test_cloud_lists_and_tighten_bit_exact(nb):
     check("tight indices", g["tight_index"].astype(np.int64), _np(t.index))
 
 
+def test_cloud_cells_bit_exact(nb):
+    """The reference's cell assignment (sim/neighbours.py:106-126, 250-265): grid geometry, cell
+    starts and the counting-sort order of the 4,096 cloud exactly as the reference wrote them."""
+    ops = nb[0]
+    g = golden("cloud_lists.npz")
+    lo, inv, nc = ops.cell_geometry(g["pos"], g["h_search"])
+    check("grid lo", g["lo"], lo)
+    check("grid inverse cell", g["inv_cell"], inv)
+    check("grid dims", g["ncell"], nc)
+    start, order = ops.build_grid(g["pos"], g["lo"], g["inv_cell"], g["ncell"])
+    check("cell starts", g["grid_start"], _np(start))
+    check("cell order", g["grid_order"].astype(np.int64), _np(order))
+
+
+def test_cells_at_262k_bit_exact(nb):
+    """The same at the 262,144-particle cloud (BASELINE's second configuration) against the
+    oracle's cell of every particle: geometry, starts and order exactly."""
+    from blackhole_nebula_simulator_b200 import ics
+    from oracle import native
+
+    ops = nb[0]
+    ic = ics.cloud(262_144, seed=1)
+    # varied search radii, so the median of an even count is the mean of two different values
+    hs = 1.4 * ic.h * np.random.default_rng(5).uniform(0.8, 1.25, len(ic.h))
+    cell, lo, inv, nc = native.grid_cells(ic.x, hs)
+    glo, ginv, gnc = ops.cell_geometry(ic.x, hs)
+    check("grid lo", lo, glo)
+    check("grid dims", nc, gnc)
+    check("grid inverse cell", inv, ginv)
+    start, order = ops.build_grid(ic.x, lo, inv, nc)
+    ref_order = np.argsort(cell, kind="stable")
+    check("cell order", ref_order, _np(order))
+    check("cell starts", np.searchsorted(cell[ref_order], np.arange(int(np.prod(nc)) + 1)),
+          _np(start))  # fmt: skip
+
+
 def test_long_and_short_rows_bit_exact(nb):
     """Rows far longer than the one-pass build's slot width (a few particles with 8x the search
     radius) beside ordinary rows, twice in a row so the second build runs with the width the first
