@@ -206,6 +206,52 @@ def roofline(prof, precision, disc, pk):
     return rf, dom
 
 
+# algorithmic bytes and FLOPs of one launch of each category, from its units (rows or
+# particles) and pairs (list entries written, in-support density evaluations, interacting force
+# pairs) per launch; None where the category has no such model
+def _category_work(cat, units, pairs, precision, disc):
+    rec = 112.0 if precision == "fp32" else 128.0  # packed per-particle records of a pair pass
+    if cat == "lists":  # sorted record read, offset written, 4 B per entry written
+        return units * (32.0 + 8.0) + pairs * 4.0, 0.0
+    if cat == "density":  # row records in, h / rho / omega out, 4 B per pair evaluation
+        return units * (48.0 + 40.0) + pairs * 4.0, pairs * FLOP_PER_DENSITY_EVAL
+    if cat == "forces":
+        return (units * (rec + 48.0) + pairs * 4.0,
+                pairs * (FLOP_PER_FORCE_PAIR + (20.0 if disc else 0.0)))  # fmt: skip
+    if cat == "flow":  # x_beg, p_half, n_beg, n_end, a in; x, p_flow, p_pred out
+        return units * (48.0 + 16.0 + 24.0 + 72.0 + 8.0), 0.0
+    if cat == "cooling":  # u, rho, dt in; u out
+        return units * 32.0, 0.0
+    if cat == "eos":  # rho, u, mask in; P, c_s out
+        return units * 33.0, 0.0
+    return None, None
+
+
+def kernel_table(prof, precision, disc, pk):
+    """Every timed category: launches, ms per launch, algorithmic GB/s and FP32 (or FP64)
+    TFLOP/s per launch with their fractions of the measured HBM peak and the nominal pipe."""
+    pipe_peak = FP32_NOMINAL_TFLOPS if precision == "fp32" else FP64_NOMINAL_TFLOPS
+    out = {}
+    for cat, d in prof.items():
+        if cat.startswith("_") or d["launches"] == 0:
+            continue
+        ms = d["ms"] / d["launches"]
+        units, pairs = d["units"] / d["launches"], d["pairs"] / d["launches"]
+        b, f = _category_work(cat, units, pairs, precision, disc)
+        row = {"launches": d["launches"], "ms_per_launch": round(ms, 4),
+               "units_per_launch": round(units), "pairs_per_launch": round(pairs)}  # fmt: skip
+        if b is not None and ms > 0:
+            gbs = b / (ms * 1e-3) / 1e9
+            row.update(bytes_per_launch=round(b), gbs=round(gbs, 1),
+                       hbm_frac=round(gbs / pk["hbm_gbs"], 4))  # fmt: skip
+        if f and ms > 0:
+            tf = f / (ms * 1e-3) / 1e12
+            row.update(flop_per_launch=round(f), tflops=round(tf, 3),
+                       pipe_frac=round(tf / pipe_peak, 4))  # fmt: skip
+        out[cat] = row
+    return out
+
+
 def combine_ranks(ms, psteps, device):
     """Replicas: the job's time is the slowest rank's, its work the sum over ranks."""
     import torch
@@ -528,13 +574,93 @@ def run_deposit(args, rank, world):
         }))  # fmt: skip
 
 
+def measure(args, name, rank, world, steps=None):
+    """One workload on this rank: the FP32 + MLP form (value, e2e, kernel categories, drift),
+    the FP64 plain form on the same workload, and on rank 0 the roofline and the CPU baseline.
+    Returns the workload's JSON object (rank 0) or None."""
+    import copy
+
+    a = copy.copy(args)
+    a.workload = name
+    a.n = args.n if name == args.workload else None
+    if steps is not None:
+        a.steps = steps
+    ms, total, prof, clocks, st, led, e2e, mlp = run_gpu(a, rank, world)
+    plain = None
+    if a.precision == "fp32" and not a.no_plain:
+        # the comparison form of the metric: FP64 pair arithmetic with the exact integrator
+        p_ms, p_total, p_prof, p_clk, p_st, p_led, _, _ = run_gpu(a, rank, world, "fp64", False,
+                                                                  e2e=False)  # fmt: skip
+        plain = {"value": p_total / (p_ms * 1e-3), "unit": "particle-steps/s",
+                 "ms_per_step": p_ms / a.steps, "dtype": "f64", "cooling": "exact integrator",
+                 "energy_rel_drift": p_led["drift_synced"],
+                 "kernel_ms": {k: round(v["ms"], 3) for k, v in p_prof.items()
+                               if not k.startswith("_")}}  # fmt: skip
+    if rank != 0:
+        return None
+    pk = peaks()
+    launches = prof.pop("_launches")
+    rf, dom = roofline(prof, a.precision, "torus" == name, pk)
+    n_full = a.n or N_FULL[name]
+    out = {
+        "value": total / (ms * 1e-3), "unit": "particle-steps/s", "steps": a.steps,
+        "ms_per_step": ms / a.steps, "config": workload_config(a, name, n_full, world),
+        "roofline": rf, "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
+        "kernel_ms": {k: round(v["ms"], 3) for k, v in prof.items()},
+        "kernel_table": kernel_table(prof, a.precision, "torus" == name, pk),
+        "mean_active": total / a.steps / max(world, 1),
+        "list_builds": st.builds, "list_reuses": st.reuses,
+        "levels_used": sorted(set(int(v) for v in st.level.unique().tolist())),
+        "mean_list_entries": (prof["lists"]["pairs"] / prof["lists"]["units"]
+                              if prof["lists"]["units"] else None),
+        "pairs_per_force_row": (prof["forces"]["pairs"] / prof["forces"]["units"]
+                                if prof["forces"]["units"] else None),
+        "h_stats": h_stats(st),
+        "disc_alpha_ss": (TORUS_ALPHA_AV * float(st.h.mean()) / (10.0 * TORUS_SCALE_HEIGHT)
+                          if name == "torus" else None),
+        "cooling": ("network (BF16 tensor cores, exact fallback; bremsstrahlung law of this "
+                    "library, parity with the reference unpinned: it has no such law)"
+                    if mlp is not None else "exact integrator"),
+        "cooling_network": mlp,
+        "energy_rel_drift": led["drift_synced"],
+        "energy_drift_over_time": led["t_synced"],
+        "energy_drift_sync_steps": led["sync_steps"],
+        "fp64_plain": plain,
+        "speedup_vs_fp64_plain": (total / (ms * 1e-3)) / plain["value"] if plain else None,
+    }  # fmt: skip
+    if not a.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_reference(a, 2, 1)
+    return out
+
+
+N_FULL = {"torus": 4_194_304, "streams": 1_048_576, "cloud": 262_144}
+# the second configuration of the metric ("at 1M & 4M"): the 1M streams, timed over more system
+# steps than the torus because its steps are short (small active sets)
+STREAMS_STEPS_PER_STEP = 10
+
+
+def workload_config(args, name, n_full, world):
+    config = {"workload": f"{name}, {n_full} particles, block time steps",
+              "particles": n_full,
+              "precision": args.precision if args.impl == "ours" else "fp64 (CPU oracle)",
+              "l2_flush": "inputs larger than L2",
+              "parallelism": f"replicas x{world}", "eos": args.eos,
+              "shock_capturing": "switch + reconstruction" if args.shock else "constant alpha"}  # fmt: skip
+    if name == "torus":
+        config["disc_alpha_av"] = TORUS_ALPHA_AV
+        config["scale_height"] = TORUS_SCALE_HEIGHT
+    return config
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="torus", choices=["torus", "streams", "cloud", "deposit"])
+    ap.add_argument("--workload", default=None, choices=["torus", "streams", "cloud", "deposit"],
+                    help="one workload only (default: the 4M torus, then the 1M streams in the "
+                         "same run as the line's streams_1m object)")  # fmt: skip
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--shock", action="store_true",
@@ -546,6 +672,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain comparison form")
     args = ap.parse_args()
+    both = args.workload is None
+    if both:
+        args.workload = "torus"
     if args.eos != "ideal" and args.workload != "cloud":
         ap.error("--eos gasrad/radiation needs a workload without cooling: --workload cloud")
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -559,78 +688,48 @@ def main():
         if world > 1 and args.impl == "ours":
             torch.distributed.destroy_process_group()
         return
-    n_full = args.n or {"torus": 4_194_304, "streams": 1_048_576, "cloud": 262_144}[args.workload]
-    config = {"workload": f"{args.workload}, {n_full} particles, block time steps",
-              "particles": n_full,
-              "precision": args.precision if args.impl == "ours" else "fp64 (CPU oracle)",
-              "l2_flush": "inputs larger than L2",
-              "parallelism": f"replicas x{world}", "eos": args.eos,
-              "shock_capturing": "switch + reconstruction" if args.shock else "constant alpha"}  # fmt: skip
-    if args.workload == "torus":
-        config["disc_alpha_av"] = TORUS_ALPHA_AV
-        config["scale_height"] = TORUS_SCALE_HEIGHT
+    n_full = args.n or N_FULL[args.workload]
+    config = workload_config(args, args.workload, n_full, world)
     metric = "particle-steps/s"
     if args.impl == "reference":
         if rank != 0:
             return
         cb = cpu_reference(args, max(1, min(args.steps, 3)), max(1, min(args.warmup, 1)))
-        print(json.dumps({"metric": metric, "value": cb["value"], "unit": "particle-steps/s",
-                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                          "higher_is_better": True, "impl": "reference", "dtype": "f64",
-                          "data": "synthetic", "config": config, "cpu_baseline": cb,
-                          "e2e": {"value": cb["value"], "unit": "particle-steps/s",
-                                  "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))  # fmt: skip
+        line = {"metric": metric, "value": cb["value"], "unit": "particle-steps/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "impl": "reference", "dtype": "f64",
+                "data": "synthetic", "config": config, "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "particle-steps/s",
+                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}  # fmt: skip
+        if both:
+            import copy
+
+            a = copy.copy(args)
+            a.workload, a.n = "streams", None
+            sb = cpu_reference(a, max(1, min(args.steps, 3)), max(1, min(args.warmup, 1)))
+            line["streams_1m"] = {"value": sb["value"], "unit": "particle-steps/s",
+                                  "config": workload_config(a, "streams", N_FULL["streams"], world),
+                                  "cpu_baseline": sb}  # fmt: skip
+        print(json.dumps(line))
         return
     if world > 1:
         import torch
 
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    ms, total, prof, clocks, st, led, e2e, mlp = run_gpu(args, rank, world)
-    plain = None
-    if args.precision == "fp32" and not args.no_plain:
-        # the comparison form of the metric: FP64 pair arithmetic with the exact integrator
-        p_ms, p_total, p_prof, p_clk, p_st, p_led, _, _ = run_gpu(args, rank, world, "fp64", False,
-                                                                  e2e=False)  # fmt: skip
-        plain = {"value": p_total / (p_ms * 1e-3), "unit": "particle-steps/s",
-                 "ms_per_step": p_ms / args.steps, "dtype": "f64", "cooling": "exact integrator",
-                 "energy_rel_drift": p_led["drift_synced"],
-                 "kernel_ms": {k: round(v["ms"], 3) for k, v in p_prof.items()
-                               if not k.startswith("_")}}  # fmt: skip
+    head = measure(args, args.workload, rank, world)
+    streams = None
+    if both:
+        streams = measure(args, "streams", rank, world, steps=args.steps * STREAMS_STEPS_PER_STEP)
     if rank == 0:
-        pk = peaks()
-        launches = prof.pop("_launches")
-        rf, dom = roofline(prof, args.precision, "torus" == args.workload, pk)
-        out = {
-            "metric": metric, "value": total / (ms * 1e-3), "unit": "particle-steps/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
-            "data": "synthetic", "config": config, "roofline": rf, "clocks": clocks, "e2e": e2e,
-            "gpu_launches": launches, "kernel_ms": {k: round(v["ms"], 3) for k, v in prof.items()},
-            "kernel_detail": {k: {"launches": v["launches"], "units_per_launch":
-                                  round(v["units"] / max(v["launches"], 1)),
-                                  "pairs_per_launch": round(v["pairs"] / max(v["launches"], 1))}
-                              for k, v in prof.items()},
-            "mean_active": total / args.steps / max(world, 1),
-            "list_builds": st.builds, "list_reuses": st.reuses,
-            "mean_list_entries": (prof["lists"]["pairs"] / prof["lists"]["units"]
-                                  if prof["lists"]["units"] else None),
-            "pairs_per_force_row": (prof["forces"]["pairs"] / prof["forces"]["units"]
-                                    if prof["forces"]["units"] else None),
-            "h_stats": h_stats(st),
-            "disc_alpha_ss": (TORUS_ALPHA_AV * float(st.h.mean()) / (10.0 * TORUS_SCALE_HEIGHT)
-                              if args.workload == "torus" else None),
-            "cooling": ("network (BF16 tensor cores, exact fallback)" if mlp is not None
-                        else "exact integrator"),
-            "cooling_network": mlp,
-            "energy_rel_drift": led["drift_synced"],
-            "energy_drift_over_time": led["t_synced"],
-            "energy_drift_sync_steps": led["sync_steps"],
-            "fp64_plain": plain,
-            "speedup_vs_fp64_plain": (total / (ms * 1e-3)) / plain["value"] if plain else None,
-        }  # fmt: skip
-        if not args.no_cpu_baseline:
-            out["cpu_baseline"] = cpu_reference(args, 2, 1)
+        out = {"metric": metric, "value": head.pop("value"), "unit": head.pop("unit"),
+               "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": head.pop("ms_per_step"), "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None,
+               "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic"}  # fmt: skip
+        head.pop("steps")
+        out.update(head)
+        if streams is not None:
+            out["streams_1m"] = streams
         print(json.dumps(out))
     if world > 1:
         torch.distributed.destroy_process_group()
