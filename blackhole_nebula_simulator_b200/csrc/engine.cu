@@ -55,7 +55,7 @@ int Engine::ensure_n(int64_t n) {
     NB_CUDA(cudaMallocHost((void**)&h_err, sizeof(int) * 4));
     NB_CUDA(cudaMalloc((void**)&bbox, sizeof(double) * 8));
     NB_CUDA(cudaMallocHost((void**)&h_red, sizeof(double) * 64));
-    NB_CUDA(cudaMalloc((void**)&d_rowmax, 4 * sizeof(unsigned long long)));
+    NB_CUDA(cudaMalloc((void**)&d_rowmax, 8 * sizeof(unsigned long long)));
     NB_CUDA(cudaMallocHost((void**)&h_build, sizeof(int64_t) * 2));
   }
   if (n <= cap_n && keys_a) return 0;
@@ -126,9 +126,23 @@ int Engine::ensure_tight(int64_t m) {
   return grow(E, tidx, cap_tidx, std::max<int64_t>(m, 1));
 }
 
-int Engine::ensure_ell(int64_t m) {
+int Engine::ensure_leaves(int64_t m) {
   Engine& E = *this;
-  return grow(E, ell, cap_ell, m);
+  if (m <= cap_leaf && leaf_cbase) return 0;
+  int64_t c = 0;
+  NB_TRY(grow(E, leaf_cbase, c, m));
+  c = 0;
+  NB_TRY(grow(E, leaf_bbase, c, m));
+  c = 0;
+  NB_TRY(grow(E, leaf_ncand, c, m));
+  cap_leaf = c;
+  return 0;
+}
+
+int Engine::ensure_tiles(int64_t ncand, int64_t nbatch) {
+  Engine& E = *this;
+  NB_TRY(grow(E, cands, cap_cands, std::max<int64_t>(ncand, 1)));
+  return grow(E, masks, cap_masks, std::max<int64_t>(nbatch * 32, 32));
 }
 
 int Engine::ensure_deposit(int64_t n) {
@@ -164,7 +178,7 @@ int Engine::ensure_sort_keys(int64_t m) {
 void Engine::release() {
   void* ps[] = {dep_k0, dep_k1, dep_i0, dep_i1, dep_buf, d_err, bbox, bbox_part, keys_a, keys_b, vals_a, counts, node_lo, node_hi, sub_lo, sub_hi,
                 cub_tmp, sort_keys, red, lists.perm, lists.inv_perm, lists.spos, lists.off,
-                lists.idx, ell, d_rowmax, tidx};
+                lists.idx, d_rowmax, tidx, leaf_cbase, leaf_bbase, leaf_ncand, cands, masks};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (h_err) cudaFreeHost(h_err);
@@ -369,6 +383,22 @@ __global__ void k_pack_sorted(int64_t n, const int32_t* __restrict__ perm,
   out[k] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], w ? w[i] : 0.0);
 }
 
+// the density pass's per-particle inputs in sorted order (masses also as floats when asked)
+__global__ void k_gather_density(int64_t n, const int32_t* __restrict__ perm,
+                                 const double* __restrict__ mass, const double* __restrict__ h0,
+                                 const double* __restrict__ hs, double* __restrict__ mass_s,
+                                 double* __restrict__ h0_s, double* __restrict__ hs_s,
+                                 float* __restrict__ massf_s) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int32_t i = perm[k];
+  const double m = mass[i];
+  mass_s[k] = m;
+  h0_s[k] = h0[i];
+  hs_s[k] = hs[i];
+  if (massf_s) massf_s[k] = (float)m;
+}
+
 __global__ void k_to_float(int64_t n, const double* __restrict__ a, float* __restrict__ out) {
   int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (k < n) out[k] = (float)a[k];
@@ -383,10 +413,12 @@ __global__ void k_pack_sorted4(int64_t n, const int32_t* __restrict__ perm, cons
   out[k] = make_double4(a ? a[i] : 0.0, b ? b[i] : 0.0, c ? c[i] : 0.0, d ? d[i] : 0.0);
 }
 
-// FP32 positions: integer cell of a uniform grid (edge `cell`, at most 1024 per axis, corner lo)
-// packed 10 bits per axis, and the float offset from the cell centre.
+// FP32 positions: the cell of a uniform grid (edge `cell`, at most 1024 per axis, corner lo) and
+// the float offset from the cell centre, as two float4 per particle: (offset, mass) and (cell
+// coordinates as exact floats, h); mass and h 0 when not given.
 __global__ void k_pack_sorted32(int64_t n, const int32_t* __restrict__ perm,
-                                const double* __restrict__ x, const double* __restrict__ box6,
+                                const double* __restrict__ x, const double* __restrict__ m,
+                                const double* __restrict__ h, const double* __restrict__ box6,
                                 float4* __restrict__ out) {
   int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -402,7 +434,8 @@ __global__ void k_pack_sorted32(int64_t n, const int32_t* __restrict__ perm,
     c[a] = ci;
     o[a] = (float)(x[3 * i + a] - (box6[a] + (ci + 0.5) * cell));
   }
-  out[k] = make_float4(o[0], o[1], o[2], __int_as_float((c[0] << 20) | (c[1] << 10) | c[2]));
+  out[2 * k] = make_float4(o[0], o[1], o[2], m ? (float)m[i] : 0.0f);
+  out[2 * k + 1] = make_float4((float)c[0], (float)c[1], (float)c[2], h ? (float)h[i] : 0.0f);
 }
 
 // the configured EOS (sim/hydro.py:119-139) for every particle, or for the particles of `mask`
@@ -597,7 +630,7 @@ int Workspace::ensure(Engine& E, int64_t n) {
   for (double** p : d3) NB_CUDA(cudaMalloc((void**)p, sizeof(double) * 3 * c));
   double4** d4[] = {&pk0, &pk1, &pk2, &pk3};
   for (double4** p : d4) NB_CUDA(cudaMalloc((void**)p, sizeof(double4) * c));
-  NB_CUDA(cudaMalloc((void**)&pk32, sizeof(float4) * c));
+  NB_CUDA(cudaMalloc((void**)&pk32, sizeof(float4) * 2 * c));
   NB_CUDA(cudaMalloc((void**)&f_mass, sizeof(float) * c));
   float4** f4s[] = {&pf1, &pf2, &pf3};
   for (float4** p : f4s) NB_CUDA(cudaMalloc((void**)p, sizeof(float4) * c));
@@ -812,16 +845,13 @@ static int density_on_lists(Engine& E, int64_t n, const double* x, const double*
   if (nrows == 0) return 0;
   int64_t ns = 0;
   NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));
-  count_launch(), k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, mass, W.d_a);
-  count_launch(), k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, h_start, W.d_b);
-  count_launch(), k_gather_d<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, h_search, W.d_c);
+  count_launch(), k_gather_density<<<grid_for(n), NB_THREADS, 0, st>>>(
+      n, L.perm, mass, h_start, h_search, W.d_a, W.d_b, W.d_c, nullptr);
   DensityParams dp{prm->kernel_id, prm->cnorm, prm->eta, prm->tol, prm->h_max};
   if (prm->precision == 1) {
     // grid over the box of the last list build (cells clamp to it; the edge is derived on the
     // device, so no host round trip)
-    count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, E.bbox, W.pk32);
-    count_launch(), k_to_float<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.d_a, W.f_mass);
-    dp.massf = W.f_mass;
+    count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, mass, nullptr, E.bbox, W.pk32);
     E.prof.begin(st);
     launch_density32<int32_t>(nrows, W.rows_s, W.pk32, E.bbox, W.d_a, W.d_b, W.d_c, L.off,
                               L.idx, dp, L.perm, h_out, rho, omega, W.iters, W.flags,
@@ -1017,7 +1047,8 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   E.prof.begin(st);
   count_launch(), k_eos<<<grid_for(n), NB_THREADS, 0, st>>>(n, s->rho, u, eos_mask, eos_of(prm), W.d_P, W.d_cs, E.d_err);
   E.prof.end(PROF_EOS, st, (double)n, 0.0);
-  if (nrows == 0) return check_device_error(E, st);
+  W.pend_err = true;  // the EOS's and the force pass's error word, read at the step's end
+  if (nrows == 0) return 0;
   int64_t ns = 0;
   NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));
   const bool sw_on = prm->viscosity && prm->visc_switch && sk.switch_on;
@@ -1080,14 +1111,18 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   fp.tighten = 1;
   const bool want_tight = sk.want_tight && prm->limiter && rows == W.rows;
   W.tight_ver = -1;
-  if (want_tight) {
+  // the FP32 form without the reconstruction walks the lists in a launch of its own that writes
+  // the interacting entries, and sums the pairs from them in a second launch (they are also
+  // the limiter's entries when it wants them, decided exactly in the FP32 test's band)
+  const bool split = prm->precision == 1 && !recon;
+  if (want_tight || split) {
     NB_TRY(E.ensure_tight(L.total));
     fp.tidx = E.tidx;
     fp.tcnt = W.i32a;
-    if (prm->precision == 1) {
-      count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, s->h, W.pk0);
-      fp.pos64 = W.pk0;
-    }
+  }
+  if (want_tight && prm->precision == 1) {
+    count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, s->h, W.pk0);
+    fp.pos64 = W.pk0;
   }
   if (recon) {
     fp.use_recon = 1;
@@ -1108,7 +1143,7 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   fo.ddudt = W.d_ddudt;
   fo.pairs = W.pairs;
   if (prm->precision == 1) {
-    count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, E.bbox, W.pk32);
+    count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, s->mass, s->h, E.bbox, W.pk32);
     E.prof.begin(st);
     launch_forces32<int32_t>(nrows, W.rows_s, W.pk32, E.bbox, W.pf1, W.pf2, W.pf3, L.off,
                              L.idx, fp, L.perm, fo, st);
@@ -1132,7 +1167,7 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
       nrows, rows, prm->viscosity, prm->disc_alpha_av, W.v_dacc, W.d_ddudt, W.d_cs, s->h,
       W.d_vsig, s->a_hydro, s->dudt, s->vsig_max, s->nu, s->disk_heating);
   NB_CUDA(cudaGetLastError());
-  return check_device_error(E, st);
+  return 0;
 }
 
 }  // namespace nbk

@@ -175,13 +175,24 @@ struct Engine {
   double* dep_buf = nullptr;
   int64_t dep_cap = 0;
   int ensure_deposit(int64_t n);
-  // one-pass list build: rows written to fixed-width slots (row_cap entries each), then packed
-  int32_t* ell = nullptr;
-  int64_t cap_ell = 0, row_cap = 256;
-  int64_t list_slots = 0;  // resident blocks of the persistent list kernel
+  int64_t list_slots = 0, cand_slots = 0;  // resident warps of the persistent list passes
   int32_t* tidx = nullptr;  // interacting entries of the active rows, in the lists' layout
   int64_t cap_tidx = 0;
+  // list build: the longest row of the last build [0], the passes' work counters [2, 3] and the
+  // candidate and batch cursors [4, 5]
   unsigned long long* d_rowmax = nullptr;
+  // list build: per query leaf the start of its candidate list and of its masks and its number
+  // of candidate sub-leaves; the candidate lists and the tests' hit masks (32 per batch)
+  int64_t *leaf_cbase = nullptr, *leaf_bbase = nullptr;
+  int32_t* leaf_ncand = nullptr;
+  int64_t cap_leaf = 0;
+  int32_t* cands = nullptr;
+  int64_t cap_cands = 0;
+  uint32_t* masks = nullptr;
+  int64_t cap_masks = 0;
+  int64_t last_cands = 0, last_batches = 0;
+  int ensure_leaves(int64_t m);
+  int ensure_tiles(int64_t ncand, int64_t nbatch);
   int64_t* h_build = nullptr;  // pinned: total entries and longest row of the last build
   double* red = nullptr;      // reduction partials (doubles)
   double* h_red = nullptr;    // pinned host copy of small reductions
@@ -194,7 +205,6 @@ struct Engine {
   int ensure_sub(int64_t m);
   int ensure_list_capacity(int64_t m);
   int ensure_sort_keys(int64_t m);
-  int ensure_ell(int64_t m);
   int ensure_tight(int64_t m);
   int ensure_cub(size_t bytes);
   void release();

@@ -330,7 +330,7 @@ __device__ __forceinline__ void mlp_hidden(const __nv_bfloat16 (*W)[MLP_H], cons
 // mode_out (optional): 0 exact (at or below the floor, or not cooled), 1 network, 2 fallback.
 // judge: every judge-th network result is compared with the exact one (|du_mlp - du_exact| / u
 // accumulated as max and sum of squares in stats[0..1], count in stats[2]).
-__global__ void __launch_bounds__(128) k_mlp_cool(int64_t n, const double* __restrict__ u_in,
+__global__ void __launch_bounds__(128, 4) k_mlp_cool(int64_t n, const double* __restrict__ u_in,
                                                   const double* __restrict__ rho,
                                                   const double* __restrict__ dt, double dt_scalar,
                                                   const float* __restrict__ w, BremsParams bp,
@@ -346,6 +346,7 @@ __global__ void __launch_bounds__(128) k_mlp_cool(int64_t n, const double* __res
   int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   int64_t nwarps = (int64_t)gridDim.x * warps;
   unsigned long long n_mlp = 0, n_fb = 0;
+  double j_e2 = 0.0, j_n = 0.0, j_max = 0.0;  // judged errors of this thread (summed per warp)
   for (int64_t base = wid * 16; base < n; base += nwarps * 16) {
     // lanes 0-15 form the scaled inputs of one particle each
     int64_t me = base + (lane & 15);
@@ -412,7 +413,9 @@ __global__ void __launch_bounds__(128) k_mlp_cool(int64_t n, const double* __res
         un = u;
       } else {
         bool ok = inside;
-        double ff = 1.0 / (1.0 + exp(-(double)f));  // the network predicts logit f
+        // the network predicts the logit f; its sigmoid in float (1e-7 of u, far inside the
+        // acceptance test below, which judges the u it implies)
+        double ff = (double)(1.0f / (1.0f + __expf(-f)));
         double um = u - ff * (u - bp.u_floor);
         if (ok) {
           // a-posteriori acceptance: the cooling rate r(u) grows with T, so the exact step du_e
@@ -440,10 +443,9 @@ __global__ void __launch_bounds__(128) k_mlp_cool(int64_t n, const double* __res
           if (judge > 0 && stats && (me % judge) == 0) {
             double ue = brems_cool_one(u, r, d, bp);
             double e = fabs(um - ue) / u;
-            atomicAdd(&stats[1], e * e);
-            atomicAdd(&stats[2], 1.0);
-            unsigned long long* mx = (unsigned long long*)&stats[0];
-            atomicMax(mx, (unsigned long long)__double_as_longlong(e));
+            j_e2 += e * e;
+            j_n += 1.0;
+            j_max = fmax(j_max, e);
           }
         } else {
           un = brems_cool_one(u, r, d, bp);
@@ -455,9 +457,26 @@ __global__ void __launch_bounds__(128) k_mlp_cool(int64_t n, const double* __res
       if (mode_out) mode_out[me] = (int8_t)mode;
     }
   }
-  if (counts) {
-    atomicAdd(&counts[0], n_mlp);
-    atomicAdd(&counts[1], n_fb);
+  // one atomic per warp for the counts and the judged statistics
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    n_mlp += __shfl_xor_sync(0xffffffffu, n_mlp, o);
+    n_fb += __shfl_xor_sync(0xffffffffu, n_fb, o);
+    j_e2 += __shfl_xor_sync(0xffffffffu, j_e2, o);
+    j_n += __shfl_xor_sync(0xffffffffu, j_n, o);
+    j_max = fmax(j_max, __shfl_xor_sync(0xffffffffu, j_max, o));
+  }
+  if (lane == 0) {
+    if (counts) {
+      atomicAdd(&counts[0], n_mlp);
+      atomicAdd(&counts[1], n_fb);
+    }
+    if (stats && j_n > 0.0) {
+      atomicAdd(&stats[1], j_e2);
+      atomicAdd(&stats[2], j_n);
+      // non-negative doubles order like their bits
+      atomicMax((unsigned long long*)&stats[0], (unsigned long long)__double_as_longlong(j_max));
+    }
   }
 }
 

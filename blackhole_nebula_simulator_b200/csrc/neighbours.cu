@@ -19,13 +19,9 @@
 namespace nbk {
 
 static constexpr int LEAF = 32;
-static constexpr int SUB = 8;  // sub-leaf: the unit each lane tests its own sphere against
+static constexpr int SUB = 8;  // sub-leaf: the unit of the candidate queue (4 per staged batch)
 static constexpr int FAN = 8;
 static constexpr int STACK = 96;
-static constexpr int QCAP = 24;  // sub-leaves a lane queues before the warp flushes
-// entries of the fixed-width row scratch of the one-pass build (int32, 24 GiB); larger builds
-// count first and fill second
-static constexpr double ELL_MAX_ENTRIES = 6.0 * 1024 * 1024 * 1024;
 
 // ---------------------------------------------------------------- bounding box
 __global__ void k_bbox_partial(int64_t n, const double* __restrict__ pos, double* __restrict__ part) {
@@ -232,208 +228,416 @@ __device__ __forceinline__ double point_gap2(double x, double y, double z, doubl
   return gx * gx + gy * gy + gz * gz;
 }
 
-// The rows of one query leaf of LEAF consecutive sorted particles, one lane per particle.  The
-// warp walks the tree of boxes with an explicit stack in shared memory (entries (level << 40) |
-// index; children pushed highest first, so candidate leaves are reached in ascending order).  At
-// each candidate leaf every lane tests its own search sphere against the leaf's sub-leaves and
-// queues the ones it reaches (shared memory, per lane, in ascending order); the warp flushes the
-// queues in lockstep, each lane walking its own sub-leaves' particles, so every row comes out
-// sorted.
-// PASS 0 counts each row's entries; PASS 1 writes them at off[k]; PASS 2 writes them into a
-// fixed-width slot of row_cap entries at k * row_cap and counts them.  Returns the row length.
-template <int PASS>
-__device__ __forceinline__ int64_t leaf_rows(int64_t leaf, int64_t n, const TreeView& tv,
-                                             const double4* __restrict__ slo,
-                                             const double4* __restrict__ shi,
-                                             const double4* __restrict__ spos,
-                                             int64_t* __restrict__ counts,
-                                             const int64_t* __restrict__ off,
-                                             int32_t* __restrict__ idx, int64_t row_cap,
-                                             int64_t* stack, int32_t (*queue)[32], int lane,
-                                             int* err) {
-  int64_t k = leaf * LEAF + lane;
-  bool valid = k < n;
-  double4 me = valid ? spos[k] : make_double4(0, 0, 0, 0);
-  double ri = 2.0 * me.w;
-  double r2i = __dmul_rn(ri, ri);
-  const double4 qlo = tv.lo[leaf], qhi = tv.hi[leaf];
-  const double qh = qlo.w;
-  int64_t m = 0, base = 0, cap = 0;
-  if (PASS == 1 && valid) {
-    base = off[k];
-    cap = off[k + 1] - base;
-  }
-  if (PASS == 2) {
-    base = k * row_cap;
-    cap = row_cap;
-  }
-  int qn = 0;  // this lane's queued sub-leaves
-  auto flush = [&]() {
-    int qmax = qn;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) qmax = max(qmax, __shfl_xor_sync(0xffffffffu, qmax, o));
-    for (int t = 0; t < qmax; ++t) {
-      if (t < qn) {
-        int64_t sb = (int64_t)queue[t][lane] * SUB;
-        int64_t se = min(sb + SUB, n);
-        for (int64_t j = sb; j < se; ++j) {
-          double4 c = spos[j];
-          double d2 = d2_exact(c.x - me.x, c.y - me.y, c.z - me.z);
-          double rj = 2.0 * c.w;
-          if (d2 < r2i || d2 < __dmul_rn(rj, rj)) {
-            if (PASS == 1) {
-              if (m < cap)
-                idx[base + m] = (int32_t)j;
-              else
-                set_error(err, ERR_LIST_OVERFLOW);
-            } else if (PASS == 2) {
-              if (m < cap) idx[base + m] = (int32_t)j;  // longer rows are redone in CSR
-            }
-            m += 1;
-          }
-        }
-      }
-    }
-    __syncwarp();
-    qn = 0;
-  };
+// The rows of one query leaf of LEAF consecutive sorted particles, one lane per particle, tested
+// tile by tile.  The warp walks the tree of boxes with an explicit stack in shared memory (entries
+// (level << 40) | index; children pushed highest first, so candidate leaves are reached in
+// ascending order) and takes, in ascending order, the sub-leaves whose boxes lie within reach of
+// the query leaf's box.  Every 4 of them (32 candidates) are staged in shared memory, one
+// candidate per lane with coalesced loads, as float offsets from the query leaf's centre, and
+// every lane tests its own particle against all 32: the whole warp stays busy on the same
+// candidates, with no per-lane queues.
+//
+// The test is the reference's FP64 r^2 < (2 h_i)^2 or r^2 < (2 h_j)^2 decided in FP32 with a
+// rigorous band.  With D the largest offset component of the query lanes and the staged batch
+// and u = 2^-24, the offsets round with error <= u D, their differences with error <= 4 u D,
+// and the float r^2 of a pair (three rounded squares and sums of terms <= 12 D^2) differs from
+// the exact one by at most 84 u D^2; the float thresholds and their subtractions add at most
+// 36 u D^2 for every threshold that can matter (r^2 <= 12 D^2).  Pairs whose float r^2 lies
+// within B = 192 u D^2 of the threshold are decided by the exact FP64 test (no fused
+// multiply-add) from the double positions; the others are certain.  So the lists are the
+// reference's bit for bit.
+//
+// Three passes share the traversal: k_lists_cand counts each query leaf's candidate sub-leaves
+// (so every leaf gets its own slice of the candidate and mask buffers), k_lists_test runs the
+// tests once, storing each lane's 32-bit hit mask per batch and its row's entry count, and
+// k_lists_expand turns the masks into the CSR entries at the rows' offsets, each row ascending
+// (batches come in ascending candidate order, a mask's bits from the lowest slot up).
+
+constexpr float BAND_U = 192.0f / 16777216.0f;  // 192 u, u = 2^-24
+
+// The query leaf's box, centre and largest search radius.
+struct QueryLeaf {
+  double4 lo, hi;
+  double cx, cy, cz;
+};
+
+__device__ __forceinline__ QueryLeaf query_leaf(const TreeView& tv, int64_t leaf) {
+  QueryLeaf q;
+  q.lo = tv.lo[leaf];
+  q.hi = tv.hi[leaf];
+  q.cx = 0.5 * (q.lo.x + q.hi.x);
+  q.cy = 0.5 * (q.lo.y + q.hi.y);
+  q.cz = 0.5 * (q.lo.z + q.hi.z);
+  return q;
+}
+
+// Walk the tree for one query leaf; on_subs(s0, mask) is called warp-uniformly for every
+// candidate leaf with its first sub-leaf s0 and the ballot of its sub-leaves within reach of the
+// query leaf's box (bit c: sub-leaf s0 + c), in ascending order.  Returns false if the stack
+// overflowed.
+template <typename F>
+__device__ __forceinline__ bool walk_candidates(int64_t n, const TreeView& tv, const QueryLeaf& q,
+                                                const double4* __restrict__ slo,
+                                                const double4* __restrict__ shi,
+                                                int64_t* stack, int lane, F&& on_subs) {
+  const unsigned FULL = 0xffffffffu;
+  const int64_t nsub = (n + SUB - 1) / SUB;
+  const double qh = q.lo.w;
   int sp = 0;
   __syncwarp();
   if (lane == 0) stack[0] = ((int64_t)(tv.nlevels - 1) << 40);
   sp = 1;
   __syncwarp();
   while (sp > 0) {
-    int64_t e = stack[sp - 1];
+    const int64_t e = stack[sp - 1];
     __syncwarp();
     sp -= 1;
-    int lvl = (int)(e >> 40);
-    int64_t node = e & ((1ll << 40) - 1);
+    const int lvl = (int)(e >> 40);
+    const int64_t node = e & ((1ll << 40) - 1);
     if (lvl == 0) {
-      // candidate leaf: queue the sub-leaves this lane's sphere reaches
-      int64_t s0 = node * (LEAF / SUB);
-      int64_t s1 = min(s0 + LEAF / SUB, (n + SUB - 1) / SUB);
-      bool near = valid;
-      if (near) {
-        // the leaf's own box first: a lane whose sphere misses it skips the sub-leaf tests
-        const double4 llo = tv.lo[node], lhi = tv.hi[node];
-        const double lreach = 2.0 * fmax(me.w, llo.w);
-        near = point_gap2(me.x, me.y, me.z, llo, lhi) < lreach * lreach * (1.0 + 1e-12);
+      const int64_t s0 = node * (LEAF / SUB);
+      const int64_t s1 = min(s0 + LEAF / SUB, nsub);
+      bool near = false;
+      if (lane < s1 - s0) {
+        const double4 blo = slo[s0 + lane], bhi = shi[s0 + lane];
+        const double reach = 2.0 * fmax(qh, blo.w);
+        near = box_gap2(q.lo, q.hi, blo, bhi) < reach * reach * (1.0 + 1e-12);
       }
-      if (near) {
-        for (int64_t sidx = s0; sidx < s1; ++sidx) {
-          double4 blo = slo[sidx], bhi = shi[sidx];
-          double reach = 2.0 * fmax(me.w, blo.w);
-          if (point_gap2(me.x, me.y, me.z, blo, bhi) < reach * reach * (1.0 + 1e-12))
-            queue[qn++][lane] = (int32_t)sidx;
-        }
-      }
-      if (__any_sync(0xffffffffu, qn > QCAP - LEAF / SUB)) flush();
+      const unsigned mk = __ballot_sync(FULL, near);
+      if (mk) on_subs(s0, mk);
       continue;
     }
-    int64_t c0 = node * FAN;
-    int64_t csize = tv.level_size[lvl - 1];
-    int64_t child = c0 + lane;
+    const int64_t c0 = node * FAN;
+    const int64_t csize = tv.level_size[lvl - 1];
+    const int64_t child = c0 + lane;
     bool hit = false;
     if (lane < FAN && child < csize) {
-      int64_t g = tv.level_off[lvl - 1] + child;
-      double4 blo = tv.lo[g], bhi = tv.hi[g];
-      double reach = 2.0 * fmax(qh, blo.w);
-      hit = box_gap2(qlo, qhi, blo, bhi) < reach * reach * (1.0 + 1e-12);
+      const int64_t g = tv.level_off[lvl - 1] + child;
+      const double4 blo = tv.lo[g], bhi = tv.hi[g];
+      const double reach = 2.0 * fmax(qh, blo.w);
+      hit = box_gap2(q.lo, q.hi, blo, bhi) < reach * reach * (1.0 + 1e-12);
     }
-    unsigned mask = __ballot_sync(0xffffffffu, hit);
-    int nh = __popc(mask);
-    if (sp + nh > STACK) {
-      set_error(err, ERR_TRAVERSAL_STACK);
-      break;
-    }
+    const unsigned mask = __ballot_sync(FULL, hit);
+    const int nh = __popc(mask);
+    if (sp + nh > STACK) return false;
     if (hit) {
-      int above = __popc(mask & ~((2u << lane) - 1u));
+      const int above = __popc(mask & ~((2u << lane) - 1u));
       stack[sp + above] = ((int64_t)(lvl - 1) << 40) | child;
     }
     __syncwarp();
     sp += nh;
   }
-  flush();
-  if (PASS != 1 && valid) counts[k] = m;
-  return valid ? m : 0;
+  return true;
 }
 
-// Persistent list kernel: each warp takes the next query leaf from `order` (heaviest first) until
-// none is left, so a few slow leaves (sparse regions whose 32 curve-consecutive particles spread
-// far) overlap with the rest instead of holding whole blocks.  PASS 2 also records the longest
-// row in *rowmax.
-template <int PASS>
-__global__ void __launch_bounds__(NB_THREADS) k_lists_sub(int64_t n, int64_t nwork,
-                                                          const int32_t* __restrict__ order,
-                                                          unsigned long long* __restrict__ next,
-                                                          TreeView tv,
-                                                          const double4* __restrict__ slo,
-                                                          const double4* __restrict__ shi,
-                                                          const double4* __restrict__ spos,
-                                                          int64_t* __restrict__ counts,
-                                                          const int64_t* __restrict__ off,
-                                                          int32_t* __restrict__ idx,
-                                                          int64_t row_cap,
-                                                          unsigned long long* __restrict__ rowmax,
-                                                          int* err) {
-  __shared__ int64_t stack_s[NB_THREADS / 32][STACK];
-  __shared__ int32_t queue_s[NB_THREADS / 32][QCAP][32];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  int64_t* stack = stack_s[wib];
-  int32_t(*queue)[32] = queue_s[wib];
+// Pass 1: the candidate sub-leaves of each query leaf, in ascending order, into its own slice of
+// the candidate buffer.  The walk goes level by level: the nodes within reach of the query box at
+// one level (a frontier in shared memory, ascending) give the next level's nodes to test, 32 at
+// a time, one per lane; the leaves within reach give the sub-leaves to test the same way, and the
+// sub-leaves within reach are the leaf's candidate list (ascending, since every frontier is).  A
+// frontier larger than its buffer sends the leaf to the depth-first walk instead, which counts
+// first and writes in a second walk.  The leaf takes its slices of the candidate and mask
+// buffers with two atomic adds (cand_at / batch_at, so slices of different leaves lie in any
+// order).  A slice that would pass the buffers' capacity is not written; the host then grows the
+// buffers from the cursors' final values and runs the pass again.
+constexpr int CAND_WARPS = 4;
+constexpr int CAND_SMEM = 1024;  // entries of a frontier buffer
+
+__global__ void __launch_bounds__(CAND_WARPS * 32) k_lists_cand(int64_t n, int64_t nwork,
+                                                           const uint64_t* __restrict__ order,
+                                                           unsigned long long* __restrict__ next,
+                                                           TreeView tv,
+                                                           const double4* __restrict__ slo,
+                                                           const double4* __restrict__ shi,
+                                                           unsigned long long* __restrict__ cand_at,
+                                                           unsigned long long* __restrict__ batch_at,
+                                                           int64_t cap_cands, int64_t cap_batches,
+                                                           int32_t* __restrict__ cands,
+                                                           int64_t* __restrict__ leaf_cbase,
+                                                           int64_t* __restrict__ leaf_bbase,
+                                                           int32_t* __restrict__ leaf_ncand,
+                                                           int* err) {
+  __shared__ int64_t stacks[CAND_WARPS][STACK];
+  __shared__ int32_t fronts[CAND_WARPS][2][CAND_SMEM];
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  int64_t* stack = stacks[threadIdx.x >> 5];
+  int32_t(*front)[CAND_SMEM] = fronts[threadIdx.x >> 5];
+  const int64_t nsub = (n + SUB - 1) / SUB;
+  while (true) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(next, 1ull);
+    t = __shfl_sync(FULL, t, 0);
+    if (t >= (unsigned long long)nwork) break;  // warp-uniform
+    const int64_t leaf = (int64_t)(order[t] & 0xffffffffull);
+    const QueryLeaf q = query_leaf(tv, leaf);
+    const double qh = q.lo.w;
+    // level by level from the root; `cur` holds the frontier (ascending node indices)
+    int cur = 0, fn = 1;
+    bool over = false;
+    __syncwarp();
+    if (lane == 0) front[0][0] = 0;
+    __syncwarp();
+    for (int lvl = tv.nlevels - 1; lvl >= 0 && !over; --lvl) {
+      // children of the frontier: nodes of level lvl - 1, or at the leaves their sub-leaves
+      const int fan = lvl > 0 ? FAN : LEAF / SUB;
+      const int64_t csize = lvl > 0 ? tv.level_size[lvl - 1] : nsub;
+      const int64_t coff = lvl > 0 ? tv.level_off[lvl - 1] : 0;
+      const double4* clo = lvl > 0 ? tv.lo : slo;
+      const double4* chi = lvl > 0 ? tv.hi : shi;
+      const int total = fn * fan;
+      int nn = 0;
+      for (int c0 = 0; c0 < total; c0 += 32) {
+        const int c = c0 + lane;
+        bool hit = false;
+        int32_t child = 0;
+        if (c < total) {
+          child = front[cur][c / fan] * fan + c % fan;
+          if (child < csize) {
+            const double4 blo = clo[coff + child], bhi = chi[coff + child];
+            const double reach = 2.0 * fmax(qh, blo.w);
+            hit = box_gap2(q.lo, q.hi, blo, bhi) < reach * reach * (1.0 + 1e-12);
+          }
+        }
+        const unsigned mk = __ballot_sync(FULL, hit);
+        if (nn + __popc(mk) > CAND_SMEM) {
+          over = true;
+          break;
+        }
+        if (hit) front[cur ^ 1][nn + __popc(mk & below)] = child;
+        nn += __popc(mk);
+      }
+      __syncwarp();
+      cur ^= 1;
+      fn = nn;
+    }
+    int64_t count = fn;
+    if (over) {
+      // a frontier outgrew its buffer: the depth-first walk counts instead
+      count = 0;
+      if (!walk_candidates(n, tv, q, slo, shi, stack, lane,
+                           [&](int64_t, unsigned mk) { count += __popc(mk); }))
+        set_error(err, ERR_TRAVERSAL_STACK);
+    }
+    const int64_t nbat = (count + 3) / 4;
+    unsigned long long cb = 0, bb = 0;
+    if (lane == 0) {
+      cb = atomicAdd(cand_at, (unsigned long long)count);
+      bb = atomicAdd(batch_at, (unsigned long long)nbat);
+    }
+    cb = __shfl_sync(FULL, cb, 0);
+    bb = __shfl_sync(FULL, bb, 0);
+    const bool fits = (int64_t)cb + count <= cap_cands && (int64_t)bb + nbat <= cap_batches;
+    if (fits) {
+      if (!over) {
+        for (int64_t c = lane; c < count; c += 32) cands[cb + c] = front[cur][c];
+      } else {
+        int64_t c2 = 0;
+        walk_candidates(n, tv, q, slo, shi, stack, lane, [&](int64_t s0, unsigned mk) {
+          const int pos = __popc(mk & below);
+          if (((mk >> lane) & 1u) && c2 + pos < count) cands[cb + c2 + pos] = (int32_t)(s0 + lane);
+          c2 += __popc(mk);
+        });
+      }
+    }
+    if (lane == 0) {
+      leaf_cbase[leaf] = (int64_t)cb;
+      leaf_bbase[leaf] = (int64_t)bb;
+      leaf_ncand[leaf] = (int32_t)count;
+    }
+    __syncwarp();
+  }
+}
+
+// Pass 2: the tests, on each leaf's candidate list.  Each batch's final hit masks go to
+// masks[(batch base + b) * 32 + lane], the rows' entry counts to counts.
+__global__ void __launch_bounds__(NB_THREADS) k_lists_test(int64_t n, int64_t nwork,
+                                                           const uint64_t* __restrict__ order,
+                                                           unsigned long long* __restrict__ next,
+                                                           TreeView tv,
+                                                           const double4* __restrict__ spos,
+                                                           const int32_t* __restrict__ cands,
+                                                           const int64_t* __restrict__ leaf_cbase,
+                                                           const int64_t* __restrict__ leaf_bbase,
+                                                           const int32_t* __restrict__ leaf_ncand,
+                                                           uint32_t* __restrict__ masks,
+                                                           int64_t* __restrict__ counts,
+                                                           unsigned long long* __restrict__ rowmax,
+                                                           int* err) {
+  __shared__ float4 cand_s[NB_THREADS / 32][32];
+  __shared__ int32_t cidx_s[NB_THREADS / 32][32];
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  float4* cand = cand_s[threadIdx.x >> 5];
+  int32_t* cidx = cidx_s[threadIdx.x >> 5];
   unsigned longest = 0;
   while (true) {
-    unsigned long long w = 0;
-    if (lane == 0) w = atomicAdd(next, 1ull);
-    w = __shfl_sync(0xffffffffu, w, 0);
-    if (w >= (unsigned long long)nwork) break;  // warp-uniform
-    int64_t leaf = order[w];
-    int64_t m = leaf_rows<PASS>(leaf, n, tv, slo, shi, spos, counts, off, idx, row_cap, stack,
-                                queue, lane, err);
-    longest = max(longest, (unsigned)m);
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(next, 1ull);
+    t = __shfl_sync(FULL, t, 0);
+    if (t >= (unsigned long long)nwork) break;  // warp-uniform
+    const int64_t leaf = (int64_t)(order[t] & 0xffffffffull);
+    const QueryLeaf q = query_leaf(tv, leaf);
+    const int64_t cbase = leaf_cbase[leaf], bbase = leaf_bbase[leaf];
+    const int64_t ncand = leaf_ncand[leaf];
+    const int64_t k = leaf * LEAF + lane;
+    const bool valid = k < n;
+    const double4 me = valid ? spos[k] : make_double4(0, 0, 0, 0);
+    float mx = 1e30f, my = 1e30f, mz = 1e30f, Dl = 0.0f, r2i_f = -1.0f;
+    const double ri = 2.0 * me.w;
+    const double r2i = __dmul_rn(ri, ri);
+    if (valid) {
+      mx = (float)(me.x - q.cx);
+      my = (float)(me.y - q.cy);
+      mz = (float)(me.z - q.cz);
+      Dl = fmaxf(fmaxf(fabsf(mx), fabsf(my)), fabsf(mz));
+      r2i_f = (float)r2i;
+    }
+    // non-negative floats order like their bits
+    const float Dq = __uint_as_float(__reduce_max_sync(FULL, __float_as_uint(Dl)));
+    int64_t m = 0;
+    for (int64_t b = 0; 4 * b < ncand; ++b) {
+      // stage: slot = lane, candidate sub-leaf 4 b + lane / 8, particle lane % 8 of it
+      const int64_t c = 4 * b + (lane >> 3);
+      const int32_t sb = c < ncand ? cands[cbase + c] : -1;
+      const int64_t j = (int64_t)sb * SUB + (lane & 7);
+      float4 cc = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+      float Dj = 0.0f;
+      int32_t jj = -1;
+      if (sb >= 0 && j < n) {
+        const double4 p = spos[j];
+        cc.x = (float)(p.x - q.cx);
+        cc.y = (float)(p.y - q.cy);
+        cc.z = (float)(p.z - q.cz);
+        const double rj = 2.0 * p.w;
+        cc.w = (float)(rj * rj);
+        Dj = fmaxf(fmaxf(fabsf(cc.x), fabsf(cc.y)), fabsf(cc.z));
+        jj = (int32_t)j;
+      }
+      const float D = fmaxf(Dq, __uint_as_float(__reduce_max_sync(FULL, __float_as_uint(Dj))));
+      // offsets beyond float's comfortable range (never in code units): every pair exactly
+      const bool wide = !(D < 1e15f);
+      const float B = wide ? 0.0f : BAND_U * D * D;
+      cc.w -= B;
+      cand[lane] = cc;
+      cidx[lane] = jj;
+      __syncwarp();
+      const float ri_lo = r2i_f - B, twoB = 2.0f * B;
+      unsigned hit = 0u, amb = 0u;
+#pragma unroll
+      for (int tt = 0; tt < 32; ++tt) {
+        const float4 e = cand[tt];
+        const float dx = e.x - mx, dy = e.y - my, dz = e.z - mz;
+        const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        const float tl = fmaxf(e.w, ri_lo);
+        hit |= d2 < tl ? 1u << tt : 0u;
+        amb |= d2 - twoB < tl ? 1u << tt : 0u;
+      }
+      if (wide) {
+        hit = 0u;
+        amb = __ballot_sync(FULL, jj >= 0);
+      }
+      if (!valid) hit = amb = 0u;
+      amb &= ~hit;
+      if (__any_sync(FULL, amb != 0u)) {
+        // the band: the reference's exact FP64 test from the double positions
+        while (amb) {
+          const int tt = __ffs(amb) - 1;
+          amb &= amb - 1u;
+          const double4 pj = spos[cidx[tt]];
+          const double d2 = d2_exact(pj.x - me.x, pj.y - me.y, pj.z - me.z);
+          const double rj = 2.0 * pj.w;
+          if (d2 < r2i || d2 < __dmul_rn(rj, rj)) hit |= 1u << tt;
+        }
+      }
+      masks[(bbase + b) * 32 + lane] = hit;
+      m += __popc(hit);
+      __syncwarp();  // the next batch overwrites the staged candidates
+    }
+    if (valid) counts[k] = m;
+    longest = max(longest, valid ? (unsigned)m : 0u);
   }
-  if (PASS == 2) {
-    unsigned mx = __reduce_max_sync(0xffffffffu, longest);
-    if (lane == 0) atomicMax(rowmax, (unsigned long long)mx);
-  }
+  const unsigned mx = __reduce_max_sync(FULL, longest);
+  if (lane == 0) atomicMax(rowmax, (unsigned long long)mx);
 }
 
-// Cost key of each query leaf for the heaviest-first order: the linear size of the region its
-// traversal covers (box extent plus twice the largest search diameter), as descending-order bits.
+// Pass 3: masks -> CSR entries.  One warp per query leaf.  The leaf's masks and candidate
+// sub-leaves are staged in shared memory a chunk of batches at a time; then row by row and batch
+// by batch, lane t takes candidate slot t of the batch: a set bit's entry goes to the row's
+// running position plus the number of set bits below it, so one coalesced store writes all of
+// a batch's entries of the row.  Each row's entries come out in ascending order (batches
+// ascending, a mask's bits from the lowest slot up), contiguous from the row's offset.
+constexpr int EXPAND_WARPS = 4;
+constexpr int EXPAND_CHUNK = 64;  // batches staged at a time
+
+__global__ void __launch_bounds__(EXPAND_WARPS * 32) k_lists_expand(int64_t n, int64_t nleaf,
+                                                             const int32_t* __restrict__ cands,
+                                                             const int64_t* __restrict__ leaf_cbase,
+                                                             const int64_t* __restrict__ leaf_bbase,
+                                                             const int32_t* __restrict__ leaf_ncand,
+                                                             const uint32_t* __restrict__ masks,
+                                                             const int64_t* __restrict__ off,
+                                                             int32_t* __restrict__ idx, int* err) {
+  // per warp: a chunk's masks (one row per batch, 32 lanes' masks) and its candidate sub-leaves
+  __shared__ uint32_t mask_s[EXPAND_WARPS][EXPAND_CHUNK][32];
+  __shared__ int32_t sub_s[EXPAND_WARPS][EXPAND_CHUNK * 4];
+  const unsigned FULL = 0xffffffffu;
+  const int64_t leaf = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (leaf >= nleaf) return;  // warp-uniform
+  uint32_t(*msk)[32] = mask_s[threadIdx.x >> 5];
+  int32_t* sub = sub_s[threadIdx.x >> 5];
+  const int64_t cbase = leaf_cbase[leaf], bbase = leaf_bbase[leaf];
+  const int64_t ncand = leaf_ncand[leaf], nbat = (ncand + 3) / 4;
+  const int64_t k0 = leaf * LEAF;
+  const int rows = (int)(n - k0 < LEAF ? n - k0 : LEAF);
+  const unsigned below = (1u << lane) - 1u;
+  // lane r keeps row r's running output position and its end
+  int64_t pos = lane < rows ? off[k0 + lane] : 0;
+  const int64_t stop = lane < rows ? off[k0 + lane + 1] : 0;
+  for (int64_t c0 = 0; c0 < nbat; c0 += EXPAND_CHUNK) {
+    const int nb = (int)(nbat - c0 < EXPAND_CHUNK ? nbat - c0 : EXPAND_CHUNK);
+    __syncwarp();
+    for (int e = lane; e < nb * 32; e += 32) msk[e >> 5][e & 31] = masks[(bbase + c0) * 32 + e];
+    for (int e = lane; e < nb * 4; e += 32) {
+      const int64_t c = 4 * c0 + e;
+      sub[e] = c < ncand ? cands[cbase + c] : 0;
+    }
+    __syncwarp();
+    for (int r = 0; r < rows; ++r) {
+      int64_t at = __shfl_sync(FULL, pos, r);  // warp-uniform from here on
+      const int64_t end = __shfl_sync(FULL, stop, r);
+      for (int b = 0; b < nb; ++b) {
+        const uint32_t m = msk[b][r];
+        if (m == 0u) continue;  // warp-uniform
+        if ((m >> lane) & 1u) {
+          const int64_t w = at + __popc(m & below);
+          if (w < end)
+            idx[w] = sub[4 * b + (lane >> 3)] * SUB + (lane & 7);
+          else
+            set_error(err, ERR_LIST_OVERFLOW);
+        }
+        at += __popc(m);
+      }
+      if (lane == r) pos = at;
+    }
+  }
+  if (lane < rows && pos != stop) set_error(err, ERR_LIST_OVERFLOW);
+}
+
+// Order key of each query leaf: its cost class (the binary exponent of the linear size of the
+// region its traversal covers, box extent plus twice the largest search diameter), heaviest
+// first, then the leaf's curve position.
 __global__ void k_leaf_cost(int64_t nleaf, const double4* __restrict__ lo,
-                            const double4* __restrict__ hi, uint32_t* __restrict__ key,
-                            int32_t* __restrict__ id) {
+                            const double4* __restrict__ hi, uint64_t* __restrict__ key) {
   int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (l >= nleaf) return;
   double4 a = lo[l], b = hi[l];
   double ext = fmax(fmax(b.x - a.x, b.y - a.y), b.z - a.z);
   float c = (float)(ext + 4.0 * a.w);
-  key[l] = ~__float_as_uint(c);  // non-negative floats order like their bits
-  id[l] = (int32_t)l;
-}
-
-// Pack the fixed-width rows into CSR: warp per row, coalesced on both sides.  Rows longer than
-// the width are left to the CSR pass over their leaves.
-__global__ void k_pack_rows(int64_t n, int64_t row_cap, const int32_t* __restrict__ ell,
-                            const int64_t* __restrict__ off, int32_t* __restrict__ idx) {
-  int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (k >= n) return;
-  int64_t b = off[k], cnt = off[k + 1] - b;
-  if (cnt > row_cap) return;
-  const int32_t* src = ell + k * row_cap;
-  for (int64_t t = lane; t < cnt; t += 32) idx[b + t] = src[t];
-}
-
-// Leaves holding a row longer than the width (unordered list; each is redone on its own).
-__global__ void k_long_leaves(int64_t n, int64_t nleaf, const int64_t* __restrict__ counts,
-                              int64_t row_cap, int32_t* __restrict__ out,
-                              unsigned long long* __restrict__ nout) {
-  int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (l >= nleaf) return;
-  bool longer = false;
-  for (int64_t k = l * LEAF; k < min((l + 1) * LEAF, n); ++k) longer |= counts[k] > row_cap;
-  if (longer) out[atomicAdd(nout, 1ull)] = (int32_t)l;
+  const uint64_t cls = 255u - ((__float_as_uint(c) >> 23) & 255u);
+  key[l] = (cls << 32) | (uint64_t)l;
 }
 
 // ---------------------------------------------------------------- export to original order
@@ -456,15 +660,25 @@ __global__ void k_export_fill(int64_t n, const int32_t* __restrict__ perm,
 }
 
 // ---------------------------------------------------------------- host orchestration
-// Resident blocks of the persistent list kernel over the whole device (fewest of its variants).
+// Synchronise the stream after a pass whose size the host needs next, and stop on a device
+// error the pass raised (so no buffer is sized from a failed pass).
+static int pending_check(Engine& E, cudaStream_t st) {
+  NB_CUDA(cudaMemcpyAsync(E.h_err, E.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  if (E.h_err[0] != 0) return check_device_error(E, st);
+  return 0;
+}
+
+// Resident blocks of the persistent list kernels over the whole device (fewest of the two).
 static int list_kernel_slots(Engine& E) {
   if (E.list_slots > 0) return 0;
-  int sms = 0, b0 = 0, b1 = 0, b2 = 0;
+  int sms = 0, b0 = 0, b1 = 0;
   NB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E.device));
-  NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_lists_sub<0>, NB_THREADS, 0));
-  NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_lists_sub<1>, NB_THREADS, 0));
-  NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_lists_sub<2>, NB_THREADS, 0));
-  E.list_slots = (int64_t)sms * std::max(1, std::min(b0, std::min(b1, b2)));
+  NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_lists_cand, CAND_WARPS * 32, 0));
+  NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_lists_test, NB_THREADS, 0));
+  // resident warps of each pass over the whole device
+  E.list_slots = (int64_t)sms * std::max(1, b1) * (NB_THREADS / 32);
+  E.cand_slots = (int64_t)sms * std::max(1, b0) * CAND_WARPS;
   return 0;
 }
 int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaStream_t st) {
@@ -516,62 +730,53 @@ int build_lists(Engine& E, int64_t n, const double* pos, const double* hs, cudaS
   int64_t nsub = (n + SUB - 1) / SUB;
   NB_TRY(E.ensure_sub(nsub));
   count_launch(), k_sub_boxes<<<grid_for(nsub), NB_THREADS, 0, st>>>(n, nsub, L.spos, E.sub_lo, E.sub_hi);
-  // query leaves heaviest first, for the persistent list kernel
-  uint32_t* cost = reinterpret_cast<uint32_t*>(E.keys_a);
-  uint32_t* cost_sorted = reinterpret_cast<uint32_t*>(E.keys_b);
-  int32_t* order = reinterpret_cast<int32_t*>(E.keys_b) + E.cap_n;  // second half of keys_b
-  count_launch(), k_leaf_cost<<<grid_for(nleaf), NB_THREADS, 0, st>>>(nleaf, E.node_lo, E.node_hi, cost, E.vals_a);
+  // query leaves by cost class, heaviest first, each class in curve order
+  uint64_t* cost = E.keys_a;
+  uint64_t* order = E.keys_b;
+  count_launch(), k_leaf_cost<<<grid_for(nleaf), NB_THREADS, 0, st>>>(nleaf, E.node_lo, E.node_hi, cost);
   tmp = 0;
-  NB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, cost, cost_sorted, E.vals_a, order, (int)nleaf, 0, 32, st));
+  NB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, cost, order, (int)nleaf, 0, 40, st));
   NB_TRY(E.ensure_cub(tmp));
   tmp = E.cub_bytes;
-  NB_CUDA(cub::DeviceRadixSort::SortPairs(E.cub_tmp, tmp, cost, cost_sorted, E.vals_a, order, (int)nleaf, 0, 32, st));
-  NB_CUDA(cudaMemsetAsync(E.d_rowmax, 0, 4 * sizeof(unsigned long long), st));
+  NB_CUDA(cub::DeviceRadixSort::SortKeys(E.cub_tmp, tmp, cost, order, (int)nleaf, 0, 40, st));
   NB_TRY(list_kernel_slots(E));
-  auto grid = [&](int64_t nwork) {
-    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((nwork * 32 + NB_THREADS - 1) / NB_THREADS, E.list_slots));
-  };
-  int64_t total = 0;
-  if ((double)n * (double)E.row_cap <= ELL_MAX_ENTRIES) {
-    // one traversal into fixed-width rows, scan, pack; the few rows longer than the width are
-    // written straight into CSR by a second traversal over their leaves only
-    NB_TRY(E.ensure_ell(n * E.row_cap));
-    count_launch(), k_lists_sub<2><<<grid(nleaf), NB_THREADS, 0, st>>>(n, nleaf, order, E.d_rowmax + 2, tv, E.sub_lo, E.sub_hi, L.spos, E.counts, nullptr, E.ell, E.row_cap, E.d_rowmax, E.d_err);
-    NB_CUDA(cudaMemsetAsync(L.off, 0, sizeof(int64_t), st));
-    tmp = E.cub_bytes;
-    NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, E.counts, L.off + 1, (int)n, st));
-    NB_CUDA(cudaMemcpyAsync(E.h_build, L.off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    NB_CUDA(cudaMemcpyAsync(E.h_build + 1, E.d_rowmax, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    NB_CUDA(cudaStreamSynchronize(st));
-    total = E.h_build[0];
-    int64_t longest = E.h_build[1];
-    NB_TRY(E.ensure_list_capacity(total));
-    count_launch(), k_pack_rows<<<grid_for(n * 32), NB_THREADS, 0, st>>>(n, E.row_cap, E.ell, L.off, L.idx);
-    if (longest > E.row_cap) {
-      int32_t* leaves = reinterpret_cast<int32_t*>(E.keys_a);  // free after the order sort
-      count_launch(), k_long_leaves<<<grid_for(nleaf), NB_THREADS, 0, st>>>(n, nleaf, E.counts, E.row_cap, leaves, E.d_rowmax + 1);
-      NB_CUDA(cudaMemcpyAsync(E.h_build + 1, E.d_rowmax + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-      NB_CUDA(cudaStreamSynchronize(st));
-      int64_t nlong = E.h_build[1];
-      count_launch(), k_lists_sub<1><<<grid(nlong), NB_THREADS, 0, st>>>(n, nlong, leaves, E.d_rowmax + 3, tv, E.sub_lo, E.sub_hi, L.spos, nullptr, L.off, L.idx, 0, nullptr, E.d_err);
-    }
-    // width for the next build: half as much again as this build's longest row (a redo of the
-    // longest leaves costs far more than idle slots, which are never read), within the scratch
-    // bound (rows beyond it take the CSR redo above)
-    int64_t widest = std::min<int64_t>(1024, (int64_t)(ELL_MAX_ENTRIES / (double)n) / 32 * 32);
-    E.row_cap = std::min<int64_t>(std::max<int64_t>((longest + longest / 2 + 31) / 32 * 32, 256), std::max<int64_t>(widest, 64));
-  } else {
-    // count, scan, fill
-    count_launch(), k_lists_sub<0><<<grid(nleaf), NB_THREADS, 0, st>>>(n, nleaf, order, E.d_rowmax + 2, tv, E.sub_lo, E.sub_hi, L.spos, E.counts, nullptr, nullptr, 0, nullptr, E.d_err);
-    NB_CUDA(cudaMemsetAsync(L.off, 0, sizeof(int64_t), st));
-    tmp = E.cub_bytes;
-    NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, E.counts, L.off + 1, (int)n, st));
-    NB_CUDA(cudaMemcpyAsync(E.h_build, L.off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    NB_CUDA(cudaStreamSynchronize(st));
-    total = E.h_build[0];
-    NB_TRY(E.ensure_list_capacity(total));
-    count_launch(), k_lists_sub<1><<<grid(nleaf), NB_THREADS, 0, st>>>(n, nleaf, order, E.d_rowmax + 3, tv, E.sub_lo, E.sub_hi, L.spos, nullptr, L.off, L.idx, 0, nullptr, E.d_err);
+  // persistent passes: at most one warp per query leaf, at most the resident warps
+  const unsigned grid = (unsigned)std::max<int64_t>(
+      1, std::min<int64_t>(nleaf, E.list_slots) / (NB_THREADS / 32));
+  const unsigned cand_grid = (unsigned)std::max<int64_t>(
+      1, std::min<int64_t>(nleaf, E.cand_slots) / CAND_WARPS);
+  // candidate lists of the query leaves, each in its own slice of the buffers (sized from the
+  // last build's totals; a pass that outgrows them is run again with buffers of its size)
+  NB_TRY(E.ensure_leaves(nleaf));
+  NB_TRY(E.ensure_tiles(E.last_cands > 0 ? E.last_cands + E.last_cands / 4 : nleaf * 512,
+                        E.last_batches > 0 ? E.last_batches + E.last_batches / 4 : nleaf * 128));
+  for (int attempt = 0;; ++attempt) {
+    NB_CUDA(cudaMemsetAsync(E.d_rowmax, 0, 8 * sizeof(unsigned long long), st));
+    count_launch(), k_lists_cand<<<cand_grid, CAND_WARPS * 32, 0, st>>>(
+        n, nleaf, order, E.d_rowmax + 2, tv, E.sub_lo, E.sub_hi, E.d_rowmax + 4, E.d_rowmax + 5,
+        E.cap_cands, E.cap_masks / 32, E.cands, E.leaf_cbase, E.leaf_bbase, E.leaf_ncand, E.d_err);
+    NB_CUDA(cudaMemcpyAsync(E.h_build, E.d_rowmax + 4, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    NB_TRY(pending_check(E, st));
+    const int64_t ncand = E.h_build[0], nbatch = E.h_build[1];
+    E.last_cands = ncand;
+    E.last_batches = nbatch;
+    if (ncand <= E.cap_cands && nbatch <= E.cap_masks / 32) break;
+    if (attempt > 0) return set_host_error(E, "list build: candidate buffers outgrown twice");
+    NB_TRY(E.ensure_tiles(ncand + ncand / 4, nbatch + nbatch / 4));
   }
+  // the tests, once: hit masks per batch and lane, entries per row
+  count_launch(), k_lists_test<<<grid, NB_THREADS, 0, st>>>(n, nleaf, order, E.d_rowmax + 3, tv, L.spos, E.cands, E.leaf_cbase, E.leaf_bbase, E.leaf_ncand, E.masks, E.counts, E.d_rowmax, E.d_err);
+  NB_CUDA(cudaMemsetAsync(L.off, 0, sizeof(int64_t), st));
+  tmp = E.cub_bytes;
+  NB_CUDA(cub::DeviceScan::InclusiveSum(E.cub_tmp, tmp, E.counts, L.off + 1, (int)n, st));
+  NB_CUDA(cudaMemcpyAsync(E.h_build, L.off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaMemcpyAsync(E.h_build + 1, E.d_rowmax, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  NB_TRY(pending_check(E, st));
+  const int64_t total = E.h_build[0];
+  NB_TRY(E.ensure_list_capacity(total));
+  // masks -> entries at the rows' offsets
+  count_launch(), k_lists_expand<<<grid_for(nleaf * 32, EXPAND_WARPS * 32), EXPAND_WARPS * 32, 0, st>>>(
+      n, nleaf, E.cands, E.leaf_cbase, E.leaf_bbase, E.leaf_ncand, E.masks, L.off, L.idx, E.d_err);
   E.prof.end(PROF_LISTS, st, (double)n, (double)total);
   L.n = n;
   L.total = total;

@@ -24,12 +24,19 @@ void launch_forces32(int64_t nrows, const int64_t* rows, const float4* pos, cons
                      ForceOut out, cudaStream_t st) {
   if (nrows <= 0) return;
   Pos32 geo{pos, 0.f, box6};
-  if (prm.use_recon && prm.use_visc)
+  if (prm.use_recon && prm.use_visc) {
     count_launch(), k_forces_g<float, Pos32, I, float4, true><<<grid_for(nrows * 8), NB_THREADS, 0, st>>>(
         nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
-  else
+  } else if (prm.tidx && prm.tcnt) {
+    // the walk, then the pairs from its entries
+    count_launch(), k_forces_g<float, Pos32, I, float4, false, 1><<<grid_for(nrows * 8), NB_THREADS, 0, st>>>(
+        nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
+    count_launch(), k_forces_g<float, Pos32, I, float4, false, 2><<<grid_for(nrows * 8), NB_THREADS, 0, st>>>(
+        nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
+  } else {
     count_launch(), k_forces_g<float, Pos32, I, float4, false><<<grid_for(nrows * 8), NB_THREADS, 0, st>>>(
         nrows, rows, geo, vm, hydro, aux, off, idx, prm, out_map, out);
+  }
 }
 
 

@@ -18,23 +18,45 @@ namespace nbk {
 // FP64: packed (x, y, z, w) doubles.  dx = x_j - x_i as the reference forms it.
 struct Pos64 {
   const double4* p;
+  static constexpr bool has_mass = false;
+  struct Own {
+    double4 a;
+  };
   __device__ __forceinline__ void ready() {}
+  __device__ __forceinline__ Own own(int64_t i) const { return Own{p[i]}; }
+  __device__ __forceinline__ void diff(const Own& o, int64_t j, double& dx, double& dy,
+                                       double& dz) const {
+    const double4 b = p[j];
+    dx = b.x - o.a.x;
+    dy = b.y - o.a.y;
+    dz = b.z - o.a.z;
+  }
   __device__ __forceinline__ void diff(int64_t i, int64_t j, double& dx, double& dy,
                                        double& dz) const {
-    double4 a = p[i], b = p[j];
-    dx = b.x - a.x;
-    dy = b.y - a.y;
-    dz = b.z - a.z;
+    diff(own(i), j, dx, dy, dz);
+  }
+  // the difference and particle j's smoothing length (from the hydro record)
+  template <typename V4>
+  __device__ __forceinline__ void diff_h(int64_t i, int64_t j, const V4* __restrict__ hydro,
+                                         double& dx, double& dy, double& dz, double& hj) const {
+    diff(own(i), j, dx, dy, dz);
+    hj = (double)hydro[j].x;
   }
 };
 
-// FP32: per particle the integer cell of a uniform grid of edge `cell` and the float offset from
-// that cell's centre; dx = (c_j - c_i) cell + (o_j - o_i) keeps full float precision at any
-// distance from the origin.
+// FP32: per particle the cell of a uniform grid of edge `cell` (at most 1024 per axis) and the
+// float offset from that cell's centre, packed as two float4: (offset x, y, z, mass) and (cell
+// x, y, z as exact small floats, h: the smoothing length where the force pass needs it).  dx = (c_j - c_i) cell + (o_j - o_i): the cell difference
+// is an exact float, and one fused multiply-add rounds the sum once, so the difference keeps full
+// float precision at any distance from the origin.
 struct Pos32 {
-  const float4* p;  // (ox, oy, oz, packed cell: 10 bits per axis)
+  const float4* p;
   float cell;
   const double* box6 = nullptr;  // grid corner and far corner; the edge is derived on the device
+  static constexpr bool has_mass = true;
+  struct Own {
+    float4 a, c;
+  };
   // edge of the grid cells: the largest side of the box over 1000, as the packing kernel uses
   __device__ __forceinline__ void ready() {
     if (box6) {
@@ -42,16 +64,28 @@ struct Pos32 {
       cell = (float)fmax(span / 1000.0, 1e-30);
     }
   }
+  __device__ __forceinline__ Own own(int64_t i) const { return Own{p[2 * i], p[2 * i + 1]}; }
+  __device__ __forceinline__ float mass(int64_t j) const { return p[2 * j].w; }
+  __device__ __forceinline__ void diff(const Own& o, int64_t j, float& dx, float& dy,
+                                       float& dz) const {
+    const float4 b = p[2 * j], cb = p[2 * j + 1];
+    dx = fmaf(cb.x - o.c.x, cell, b.x - o.a.x);
+    dy = fmaf(cb.y - o.c.y, cell, b.y - o.a.y);
+    dz = fmaf(cb.z - o.c.z, cell, b.z - o.a.z);
+  }
   __device__ __forceinline__ void diff(int64_t i, int64_t j, float& dx, float& dy,
                                        float& dz) const {
-    float4 a = p[i], b = p[j];
-    int ca = __float_as_int(a.w), cb = __float_as_int(b.w);
-    float ex = (float)(((cb >> 20) & 1023) - ((ca >> 20) & 1023));
-    float ey = (float)(((cb >> 10) & 1023) - ((ca >> 10) & 1023));
-    float ez = (float)((cb & 1023) - (ca & 1023));
-    dx = fmaf(ex, cell, b.x - a.x);
-    dy = fmaf(ey, cell, b.y - a.y);
-    dz = fmaf(ez, cell, b.z - a.z);
+    diff(own(i), j, dx, dy, dz);
+  }
+  // the difference and particle j's smoothing length, from the same record
+  template <typename V4>
+  __device__ __forceinline__ void diff_h(int64_t i, int64_t j, const V4* __restrict__,
+                                         float& dx, float& dy, float& dz, float& hj) const {
+    const float4 a = p[2 * i], ca = p[2 * i + 1], b = p[2 * j], cb = p[2 * j + 1];
+    dx = fmaf(cb.x - ca.x, cell, b.x - a.x);
+    dy = fmaf(cb.y - ca.y, cell, b.y - a.y);
+    dz = fmaf(cb.z - ca.z, cell, b.z - a.z);
+    hj = cb.w;
   }
 };
 
@@ -259,11 +293,16 @@ __device__ __forceinline__ double group_total(const Acc<float>& a) {
 
 template <typename R>
 struct DensityEntry;
+#ifndef DENSITY_CAP
+#define DENSITY_CAP 112
+#endif
 template <>
 struct DensityEntry<float> {
   using T = float2;
-  static constexpr int CAP = 240;     // in-range entries a row keeps in shared memory
-  static constexpr int BLOCKS = 7;    // resident blocks per SM: 7 x (30 KiB + 1 KiB) of shared
+  // entries inside r_in a row keeps in shared memory: 16 rows x 112 x 8 B = 14 KiB per block, so
+  // 8 resident blocks (the register limit) leave most of the SM's L1 to the gathered records
+  static constexpr int CAP = DENSITY_CAP;
+  static constexpr int BLOCKS = 8;
 };
 template <>
 struct DensityEntry<double> {
@@ -277,10 +316,12 @@ constexpr int DENSITY_THREADS = 128;  // 16 rows per block
 #endif
 
 // Eight lanes per row, four rows per warp.  The lanes of a row split its list (entry e to lane
-// e mod 8, coalesced index loads) and store the distance and mass of every entry inside the search
-// radius in shared memory, in list order; each Newton iteration then sums the kernel terms over
-// that cache and reduces across the eight lanes, so the lanes of a row take the same Newton steps.
-// Rows with more in-range entries than the cache holds re-walk their list in every sum.
+// e mod 8, coalesced index loads) and store the distance and mass of every entry inside r_in =
+// 2.1 h_start (the Newton iterates stay near the start h) in shared memory, in list order; each
+// Newton iteration then sums the kernel terms over that cache and reduces across the eight lanes,
+// so the lanes of a row take the same Newton steps.  A sum at an h whose support reaches past
+// r_in adds the entries beyond it from the list (the same distances, recomputed); rows with more
+// entries inside r_in than the cache holds re-walk their list in every sum.
 template <typename R, typename PosT, typename I>
 __global__ void __launch_bounds__(DENSITY_THREADS, DensityEntry<R>::BLOCKS)
     k_density(int64_t nrows, const int64_t* __restrict__ rows, PosT geo_in,
@@ -310,10 +351,22 @@ __global__ void __launch_bounds__(DENSITY_THREADS, DensityEntry<R>::BLOCKS)
     e0 = off[i];
     e1 = off[i + 1];
   }
+  const typename PosT::Own me_rec = geo.own(i);  // the row's own record, loaded once
+  auto mass_of = [&](int64_t j) -> R {
+    if constexpr (PosT::has_mass)
+      return (R)geo.mass(j);
+    else
+      return prm.massf ? (R)prm.massf[j] : (R)mass[j];
+  };
   const double r_max = 2.0 * hs;
   const R r2max = (R)(r_max * r_max);
   const int kid = prm.kid;
   const R cn = (R)prm.cnorm;
+  // the Newton iterates stay near the start h0 (the previous step's h): entries inside
+  // r_in = 2.1 h0 are cached, and a sum at h adds the others only when r_in / h < 2 (else every
+  // one of them has q >= 2, a zero term)
+  const double h_first = live ? fmin(h_start[i], hs) : 1.0;
+  const R r_in = (R)(2.1 * h_first);
   // distances and masses of the entries inside r_max (sim/sph.py:231-248), in list order
   const unsigned len = (unsigned)(e1 - e0);
   const unsigned maxlen = __reduce_max_sync(FULL, len);
@@ -338,7 +391,7 @@ __global__ void __launch_bounds__(DENSITY_THREADS, DensityEntry<R>::BLOCKS)
       mm[u] = R(0);
       if (jj[u] >= 0) {
         R dx, dy, dz;
-        geo.diff(i, jj[u], dx, dy, dz);
+        geo.diff(me_rec, jj[u], dx, dy, dz);
         R d2 = sqdist(dx, dy, dz);
         if (d2 < r2max) {
           inr[u] = true;
@@ -348,12 +401,13 @@ __global__ void __launch_bounds__(DENSITY_THREADS, DensityEntry<R>::BLOCKS)
     }
 #pragma unroll
     for (int u = 0; u < U; ++u)
-      if (inr[u]) mm[u] = prm.massf ? (R)prm.massf[jj[u]] : (R)mass[jj[u]];
+      if (inr[u]) mm[u] = mass_of(jj[u]);
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      unsigned seg = (__ballot_sync(FULL, inr[u]) >> (8 * g)) & 0xffu;
-      int pos = cnt + __popc(seg & ((1u << gl) - 1u));
-      if (inr[u] && pos < CAP) {
+      const bool inner = inr[u] && rr[u] < r_in;
+      const unsigned seg = (__ballot_sync(FULL, inner) >> (8 * g)) & 0xffu;
+      const int pos = cnt + __popc(seg & ((1u << gl) - 1u));
+      if (inner && pos < CAP) {  // overflow: the walk below instead
         E2 v;
         v.x = rr[u];
         v.y = mm[u];
@@ -387,14 +441,25 @@ __global__ void __launch_bounds__(DENSITY_THREADS, DensityEntry<R>::BLOCKS)
           E2 v = cache[t];
           term(v.x, v.y);
         }
+        if (!(r_in * inv_h >= R(2)))
+          for (int64_t e = e0 + gl; e < e1; e += 8) {  // the entries beyond r_in
+            int64_t j = (int64_t)idx[e];
+            R dx, dy, dz;
+            geo.diff(me_rec, j, dx, dy, dz);
+            R d2 = sqdist(dx, dy, dz);
+            if (!(d2 < r2max)) continue;
+            const R rj = sqrt(d2);
+            if (rj < r_in) continue;
+            term(rj, mass_of(j));
+          }
       } else {
         for (int64_t e = e0 + gl; e < e1; e += 8) {
           int64_t j = (int64_t)idx[e];
           R dx, dy, dz;
-          geo.diff(i, j, dx, dy, dz);
+          geo.diff(me_rec, j, dx, dy, dz);
           R d2 = sqdist(dx, dy, dz);
           if (!(d2 < r2max)) continue;
-          term(sqrt(d2), prm.massf ? (R)prm.massf[j] : (R)mass[j]);
+          term(sqrt(d2), mass_of(j));
         }
       }
     }
@@ -478,9 +543,20 @@ constexpr int FORCE_QUEUE = 64;  // interacting entries a row queues before its 
 // Fused pressure + artificial viscosity (+ conductivity) + P dV (+ disc viscosity) pass.  Eight
 // lanes per row (lanes 8g .. 8g+7 of a warp), each taking every eighth list entry; the pair terms
 // are summed per lane and then over the row's lanes.
-template <typename R, typename PosT, typename I, typename V4, bool RECON>
-__global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? (RECON ? 2 : FORCE_BLOCKS_PER_SM_FP32)
-                                                             : (RECON ? 1 : 2))
+// MODE 0: the walk queues the interacting entries and drains them into the pair terms as it
+// goes.  The same pass can run as two launches: MODE 1 only walks, writing every row's
+// interacting entries (self included, list order) to prm.tidx / prm.tcnt, with few registers
+// and so many resident warps to hide the walk's dependent loads; MODE 2 then reads those
+// entries, every lane busy on pair terms, with no walk state alive beside the accumulators.
+template <int MODE, typename R, bool RECON>
+struct ForceBlocks {
+  static constexpr int value = MODE == 1 ? 6
+                               : sizeof(R) == 4 ? (RECON ? 2 : FORCE_BLOCKS_PER_SM_FP32)
+                                                : (RECON ? 1 : 2);
+};
+
+template <typename R, typename PosT, typename I, typename V4, bool RECON, int MODE = 0>
+__global__ void __launch_bounds__(NB_THREADS, (ForceBlocks<MODE, R, RECON>::value))
     k_forces_g(int64_t nrows, const int64_t* __restrict__ rows, PosT geo_in,
              const V4* __restrict__ vm,    // (vx, vy, vz, mass)
              const V4* __restrict__ hydro, // (h, rho, omega, P)
@@ -750,10 +826,22 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? (RECON ? 2 : FORC
   // written out for the level limiter: exactly the reference's FP64 test, which the FP32 form
   // takes from prm.pos64 where its float test falls within 1e-5 of the boundary
   int m_tot = 0;
+  if constexpr (MODE == 2) {
+    // the interacting entries the walk launch wrote (self included: skipped here)
+    const int cnt = live ? prm.tcnt[q] : 0;
+    for (int k2 = gl; k2 < cnt; k2 += 8) {
+      const int64_t b = (int64_t)ld_stream(prm.tidx + e_beg + k2);
+      if (b == a) continue;
+      if constexpr (sizeof(R) == 4)
+        pair_fast(b);
+      else
+        pair(b);
+    }
+  }
   // FORCE_UNROLL rounds of eight entries at a time: their index and position loads are issued
   // together, then the rounds are queued one after the other in list order
   constexpr int FU = FORCE_UNROLL;
-  for (unsigned base = 0; base < maxlen; base += 8 * FU) {
+  for (unsigned base = 0; MODE != 2 && base < maxlen; base += 8 * FU) {
     int64_t bb[FU];
     bool take[FU], tight[FU];
 #pragma unroll
@@ -770,9 +858,8 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? (RECON ? 2 : FORC
         if (b != a) {
           bool tk = true;
           if (prm.tighten) {
-            R ddx, ddy, ddz;
-            geo.diff(a, b, ddx, ddy, ddz);
-            const R h_b = (R)hydro[b].x;
+            R ddx, ddy, ddz, h_b;
+            geo.diff_h(a, b, hydro, ddx, ddy, ddz, h_b);
             R rr = R(2) * (h_a > h_b ? h_a : h_b);
             const R d2 = sqdist(ddx, ddy, ddz), r2 = rr * rr;
             tk = d2 < r2;
@@ -794,9 +881,11 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? (RECON ? 2 : FORC
     }
 #pragma unroll
     for (int u = 0; u < FU; ++u) {
-      unsigned seg = (__ballot_sync(FULL, take[u]) >> (8 * g)) & 0xffu;
-      if (take[u]) pq[pc + __popc(seg & ((1u << gl) - 1u))] = (int32_t)bb[u];
-      pc += __popc(seg);
+      if constexpr (MODE == 0) {
+        unsigned seg = (__ballot_sync(FULL, take[u]) >> (8 * g)) & 0xffu;
+        if (take[u]) pq[pc + __popc(seg & ((1u << gl) - 1u))] = (int32_t)bb[u];
+        pc += __popc(seg);
+      }
       if (prm.tidx) {
         const unsigned tseg = (__ballot_sync(FULL, tight[u]) >> (8 * g)) & 0xffu;
         if (tight[u])
@@ -804,10 +893,11 @@ __global__ void __launch_bounds__(NB_THREADS, sizeof(R) == 4 ? (RECON ? 2 : FORC
         m_tot += __popc(tseg);
       }
     }
-    if (__any_sync(FULL, pc > FORCE_QUEUE - 8)) drain();
+    if (MODE == 0 && __any_sync(FULL, pc > FORCE_QUEUE - 8)) drain();
   }
-  drain();
-  if (prm.tcnt && live && gl == 0) prm.tcnt[q] = m_tot;
+  if constexpr (MODE == 0) drain();
+  if (MODE != 2 && prm.tcnt && live && gl == 0) prm.tcnt[q] = m_tot;
+  if constexpr (MODE == 1) return;  // the walk launch writes only the entries and counts
   // sums over the row's eight lanes (uniform flags: every lane takes part in every reduction)
   double s_ax = 0, s_ay = 0, s_az = 0, s_work = 0, s_heat = 0, s_vheat = 0, s_cheat = 0;
   double s_dax = 0, s_day = 0, s_daz = 0, s_dheat = 0;
