@@ -621,7 +621,12 @@ def measure(args, name, rank, world, steps=None):
         "cooling": ("network (BF16 tensor cores, exact fallback; bremsstrahlung law of this "
                     "library, parity with the reference unpinned: it has no such law)"
                     if mlp is not None else "exact integrator"),
-        "cooling_network": mlp,
+        "cooling_network": (dict(mlp, gain=(
+            "net cost: the exact integrator of this library's bremsstrahlung law is a closed "
+            "form; cooling category ms per step with the network "
+            f"{prof['cooling']['ms'] / a.steps:.3f} vs {plain['kernel_ms']['cooling'] / a.steps:.3f} "
+            "with the exact integrator (FP64 plain)" if plain else "net cost (closed-form law)"))
+                            if mlp is not None else None),
         "energy_rel_drift": led["drift_synced"],
         "energy_drift_over_time": led["t_synced"],
         "energy_drift_sync_steps": led["sync_steps"],

@@ -1001,6 +1001,10 @@ int mark_rows(Engine& E, int64_t nrows, const int64_t* rows, int tight, const do
   return 0;
 }
 
+int sorted_rows(Engine& E, int64_t nrows, const int64_t* rows, int64_t* ns, cudaStream_t st) {
+  return rows_sorted(E, E.lists.n, nrows, rows, ns, st);
+}
+
 int sorted_rows_and_pack(Engine& E, int64_t nrows, const int64_t* rows, const double* x,
                          const double* h, int64_t* ns, cudaStream_t st) {
   Lists& L = E.lists;

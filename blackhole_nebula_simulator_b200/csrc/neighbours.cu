@@ -570,6 +570,9 @@ __global__ void __launch_bounds__(NB_THREADS) k_lists_test(int64_t n, int64_t nw
 // ascending, a mask's bits from the lowest slot up), contiguous from the row's offset.
 constexpr int EXPAND_WARPS = 4;
 constexpr int EXPAND_CHUNK = 64;  // batches staged at a time
+#ifndef EXPAND_UNROLL
+#define EXPAND_UNROLL 4
+#endif
 
 __global__ void __launch_bounds__(EXPAND_WARPS * 32) k_lists_expand(int64_t n, int64_t nleaf,
                                                              const int32_t* __restrict__ cands,
@@ -608,17 +611,24 @@ __global__ void __launch_bounds__(EXPAND_WARPS * 32) k_lists_expand(int64_t n, i
     for (int r = 0; r < rows; ++r) {
       int64_t at = __shfl_sync(FULL, pos, r);  // warp-uniform from here on
       const int64_t end = __shfl_sync(FULL, stop, r);
-      for (int b = 0; b < nb; ++b) {
-        const uint32_t m = msk[b][r];
-        if (m == 0u) continue;  // warp-uniform
-        if ((m >> lane) & 1u) {
-          const int64_t w = at + __popc(m & below);
-          if (w < end)
-            idx[w] = sub[4 * b + (lane >> 3)] * SUB + (lane & 7);
-          else
-            set_error(err, ERR_LIST_OVERFLOW);
+      // EXPAND_UNROLL batches' masks are read together, then written one after the other
+      for (int b0 = 0; b0 < nb; b0 += EXPAND_UNROLL) {
+        uint32_t mm[EXPAND_UNROLL];
+#pragma unroll
+        for (int u = 0; u < EXPAND_UNROLL; ++u) mm[u] = b0 + u < nb ? msk[b0 + u][r] : 0u;
+#pragma unroll
+        for (int u = 0; u < EXPAND_UNROLL; ++u) {
+          const uint32_t m = mm[u];
+          if (m == 0u) continue;  // warp-uniform
+          if ((m >> lane) & 1u) {
+            const int64_t w = at + __popc(m & below);
+            if (w < end)
+              idx[w] = sub[4 * (b0 + u) + (lane >> 3)] * SUB + (lane & 7);
+            else
+              set_error(err, ERR_LIST_OVERFLOW);
+          }
+          at += __popc(m);
         }
-        at += __popc(m);
       }
       if (lane == r) pos = at;
     }

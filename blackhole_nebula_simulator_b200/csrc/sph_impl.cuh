@@ -37,10 +37,15 @@ struct Pos64 {
   }
   // the difference and particle j's smoothing length (from the hydro record)
   template <typename V4>
+  __device__ __forceinline__ void diff_h(const Own& o, int64_t j, const V4* __restrict__ hydro,
+                                         double& dx, double& dy, double& dz, double& hj) const {
+    diff(o, j, dx, dy, dz);
+    hj = (double)hydro[j].x;
+  }
+  template <typename V4>
   __device__ __forceinline__ void diff_h(int64_t i, int64_t j, const V4* __restrict__ hydro,
                                          double& dx, double& dy, double& dz, double& hj) const {
-    diff(own(i), j, dx, dy, dz);
-    hj = (double)hydro[j].x;
+    diff_h(own(i), j, hydro, dx, dy, dz, hj);
   }
 };
 
@@ -79,13 +84,18 @@ struct Pos32 {
   }
   // the difference and particle j's smoothing length, from the same record
   template <typename V4>
-  __device__ __forceinline__ void diff_h(int64_t i, int64_t j, const V4* __restrict__,
+  __device__ __forceinline__ void diff_h(const Own& o, int64_t j, const V4* __restrict__,
                                          float& dx, float& dy, float& dz, float& hj) const {
-    const float4 a = p[2 * i], ca = p[2 * i + 1], b = p[2 * j], cb = p[2 * j + 1];
-    dx = fmaf(cb.x - ca.x, cell, b.x - a.x);
-    dy = fmaf(cb.y - ca.y, cell, b.y - a.y);
-    dz = fmaf(cb.z - ca.z, cell, b.z - a.z);
+    const float4 b = p[2 * j], cb = p[2 * j + 1];
+    dx = fmaf(cb.x - o.c.x, cell, b.x - o.a.x);
+    dy = fmaf(cb.y - o.c.y, cell, b.y - o.a.y);
+    dz = fmaf(cb.z - o.c.z, cell, b.z - o.a.z);
     hj = cb.w;
+  }
+  template <typename V4>
+  __device__ __forceinline__ void diff_h(int64_t i, int64_t j, const V4* __restrict__ hydro,
+                                         float& dx, float& dy, float& dz, float& hj) const {
+    diff_h(own(i), j, hydro, dx, dy, dz, hj);
   }
 };
 
@@ -294,12 +304,12 @@ __device__ __forceinline__ double group_total(const Acc<float>& a) {
 template <typename R>
 struct DensityEntry;
 #ifndef DENSITY_CAP
-#define DENSITY_CAP 112
+#define DENSITY_CAP 128
 #endif
 template <>
 struct DensityEntry<float> {
   using T = float2;
-  // entries inside r_in a row keeps in shared memory: 16 rows x 112 x 8 B = 14 KiB per block, so
+  // entries inside r_in a row keeps in shared memory: 16 rows x 128 x 8 B = 16 KiB per block, so
   // 8 resident blocks (the register limit) leave most of the SM's L1 to the gathered records
   static constexpr int CAP = DENSITY_CAP;
   static constexpr int BLOCKS = 8;
@@ -533,11 +543,22 @@ constexpr int FORCE_QUEUE = 64;  // interacting entries a row queues before its 
 #ifndef FORCE_UNROLL
 #define FORCE_UNROLL 4
 #endif
-// resident blocks per SM the FP32 force pass is compiled for (registers: 65536 / (256 * 3) = 85;
-// the FP64 form keeps 2, its doubles would spill; the reconstruction forms, with two 3x3
-// gradients per pair, 2 and 1)
+// rounds of eight entries the walk launch (MODE 1) issues at once, and its resident blocks
+#ifndef WALK_UNROLL
+#define WALK_UNROLL 4
+#endif
+#ifndef WALK_BLOCKS
+#define WALK_BLOCKS 6
+#endif
+#ifndef WALK_OWN
+#define WALK_OWN 0  // 1: the walk launch keeps the row's own record in registers
+#endif
+// resident blocks per SM of the FP32 force pass (registers: 65536 / (256 * 4) = 64, a few spilled;
+// measured on the 4M torus 4.26 ms per launch against 4.59 with 3 blocks and 80 registers and
+// 5.63 with 2); the FP64 form keeps 2, its doubles would spill; the reconstruction forms, with
+// two 3x3 gradients per pair, 2 and 1
 #ifndef FORCE_BLOCKS_PER_SM_FP32
-#define FORCE_BLOCKS_PER_SM_FP32 3
+#define FORCE_BLOCKS_PER_SM_FP32 4
 #endif
 
 // Fused pressure + artificial viscosity (+ conductivity) + P dV (+ disc viscosity) pass.  Eight
@@ -550,7 +571,7 @@ constexpr int FORCE_QUEUE = 64;  // interacting entries a row queues before its 
 // entries, every lane busy on pair terms, with no walk state alive beside the accumulators.
 template <int MODE, typename R, bool RECON>
 struct ForceBlocks {
-  static constexpr int value = MODE == 1 ? 6
+  static constexpr int value = MODE == 1 ? WALK_BLOCKS
                                : sizeof(R) == 4 ? (RECON ? 2 : FORCE_BLOCKS_PER_SM_FP32)
                                                 : (RECON ? 1 : 2);
 };
@@ -840,7 +861,8 @@ __global__ void __launch_bounds__(NB_THREADS, (ForceBlocks<MODE, R, RECON>::valu
   }
   // FORCE_UNROLL rounds of eight entries at a time: their index and position loads are issued
   // together, then the rounds are queued one after the other in list order
-  constexpr int FU = FORCE_UNROLL;
+  constexpr int FU = MODE == 1 ? WALK_UNROLL : FORCE_UNROLL;
+  const typename PosT::Own me_walk = geo.own(a);
   for (unsigned base = 0; MODE != 2 && base < maxlen; base += 8 * FU) {
     int64_t bb[FU];
     bool take[FU], tight[FU];
@@ -859,7 +881,10 @@ __global__ void __launch_bounds__(NB_THREADS, (ForceBlocks<MODE, R, RECON>::valu
           bool tk = true;
           if (prm.tighten) {
             R ddx, ddy, ddz, h_b;
-            geo.diff_h(a, b, hydro, ddx, ddy, ddz, h_b);
+            if constexpr (MODE == 1 && WALK_OWN)
+              geo.diff_h(me_walk, b, hydro, ddx, ddy, ddz, h_b);
+            else
+              geo.diff_h(a, b, hydro, ddx, ddy, ddz, h_b);
             R rr = R(2) * (h_a > h_b ? h_a : h_b);
             const R d2 = sqdist(ddx, ddy, ddz), r2 = rr * rr;
             tk = d2 < r2;

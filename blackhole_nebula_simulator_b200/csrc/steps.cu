@@ -545,7 +545,10 @@ __global__ void k_limit_sweep_t(int64_t nrows, const int64_t* __restrict__ rows_
 }
 
 // _wake_targets (sim/blocks.py:356-364): need[j] = max over active i of level_i - max_gap, over
-// the rows' interacting entries into a sorted need array (eight lanes per row)
+// the rows' interacting entries into a sorted need array (eight lanes per row).  k_cut_steps acts
+// on j only where need[j] > level[j], so a contribution that is not above j's own level cannot
+// change what it does and is skipped (a load instead of an atomic): need[j] stays below or at
+// level[j] exactly where it did, and keeps its maximum where it is above.
 __global__ void k_wake_need_t(int64_t nrows, const int64_t* __restrict__ rows_s,
                               const int64_t* __restrict__ off, const int32_t* __restrict__ tidx,
                               const int32_t* __restrict__ tcnt, const int64_t* __restrict__ level_s,
@@ -557,7 +560,10 @@ __global__ void k_wake_need_t(int64_t nrows, const int64_t* __restrict__ rows_s,
   int64_t k = rows_s[q];
   long long v = (long long)(level_s[k] - max_gap);
   const int32_t* tl = tidx + off[k];
-  for (int c = gl; c < tcnt[q]; c += 8) atomicMax((long long*)&need_s[tl[c]], v);
+  for (int c = gl; c < tcnt[q]; c += 8) {
+    const int32_t j = tl[c];
+    if (v > (long long)level_s[j]) atomicMax((long long*)&need_s[j], v);
+  }
 }
 
 __global__ void k_gather_i64(int64_t n, const int32_t* __restrict__ perm, const int64_t* __restrict__ a,
@@ -665,13 +671,17 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
   W.pend_err = true;  // read with the first limiter sweep's flag (or by the landing check)
   int64_t ns = 0;
   if (prm->limiter) {
-    // curve-ordered rows, sorted (x, h) and a sorted copy of the levels
-    NB_TRY(sorted_rows_and_pack(E, nrows, rows, s->x, s->h, &ns, st));
-    count_launch(), k_gather_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, W.i_lvl);
     // the rows' interacting entries, once for every sweep and the wake-up walk (already written
-    // by the force pass of these rows on these lists, when it ran just before)
+    // by the force pass of these rows on these lists, when it ran just before); the sorted
+    // (x, h) are needed only to find them here
     const bool have_tight = rows == W.rows && W.tight_ver == W.rows_ver &&
                             W.tight_gen == L.gen && W.tight_n == nrows;
+    // curve-ordered rows, and a sorted copy of the levels
+    if (have_tight)
+      NB_TRY(sorted_rows(E, nrows, rows, &ns, st));
+    else
+      NB_TRY(sorted_rows_and_pack(E, nrows, rows, s->x, s->h, &ns, st));
+    count_launch(), k_gather_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, W.i_lvl);
     if (!have_tight) {
       NB_TRY(E.ensure_tight(L.total));
       count_launch(), k_tight_rows<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,

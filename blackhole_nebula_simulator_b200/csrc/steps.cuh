@@ -54,6 +54,7 @@ int block_land(Engine& E, nb_state* s, const nb_params* prm, cudaStream_t st);
 int mark_rows(Engine& E, int64_t nrows, const int64_t* rows, int tight, const double* x,
               const double* h, uint8_t* mark, cudaStream_t st);
 // rows as ascending sorted positions in E.ws.rows_s (count ns) and E.ws.pk0 = sorted (x, h)
+int sorted_rows(Engine& E, int64_t nrows, const int64_t* rows, int64_t* ns, cudaStream_t st);
 int sorted_rows_and_pack(Engine& E, int64_t nrows, const int64_t* rows, const double* x,
                          const double* h, int64_t* ns, cudaStream_t st);
 // checks read at the next host synchronisation (see Workspace::pend_*)

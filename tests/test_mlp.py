@@ -90,7 +90,7 @@ def test_gradients_match_oracle(gpu):
 def test_training_inference_checks_and_gain(gpu):
     """Train on 4M samples, then: accepted network results within 1e-3 u of the exact integrator,
     inputs outside the hull and failed checks fall back to it, and the time of the network step
-    beside the exact step on the same 4M particles (what the network gains, or costs)."""
+    beside the exact step on the same 4M particles: the network is the slower (a net cost)."""
     import torch
 
     _lib, cooling, ctx, ptr, stream = gpu
@@ -134,3 +134,9 @@ def test_training_inference_checks_and_gain(gpu):
         times[name] = (time.perf_counter() - t0) / 5
     print(f"exact {times['exact'] * 1e3:.3f} ms, network {times['network'] * 1e3:.3f} ms "
           f"per {n} particles: gain x{times['exact'] / times['network']:.2f}")
+    # What the network gains: nothing in time.  The exact integrator of this bremsstrahlung law
+    # is a closed form (an arctangent falling linearly in rho dt), so one evaluation per
+    # particle beats the network's four layers and its a-posteriori check; the bench line and
+    # the design notes state the network as a net cost, and this is the measurement behind it.
+    check("the network costs more than the closed-form exact integrator", True,
+          times["network"] > times["exact"])  # fmt: skip
