@@ -290,6 +290,7 @@ def run_gpu(args, rank, world, precision=None, use_mlp=None, e2e=True):
     _lib.check(c, _lib.lib().nb_profile(c, 1))
     steps0 = st.particle_steps
     launches0 = _lib.lib().nb_launch_count()
+    syncs0 = _lib.lib().nb_sync_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(dev.index) as clk:
         e0.record(stream)
@@ -298,8 +299,10 @@ def run_gpu(args, rank, world, precision=None, use_mlp=None, e2e=True):
         e1.record(stream)
         torch.cuda.synchronize()
     launches = _lib.lib().nb_launch_count() - launches0
+    syncs = _lib.lib().nb_sync_count() - syncs0
     prof = profile_read(c)
     prof["_launches"] = launches
+    prof["_syncs"] = syncs
     _lib.check(c, _lib.lib().nb_profile(c, 0))
     ms = e0.elapsed_time(e1)
     psteps = st.particle_steps - steps0
@@ -600,12 +603,14 @@ def measure(args, name, rank, world, steps=None):
         return None
     pk = peaks()
     launches = prof.pop("_launches")
+    syncs = prof.pop("_syncs")
     rf, dom = roofline(prof, a.precision, "torus" == name, pk)
     n_full = a.n or N_FULL[name]
     out = {
         "value": total / (ms * 1e-3), "unit": "particle-steps/s", "steps": a.steps,
         "ms_per_step": ms / a.steps, "config": workload_config(a, name, n_full, world),
         "roofline": rf, "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
+        "host_syncs_per_step": syncs / a.steps,
         "kernel_ms": {k: round(v["ms"], 3) for k, v in prof.items()},
         "kernel_table": kernel_table(prof, a.precision, "torus" == name, pk),
         "mean_active": total / a.steps / max(world, 1),

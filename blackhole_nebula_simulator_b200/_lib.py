@@ -77,6 +77,7 @@ _SIGS = {
     "nb_state_size": (_i64, []),
     "nb_params_size": (_i64, []),
     "nb_launch_count": (_i64, []),
+    "nb_sync_count": (_i64, []),
     "nb_reset_cache": (_int, [_vp]),
     "nb_profile": (_int, [_vp, _int]),
     "nb_profile_read": (_int, [_vp, _c.POINTER(_dbl)]),

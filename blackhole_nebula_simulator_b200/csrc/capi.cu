@@ -15,6 +15,7 @@
 
 namespace nbk {
 unsigned long long g_launch_count = 0;
+unsigned long long g_sync_count = 0;
 }
 
 using nbk::Engine;
@@ -123,6 +124,7 @@ int64_t nb_state_size(void) { return (int64_t)sizeof(nb_state); }
 int64_t nb_params_size(void) { return (int64_t)sizeof(nb_params); }
 
 int64_t nb_launch_count(void) { return (int64_t)__atomic_load_n(&nbk::g_launch_count, __ATOMIC_RELAXED); }
+int64_t nb_sync_count(void) { return (int64_t)__atomic_load_n(&nbk::g_sync_count, __ATOMIC_RELAXED); }
 
 nb_ctx* nb_create(int device) {
   nb_ctx* c = new (std::nothrow) nb_ctx();
@@ -397,7 +399,7 @@ int nb_glf_step_many(nb_ctx* ctx, int64_t n, const double* x, const double* p, c
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceReduce::Min(E.cub_tmp, tmp, it, E.ws.d_i64, (int)n, st));
   NB_CUDA(cudaMemcpyAsync(E.ws.h_i64, E.ws.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(nbk::host_sync(st));
   int64_t w = E.ws.h_i64[0];
   if (w >= 0) return 0;
   nbk::set_host_error(E, w == -1   ? "stage 1 (p_half) did not converge in 10 iterations: time step too large"
@@ -414,7 +416,7 @@ int nb_integrate_orbit(nb_ctx* ctx, int norb, const double* state0, double dt_ma
   nbk::launch_integrate_orbit(norb, state0, dt_max, eta, n_end, max_records, t_out, s_out, it_out,
                               nrec, S(stream));
   NB_CUDA(cudaGetLastError());
-  NB_CUDA(cudaStreamSynchronize(S(stream)));
+  NB_CUDA(nbk::host_sync(S(stream)));
   return 0;
 }
 
@@ -504,7 +506,7 @@ static int deposit_finish_host(nbk::Engine& E, double* outside, int64_t* n_trili
   NB_CUDA(cudaGetLastError());
   NB_CUDA(cudaMemcpyAsync(outside, E.ws.d_scal, sizeof(double), cudaMemcpyDeviceToHost, st));
   NB_CUDA(cudaMemcpyAsync(n_trilinear, E.ws.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(nbk::host_sync(st));
   return 0;
 }
 
@@ -591,7 +593,7 @@ int nb_ledger(nb_ctx* ctx, int64_t n, const double* x, const double* p, const do
   NB_TRY(E.ws.ensure(E, std::max<int64_t>(n, 1)));
   nbk::launch_ledger(n, x, p, u, mass, E.red, E.ws.d_tmp, st);
   NB_CUDA(cudaMemcpyAsync(E.ws.h_dbl, E.ws.d_tmp, sizeof(double) * 9, cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(nbk::host_sync(st));
   for (int t = 0; t < 9; ++t) out[t] = E.ws.h_dbl[t];
   return 0;
 }

@@ -92,6 +92,14 @@ inline int count_launch() {
   return 0;
 }
 
+// Host waits on a stream (read through nb_sync_count): each is a round trip that leaves the GPU
+// idle until the host launches again.
+extern unsigned long long g_sync_count;
+inline cudaError_t host_sync(cudaStream_t st) {
+  __atomic_add_fetch(&g_sync_count, 1ull, __ATOMIC_RELAXED);
+  return cudaStreamSynchronize(st);
+}
+
 inline unsigned grid_for(int64_t n, int threads = NB_THREADS) {
   int64_t b = (n + threads - 1) / threads;
   return (unsigned)(b > 0 ? b : 1);

@@ -190,7 +190,7 @@ void Engine::release() {
 
 int check_device_error(Engine& E, cudaStream_t st) {
   NB_CUDA(cudaMemcpyAsync(E.h_err, E.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(host_sync(st));
   E.ws.pend_err = false;  // this read covers a deferred check of the same word
   NB_CUDA(cudaGetLastError());
   int code = E.h_err[0];
@@ -822,14 +822,14 @@ int pending_flush(Engine& E, cudaStream_t st) {
   Workspace& W = E.ws;
   if (!W.pend_err && !W.pend_glf && !W.pend_erad && !W.pend_woken) return 0;
   NB_TRY(pending_enqueue(E, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(host_sync(st));
   return pending_finish(E, st);
 }
 
 static int read_int(Engine& E, int* d, int* out, cudaStream_t st) {
   NB_CUDA(cudaMemcpyAsync(E.ws.h_int, d, sizeof(int), cudaMemcpyDeviceToHost, st));
   NB_TRY(pending_enqueue(E, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(host_sync(st));
   *out = E.ws.h_int[0];
   return pending_finish(E, st);
 }
@@ -1031,7 +1031,7 @@ int select_mask(Engine& E, int64_t n, const uint8_t* mask, int64_t* out, int64_t
   NB_CUDA(cub::DeviceSelect::Flagged(E.cub_tmp, tmp, W.i_tmp, mask, out, W.d_i64, (int)n, st));
   NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   NB_TRY(pending_enqueue(E, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(host_sync(st));
   *count = W.h_i64[0];
   return pending_finish(E, st);
 }

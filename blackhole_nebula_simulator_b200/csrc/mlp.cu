@@ -232,7 +232,7 @@ static int mlp_grad(Engine& E, MlpBuffers& M, int64_t B, const float* X, const f
     count_launch(), k_sum_f<<<1, NB_THREADS, 0, st>>>(B, M.se, M.red);
     double h = 0;
     NB_CUDA(cudaMemcpyAsync(&h, M.red, sizeof(double), cudaMemcpyDeviceToHost, st));
-    NB_CUDA(cudaStreamSynchronize(st));
+    NB_CUDA(host_sync(st));
     *loss = h / (double)B;
   }
   NB_CUDA(cudaGetLastError());
@@ -565,7 +565,7 @@ int mlp_train(Engine& E, const nb_mlp_params* mp, int64_t nsamp, int64_t batch, 
     }
     if (loss_hist) loss_hist[ep] = (float)ep_loss;
   }
-  cudaStreamSynchronize(st);
+  host_sync(st);
   cudaFree(X);
   cudaFree(Y);
   cudaFree(g);
@@ -643,7 +643,7 @@ int nb_mlp_weights(nb_ctx* ctx, float* w_out, const float* w_in, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   if (w_out) NB_CUDA(cudaMemcpyAsync(w_out, M->w, sizeof(float) * nbk::MLP_NPARAM, cudaMemcpyDeviceToDevice, st));
   if (w_in) NB_CUDA(cudaMemcpyAsync(M->w, w_in, sizeof(float) * nbk::MLP_NPARAM, cudaMemcpyDeviceToDevice, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(nbk::host_sync(st));
   return 0;
 }
 

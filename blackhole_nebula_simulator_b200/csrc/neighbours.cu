@@ -242,9 +242,11 @@ __device__ __forceinline__ double point_gap2(double x, double y, double z, doubl
 // and u = 2^-24, the offsets round with error <= u D, their differences with error <= 4 u D,
 // and the float r^2 of a pair (three rounded squares and sums of terms <= 12 D^2) differs from
 // the exact one by at most 84 u D^2; the float thresholds and their subtractions add at most
-// 36 u D^2 for every threshold that can matter (r^2 <= 12 D^2).  Pairs whose float r^2 lies
-// within B = 192 u D^2 of the threshold are decided by the exact FP64 test (no fused
-// multiply-add) from the double positions; the others are certain.  So the lists are the
+// 36 u D^2 for every threshold that can matter (r^2 <= 12 D^2).  With B = 192 u D^2 and the
+// float threshold T lowered by B, q = fl(r^2 - (T - B)) < 0 is a certain hit (the sign of a
+// rounded difference is exact, and r^2 + 84 u D^2 < T - B + 36 u D^2 < T) and q >= 2 B a
+// certain miss (r^2 >= T - B + 2 B (1 - u) - 120 u D^2 > T); pairs in between are decided by
+// the exact FP64 test (no fused multiply-add) from the double positions.  So the lists are the
 // reference's bit for bit.
 //
 // Three passes share the traversal: k_lists_cand counts each query leaf's candidate sub-leaves
@@ -341,7 +343,9 @@ __device__ __forceinline__ bool walk_candidates(int64_t n, const TreeView& tv, c
 // order).  A slice that would pass the buffers' capacity is not written; the host then grows the
 // buffers from the cursors' final values and runs the pass again.
 constexpr int CAND_WARPS = 4;
-constexpr int CAND_SMEM = 1024;  // entries of a frontier buffer
+#ifndef CAND_SMEM
+#define CAND_SMEM 1024  // entries of a frontier buffer
+#endif
 
 __global__ void __launch_bounds__(CAND_WARPS * 32) k_lists_cand(int64_t n, int64_t nwork,
                                                            const uint64_t* __restrict__ order,
@@ -452,7 +456,10 @@ __global__ void __launch_bounds__(CAND_WARPS * 32) k_lists_cand(int64_t n, int64
 
 // Pass 2: the tests, on each leaf's candidate list.  Each batch's final hit masks go to
 // masks[(batch base + b) * 32 + lane], the rows' entry counts to counts.
-__global__ void __launch_bounds__(NB_THREADS) k_lists_test(int64_t n, int64_t nwork,
+#ifndef TEST_BLOCKS_PER_SM
+#define TEST_BLOCKS_PER_SM 3
+#endif
+__global__ void __launch_bounds__(NB_THREADS, TEST_BLOCKS_PER_SM) k_lists_test(int64_t n, int64_t nwork,
                                                            const uint64_t* __restrict__ order,
                                                            unsigned long long* __restrict__ next,
                                                            TreeView tv,
@@ -524,22 +531,32 @@ __global__ void __launch_bounds__(NB_THREADS) k_lists_test(int64_t n, int64_t nw
       cidx[lane] = jj;
       __syncwarp();
       const float ri_lo = r2i_f - B, twoB = 2.0f * B;
-      unsigned hit = 0u, amb = 0u;
+      // q = r^2 - (threshold - B) of each candidate: its sign bit is a certain hit, shifted into
+      // the mask (candidate 31 first, so bit tt is candidate tt); the smallest non-negative q
+      // (signed floats' bits sort above every non-negative float's) tells whether any lies in
+      // the band 0 <= q < 2B
+      unsigned hit = 0u, closest = 0xffffffffu;
 #pragma unroll
-      for (int tt = 0; tt < 32; ++tt) {
+      for (int tt = 31; tt >= 0; --tt) {
         const float4 e = cand[tt];
         const float dx = e.x - mx, dy = e.y - my, dz = e.z - mz;
-        const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-        const float tl = fmaxf(e.w, ri_lo);
-        hit |= d2 < tl ? 1u << tt : 0u;
-        amb |= d2 - twoB < tl ? 1u << tt : 0u;
+        const float q = fmaf(dz, dz, fmaf(dy, dy, dx * dx)) - fmaxf(e.w, ri_lo);
+        hit = __funnelshift_l(__float_as_uint(q), hit, 1);
+        closest = min(closest, __float_as_uint(q));
       }
+      unsigned amb = 0u;
       if (wide) {
         hit = 0u;
         amb = __ballot_sync(FULL, jj >= 0);
+      } else if (__any_sync(FULL, valid && closest < __float_as_uint(twoB))) {
+        for (int tt = 0; tt < 32; ++tt) {
+          const float4 e = cand[tt];
+          const float dx = e.x - mx, dy = e.y - my, dz = e.z - mz;
+          const float q = fmaf(dz, dz, fmaf(dy, dy, dx * dx)) - fmaxf(e.w, ri_lo);
+          amb |= q >= 0.0f && q < twoB ? 1u << tt : 0u;
+        }
       }
       if (!valid) hit = amb = 0u;
-      amb &= ~hit;
       if (__any_sync(FULL, amb != 0u)) {
         // the band: the reference's exact FP64 test from the double positions
         while (amb) {
@@ -562,17 +579,24 @@ __global__ void __launch_bounds__(NB_THREADS) k_lists_test(int64_t n, int64_t nw
   if (lane == 0) atomicMax(rowmax, (unsigned long long)mx);
 }
 
-// Pass 3: masks -> CSR entries.  One warp per query leaf.  The leaf's masks and candidate
-// sub-leaves are staged in shared memory a chunk of batches at a time; then row by row and batch
-// by batch, lane t takes candidate slot t of the batch: a set bit's entry goes to the row's
-// running position plus the number of set bits below it, so one coalesced store writes all of
-// a batch's entries of the row.  Each row's entries come out in ascending order (batches
-// ascending, a mask's bits from the lowest slot up), contiguous from the row's offset.
-constexpr int EXPAND_WARPS = 4;
-constexpr int EXPAND_CHUNK = 64;  // batches staged at a time
-#ifndef EXPAND_UNROLL
-#define EXPAND_UNROLL 4
+// Pass 3: masks -> CSR entries.  One warp per query leaf.  The leaf's masks (all 32 rows) and
+// candidate sub-leaves are staged in shared memory a chunk of batches at a time; then the warp
+// takes the rows one after the other, with lane b on batch b of a round of 32: the batches'
+// entry counts are scanned across the lanes, and for each batch with entries, in ascending
+// order, lane c writes candidate c's entry (if its bit is set) into the row's buffer at the
+// batch's start plus the number of set bits below c.  The buffer goes out with coalesced stores,
+// so each row's entries of a chunk are written as one contiguous run soon after each other
+// (short-lived partial lines in L2 would otherwise be written back to DRAM more than once).
+// Each row's entries come out in ascending order (batches ascending, candidates ascending within
+// a batch), contiguous from the row's offset.
+#ifndef EXPAND_WARPS
+#define EXPAND_WARPS 2
 #endif
+#ifndef EXPAND_CHUNK
+#define EXPAND_CHUNK 64  // batches staged at a time
+#endif
+constexpr int EXPAND_ROWBUF = 1024;  // a row's buffer: the most entries of one round (32 x 32)
+constexpr int EXPAND_STRIDE = 33;    // padded mask rows: lane b reading row r of batch b is conflict-free
 
 __global__ void __launch_bounds__(EXPAND_WARPS * 32) k_lists_expand(int64_t n, int64_t nleaf,
                                                              const int32_t* __restrict__ cands,
@@ -582,27 +606,29 @@ __global__ void __launch_bounds__(EXPAND_WARPS * 32) k_lists_expand(int64_t n, i
                                                              const uint32_t* __restrict__ masks,
                                                              const int64_t* __restrict__ off,
                                                              int32_t* __restrict__ idx, int* err) {
-  // per warp: a chunk's masks (one row per batch, 32 lanes' masks) and its candidate sub-leaves
-  __shared__ uint32_t mask_s[EXPAND_WARPS][EXPAND_CHUNK][32];
+  __shared__ uint32_t msk_s[EXPAND_WARPS][EXPAND_CHUNK * EXPAND_STRIDE];
   __shared__ int32_t sub_s[EXPAND_WARPS][EXPAND_CHUNK * 4];
+  __shared__ int32_t row_s[EXPAND_WARPS][EXPAND_ROWBUF];
   const unsigned FULL = 0xffffffffu;
   const int64_t leaf = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (leaf >= nleaf) return;  // warp-uniform
-  uint32_t(*msk)[32] = mask_s[threadIdx.x >> 5];
+  uint32_t* msk = msk_s[threadIdx.x >> 5];
   int32_t* sub = sub_s[threadIdx.x >> 5];
+  int32_t* rowbuf = row_s[threadIdx.x >> 5];
+  const unsigned below = (1u << lane) - 1u;
   const int64_t cbase = leaf_cbase[leaf], bbase = leaf_bbase[leaf];
   const int64_t ncand = leaf_ncand[leaf], nbat = (ncand + 3) / 4;
   const int64_t k0 = leaf * LEAF;
   const int rows = (int)(n - k0 < LEAF ? n - k0 : LEAF);
-  const unsigned below = (1u << lane) - 1u;
   // lane r keeps row r's running output position and its end
   int64_t pos = lane < rows ? off[k0 + lane] : 0;
   const int64_t stop = lane < rows ? off[k0 + lane + 1] : 0;
   for (int64_t c0 = 0; c0 < nbat; c0 += EXPAND_CHUNK) {
     const int nb = (int)(nbat - c0 < EXPAND_CHUNK ? nbat - c0 : EXPAND_CHUNK);
     __syncwarp();
-    for (int e = lane; e < nb * 32; e += 32) msk[e >> 5][e & 31] = masks[(bbase + c0) * 32 + e];
+    for (int e = lane; e < nb * 32; e += 32)
+      msk[(e >> 5) * EXPAND_STRIDE + (e & 31)] = masks[(bbase + c0) * 32 + e];
     for (int e = lane; e < nb * 4; e += 32) {
       const int64_t c = 4 * c0 + e;
       sub[e] = c < ncand ? cands[cbase + c] : 0;
@@ -611,25 +637,50 @@ __global__ void __launch_bounds__(EXPAND_WARPS * 32) k_lists_expand(int64_t n, i
     for (int r = 0; r < rows; ++r) {
       int64_t at = __shfl_sync(FULL, pos, r);  // warp-uniform from here on
       const int64_t end = __shfl_sync(FULL, stop, r);
-      // EXPAND_UNROLL batches' masks are read together, then written one after the other
-      for (int b0 = 0; b0 < nb; b0 += EXPAND_UNROLL) {
-        uint32_t mm[EXPAND_UNROLL];
+      int filled = 0;
+      for (int b0 = 0; b0 < nb; b0 += 32) {
+        const uint32_t m = b0 + lane < nb ? msk[(b0 + lane) * EXPAND_STRIDE + r] : 0u;
+        const int cnt = __popc(m);
+        int incl = cnt;
 #pragma unroll
-        for (int u = 0; u < EXPAND_UNROLL; ++u) mm[u] = b0 + u < nb ? msk[b0 + u][r] : 0u;
-#pragma unroll
-        for (int u = 0; u < EXPAND_UNROLL; ++u) {
-          const uint32_t m = mm[u];
-          if (m == 0u) continue;  // warp-uniform
-          if ((m >> lane) & 1u) {
-            const int64_t w = at + __popc(m & below);
-            if (w < end)
-              idx[w] = sub[4 * (b0 + u) + (lane >> 3)] * SUB + (lane & 7);
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(FULL, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        if (filled + total > EXPAND_ROWBUF) {  // write out what the buffer holds
+          __syncwarp();
+          for (int e = lane; e < filled; e += 32) {
+            if (at + e < end)
+              idx[at + e] = rowbuf[e];
             else
               set_error(err, ERR_LIST_OVERFLOW);
           }
-          at += __popc(m);
+          at += filled;
+          filled = 0;
+          __syncwarp();
         }
+        const int start = filled + incl - cnt;
+        unsigned nz = __ballot_sync(FULL, m != 0u);
+        while (nz) {
+          const int bb = __ffs(nz) - 1;
+          nz &= nz - 1u;
+          const uint32_t mb = __shfl_sync(FULL, m, bb);
+          const int sb = __shfl_sync(FULL, start, bb);
+          if ((mb >> lane) & 1u)
+            rowbuf[sb + __popc(mb & below)] = sub[4 * (b0 + bb) + (lane >> 3)] * SUB + (lane & 7);
+        }
+        filled += total;
       }
+      __syncwarp();
+      for (int e = lane; e < filled; e += 32) {
+        if (at + e < end)
+          idx[at + e] = rowbuf[e];
+        else
+          set_error(err, ERR_LIST_OVERFLOW);
+      }
+      at += filled;
+      __syncwarp();
       if (lane == r) pos = at;
     }
   }
@@ -674,7 +725,7 @@ __global__ void k_export_fill(int64_t n, const int32_t* __restrict__ perm,
 // error the pass raised (so no buffer is sized from a failed pass).
 static int pending_check(Engine& E, cudaStream_t st) {
   NB_CUDA(cudaMemcpyAsync(E.h_err, E.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(host_sync(st));
   if (E.h_err[0] != 0) return check_device_error(E, st);
   return 0;
 }
@@ -918,7 +969,7 @@ int cell_geometry(Engine& E, int64_t n, const double* pos, const double* h, doub
   NB_CUDA(cudaMemcpyAsync(box, E.bbox, sizeof(box), cudaMemcpyDeviceToHost, st));
   NB_CUDA(cudaMemcpyAsync(mid, h_sorted + (n - 1) / 2, sizeof(double) * (n % 2 ? 1 : 2),
                           cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(host_sync(st));
   // numpy's median: the middle value, or the mean of the two middle values for even n
   const double median = n % 2 ? mid[0] : (mid[0] + mid[1]) / 2.0;
   double span[3], smax = 0.0;

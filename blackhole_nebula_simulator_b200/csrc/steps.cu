@@ -208,7 +208,7 @@ static int glf_status(Engine& E, int64_t n, const int64_t* iters, cudaStream_t s
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceReduce::Min(E.cub_tmp, tmp, iters, E.ws.d_i64, (int)n, st));
   NB_CUDA(cudaMemcpyAsync(E.ws.h_i64, E.ws.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(host_sync(st));
   int64_t worst = E.ws.h_i64[0];
   if (worst >= 0) return 0;
   const char* msg = worst == -1   ? "stage 1 (p_half) did not converge in 10 iterations: time step too large"
@@ -226,7 +226,7 @@ static int sum_doubles(Engine& E, int64_t n, const double* a, double* out, cudaS
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceReduce::Sum(E.cub_tmp, tmp, a, E.ws.d_tmp, (int)n, st));
   NB_CUDA(cudaMemcpyAsync(E.ws.h_dbl, E.ws.d_tmp, sizeof(double), cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(host_sync(st));
   *out = E.ws.h_dbl[0];
   return 0;
 }
@@ -323,7 +323,7 @@ int coupled_stable_dt(Engine& E, nb_state* s, const nb_params* prm, double* dt, 
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceReduce::Min(E.cub_tmp, tmp, W.d_b, W.d_tmp, (int)n, st));
   NB_CUDA(cudaMemcpyAsync(W.h_dbl, W.d_tmp, sizeof(double), cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(host_sync(st));
   *dt = W.h_dbl[0];
   return 0;
 }
@@ -700,7 +700,7 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
             ns, W.rows_s, L.off, E.tidx, W.i32a, prm->max_gap, W.i_lvl, W.d_int + b);
       NB_CUDA(cudaMemcpyAsync(W.h_int, W.d_int + batch - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
       NB_TRY(pending_enqueue(E, st));
-      NB_CUDA(cudaStreamSynchronize(st));
+      NB_CUDA(host_sync(st));
       NB_TRY(pending_finish(E, st));
       if (W.h_int[0] == 0) {
         settled = true;
@@ -765,7 +765,7 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   size_t tmp = E.cub_bytes;
   NB_CUDA(cub::DeviceReduce::Min(E.cub_tmp, tmp, s->n_end, W.d_i64, (int)n, st));
   NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(host_sync(st));
   int64_t n_next = W.h_i64[0];
   // flow of every particle from its step start; predictor momenta; active flags
   E.prof.begin(st);
@@ -943,7 +943,7 @@ int block_wake_doomed(Engine& E, nb_state* s, int64_t nrows, const int64_t* rows
       n, s->tick_n, s->tick, end, label, s->n_end, s->level, s->p_half, s->u_half, s->a_hydro,
       s->dudt, reinterpret_cast<unsigned long long*>(W.d_i64), heat_of(s));
   NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  NB_CUDA(cudaStreamSynchronize(st));
+  NB_CUDA(host_sync(st));
   s->woken += W.h_i64[0];
   return check_device_error(E, st);
 }

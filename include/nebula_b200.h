@@ -117,6 +117,8 @@ NB_API int64_t nb_state_size(void);
 NB_API int64_t nb_params_size(void);
 /* Number of this library's own kernels launched so far by this process (all contexts). */
 NB_API int64_t nb_launch_count(void);
+/* Number of host waits on a stream this library has made so far (all contexts). */
+NB_API int64_t nb_sync_count(void);
 
 /* ---------------------------------------------------------------- operators
  * One-for-one replacements of the reference's inner functions (sim/neighbours.py, sim/sph.py,
