@@ -38,12 +38,24 @@ FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes
 FP64_NOMINAL_TFLOPS = FP32_NOMINAL_TFLOPS / 2.0
 FLOP_PER_DENSITY_EVAL = 25.0  # distance + kernel + two sums per pair evaluation
 FLOP_PER_FORCE_PAIR = 75.0  # pressure + viscosity + P dV (+20 with disc viscosity)
-# DRAM bytes (read + write) per row of one launch, from ncu captures of the FP32 kernels on the
-# 1,048,576-particle torus (profiles/k_forces_g_torus1m.md, profiles/k_density_torus1m.md),
-# scaled to a launch by its rows; for a list build, the traversal's bytes per particle from the
-# capture of a whole-set build (profiles/k_lists_sub_torus1m.md: 404.0 MB read + 1,289.2 MB
-# written over 1,048,576 rows; the same FP64 kernel in both forms)
-DRAM_BYTES_PER_ROW = {"forces": 1768.0, "density": 1003.0, "lists": 1615.0}
+# DRAM bytes (read + write) per row of one launch, from ncu captures (cold caches) of the FP32
+# kernels on the 1,048,576-particle torus, scaled to a launch by its rows: density 199.9 MB over
+# 195,200 rows; forces (walk + pair launches) 1,347 + 1,007 MB over 1,045,504 rows; a list build
+# (candidate, test and expansion passes of a build after the start, 163 entries per row)
+# 1,273 MB over 1,048,576 particles
+DRAM_BYTES_PER_ROW = {"forces": 2251.0, "density": 1024.0, "lists": 1214.0}
+# What the ncu counters of the same captures show limits each kernel (the roofline's ceiling
+# stays the HBM copy bandwidth; none of these kernels is a contraction)
+LIMITER = {
+    "lists": "issue: the test pass at 80 % issue active (FMA 45 %, ALU 42 %), the expansion at "
+             "64 %; the candidate pass latency bound (long-scoreboard 2.9 per issue at 26 % warp "
+             "occupancy); DRAM 0.1-9 % of peak",
+    "density": "latency: long-scoreboard stalls 4.2 per issue on the gathered records, 66 % "
+               "issue active at 43 % warp occupancy, DRAM 8 % of peak",
+    "forces": "latency: the walk launch stalls 11.5 per issue on the gathered records (DRAM 21 %); "
+              "the pair launch runs the FMA pipe at 36 % with 43 % warp occupancy",
+    "flow": "FP64 pipe 69-71 % (the double-precision flow update), DRAM 25-29 %",
+}
 
 
 def peaks():
@@ -197,7 +209,7 @@ def roofline(prof, precision, disc, pk):
     rf = {"bound": "hbm", "kernel": dom, "achieved": round(gbs, 2), "peak": pk["hbm_gbs"],
           "unit": "GB/s", "frac": round(gbs / pk["hbm_gbs"], 4), "traffic": traffic,
           "peak_source": pk["source"], "ms_per_launch": round(ms, 4),
-          "bytes_per_launch": bytes_}  # fmt: skip
+          "bytes_per_launch": bytes_, "limiter": LIMITER.get(dom)}  # fmt: skip
     if flops:
         tf = flops / (ms * 1e-3) / 1e12
         rf["pipe"] = {"unit": "TFLOP/s", "achieved": round(tf, 3), "peak": round(pipe_peak, 2),
@@ -248,6 +260,8 @@ def kernel_table(prof, precision, disc, pk):
             tf = f / (ms * 1e-3) / 1e12
             row.update(flop_per_launch=round(f), tflops=round(tf, 3),
                        pipe_frac=round(tf / pipe_peak, 4))  # fmt: skip
+        if cat in LIMITER:
+            row["limiter"] = LIMITER[cat]
         out[cat] = row
     return out
 

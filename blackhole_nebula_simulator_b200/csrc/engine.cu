@@ -5,6 +5,7 @@
 // Hilbert-curve order; the pair passes read packed copies in that order (coalesced, cache-friendly) and
 // scatter their results back to the caller's order.
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <cmath>
 #include <vector>
@@ -416,15 +417,11 @@ __global__ void k_pack_sorted4(int64_t n, const int32_t* __restrict__ perm, cons
 // FP32 positions: the cell of a uniform grid (edge `cell`, at most 1024 per axis, corner lo) and
 // the float offset from the cell centre, as two float4 per particle: (offset, mass) and (cell
 // coordinates as exact floats, h); mass and h 0 when not given.
-__global__ void k_pack_sorted32(int64_t n, const int32_t* __restrict__ perm,
-                                const double* __restrict__ x, const double* __restrict__ m,
-                                const double* __restrict__ h, const double* __restrict__ box6,
-                                float4* __restrict__ out) {
-  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (k >= n) return;
+__device__ __forceinline__ void pos32_record(const double* __restrict__ x, int64_t i,
+                                             const double* __restrict__ box6, float w0, float w1,
+                                             float4* __restrict__ out) {
   double span = fmax(fmax(box6[3] - box6[0], box6[4] - box6[1]), box6[5] - box6[2]);
   const double cell = fmax(span / 1000.0, 1e-30);
-  int64_t i = perm[k];
   int c[3];
   float o[3];
   for (int a = 0; a < 3; ++a) {
@@ -434,8 +431,60 @@ __global__ void k_pack_sorted32(int64_t n, const int32_t* __restrict__ perm,
     c[a] = ci;
     o[a] = (float)(x[3 * i + a] - (box6[a] + (ci + 0.5) * cell));
   }
-  out[2 * k] = make_float4(o[0], o[1], o[2], m ? (float)m[i] : 0.0f);
-  out[2 * k + 1] = make_float4((float)c[0], (float)c[1], (float)c[2], h ? (float)h[i] : 0.0f);
+  out[0] = make_float4(o[0], o[1], o[2], w0);
+  out[1] = make_float4((float)c[0], (float)c[1], (float)c[2], w1);
+}
+
+__global__ void k_pack_sorted32(int64_t n, const int32_t* __restrict__ perm,
+                                const double* __restrict__ x, const double* __restrict__ m,
+                                const double* __restrict__ h, const double* __restrict__ box6,
+                                float4* __restrict__ out) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int64_t i = perm[k];
+  pos32_record(x, i, box6, m ? (float)m[i] : 0.0f, h ? (float)h[i] : 0.0f, out + 2 * k);
+}
+
+// The FP32 density pass's sorted inputs in one pass: k_gather_density's mass, h_start and
+// h_search, and the position records (offset, m) (cell, 0).
+__global__ void k_pack_density32(int64_t n, const int32_t* __restrict__ perm,
+                                 const double* __restrict__ x, const double* __restrict__ mass,
+                                 const double* __restrict__ h0, const double* __restrict__ hs,
+                                 const double* __restrict__ box6, double* __restrict__ mass_s,
+                                 double* __restrict__ h0_s, double* __restrict__ hs_s,
+                                 float4* __restrict__ pk32) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int32_t i = perm[k];
+  const double m = mass[i];
+  mass_s[k] = m;
+  h0_s[k] = h0[i];
+  hs_s[k] = hs[i];
+  pos32_record(x, i, box6, (float)m, 0.0f, pk32 + 2 * k);
+}
+
+// The FP32 force pass's sorted inputs in one pass (the switch and the reconstruction off): the
+// position records (offset, m) (cell, h), the records (v, m), (h, rho, omega, P), (u, c_s, alpha)
+// and, when pk0 is given, the double (x, h) of the exact band test.
+__global__ void k_pack_force32(int64_t n, const int32_t* __restrict__ perm,
+                               const double* __restrict__ x, const double* __restrict__ m,
+                               const double* __restrict__ h, const double* __restrict__ box6,
+                               const double* __restrict__ vel, const double* __restrict__ rho,
+                               const double* __restrict__ omega, const double* __restrict__ P,
+                               const double* __restrict__ u, const double* __restrict__ cs,
+                               const double* __restrict__ alpha, float4* __restrict__ pk32,
+                               float4* __restrict__ pf1, float4* __restrict__ pf2,
+                               float4* __restrict__ pf3, double4* __restrict__ pk0) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int64_t i = perm[k];
+  const double hi = h[i];
+  const float mi = (float)m[i];
+  pos32_record(x, i, box6, mi, (float)hi, pk32 + 2 * k);
+  pf1[k] = make_float4((float)vel[3 * i], (float)vel[3 * i + 1], (float)vel[3 * i + 2], mi);
+  pf2[k] = make_float4((float)hi, (float)rho[i], (float)omega[i], (float)P[i]);
+  pf3[k] = make_float4((float)u[i], (float)cs[i], alpha ? (float)alpha[i] : 0.f, 0.f);
+  if (pk0) pk0[k] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], hi);
 }
 
 // the configured EOS (sim/hydro.py:119-139) for every particle, or for the particles of `mask`
@@ -761,9 +810,9 @@ static int rows_sorted(Engine& E, int64_t n, int64_t nrows, const int64_t* rows,
   NB_CUDA(cudaMemsetAsync(W.m_x, 0, n, st));
   count_launch(), k_mask_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, n, W.m_x, E.d_err);
   count_launch(), k_sorted_mask<<<grid_for(n), NB_THREADS, 0, st>>>(n, E.lists.perm, W.m_x, W.m_sorted);
-  count_launch(), k_iota64<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.i_tmp);
   size_t tmp = E.cub_bytes;
-  NB_CUDA(cub::DeviceSelect::Flagged(E.cub_tmp, tmp, W.i_tmp, W.m_sorted, W.rows_s, W.d_i64 + 4, (int)n, st));
+  NB_CUDA(cub::DeviceSelect::Flagged(E.cub_tmp, tmp, thrust::counting_iterator<int64_t>(0), W.m_sorted,
+                                     W.rows_s, W.d_i64 + 4, (int)n, st));
   count_launch(), k_rows_count_check<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, W.d_i64 + 4, W.rows_s, E.d_err);
   W.pend_err = true;
   *count = nrows;
@@ -845,18 +894,19 @@ static int density_on_lists(Engine& E, int64_t n, const double* x, const double*
   if (nrows == 0) return 0;
   int64_t ns = 0;
   NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));
-  count_launch(), k_gather_density<<<grid_for(n), NB_THREADS, 0, st>>>(
-      n, L.perm, mass, h_start, h_search, W.d_a, W.d_b, W.d_c, nullptr);
   DensityParams dp{prm->kernel_id, prm->cnorm, prm->eta, prm->tol, prm->h_max};
   if (prm->precision == 1) {
     // grid over the box of the last list build (cells clamp to it; the edge is derived on the
     // device, so no host round trip)
-    count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, mass, nullptr, E.bbox, W.pk32);
+    count_launch(), k_pack_density32<<<grid_for(n), NB_THREADS, 0, st>>>(
+        n, L.perm, x, mass, h_start, h_search, E.bbox, W.d_a, W.d_b, W.d_c, W.pk32);
     E.prof.begin(st);
     launch_density32<int32_t>(nrows, W.rows_s, W.pk32, E.bbox, W.d_a, W.d_b, W.d_c, L.off,
                               L.idx, dp, L.perm, h_out, rho, omega, W.iters, W.flags,
                               E.prof.on ? W.pairs : nullptr, st);
   } else {
+    count_launch(), k_gather_density<<<grid_for(n), NB_THREADS, 0, st>>>(
+        n, L.perm, mass, h_start, h_search, W.d_a, W.d_b, W.d_c, nullptr);
     count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, nullptr, W.pk0);
     E.prof.begin(st);
     launch_density64<int32_t>(nrows, W.rows_s, W.pk0, W.d_a, W.d_b, W.d_c, L.off, L.idx, dp,
@@ -1024,15 +1074,17 @@ void mask_or(int64_t n, const uint8_t* a, uint8_t* b, cudaStream_t st) {
 }
 
 int select_mask(Engine& E, int64_t n, const uint8_t* mask, int64_t* out, int64_t* count,
-                cudaStream_t st) {
+                cudaStream_t st, int64_t* also) {
   Workspace& W = E.ws;
-  count_launch(), k_iota64<<<grid_for(n), NB_THREADS, 0, st>>>(n, W.i_tmp);
   size_t tmp = E.cub_bytes;
-  NB_CUDA(cub::DeviceSelect::Flagged(E.cub_tmp, tmp, W.i_tmp, mask, out, W.d_i64, (int)n, st));
-  NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cub::DeviceSelect::Flagged(E.cub_tmp, tmp, thrust::counting_iterator<int64_t>(0), mask, out,
+                                     W.d_i64, (int)n, st));
+  // the count, and W.d_i64[1] when the caller left a value there to read with it
+  NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t) * (also ? 2 : 1), cudaMemcpyDeviceToHost, st));
   NB_TRY(pending_enqueue(E, st));
   NB_CUDA(host_sync(st));
   *count = W.h_i64[0];
+  if (also) *also = W.h_i64[1];
   return pending_finish(E, st);
 }
 
@@ -1057,7 +1109,9 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));
   const bool sw_on = prm->viscosity && prm->visc_switch && sk.switch_on;
   const bool recon = prm->viscosity && prm->recon;
-  if (prm->precision == 1) {
+  // FP32 without the switch and the reconstruction: every sorted input in one pass below
+  const bool fused_pack = prm->precision == 1 && !sw_on && !recon;
+  if (prm->precision == 1 && !fused_pack) {
     count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, vel, s->mass, nullptr, nullptr, 1, W.pf1);
     count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->h, s->rho, s->omega, W.d_P, 0, W.pf2);
   }
@@ -1097,9 +1151,10 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
     if (recon && prm->precision == 1)
       count_launch(), k_to_float<<<grid_for(9 * n), NB_THREADS, 0, st>>>(9 * n, W.gvel, W.gvel32);
   }
-  if (prm->precision == 1)
-    count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, 0, W.pf3);
-  else
+  if (prm->precision == 1) {
+    if (!fused_pack)
+      count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, 0, W.pf3);
+  } else
     count_launch(), k_pack_sorted4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, u, W.d_cs, s->alpha, nullptr, W.pk3);
   ForceParams fp{};
   fp.kid = prm->kernel_id;
@@ -1125,7 +1180,7 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
     fp.tcnt = W.i32a;
   }
   if (want_tight && prm->precision == 1) {
-    count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, s->h, W.pk0);
+    if (!fused_pack) count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, s->h, W.pk0);
     fp.pos64 = W.pk0;
   }
   if (recon) {
@@ -1147,7 +1202,12 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   fo.ddudt = W.d_ddudt;
   fo.pairs = W.pairs;
   if (prm->precision == 1) {
-    count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, s->mass, s->h, E.bbox, W.pk32);
+    if (fused_pack)
+      count_launch(), k_pack_force32<<<grid_for(n), NB_THREADS, 0, st>>>(
+          n, L.perm, s->x, s->mass, s->h, E.bbox, vel, s->rho, s->omega, W.d_P, u, W.d_cs, s->alpha,
+          W.pk32, W.pf1, W.pf2, W.pf3, want_tight ? W.pk0 : nullptr);
+    else
+      count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, s->mass, s->h, E.bbox, W.pk32);
     E.prof.begin(st);
     launch_forces32<int32_t>(nrows, W.rows_s, W.pk32, E.bbox, W.pf1, W.pf2, W.pf3, L.off,
                              L.idx, fp, L.perm, fo, st);

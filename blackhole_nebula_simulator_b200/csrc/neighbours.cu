@@ -12,6 +12,7 @@
 //
 // Rows come out in sorted (curve) order with each row's entries in ascending sorted index.
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include "common.cuh"
 #include "engine.cuh"
@@ -346,6 +347,9 @@ constexpr int CAND_WARPS = 4;
 #ifndef CAND_SMEM
 #define CAND_SMEM 1024  // entries of a frontier buffer
 #endif
+#ifndef CAND_UNROLL
+#define CAND_UNROLL 1
+#endif
 
 __global__ void __launch_bounds__(CAND_WARPS * 32) k_lists_cand(int64_t n, int64_t nwork,
                                                            const uint64_t* __restrict__ order,
@@ -392,25 +396,38 @@ __global__ void __launch_bounds__(CAND_WARPS * 32) k_lists_cand(int64_t n, int64
       const double4* chi = lvl > 0 ? tv.hi : shi;
       const int total = fn * fan;
       int nn = 0;
-      for (int c0 = 0; c0 < total; c0 += 32) {
-        const int c = c0 + lane;
-        bool hit = false;
-        int32_t child = 0;
-        if (c < total) {
-          child = front[cur][c / fan] * fan + c % fan;
-          if (child < csize) {
-            const double4 blo = clo[coff + child], bhi = chi[coff + child];
-            const double reach = 2.0 * fmax(qh, blo.w);
-            hit = box_gap2(q.lo, q.hi, blo, bhi) < reach * reach * (1.0 + 1e-12);
+      // CAND_UNROLL rounds of 32 children per pass: their box loads are issued together
+      for (int c0 = 0; c0 < total && !over; c0 += 32 * CAND_UNROLL) {
+        bool hit[CAND_UNROLL];
+        int32_t child[CAND_UNROLL];
+        double4 blo[CAND_UNROLL], bhi[CAND_UNROLL];
+#pragma unroll
+        for (int u = 0; u < CAND_UNROLL; ++u) {
+          const int c = c0 + 32 * u + lane;
+          child[u] = c < total ? front[cur][c / fan] * fan + c % fan : -1;
+          hit[u] = child[u] >= 0 && child[u] < csize;
+          if (hit[u]) {
+            blo[u] = clo[coff + child[u]];
+            bhi[u] = chi[coff + child[u]];
           }
         }
-        const unsigned mk = __ballot_sync(FULL, hit);
-        if (nn + __popc(mk) > CAND_SMEM) {
-          over = true;
-          break;
+#pragma unroll
+        for (int u = 0; u < CAND_UNROLL; ++u) {
+          if (hit[u]) {
+            const double reach = 2.0 * fmax(qh, blo[u].w);
+            hit[u] = box_gap2(q.lo, q.hi, blo[u], bhi[u]) < reach * reach * (1.0 + 1e-12);
+          }
         }
-        if (hit) front[cur ^ 1][nn + __popc(mk & below)] = child;
-        nn += __popc(mk);
+#pragma unroll
+        for (int u = 0; u < CAND_UNROLL; ++u) {
+          const unsigned mk = __ballot_sync(FULL, hit[u]);
+          if (nn + __popc(mk) > CAND_SMEM) {
+            over = true;
+            break;
+          }
+          if (hit[u]) front[cur ^ 1][nn + __popc(mk & below)] = child[u];
+          nn += __popc(mk);
+        }
       }
       __syncwarp();
       cur ^= 1;
@@ -579,24 +596,36 @@ __global__ void __launch_bounds__(NB_THREADS, TEST_BLOCKS_PER_SM) k_lists_test(i
   if (lane == 0) atomicMax(rowmax, (unsigned long long)mx);
 }
 
+// Position of the k-th set bit (k from 0) of m, for k < popc(m): halving by population count.
+__device__ __forceinline__ int nth_set_bit(uint32_t m, int k) {
+  int p = 0;
+  int c = __popc(m & 0xffffu);
+  if (k >= c) { k -= c; p += 16; m >>= 16; }
+  c = __popc(m & 0xffu);
+  if (k >= c) { k -= c; p += 8; m >>= 8; }
+  c = __popc(m & 0xfu);
+  if (k >= c) { k -= c; p += 4; m >>= 4; }
+  c = __popc(m & 0x3u);
+  if (k >= c) { k -= c; p += 2; m >>= 2; }
+  if (k >= (int)(m & 1u)) p += 1;
+  return p;
+}
+
 // Pass 3: masks -> CSR entries.  One warp per query leaf.  The leaf's masks (all 32 rows) and
 // candidate sub-leaves are staged in shared memory a chunk of batches at a time; then the warp
-// takes the rows one after the other, with lane b on batch b of a round of 32: the batches'
-// entry counts are scanned across the lanes, and for each batch with entries, in ascending
-// order, lane c writes candidate c's entry (if its bit is set) into the row's buffer at the
-// batch's start plus the number of set bits below c.  The buffer goes out with coalesced stores,
-// so each row's entries of a chunk are written as one contiguous run soon after each other
-// (short-lived partial lines in L2 would otherwise be written back to DRAM more than once).
-// Each row's entries come out in ascending order (batches ascending, candidates ascending within
-// a batch), contiguous from the row's offset.
+// takes the rows one after the other, 32 batches at a time with lane b on batch b: the batches'
+// entry counts are scanned across the lanes, and the row's entries of those batches are written
+// 32 at a time, lane s taking entry s: its batch is found by a binary search over the scanned
+// counts, its candidate as the set bit of that rank in the batch's mask.  Every store writes 32
+// consecutive entries of one row, and each row's entries come out in ascending order (batches
+// ascending, a mask's bits from the lowest slot up), contiguous from the row's offset.
 #ifndef EXPAND_WARPS
-#define EXPAND_WARPS 2
+#define EXPAND_WARPS 4
 #endif
 #ifndef EXPAND_CHUNK
 #define EXPAND_CHUNK 64  // batches staged at a time
 #endif
-constexpr int EXPAND_ROWBUF = 1024;  // a row's buffer: the most entries of one round (32 x 32)
-constexpr int EXPAND_STRIDE = 33;    // padded mask rows: lane b reading row r of batch b is conflict-free
+constexpr int EXPAND_STRIDE = 33;  // padded mask rows: lane b reading row r of batch b is conflict-free
 
 __global__ void __launch_bounds__(EXPAND_WARPS * 32) k_lists_expand(int64_t n, int64_t nleaf,
                                                              const int32_t* __restrict__ cands,
@@ -608,15 +637,12 @@ __global__ void __launch_bounds__(EXPAND_WARPS * 32) k_lists_expand(int64_t n, i
                                                              int32_t* __restrict__ idx, int* err) {
   __shared__ uint32_t msk_s[EXPAND_WARPS][EXPAND_CHUNK * EXPAND_STRIDE];
   __shared__ int32_t sub_s[EXPAND_WARPS][EXPAND_CHUNK * 4];
-  __shared__ int32_t row_s[EXPAND_WARPS][EXPAND_ROWBUF];
   const unsigned FULL = 0xffffffffu;
   const int64_t leaf = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (leaf >= nleaf) return;  // warp-uniform
   uint32_t* msk = msk_s[threadIdx.x >> 5];
   int32_t* sub = sub_s[threadIdx.x >> 5];
-  int32_t* rowbuf = row_s[threadIdx.x >> 5];
-  const unsigned below = (1u << lane) - 1u;
   const int64_t cbase = leaf_cbase[leaf], bbase = leaf_bbase[leaf];
   const int64_t ncand = leaf_ncand[leaf], nbat = (ncand + 3) / 4;
   const int64_t k0 = leaf * LEAF;
@@ -637,50 +663,36 @@ __global__ void __launch_bounds__(EXPAND_WARPS * 32) k_lists_expand(int64_t n, i
     for (int r = 0; r < rows; ++r) {
       int64_t at = __shfl_sync(FULL, pos, r);  // warp-uniform from here on
       const int64_t end = __shfl_sync(FULL, stop, r);
-      int filled = 0;
       for (int b0 = 0; b0 < nb; b0 += 32) {
         const uint32_t m = b0 + lane < nb ? msk[(b0 + lane) * EXPAND_STRIDE + r] : 0u;
-        const int cnt = __popc(m);
-        int incl = cnt;
+        int incl = __popc(m);
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
           const int v = __shfl_up_sync(FULL, incl, o);
           if (lane >= o) incl += v;
         }
         const int total = __shfl_sync(FULL, incl, 31);
-        if (filled + total > EXPAND_ROWBUF) {  // write out what the buffer holds
-          __syncwarp();
-          for (int e = lane; e < filled; e += 32) {
-            if (at + e < end)
-              idx[at + e] = rowbuf[e];
+        for (int base = 0; base < total; base += 32) {
+          const int s = base + lane;
+          // batch of entry s: the number of batches whose inclusive count is <= s (< 32 for
+          // s < total; the probes stay within lanes 0..30)
+          int j = 0;
+#pragma unroll
+          for (int step = 16; step > 0; step >>= 1)
+            if (__shfl_sync(FULL, incl, j + step - 1) <= s) j += step;
+          const uint32_t mb = __shfl_sync(FULL, m, j);
+          const int first = __shfl_sync(FULL, incl, j) - __popc(mb);
+          if (s < total) {
+            const int t = nth_set_bit(mb, s - first);
+            const int64_t w = at + s;
+            if (w < end)
+              idx[w] = sub[4 * (b0 + j) + (t >> 3)] * SUB + (t & 7);
             else
               set_error(err, ERR_LIST_OVERFLOW);
           }
-          at += filled;
-          filled = 0;
-          __syncwarp();
         }
-        const int start = filled + incl - cnt;
-        unsigned nz = __ballot_sync(FULL, m != 0u);
-        while (nz) {
-          const int bb = __ffs(nz) - 1;
-          nz &= nz - 1u;
-          const uint32_t mb = __shfl_sync(FULL, m, bb);
-          const int sb = __shfl_sync(FULL, start, bb);
-          if ((mb >> lane) & 1u)
-            rowbuf[sb + __popc(mb & below)] = sub[4 * (b0 + bb) + (lane >> 3)] * SUB + (lane & 7);
-        }
-        filled += total;
+        at += total;
       }
-      __syncwarp();
-      for (int e = lane; e < filled; e += 32) {
-        if (at + e < end)
-          idx[at + e] = rowbuf[e];
-        else
-          set_error(err, ERR_LIST_OVERFLOW);
-      }
-      at += filled;
-      __syncwarp();
       if (lane == r) pos = at;
     }
   }
@@ -996,7 +1008,10 @@ size_t cub_bytes_needed(int64_t n, int64_t m) {
                                        m, (int)n, (int64_t*)nullptr, (int64_t*)nullptr);
   cub::DeviceSelect::Flagged((void*)nullptr, d, (int64_t*)nullptr, (const uint8_t*)nullptr,
                              (int64_t*)nullptr, (int64_t*)nullptr, (int)n);
-  return std::max(std::max(a, b), std::max(c, d)) + 256;
+  size_t e = 0;
+  cub::DeviceSelect::Flagged((void*)nullptr, e, thrust::counting_iterator<int64_t>(0),
+                             (const uint8_t*)nullptr, (int64_t*)nullptr, (int64_t*)nullptr, (int)n);
+  return std::max(std::max(std::max(a, b), std::max(c, d)), e) + 256;
 }
 
 }  // namespace nbk

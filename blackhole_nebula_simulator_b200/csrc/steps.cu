@@ -331,25 +331,33 @@ int coupled_stable_dt(Engine& E, nb_state* s, const nb_params* prm, double* dt, 
 // ---------------------------------------------------------------- block steps
 // gravity flow of every particle to tick n_next from its step start, the predictor momentum,
 // and the active flags (sim/blocks.py:506-517)
-__global__ void k_block_flow(int64_t n, int64_t n_next, double tick,
+__global__ void k_block_flow(int64_t n, const int64_t* __restrict__ n_next_p, double tick,
                              const double* __restrict__ x_beg, const double* __restrict__ p_half,
                              const int64_t* __restrict__ n_beg, const int64_t* __restrict__ n_end,
                              const double* __restrict__ a, double* __restrict__ x,
                              double* __restrict__ p_flow, double* __restrict__ p_pred,
-                             int64_t* __restrict__ iters, uint8_t* __restrict__ active) {
+                             double* __restrict__ v_eval, int64_t* __restrict__ iters,
+                             uint8_t* __restrict__ active) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const int64_t n_next = *n_next_p;
   double s = (double)(n_next - n_beg[i]) * tick;
   double half_len = 0.5 * (double)(n_end[i] - n_beg[i]) * tick;
   double xb[3] = {x_beg[3 * i], x_beg[3 * i + 1], x_beg[3 * i + 2]};
   double pb[3] = {p_half[3 * i], p_half[3 * i + 1], p_half[3 * i + 2]};
-  double xo[3], po[3];
+  double xo[3], po[3], pp[3];
   iters[i] = glf_one(xb, pb, s, xo, po);
   double lag = s - half_len;
   for (int c = 0; c < 3; ++c) {
+    pp[c] = po[c] + lag * a[3 * i + c];
     x[3 * i + c] = xo[c];
     p_flow[3 * i + c] = po[c];
-    p_pred[3 * i + c] = po[c] + lag * a[3 * i + c];
+    p_pred[3 * i + c] = pp[c];
+  }
+  if (v_eval) {  // the velocity of the predicted momentum at the new position (k_v_from_p's)
+    double w[3];
+    gn_dh_dp(xo, pp, w);
+    for (int c = 0; c < 3; ++c) v_eval[3 * i + c] = w[c];
   }
   active[i] = n_end[i] == n_next;
 }
@@ -763,15 +771,14 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
   int64_t n = s->n;
   NB_TRY(W.ensure(E, n));
   size_t tmp = E.cub_bytes;
-  NB_CUDA(cub::DeviceReduce::Min(E.cub_tmp, tmp, s->n_end, W.d_i64, (int)n, st));
-  NB_CUDA(cudaMemcpyAsync(W.h_i64, W.d_i64, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  NB_CUDA(host_sync(st));
-  int64_t n_next = W.h_i64[0];
+  // the earliest step end stays on the device for the flow and the active flags; the host reads
+  // it with the active count
+  NB_CUDA(cub::DeviceReduce::Min(E.cub_tmp, tmp, s->n_end, W.d_i64 + 1, (int)n, st));
   // flow of every particle from its step start; predictor momenta; active flags
   E.prof.begin(st);
-  count_launch(), k_block_flow<<<grid_for(n, 128), 128, 0, st>>>(n, n_next, s->tick, s->x_beg, s->p_half, s->n_beg,
+  count_launch(), k_block_flow<<<grid_for(n, 128), 128, 0, st>>>(n, W.d_i64 + 1, s->tick, s->x_beg, s->p_half, s->n_beg,
                                                  s->n_end, s->a_hydro, s->x, W.v_flow, W.v_pred,
-                                                 W.iters, W.m_rows);
+                                                 W.v_eval, W.iters, W.m_rows);
   E.prof.end(PROF_FLOW, st, (double)n, 0.0);
   {
     // the flow's worst iteration code, read with the active count just below
@@ -779,8 +786,8 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
     NB_CUDA(cub::DeviceReduce::Min(E.cub_tmp, tmp2, W.iters, W.d_scal_i, (int)n, st));
     W.pend_glf = true;
   }
-  int64_t nrows = 0;
-  NB_TRY(select_mask(E, n, W.m_rows, W.rows, &nrows, st));
+  int64_t nrows = 0, n_next = 0;
+  NB_TRY(select_mask(E, n, W.m_rows, W.rows, &nrows, st, &n_next));
   W.rows_ver += 1;
   E.prof.begin(st);
   if (prm->cooling == 3 && nrows > 0) {
@@ -801,8 +808,7 @@ int block_advance(Engine& E, nb_state* s, const nb_params* prm, int64_t* rows_ou
     NB_CUDA(cub::DeviceReduce::Sum(E.cub_tmp, tmp2, W.d_dm, W.d_scal, (int)n, st));
     W.pend_erad = &s->e_radiated;
   }
-  s->tick_n = n_next;
-  launch_v_from_p(n, s->x, W.v_pred, W.v_eval, st);
+  s->tick_n = n_next;  // W.v_eval: written by the flow kernel
   ShockStep sk;
   sk.switch_on = 1;
   sk.n_beg = s->n_beg;

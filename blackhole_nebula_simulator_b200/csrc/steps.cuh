@@ -27,8 +27,10 @@ struct ShockStep {
 int compute_density(Engine& E, int64_t n, const double* x, const double* mass, double* h,
                     double* rho, double* omega, int64_t nrows, const int64_t* rows,
                     const nb_params* prm, int64_t* builds, int64_t* reuses, cudaStream_t st);
+// out = the indices of mask's set entries, ascending; count read on the host (with W.d_i64[1]
+// into *also when given)
 int select_mask(Engine& E, int64_t n, const uint8_t* mask, int64_t* out, int64_t* count,
-                cudaStream_t st);
+                cudaStream_t st, int64_t* also = nullptr);
 int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, int64_t nrows,
                   const int64_t* rows, const nb_params* prm, const uint8_t* touched,
                   const ShockStep& sk, cudaStream_t st);
