@@ -465,19 +465,22 @@ __global__ void k_pack_density32(int64_t n, const int32_t* __restrict__ perm,
 
 // The FP32 force pass's sorted inputs in one pass (the switch and the reconstruction off): the
 // position records (offset, m) (cell, h), the records (v, m), (h, rho, omega, P), (u, c_s, alpha)
-// and, when pk0 is given, the double (x, h) of the exact band test.
+// and, when pk0 is given, the double (x, h) of the exact band test; with `only`, the records of
+// its particles alone.
 __global__ void k_pack_force32(int64_t n, const int32_t* __restrict__ perm,
                                const double* __restrict__ x, const double* __restrict__ m,
                                const double* __restrict__ h, const double* __restrict__ box6,
                                const double* __restrict__ vel, const double* __restrict__ rho,
                                const double* __restrict__ omega, const double* __restrict__ P,
                                const double* __restrict__ u, const double* __restrict__ cs,
-                               const double* __restrict__ alpha, float4* __restrict__ pk32,
-                               float4* __restrict__ pf1, float4* __restrict__ pf2,
-                               float4* __restrict__ pf3, double4* __restrict__ pk0) {
+                               const double* __restrict__ alpha, const uint8_t* __restrict__ only,
+                               float4* __restrict__ pk32, float4* __restrict__ pf1,
+                               float4* __restrict__ pf2, float4* __restrict__ pf3,
+                               double4* __restrict__ pk0) {
   int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (k >= n) return;
   const int64_t i = perm[k];
+  if (only && !only[i]) return;  // a record the pass does not read
   const double hi = h[i];
   const float mi = (float)m[i];
   pos32_record(x, i, box6, mi, (float)hi, pk32 + 2 * k);
@@ -568,15 +571,19 @@ __global__ void k_mark_s(int64_t nrows, const int64_t* __restrict__ rows_s,
 // if it is a row or a row is among its own entries.  Eight lanes per particle scan its list until
 // one of them meets a row, and the mark goes straight to the caller's order.  Cheaper than
 // scattering marks when a large share of the particles are rows.
+// With `tight`, only rows within 2 max(h_k, h_row) count (pk: sorted (x, h)), the same exact
+// test k_mark_s makes from the row's side (the squared differences do not depend on the sign).
 __global__ void k_mark_gather(int64_t n, const int64_t* __restrict__ off,
                               const int32_t* __restrict__ idx, const uint8_t* __restrict__ row_s,
-                              const int32_t* __restrict__ perm, uint8_t* __restrict__ mark) {
+                              const int32_t* __restrict__ perm, int tight,
+                              const double4* __restrict__ pk, uint8_t* __restrict__ mark) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   int64_t k = t >> 3;
   const int gl = (int)(t & 7), g = (int)((threadIdx.x & 31) >> 3);
   const bool live = k < n;
   if (!__any_sync(0xffffffffu, live)) return;  // warp-uniform
   bool hit = live && row_s[k];
+  const double4 me = tight && live ? pk[k] : make_double4(0, 0, 0, 0);
   const int64_t e0 = live ? off[k] : 0, e1 = live ? off[k + 1] : 0;
   for (int64_t b = e0; ; b += 8) {
     unsigned grp = (__ballot_sync(0xffffffffu, hit) >> (8 * g)) & 0xffu;
@@ -585,7 +592,17 @@ __global__ void k_mark_gather(int64_t n, const int64_t* __restrict__ off,
       hit = grp != 0;
       break;
     }
-    if (more && b + gl < e1) hit = hit || row_s[ld_stream(idx + b + gl)];
+    if (more && b + gl < e1) {
+      const int32_t j = ld_stream(idx + b + gl);
+      bool near = row_s[j];
+      if (near && tight) {
+        const double4 o = pk[j];
+        const double d2 = d2_exact(o.x - me.x, o.y - me.y, o.z - me.z);
+        const double rr = 2.0 * fmax(me.w, o.w);
+        near = d2 < rr * rr;
+      }
+      hit = hit || near;
+    }
   }
   if (live && gl == 0 && hit) mark[perm[k]] = 1;
 }
@@ -1038,12 +1055,14 @@ int mark_rows(Engine& E, int64_t nrows, const int64_t* rows, int tight, const do
   Workspace& W = E.ws;
   int64_t n = L.n, ns = 0;
   NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));
-  if (!tight && nrows * 4 > n) {
-    // most particles are rows: gather (W.m_sorted holds the rows' sorted mask)
-    count_launch(), k_mark_gather<<<grid_for(n * 8), NB_THREADS, 0, st>>>(n, L.off, L.idx, W.m_sorted, L.perm, mark);
+  if (tight) count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, h, W.pk0);
+  if (nrows * 4 > n) {
+    // most particles are rows: each particle looks for a row among its own entries (the lists
+    // are symmetric) and stops at the first; W.m_sorted holds the rows' sorted mask
+    count_launch(), k_mark_gather<<<grid_for(n * 8), NB_THREADS, 0, st>>>(n, L.off, L.idx, W.m_sorted, L.perm,
+                                                                        tight, W.pk0, mark);
     return 0;
   }
-  if (tight) count_launch(), k_pack_sorted<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, x, h, W.pk0);
   NB_CUDA(cudaMemsetAsync(W.m_smark, 0, n, st));
   count_launch(), k_mark_s<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, tight,
                                                                W.pk0, W.m_smark);
@@ -1109,8 +1128,10 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
   NB_TRY(rows_sorted(E, n, nrows, rows, &ns, st));
   const bool sw_on = prm->viscosity && prm->visc_switch && sk.switch_on;
   const bool recon = prm->viscosity && prm->recon;
-  // FP32 without the switch and the reconstruction: every sorted input in one pass below
+  // FP32 without the switch and the reconstruction: every sorted input in one pass below, for
+  // the touched particles only when they hold every list entry of the rows and are few
   const bool fused_pack = prm->precision == 1 && !sw_on && !recon;
+  const bool sparse_pack = fused_pack && touched && sk.touched_covers_lists && nrows * 8 < n;
   if (prm->precision == 1 && !fused_pack) {
     count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, vel, s->mass, nullptr, nullptr, 1, W.pf1);
     count_launch(), k_pack_sorted_f4<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->h, s->rho, s->omega, W.d_P, 0, W.pf2);
@@ -1205,7 +1226,7 @@ int engine_forces(Engine& E, nb_state* s, const double* vel, const double* u, in
     if (fused_pack)
       count_launch(), k_pack_force32<<<grid_for(n), NB_THREADS, 0, st>>>(
           n, L.perm, s->x, s->mass, s->h, E.bbox, vel, s->rho, s->omega, W.d_P, u, W.d_cs, s->alpha,
-          W.pk32, W.pf1, W.pf2, W.pf3, want_tight ? W.pk0 : nullptr);
+          sparse_pack ? touched : nullptr, W.pk32, W.pf1, W.pf2, W.pf3, want_tight ? W.pk0 : nullptr);
     else
       count_launch(), k_pack_sorted32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->x, s->mass, s->h, E.bbox, W.pk32);
     E.prof.begin(st);

@@ -112,6 +112,7 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
     E.prof.end(PROF_MARKS, st, (double)nrows, 0.0);
   }
   NB_CUDA(cudaMemsetAsync(W.m_done, 0, n, st));
+  const int64_t builds_in = s->builds;
   bool settled = false;
   for (int it = 0; it < 8; ++it) {
     int64_t ntodo = 0;
@@ -151,7 +152,9 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
   }
   if (prm->viscosity && !prm->visc_switch)
     count_launch(), k_set_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, prm->alpha_const, s->alpha);
-  return engine_forces(E, s, vel, u, nrows, rows, prm, W.m_done, sk, st);
+  ShockStep sk2 = sk;
+  sk2.touched_covers_lists = s->builds == builds_in;  // no rebuild since the first marking
+  return engine_forces(E, s, vel, u, nrows, rows, prm, W.m_done, sk2, st);
 }
 
 // ---------------------------------------------------------------- shared step

@@ -22,6 +22,9 @@ struct ShockStep {
   double tick = 0.0;
   int recon_full = 0;
   int want_tight = 0;  // block steps: the force pass also writes the rows' interacting entries
+  // the touched set holds every list entry of the rows (marked on the lists the force pass
+  // walks), so the force pass reads records of touched particles only
+  int touched_covers_lists = 0;
 };
 
 int compute_density(Engine& E, int64_t n, const double* x, const double* mass, double* h,
