@@ -264,12 +264,38 @@ __global__ void k_hsearch(int64_t n, const double* __restrict__ hg, double h_max
   hs[i] = fmin(hg[i], h_max) * skin;
 }
 
-__global__ void k_disp(int64_t n, const double* __restrict__ x, const double* __restrict__ xr,
-                       double* __restrict__ disp) {
+// The displacements since the last build, and their largest value into *dmax (as the bits of a
+// non-negative double, which order like the values; *dmax starts at 0).
+__global__ void __launch_bounds__(NB_THREADS) k_disp(int64_t n, const double* __restrict__ x,
+                                                     const double* __restrict__ xr,
+                                                     double* __restrict__ disp,
+                                                     unsigned long long* __restrict__ dmax) {
+  __shared__ unsigned long long wmax[NB_THREADS / 32];
+  const unsigned FULL = 0xffffffffu;
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double dx = x[3 * i] - xr[3 * i], dy = x[3 * i + 1] - xr[3 * i + 1], dz = x[3 * i + 2] - xr[3 * i + 2];
-  disp[i] = sqrt(dx * dx + dy * dy + dz * dz);
+  unsigned long long key = 0ull;
+  if (i < n) {
+    double dx = x[3 * i] - xr[3 * i], dy = x[3 * i + 1] - xr[3 * i + 1], dz = x[3 * i + 2] - xr[3 * i + 2];
+    const double d = sqrt(dx * dx + dy * dy + dz * dz);
+    disp[i] = d;
+    key = (unsigned long long)__double_as_longlong(d);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long v = __shfl_xor_sync(FULL, key, o);
+    key = v > key ? v : key;
+  }
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = key;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    key = threadIdx.x < NB_THREADS / 32 ? wmax[threadIdx.x] : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long v = __shfl_xor_sync(FULL, key, o);
+      key = v > key ? v : key;
+    }
+    if (threadIdx.x == 0) atomicMax(dmax, key);
+  }
 }
 
 // The TOPK largest displacements with their indices, in descending order and, among equal values,
@@ -717,8 +743,9 @@ int Workspace::ensure(Engine& E, int64_t n) {
   NB_CUDA(cudaMallocHost((void**)&h_int, sizeof(int) * 16));
   NB_CUDA(cudaMallocHost((void**)&h_i64, sizeof(int64_t) * 16));
   NB_CUDA(cudaMallocHost((void**)&h_dbl, sizeof(double) * 80));
-  NB_CUDA(cudaMalloc((void**)&d_scal, sizeof(double) * 8));
-  NB_CUDA(cudaMalloc((void**)&d_scal_i, sizeof(int64_t) * 8));
+  NB_CUDA(cudaMalloc((void**)&d_scal_i, sizeof(int64_t) * 16));
+  d_scal = reinterpret_cast<double*>(d_scal_i + 8);
+  NB_CUDA(cudaMallocHost((void**)&h_scal, sizeof(int64_t) * 16));
   cap = c;
   if (cache.cap < c) {
     if (cache.x_ref) cudaFree(cache.x_ref);
@@ -761,13 +788,13 @@ void Workspace::release() {
                 d_dm, d_tmp, d_uh, v_flow, v_pred, v_eval, v_dacc, v_tmp, pk0, pk1, pk2, pk3, pk32,
                 pf1, pf2, pf3, m_x, m_sorted, m_smark, f_mass,
                 rows, rows_s, rows2, iters, flags, need, i_tmp, pairs, i_lvl, i_tmp2, m_rows, m_done, m_need,
-                m_tmp, i32a, i32b, dk_b, d_int, d_i64, tk_key0, tk_key1, tk_idx0, tk_idx1, d_scal,
-                d_scal_i};
+                m_tmp, i32a, i32b, dk_b, d_int, d_i64, tk_key0, tk_key1, tk_idx0, tk_idx1, d_scal_i};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (h_int) cudaFreeHost(h_int);
   if (h_i64) cudaFreeHost(h_i64);
   if (h_dbl) cudaFreeHost(h_dbl);
+  if (h_scal) cudaFreeHost(h_scal);
   *this = Workspace{cache};
 }
 
@@ -845,28 +872,26 @@ static int rows_sorted(Engine& E, int64_t n, int64_t nrows, const int64_t* rows,
 int pending_enqueue(Engine& E, cudaStream_t st) {
   Workspace& W = E.ws;
   if (W.pend_err) NB_CUDA(cudaMemcpyAsync(E.h_err, E.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
-  if (W.pend_glf)
-    NB_CUDA(cudaMemcpyAsync(W.h_i64 + 8, W.d_scal_i, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  if (W.pend_erad)
-    NB_CUDA(cudaMemcpyAsync(W.h_dbl + 72, W.d_scal, sizeof(double), cudaMemcpyDeviceToHost, st));
-  if (W.pend_woken)
-    NB_CUDA(cudaMemcpyAsync(W.h_i64 + 10, W.d_scal_i + 2, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  // the flow's worst iteration code (d_scal_i[0]), the wake-up count (d_scal_i[2]) and the
+  // radiated energy (d_scal[0] = word 8 of the same allocation) in one copy
+  if (W.pend_glf || W.pend_erad || W.pend_woken)
+    NB_CUDA(cudaMemcpyAsync(W.h_scal, W.d_scal_i, sizeof(int64_t) * 9, cudaMemcpyDeviceToHost, st));
   return 0;
 }
 
 int pending_finish(Engine& E, cudaStream_t st) {
   Workspace& W = E.ws;
   if (W.pend_erad) {
-    *W.pend_erad += W.h_dbl[72];
+    *W.pend_erad += reinterpret_cast<const double*>(W.h_scal)[8];
     W.pend_erad = nullptr;
   }
   if (W.pend_woken) {
-    *W.pend_woken += W.h_i64[10];
+    *W.pend_woken += W.h_scal[2];
     W.pend_woken = nullptr;
   }
   if (W.pend_glf) {
     W.pend_glf = false;
-    int64_t worst = W.h_i64[8];
+    int64_t worst = W.h_scal[0];
     if (worst < 0) {
       const char* msg = worst == -1   ? "stage 1 (p_half) did not converge in 10 iterations: time step too large"
                         : worst == -2 ? "stage 2 (x1) did not converge in 10 iterations: time step too large"
@@ -946,8 +971,22 @@ static int reuse_limits(Engine& E, int64_t n, const double* x, const double* hg,
   Workspace& W = E.ws;
   Cache& C = W.cache;
   *ok = 0;
-  count_launch(), k_disp<<<grid_for(n), NB_THREADS, 0, st>>>(n, x, C.x_ref, W.d_disp);
-  // the largest displacements (descending; ties by index) into W.dk_b / W.i32b
+  // the largest displacement into W.dk_b[0]: the test without a fast set needs no more
+  NB_CUDA(cudaMemsetAsync(W.dk_b, 0, sizeof(double), st));
+  count_launch(), k_disp<<<grid_for(n), NB_THREADS, 0, st>>>(n, x, C.x_ref, W.d_disp,
+                                                            reinterpret_cast<unsigned long long*>(W.dk_b));
+  {
+    NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
+    count_launch(), k_reuse_test<<<grid_for(n), NB_THREADS, 0, st>>>(n, C.hs, W.d_disp, W.dk_b, hg, W.m_rows,
+                                                     W.d_heff, W.d_hlim, W.d_int);
+    int fail = 0;
+    NB_TRY(read_int(E, W.d_int, &fail, st));
+    if (!fail) {
+      *ok = 1;
+      return 0;
+    }
+  }
+  // the largest displacements (descending; ties by index) into W.dk_b / W.i32b for the fast sets
   {
     int64_t count = n;
     unsigned long long *kin = nullptr, *kout = W.tk_key0;
@@ -970,7 +1009,7 @@ static int reuse_limits(Engine& E, int64_t n, const double* x, const double* hg,
     count_launch(), k_topk_out<<<1, 128, 0, st>>>((int)std::min<int64_t>(n, TOPK), kout, iout, W.dk_b, W.i32b);
   }
   int top = (int)std::min<int64_t>(n, TOPK);
-  static const int FAST[] = {0, 1, 2, 4, 8, 16, 32, 64};
+  static const int FAST[] = {1, 2, 4, 8, 16, 32, 64};  // no fast set: tested above
   for (int nf : FAST) {
     if (nf >= top) break;
     NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
@@ -979,10 +1018,6 @@ static int reuse_limits(Engine& E, int64_t n, const double* x, const double* hg,
     int fail = 0;
     NB_TRY(read_int(E, W.d_int, &fail, st));
     if (fail) continue;
-    if (nf == 0) {
-      *ok = 1;
-      return 0;
-    }
     NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
     count_launch(), k_fast_complete<<<nf, NB_THREADS, 0, st>>>(n, nf, W.i32b, x, W.d_hlim, E.lists.inv_perm,
                                                E.lists.off, E.lists.idx, W.d_int);

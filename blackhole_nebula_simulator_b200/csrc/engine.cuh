@@ -67,6 +67,7 @@ struct Workspace {
   int* h_int = nullptr;
   int64_t* h_i64 = nullptr;
   double* h_dbl = nullptr;
+  int64_t* h_scal = nullptr;  // host copy of d_scal_i[0..8) and d_scal[0] (one read for all three)
   // W.rows (the active rows of the current step) changes version whenever it is rewritten; the
   // sorted copy in rows_s is kept while the rows and the lists stay the same
   int64_t rows_ver = 0, rs_ver = -1, rs_gen = -1, rs_n = -1, rs_count = 0;
@@ -79,7 +80,7 @@ struct Workspace {
   bool pend_err = false, pend_glf = false;
   double* pend_erad = nullptr;
   int64_t* pend_woken = nullptr;  // the level choice's wake-up count (d_scal_i[2]) to add here
-  double* d_scal = nullptr;
+  double* d_scal = nullptr;    // = (double*)(d_scal_i + 8): one allocation, read in one copy
   int64_t* d_scal_i = nullptr;
   // switch and velocity reconstruction only (allocated on first use): sorted accelerations and
   // the sorted velocity gradients (9 per particle; float copy for the FP32 force pass)
