@@ -659,8 +659,10 @@ def measure(args, name, rank, world, steps=None):
 
 N_FULL = {"torus": 4_194_304, "streams": 1_048_576, "cloud": 262_144}
 # the second configuration of the metric ("at 1M & 4M"): the 1M streams, timed over more system
-# steps than the torus because its steps are short (small active sets)
-STREAMS_STEPS_PER_STEP = 10
+# steps than the torus because its steps are short (small active sets, about a millisecond each,
+# bound by the host that launches them: 300 steps keep one slow host moment from moving the
+# number)
+STREAMS_STEPS_PER_STEP = 30
 
 
 def workload_config(args, name, n_full, world):

@@ -964,27 +964,39 @@ static int density_on_lists(Engine& E, int64_t n, const double* x, const double*
   return 0;
 }
 
-// sim/sph.py:117-147 (_reuse_limits): returns 1 with W.d_heff filled if the cached lists are
-// provably complete for the search limits h_eff, else 0.
-static int reuse_limits(Engine& E, int64_t n, const double* x, const double* hg, int* ok,
-                        cudaStream_t st) {
+// The first reuse test (no fast set: the largest displacement outside it is the largest of
+// all, reduced into W.dk_b[0] by the displacement pass) for the rows of `mask`; its failure
+// flag goes to *fail (zeroed here), read by the caller with its next round trip.  hg_in: the
+// caller's h guesses, copied to W.d_hg for the tests and the solve (null: W.d_hg holds them).
+int reuse_first_test(Engine& E, int64_t n, const double* x, const double* hg_in,
+                     const uint8_t* mask, int* fail, cudaStream_t st) {
   Workspace& W = E.ws;
   Cache& C = W.cache;
-  *ok = 0;
-  // the largest displacement into W.dk_b[0]: the test without a fast set needs no more
+  if (hg_in) NB_CUDA(cudaMemcpyAsync(W.d_hg, hg_in, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   NB_CUDA(cudaMemsetAsync(W.dk_b, 0, sizeof(double), st));
   count_launch(), k_disp<<<grid_for(n), NB_THREADS, 0, st>>>(n, x, C.x_ref, W.d_disp,
                                                             reinterpret_cast<unsigned long long*>(W.dk_b));
-  {
-    NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
-    count_launch(), k_reuse_test<<<grid_for(n), NB_THREADS, 0, st>>>(n, C.hs, W.d_disp, W.dk_b, hg, W.m_rows,
-                                                     W.d_heff, W.d_hlim, W.d_int);
-    int fail = 0;
-    NB_TRY(read_int(E, W.d_int, &fail, st));
-    if (!fail) {
-      *ok = 1;
-      return 0;
-    }
+  NB_CUDA(cudaMemsetAsync(fail, 0, sizeof(int), st));
+  count_launch(), k_reuse_test<<<grid_for(n), NB_THREADS, 0, st>>>(n, C.hs, W.d_disp, W.dk_b, W.d_hg, mask,
+                                                   W.d_heff, W.d_hlim, fail);
+  return 0;
+}
+
+// sim/sph.py:117-147 (_reuse_limits): returns 1 with W.d_heff filled if the cached lists are
+// provably complete for the search limits h_eff, else 0.  first_fail: the first test's outcome
+// when it ran already (reuse_first_test), -1 to run it here.
+static int reuse_limits(Engine& E, int64_t n, const double* x, const uint8_t* mask,
+                        int first_fail, int* ok, cudaStream_t st) {
+  Workspace& W = E.ws;
+  Cache& C = W.cache;
+  *ok = 0;
+  if (first_fail < 0) {
+    NB_TRY(reuse_first_test(E, n, x, nullptr, mask, W.d_int, st));
+    NB_TRY(read_int(E, W.d_int, &first_fail, st));
+  }
+  if (!first_fail) {
+    *ok = 1;
+    return 0;
   }
   // the largest displacements (descending; ties by index) into W.dk_b / W.i32b for the fast sets
   {
@@ -1013,7 +1025,7 @@ static int reuse_limits(Engine& E, int64_t n, const double* x, const double* hg,
   for (int nf : FAST) {
     if (nf >= top) break;
     NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));
-    count_launch(), k_reuse_test<<<grid_for(n), NB_THREADS, 0, st>>>(n, C.hs, W.d_disp, W.dk_b + nf, hg, W.m_rows,
+    count_launch(), k_reuse_test<<<grid_for(n), NB_THREADS, 0, st>>>(n, C.hs, W.d_disp, W.dk_b + nf, W.d_hg, mask,
                                                      W.d_heff, W.d_hlim, W.d_int);
     int fail = 0;
     NB_TRY(read_int(E, W.d_int, &fail, st));
@@ -1036,16 +1048,21 @@ static int reuse_limits(Engine& E, int64_t n, const double* x, const double* hg,
 // guess for every particle; rows get their solved h, and rho / omega.
 int compute_density(Engine& E, int64_t n, const double* x, const double* mass, double* h,
                     double* rho, double* omega, int64_t nrows, const int64_t* rows,
-                    const nb_params* prm, int64_t* builds, int64_t* reuses, cudaStream_t st) {
+                    const nb_params* prm, int64_t* builds, int64_t* reuses, cudaStream_t st,
+                    const uint8_t* rows_mask, int first_fail) {
   Workspace& W = E.ws;
   Cache& C = W.cache;
   NB_TRY(W.ensure(E, n));
-  NB_CUDA(cudaMemsetAsync(W.m_rows, 0, n, st));
-  count_launch(), k_mask_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, n, W.m_rows, E.d_err);
-  NB_CUDA(cudaMemcpyAsync(W.d_hg, h, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  const uint8_t* mask = rows_mask;
+  if (first_fail < 0) {
+    NB_CUDA(cudaMemsetAsync(W.m_rows, 0, n, st));
+    count_launch(), k_mask_rows<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, n, W.m_rows, E.d_err);
+    NB_CUDA(cudaMemcpyAsync(W.d_hg, h, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    mask = W.m_rows;
+  }
   if (C.valid && C.n == n && n > 0 && E.lists.n == n) {
     int ok = 0;
-    NB_TRY(reuse_limits(E, n, x, W.d_hg, &ok, st));
+    NB_TRY(reuse_limits(E, n, x, mask, first_fail, &ok, st));
     if (ok) {
       NB_TRY(density_on_lists(E, n, x, mass, W.d_hg, W.d_heff, nrows, rows, prm, h, rho, omega, st));
       NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int), st));

@@ -116,14 +116,26 @@ int hydro_rows(Engine& E, nb_state* s, const nb_params* prm, int64_t nrows, cons
   bool settled = false;
   for (int it = 0; it < 8; ++it) {
     int64_t ntodo = 0;
-    NB_TRY(select_mask(E, n, W.m_need, W.rows2, &ntodo, st));
+    // on cached lists, the first reuse test runs on the todo mask before its count is read, and
+    // its outcome comes back with the count (W.d_i64[1])
+    int first_fail = -1;
+    const bool pre = it == 0 && W.cache.valid && W.cache.n == n && E.lists.n == n && n > 0;
+    if (pre) {
+      NB_CUDA(cudaMemsetAsync(W.d_i64 + 1, 0, sizeof(int64_t), st));
+      NB_TRY(reuse_first_test(E, n, s->x, s->h, W.m_need, reinterpret_cast<int*>(W.d_i64 + 1), st));
+      int64_t fail64 = 0;
+      NB_TRY(select_mask(E, n, W.m_need, W.rows2, &ntodo, st, &fail64));
+      first_fail = fail64 != 0;
+    } else {
+      NB_TRY(select_mask(E, n, W.m_need, W.rows2, &ntodo, st));
+    }
     if (ntodo == 0) {
       settled = true;
       break;
     }
     const int64_t builds0 = s->builds;
     NB_TRY(compute_density(E, n, s->x, s->mass, s->h, s->rho, s->omega, ntodo, W.rows2, prm,
-                           &s->builds, &s->reuses, st));
+                           &s->builds, &s->reuses, st, pre ? W.m_need : nullptr, first_fail));
     mask_or(n, W.m_need, W.m_done, st);
     // Reused lists are complete for every pair within 2 max(h_i, h_j) at the new h (the reuse
     // test proves it for the search limits the solve was capped at), so the interacting

@@ -27,9 +27,14 @@ struct ShockStep {
   int touched_covers_lists = 0;
 };
 
+// rows_mask / first_fail: the rows' mask and the first reuse test's outcome when
+// reuse_first_test ran on it already (first_fail -1: neither)
 int compute_density(Engine& E, int64_t n, const double* x, const double* mass, double* h,
                     double* rho, double* omega, int64_t nrows, const int64_t* rows,
-                    const nb_params* prm, int64_t* builds, int64_t* reuses, cudaStream_t st);
+                    const nb_params* prm, int64_t* builds, int64_t* reuses, cudaStream_t st,
+                    const uint8_t* rows_mask = nullptr, int first_fail = -1);
+int reuse_first_test(Engine& E, int64_t n, const double* x, const double* hg_in,
+                     const uint8_t* mask, int* fail, cudaStream_t st);
 // out = the indices of mask's set entries, ascending; count read on the host (with W.d_i64[1]
 // into *also when given)
 int select_mask(Engine& E, int64_t n, const uint8_t* mask, int64_t* out, int64_t* count,
