@@ -300,6 +300,11 @@ __device__ __forceinline__ uint32_t ld2(const __nv_bfloat16* p) {
 }
 
 // One hidden layer on tensor cores: in (hi, lo) fragments for 4 k-steps -> out fragments.
+// SiLU for inference: the reciprocal of 1 + e^-z by the fast approximate division (within 2
+// ulp; the training pass uses the IEEE division, a difference far below the BF16 rounding of the
+// activations that follows)
+__device__ __forceinline__ float silu_inf(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+
 __device__ __forceinline__ void mlp_hidden(const __nv_bfloat16 (*W)[MLP_H], const float* bias,
                                            const uint32_t ahi[4][4], const uint32_t alo[4][4],
                                            uint32_t ohi[4][4], uint32_t olo[4][4], int g, int t) {
@@ -314,10 +319,10 @@ __device__ __forceinline__ void mlp_hidden(const __nv_bfloat16 (*W)[MLP_H], cons
       mma16816(d0, d1, d2, d3, ahi[kk][0], ahi[kk][1], ahi[kk][2], ahi[kk][3], b0, b1);
       mma16816(d0, d1, d2, d3, alo[kk][0], alo[kk][1], alo[kk][2], alo[kk][3], b0, b1);
     }
-    d0 = silu(d0);
-    d1 = silu(d1);
-    d2 = silu(d2);
-    d3 = silu(d3);
+    d0 = silu_inf(d0);
+    d1 = silu_inf(d1);
+    d2 = silu_inf(d2);
+    d3 = silu_inf(d3);
     // n-tile j is half of the next layer's k-step j/2: rows g (regs 0/2) and g+8 (regs 1/3)
     int kk = j >> 1, hsel = (j & 1) * 2;
     split2(d0, d1, ohi[kk][hsel], olo[kk][hsel]);
@@ -382,10 +387,10 @@ __global__ void __launch_bounds__(128, 4) k_mlp_cool(int64_t n, const double* __
       uint32_t b0 = ld2(&S.w1[j * 8 + g][2 * t]);
       uint32_t b1 = ld2(&S.w1[j * 8 + g][8 + 2 * t]);
       mma16816(d0, d1, d2, d3, a[0], a[1], a[2], a[3], b0, b1);
-      d0 = silu(d0);
-      d1 = silu(d1);
-      d2 = silu(d2);
-      d3 = silu(d3);
+      d0 = silu_inf(d0);
+      d1 = silu_inf(d1);
+      d2 = silu_inf(d2);
+      d3 = silu_inf(d3);
       int kk = j >> 1, hsel = (j & 1) * 2;
       split2(d0, d1, h1hi[kk][hsel], h1lo[kk][hsel]);
       split2(d2, d3, h1hi[kk][hsel + 1], h1lo[kk][hsel + 1]);

@@ -347,9 +347,6 @@ constexpr int CAND_WARPS = 4;
 #ifndef CAND_SMEM
 #define CAND_SMEM 1024  // entries of a frontier buffer
 #endif
-#ifndef CAND_UNROLL
-#define CAND_UNROLL 1
-#endif
 
 __global__ void __launch_bounds__(CAND_WARPS * 32) k_lists_cand(int64_t n, int64_t nwork,
                                                            const uint64_t* __restrict__ order,
@@ -396,38 +393,25 @@ __global__ void __launch_bounds__(CAND_WARPS * 32) k_lists_cand(int64_t n, int64
       const double4* chi = lvl > 0 ? tv.hi : shi;
       const int total = fn * fan;
       int nn = 0;
-      // CAND_UNROLL rounds of 32 children per pass: their box loads are issued together
-      for (int c0 = 0; c0 < total && !over; c0 += 32 * CAND_UNROLL) {
-        bool hit[CAND_UNROLL];
-        int32_t child[CAND_UNROLL];
-        double4 blo[CAND_UNROLL], bhi[CAND_UNROLL];
-#pragma unroll
-        for (int u = 0; u < CAND_UNROLL; ++u) {
-          const int c = c0 + 32 * u + lane;
-          child[u] = c < total ? front[cur][c / fan] * fan + c % fan : -1;
-          hit[u] = child[u] >= 0 && child[u] < csize;
-          if (hit[u]) {
-            blo[u] = clo[coff + child[u]];
-            bhi[u] = chi[coff + child[u]];
+      for (int c0 = 0; c0 < total; c0 += 32) {
+        const int c = c0 + lane;
+        bool hit = false;
+        int32_t child = 0;
+        if (c < total) {
+          child = front[cur][c / fan] * fan + c % fan;
+          if (child < csize) {
+            const double4 blo = clo[coff + child], bhi = chi[coff + child];
+            const double reach = 2.0 * fmax(qh, blo.w);
+            hit = box_gap2(q.lo, q.hi, blo, bhi) < reach * reach * (1.0 + 1e-12);
           }
         }
-#pragma unroll
-        for (int u = 0; u < CAND_UNROLL; ++u) {
-          if (hit[u]) {
-            const double reach = 2.0 * fmax(qh, blo[u].w);
-            hit[u] = box_gap2(q.lo, q.hi, blo[u], bhi[u]) < reach * reach * (1.0 + 1e-12);
-          }
+        const unsigned mk = __ballot_sync(FULL, hit);
+        if (nn + __popc(mk) > CAND_SMEM) {
+          over = true;
+          break;
         }
-#pragma unroll
-        for (int u = 0; u < CAND_UNROLL; ++u) {
-          const unsigned mk = __ballot_sync(FULL, hit[u]);
-          if (nn + __popc(mk) > CAND_SMEM) {
-            over = true;
-            break;
-          }
-          if (hit[u]) front[cur ^ 1][nn + __popc(mk & below)] = child[u];
-          nn += __popc(mk);
-        }
+        if (hit) front[cur ^ 1][nn + __popc(mk & below)] = child;
+        nn += __popc(mk);
       }
       __syncwarp();
       cur ^= 1;
