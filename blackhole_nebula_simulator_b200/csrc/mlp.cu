@@ -299,12 +299,12 @@ __device__ __forceinline__ uint32_t ld2(const __nv_bfloat16* p) {
   return *reinterpret_cast<const uint32_t*>(p);
 }
 
-// One hidden layer on tensor cores: in (hi, lo) fragments for 4 k-steps -> out fragments.
 // SiLU for inference: the reciprocal of 1 + e^-z by the fast approximate division (within 2
 // ulp; the training pass uses the IEEE division, a difference far below the BF16 rounding of the
 // activations that follows)
 __device__ __forceinline__ float silu_inf(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 
+// One hidden layer on tensor cores: in (hi, lo) fragments for 4 k-steps -> out fragments.
 __device__ __forceinline__ void mlp_hidden(const __nv_bfloat16 (*W)[MLP_H], const float* bias,
                                            const uint32_t ahi[4][4], const uint32_t alo[4][4],
                                            uint32_t ohi[4][4], uint32_t olo[4][4], int g, int t) {
