@@ -352,66 +352,76 @@ __global__ void __launch_bounds__(128, 4) k_mlp_cool(int64_t n, const double* __
   int64_t nwarps = (int64_t)gridDim.x * warps;
   unsigned long long n_mlp = 0, n_fb = 0;
   double j_e2 = 0.0, j_n = 0.0, j_max = 0.0;  // judged errors of this thread (summed per warp)
-  for (int64_t base = wid * 16; base < n; base += nwarps * 16) {
-    // lanes 0-15 form the scaled inputs of one particle each
-    int64_t me = base + (lane & 15);
+  for (int64_t base = wid * 32; base < n; base += nwarps * 32) {
+    // lane l: the scaled inputs and, after the two tiles below, the network's f of particle
+    // base + l; the tensor tiles take rows 0-15 (lanes 0-15's inputs) and then rows 16-31
+    int64_t me = base + lane;
     bool have = me < n;
     double u = have ? u_in[me] : 1.0, r = have ? rho[me] : 1.0;
     double d = have ? (dt ? dt[me] : dt_scalar) : 1.0;
     float x[3] = {0.f, 0.f, 0.f};
     bool inside = have && mlp_inputs(u, r, d, bp, hl, x);
     bool hot = have && (bp.tfac * u > bp.t_floor) && d > 0;
-    // layer 1 (K = 16: x high parts in cols 0-2, remainders in cols 3-5)
-    float xr[2][3];
+    float f_a = 0.f, f_b = 0.f;
+#pragma unroll 1
+    for (int tile = 0; tile < 2; ++tile) {
+      // layer 1 (K = 16: x high parts in cols 0-2, remainders in cols 3-5)
+      float xr[2][3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      xr[0][c] = __shfl_sync(0xffffffffu, x[c], g);
-      xr[1][c] = __shfl_sync(0xffffffffu, x[c], g + 8);
-    }
-    uint32_t a[4] = {0u, 0u, 0u, 0u};
+      for (int c = 0; c < 3; ++c) {
+        xr[0][c] = __shfl_sync(0xffffffffu, x[c], 16 * tile + g);
+        xr[1][c] = __shfl_sync(0xffffffffu, x[c], 16 * tile + g + 8);
+      }
+      uint32_t a[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-    for (int rr = 0; rr < 2; ++rr) {
-      float hi0 = __bfloat162float(__float2bfloat16(xr[rr][0]));
-      float hi1 = __bfloat162float(__float2bfloat16(xr[rr][1]));
-      float hi2 = __bfloat162float(__float2bfloat16(xr[rr][2]));
-      float c6[6] = {hi0, hi1, hi2, xr[rr][0] - hi0, xr[rr][1] - hi1, xr[rr][2] - hi2};
-      // a0/a1: cols 2t, 2t+1 of rows g / g+8 (a2, a3: cols 8+ are zero)
-      float e0 = 2 * t < 6 ? c6[2 * t] : 0.f, e1 = 2 * t + 1 < 6 ? c6[2 * t + 1] : 0.f;
-      a[rr] = pack_bf16(e0, e1);
-    }
-    uint32_t h1hi[4][4], h1lo[4][4];
+      for (int rr = 0; rr < 2; ++rr) {
+        float hi0 = __bfloat162float(__float2bfloat16(xr[rr][0]));
+        float hi1 = __bfloat162float(__float2bfloat16(xr[rr][1]));
+        float hi2 = __bfloat162float(__float2bfloat16(xr[rr][2]));
+        float c6[6] = {hi0, hi1, hi2, xr[rr][0] - hi0, xr[rr][1] - hi1, xr[rr][2] - hi2};
+        // a0/a1: cols 2t, 2t+1 of rows g / g+8 (a2, a3: cols 8+ are zero)
+        float e0 = 2 * t < 6 ? c6[2 * t] : 0.f, e1 = 2 * t + 1 < 6 ? c6[2 * t + 1] : 0.f;
+        a[rr] = pack_bf16(e0, e1);
+      }
+      uint32_t h1hi[4][4], h1lo[4][4];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      float c0 = S.b1[j * 8 + 2 * t], c1 = S.b1[j * 8 + 2 * t + 1];
-      float d0 = c0, d1 = c1, d2 = c0, d3 = c1;
-      uint32_t b0 = ld2(&S.w1[j * 8 + g][2 * t]);
-      uint32_t b1 = ld2(&S.w1[j * 8 + g][8 + 2 * t]);
-      mma16816(d0, d1, d2, d3, a[0], a[1], a[2], a[3], b0, b1);
-      d0 = silu_inf(d0);
-      d1 = silu_inf(d1);
-      d2 = silu_inf(d2);
-      d3 = silu_inf(d3);
-      int kk = j >> 1, hsel = (j & 1) * 2;
-      split2(d0, d1, h1hi[kk][hsel], h1lo[kk][hsel]);
-      split2(d2, d3, h1hi[kk][hsel + 1], h1lo[kk][hsel + 1]);
-    }
-    uint32_t h2hi[4][4], h2lo[4][4];
-    mlp_hidden(S.w2, S.b2, h1hi, h1lo, h2hi, h2lo, g, t);
-    mlp_hidden(S.w3, S.b3, h2hi, h2lo, h1hi, h1lo, g, t);
-    // output layer: one n-tile, only column 0 is real
-    float o0 = S.b4, o1 = 0.f, o2 = S.b4, o3 = 0.f;
+      for (int j = 0; j < 8; ++j) {
+        float c0 = S.b1[j * 8 + 2 * t], c1 = S.b1[j * 8 + 2 * t + 1];
+        float d0 = c0, d1 = c1, d2 = c0, d3 = c1;
+        uint32_t b0 = ld2(&S.w1[j * 8 + g][2 * t]);
+        uint32_t b1 = ld2(&S.w1[j * 8 + g][8 + 2 * t]);
+        mma16816(d0, d1, d2, d3, a[0], a[1], a[2], a[3], b0, b1);
+        d0 = silu_inf(d0);
+        d1 = silu_inf(d1);
+        d2 = silu_inf(d2);
+        d3 = silu_inf(d3);
+        int kk = j >> 1, hsel = (j & 1) * 2;
+        split2(d0, d1, h1hi[kk][hsel], h1lo[kk][hsel]);
+        split2(d2, d3, h1hi[kk][hsel + 1], h1lo[kk][hsel + 1]);
+      }
+      uint32_t h2hi[4][4], h2lo[4][4];
+      mlp_hidden(S.w2, S.b2, h1hi, h1lo, h2hi, h2lo, g, t);
+      mlp_hidden(S.w3, S.b3, h2hi, h2lo, h1hi, h1lo, g, t);
+      // output layer: one n-tile, only column 0 is real
+      float o0 = S.b4, o1 = 0.f, o2 = S.b4, o3 = 0.f;
 #pragma unroll
-    for (int kk = 0; kk < 4; ++kk) {
-      uint32_t b0 = ld2(&S.w4[g][kk * 16 + 2 * t]);
-      uint32_t b1 = ld2(&S.w4[g][kk * 16 + 8 + 2 * t]);
-      mma16816(o0, o1, o2, o3, h1hi[kk][0], h1hi[kk][1], h1hi[kk][2], h1hi[kk][3], b0, b1);
-      mma16816(o0, o1, o2, o3, h1lo[kk][0], h1lo[kk][1], h1lo[kk][2], h1lo[kk][3], b0, b1);
+      for (int kk = 0; kk < 4; ++kk) {
+        uint32_t b0 = ld2(&S.w4[g][kk * 16 + 2 * t]);
+        uint32_t b1 = ld2(&S.w4[g][kk * 16 + 8 + 2 * t]);
+        mma16816(o0, o1, o2, o3, h1hi[kk][0], h1hi[kk][1], h1hi[kk][2], h1hi[kk][3], b0, b1);
+        mma16816(o0, o1, o2, o3, h1lo[kk][0], h1lo[kk][1], h1lo[kk][2], h1lo[kk][3], b0, b1);
+      }
+      // lanes with t == 0 hold f of rows g (o0) and g + 8 (o2) of the tile; lane l takes row l % 16
+      float f_lo = __shfl_sync(0xffffffffu, o0, (lane & 7) * 4);
+      float f_hi = __shfl_sync(0xffffffffu, o2, ((lane & 7)) * 4);
+      const float f_row = (lane & 15) < 8 ? f_lo : f_hi;
+      if (tile == 0)
+        f_a = f_row;
+      else
+        f_b = f_row;
     }
-    // lanes with t == 0 hold f of rows g (o0) and g + 8 (o2); move them to lanes 0-15
-    float f_lo = __shfl_sync(0xffffffffu, o0, (lane & 7) * 4);
-    float f_hi = __shfl_sync(0xffffffffu, o2, ((lane & 7)) * 4);
-    float f = (lane & 15) < 8 ? f_lo : f_hi;
-    if (lane < 16 && have) {
+    const float f = lane < 16 ? f_a : f_b;
+    if (have) {
       double un;
       int mode = 0;
       if (!hot) {
@@ -587,7 +597,7 @@ int mlp_cool(Engine& E, int64_t n, const double* u, const double* rho, const dou
   if (n <= 0) return 0;
   MlpState* M;
   NB_TRY(mlp_state(E, &M));
-  int blocks = (int)std::min<int64_t>((n + 63) / 64, 148 * 16);
+  int blocks = (int)std::min<int64_t>((n + 127) / 128, 148 * 16);
   count_launch(), k_mlp_cool<<<blocks, 128, 0, st>>>(n, u, rho, dt, dt_scalar, M->w, brems_of_mlp(mp),
                                                      hull_of(mp), mp->judge, u_out, mode, M->counts,
                                                      M->stats);
