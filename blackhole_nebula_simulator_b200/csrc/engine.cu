@@ -249,13 +249,6 @@ __global__ void k_pack_sorted_f4(int64_t n, const int32_t* __restrict__ perm,
                          d ? (float)d[i] : 0.f);
 }
 
-__global__ void k_rows_to_sorted(int64_t nrows, const int64_t* __restrict__ rows,
-                                 const int32_t* __restrict__ inv_perm, int64_t* __restrict__ out) {
-  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= nrows) return;
-  out[q] = inv_perm[rows[q]];
-}
-
 // h_search = min(min(h_guess, h_max) * skin, cap) (sim/sph.py:373)
 __global__ void k_hsearch(int64_t n, const double* __restrict__ hg, double h_max, double skin,
                           double* __restrict__ hs) {
@@ -391,13 +384,6 @@ __global__ void k_fast_complete(int64_t n, int nfast, const int32_t* __restrict_
       if (a >= hi || idx[a] != key) atomicOr(fail, 1);
     }
   }
-}
-
-__global__ void k_gather_d(int64_t n, const int32_t* __restrict__ perm, const double* __restrict__ a,
-                           double* __restrict__ out) {
-  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  out[k] = a[perm[k]];
 }
 
 // sorted packs for the pair passes
@@ -639,29 +625,6 @@ __global__ void k_unsort_marks(int64_t n, const int32_t* __restrict__ perm,
   if (k < n && mark_s[k]) mark[perm[k]] = 1;
 }
 
-// touched sets: mark the rows and their list entries (optionally only interacting pairs)
-__global__ void k_mark(int64_t nrows, const int64_t* __restrict__ rows,
-                       const int32_t* __restrict__ perm, const int32_t* __restrict__ inv_perm,
-                       const int64_t* __restrict__ off, const int32_t* __restrict__ idx, int tight,
-                       const double* __restrict__ x, const double* __restrict__ h,
-                       uint8_t* __restrict__ mark) {
-  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= nrows) return;
-  int64_t i = rows[q];
-  int64_t k = inv_perm[i];
-  mark[i] = 1;
-  double xi0 = x[3 * i], xi1 = x[3 * i + 1], xi2 = x[3 * i + 2], hi = h[i];
-  for (int64_t e = off[k]; e < off[k + 1]; ++e) {
-    int64_t j = perm[idx[e]];
-    if (tight) {
-      double d2 = d2_exact(x[3 * j] - xi0, x[3 * j + 1] - xi1, x[3 * j + 2] - xi2);
-      double rr = 2.0 * fmax(hi, h[j]);
-      if (!(d2 < rr * rr)) continue;
-    }
-    mark[j] = 1;
-  }
-}
-
 __global__ void k_mask_and_not(int64_t n, const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
                                uint8_t* __restrict__ out) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -673,11 +636,6 @@ __global__ void k_mask_or(int64_t n, const uint8_t* __restrict__ a, uint8_t* __r
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   b[i] = b[i] | a[i];
-}
-
-__global__ void k_iota64(int64_t n, int64_t* __restrict__ out) {
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) out[i] = i;
 }
 
 // rows with flag 2 (FLAG_SEARCH_TOO_SMALL): double their search; every row restarts from its h
@@ -796,12 +754,6 @@ void Workspace::release() {
   if (h_dbl) cudaFreeHost(h_dbl);
   if (h_scal) cudaFreeHost(h_scal);
   *this = Workspace{cache};
-}
-
-__global__ void k_gather_rows_i64(int64_t nrows, const int64_t* __restrict__ rows,
-                                  const int64_t* __restrict__ a, int64_t* __restrict__ out) {
-  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q < nrows) out[q] = a[rows[q]];
 }
 
 // sum of a[rows] into E.ws.h_i64[0] (profiling only)

@@ -199,15 +199,6 @@ __global__ void k_cool_shared(int64_t n, int law, const double* __restrict__ x0,
   u_half[i] = un;
 }
 
-// dm = m (u_half - u_cooled); u_half <- u_cooled
-__global__ void k_dm_shared(int64_t n, const double* __restrict__ m, const double* __restrict__ uc,
-                            double* __restrict__ u_half, double* __restrict__ dm) {
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  dm[i] = m[i] * (u_half[i] - uc[i]);
-  u_half[i] = uc[i];
-}
-
 __global__ void k_pred_shared(int64_t n, const double* __restrict__ p_flow,
                               const double* __restrict__ a, const double* __restrict__ u_half,
                               const double* __restrict__ dudt, double half,
