@@ -531,29 +531,30 @@ __global__ void k_tight_rows(int64_t nrows, const int64_t* __restrict__ rows_s,
 // above the start is unique, so in-place sweeps reach the reference's levels
 __global__ void k_limit_sweep_t(int64_t nrows, const int64_t* __restrict__ rows_s,
                                 const int64_t* __restrict__ off, const int32_t* __restrict__ tidx,
-                                const int32_t* __restrict__ tcnt, int64_t max_gap,
-                                int64_t* level_s, int* changed) {
+                                const int32_t* __restrict__ tcnt, int max_gap,
+                                int32_t* level_s, int* changed) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   int64_t q = t >> 3;
   const int gl = (int)(t & 7);
   const bool live = q < nrows;
-  int64_t k = 0, need = INT64_MIN;
+  int64_t k = 0;
+  int need = INT_MIN;
   if (live) {
     k = rows_s[q];
-    need = ((volatile int64_t*)level_s)[k];
+    need = ((volatile int32_t*)level_s)[k];
     const int32_t* tl = tidx + off[k];
     for (int c = gl; c < tcnt[q]; c += 8) {
-      int64_t lj = ((volatile int64_t*)level_s)[tl[c]];
+      int lj = ((volatile int32_t*)level_s)[tl[c]];
       if (lj - max_gap > need) need = lj - max_gap;
     }
   }
 #pragma unroll
   for (int o = 4; o > 0; o >>= 1) {
-    int64_t other = __shfl_xor_sync(0xffffffffu, need, o);
+    int other = __shfl_xor_sync(0xffffffffu, need, o);
     need = other > need ? other : need;
   }
-  if (live && gl == 0 && need > ((volatile int64_t*)level_s)[k]) {
-    atomicMax((long long*)&level_s[k], (long long)need);
+  if (live && gl == 0 && need > ((volatile int32_t*)level_s)[k]) {
+    atomicMax(&level_s[k], need);
     *changed = 1;
   }
 }
@@ -565,38 +566,44 @@ __global__ void k_limit_sweep_t(int64_t nrows, const int64_t* __restrict__ rows_
 // level[j] exactly where it did, and keeps its maximum where it is above.
 __global__ void k_wake_need_t(int64_t nrows, const int64_t* __restrict__ rows_s,
                               const int64_t* __restrict__ off, const int32_t* __restrict__ tidx,
-                              const int32_t* __restrict__ tcnt, const int64_t* __restrict__ level_s,
-                              int64_t max_gap, int64_t* __restrict__ need_s) {
+                              const int32_t* __restrict__ tcnt, const int32_t* __restrict__ level_s,
+                              int max_gap, int32_t* __restrict__ need_s) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   int64_t q = t >> 3;
   const int gl = (int)(t & 7);
   if (q >= nrows) return;
   int64_t k = rows_s[q];
-  long long v = (long long)(level_s[k] - max_gap);
+  const int v = level_s[k] - max_gap;
   const int32_t* tl = tidx + off[k];
   for (int c = gl; c < tcnt[q]; c += 8) {
     const int32_t j = tl[c];
-    if (v > (long long)level_s[j]) atomicMax((long long*)&need_s[j], v);
+    if (v > level_s[j]) atomicMax(&need_s[j], v);
   }
 }
 
-__global__ void k_gather_i64(int64_t n, const int32_t* __restrict__ perm, const int64_t* __restrict__ a,
-                             int64_t* __restrict__ out) {
+// levels (at most K_MAX) in sorted order as 32-bit integers, for the sweeps' gathers
+__global__ void k_gather_level32(int64_t n, const int32_t* __restrict__ perm,
+                                 const int64_t* __restrict__ a, int32_t* __restrict__ out) {
   int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (k < n) out[k] = a[perm[k]];
+  if (k < n) out[k] = (int32_t)a[perm[k]];
 }
 
-__global__ void k_scatter_rows_i64(int64_t nrows, const int64_t* __restrict__ rows_s,
-                                   const int32_t* __restrict__ perm, const int64_t* __restrict__ a_s,
-                                   int64_t* __restrict__ a) {
+__global__ void k_fill_i32(int64_t n, int32_t v, int32_t* __restrict__ a) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
+__global__ void k_scatter_rows_level32(int64_t nrows, const int64_t* __restrict__ rows_s,
+                                       const int32_t* __restrict__ perm,
+                                       const int32_t* __restrict__ a_s, int64_t* __restrict__ a) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= nrows) return;
   int64_t k = rows_s[q];
   a[perm[k]] = a_s[k];
 }
 
-__global__ void k_scatter_i64(int64_t n, const int32_t* __restrict__ perm, const int64_t* __restrict__ a_s,
-                              int64_t* __restrict__ a) {
+__global__ void k_scatter_level32(int64_t n, const int32_t* __restrict__ perm,
+                                  const int32_t* __restrict__ a_s, int64_t* __restrict__ a) {
   int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (k < n) a[perm[k]] = a_s[k];
 }
@@ -677,6 +684,9 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
   Workspace& W = E.ws;
   Lists& L = E.lists;
   int64_t n = s->n;
+  // sorted levels and wake-up needs as 32-bit integers in the int64 scratch arrays
+  int32_t* lvl_s = reinterpret_cast<int32_t*>(W.i_lvl);
+  int32_t* need_s = reinterpret_cast<int32_t*>(W.i_tmp2);
   if (nrows == 0) return 0;
   count_launch(), k_wanted_levels<<<grid_for(nrows), NB_THREADS, 0, st>>>(
       nrows, rows, s->tick_n, prm->dt_max, s->h, s->vsig_max, s->a_hydro,
@@ -695,7 +705,7 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
       NB_TRY(sorted_rows(E, nrows, rows, &ns, st));
     else
       NB_TRY(sorted_rows_and_pack(E, nrows, rows, s->x, s->h, &ns, st));
-    count_launch(), k_gather_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, W.i_lvl);
+    count_launch(), k_gather_level32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, lvl_s);
     if (!have_tight) {
       NB_TRY(E.ensure_tight(L.total));
       count_launch(), k_tight_rows<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, L.idx, W.pk0,
@@ -711,7 +721,7 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
       NB_CUDA(cudaMemsetAsync(W.d_int, 0, sizeof(int) * batch, st));
       for (int b = 0; b < batch; ++b)
         count_launch(), k_limit_sweep_t<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(
-            ns, W.rows_s, L.off, E.tidx, W.i32a, prm->max_gap, W.i_lvl, W.d_int + b);
+            ns, W.rows_s, L.off, E.tidx, W.i32a, (int)prm->max_gap, lvl_s, W.d_int + b);
       NB_CUDA(cudaMemcpyAsync(W.h_int, W.d_int + batch - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
       NB_TRY(pending_enqueue(E, st));
       NB_CUDA(host_sync(st));
@@ -722,17 +732,17 @@ static int choose_levels_and_open(Engine& E, nb_state* s, const nb_params* prm, 
       }
     }
     if (!settled) return set_host_error(E, "level limiter did not settle");
-    count_launch(), k_scatter_rows_i64<<<grid_for(ns), NB_THREADS, 0, st>>>(ns, W.rows_s, L.perm, W.i_lvl, s->level);
+    count_launch(), k_scatter_rows_level32<<<grid_for(ns), NB_THREADS, 0, st>>>(ns, W.rows_s, L.perm, lvl_s, s->level);
   }
   count_launch(), k_land<<<grid_for(nrows), NB_THREADS, 0, st>>>(nrows, rows, s->tick_n, s->n_stop, s->level, E.d_err);
   W.pend_err = true;  // read with the wake-up count (the kernels below skip their writes on it)
   if (prm->limiter) {
     // levels after _land, sorted; need in sorted order, then back to the caller's order
-    count_launch(), k_gather_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, W.i_lvl);
-    count_launch(), k_fill_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, -1, W.i_tmp2);
+    count_launch(), k_gather_level32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, s->level, lvl_s);
+    count_launch(), k_fill_i32<<<grid_for(n), NB_THREADS, 0, st>>>(n, -1, need_s);
     count_launch(), k_wake_need_t<<<grid_for(ns * 8), NB_THREADS, 0, st>>>(ns, W.rows_s, L.off, E.tidx, W.i32a,
-                                                                     W.i_lvl, prm->max_gap, W.i_tmp2);
-    count_launch(), k_scatter_i64<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, W.i_tmp2, W.need);
+                                                                     lvl_s, (int)prm->max_gap, need_s);
+    count_launch(), k_scatter_level32<<<grid_for(n), NB_THREADS, 0, st>>>(n, L.perm, need_s, W.need);
     // the wake-up count is read with the step's last checks (no round trip of its own)
     if (W.pend_woken) NB_TRY(pending_flush(E, st));
     NB_CUDA(cudaMemsetAsync(W.d_scal_i + 2, 0, sizeof(int64_t), st));
