@@ -48,8 +48,10 @@ DRAM_BYTES_PER_ROW = {"forces": 2251.0, "density": 1024.0, "lists": 1214.0}
 # stays the HBM copy bandwidth; none of these kernels is a contraction)
 LIMITER = {
     "lists": "issue: the test pass at 80 % issue active (FMA 45 %, ALU 42 %), the expansion at "
-             "64 %; the candidate pass latency bound (long-scoreboard 2.9 per issue at 26 % warp "
+             "64 %; the candidate pass latency bound (long-scoreboard 3.2 per issue at 24 % warp "
              "occupancy); DRAM 0.1-9 % of peak",
+    "cooling": "issue and shared-memory latency: 39 % issue active at 24 % warp occupancy (128 "
+               "registers), tensor pipe 19.5 %, FP64 pipe 6.4 % (the check)",
     "density": "latency: long-scoreboard stalls 4.2 per issue on the gathered records, 66 % "
                "issue active at 43 % warp occupancy, DRAM 8 % of peak",
     "forces": "latency: the walk launch stalls 11.5 per issue on the gathered records (DRAM 21 %); "
