@@ -71,7 +71,7 @@ def test_cloud_cells_bit_exact(nb):
 
 
 def test_cells_at_262k_bit_exact(nb):
-    """The same at the 262,144-particle cloud (BASELINE's second configuration) against the
+    """The same at the 262,144-particle cloud (the uniform cloud of the FP32 tests) against the
     oracle's cell of every particle: geometry, starts and order exactly."""
     from blackhole_nebula_simulator_b200 import ics
     from oracle import native
