@@ -335,7 +335,10 @@ __device__ __forceinline__ void mlp_hidden(const __nv_bfloat16 (*W)[MLP_H], cons
 // mode_out (optional): 0 exact (at or below the floor, or not cooled), 1 network, 2 fallback.
 // judge: every judge-th network result is compared with the exact one (|du_mlp - du_exact| / u
 // accumulated as max and sum of squares in stats[0..1], count in stats[2]).
-__global__ void __launch_bounds__(128, 4) k_mlp_cool(int64_t n, const double* __restrict__ u_in,
+#ifndef MLP_BLOCKS_PER_SM
+#define MLP_BLOCKS_PER_SM 4  // 128 registers (a few spilled); 5 blocks spill 208 B
+#endif
+__global__ void __launch_bounds__(128, MLP_BLOCKS_PER_SM) k_mlp_cool(int64_t n, const double* __restrict__ u_in,
                                                   const double* __restrict__ rho,
                                                   const double* __restrict__ dt, double dt_scalar,
                                                   const float* __restrict__ w, BremsParams bp,
