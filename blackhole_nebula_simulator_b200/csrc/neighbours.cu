@@ -600,10 +600,11 @@ __device__ __forceinline__ int nth_set_bit(uint32_t m, int k) {
 // takes the rows one after the other, 32 batches at a time with lane b on batch b: the batches'
 // entry counts are scanned across the lanes, and the row's entries of those batches are written
 // 32 at a time, lane s taking entry s: its batch is found by a binary search over the scanned
-// counts, its candidate as the set bit of that rank in the batch's mask.  Every store writes 32
-// consecutive entries of one row, and each row's entries come out in ascending order (batches
-// ascending, a mask's bits from the lowest slot up), contiguous from the row's offset.
-// warps per block and batches staged at a time: measured on the 4M torus (list build ms per
+// counts, its candidate as the set bit of that rank in the batch's mask.  Every store writes up
+// to 32 consecutive entries of one row, and each row's entries come out in ascending order
+// (batches ascending, a mask's bits from the lowest slot up), contiguous from the row's offset.
+//
+// Warps per block and batches staged at a time: measured on the 4M torus (list build ms per
 // build) 10.45 with 8 warps and 32 batches, 10.86 with 4 and 32, 11.35 with 4 and 64, 11.68
 // with 2 and 64 (37.9 KB of shared memory per block for 8 x 32 and 4 x 64)
 #ifndef EXPAND_WARPS
