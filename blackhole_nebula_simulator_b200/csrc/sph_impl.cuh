@@ -321,6 +321,8 @@ struct DensityEntry<double> {
   static constexpr int BLOCKS = 4;
 };
 constexpr int DENSITY_THREADS = 128;  // 16 rows per block
+// rounds of 8 entries the list walk loads at once: 4 measured 3.55 ms per density launch on the
+// 4M torus against 3.88 with 2 and 3.75 with 8
 #ifndef DENSITY_UNROLL
 #define DENSITY_UNROLL 4
 #endif
